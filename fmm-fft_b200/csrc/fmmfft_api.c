@@ -1,0 +1,223 @@
+/*
+ * Public C-ABI of libfmmfft_b200.so (declared in include/fmmfft.h): the reference-compatible
+ * entry points getwlen2 / getvlen / mfti / mft (src/fmmfft.c:1160, :1110, :337, :980) and the
+ * native plan API.  Host code only; device work is delegated to fmmfft_kernels.cu.
+ */
+#include <pthread.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../../include/fmmfft.h"
+#include "fmmfft_internal.h"
+
+struct fmmfft_plan_s {
+  long N, P, M, T, b;
+  int precision;
+  size_t device_bytes;
+  fmmk_state *dev;
+};
+
+/* ------------------------------------------------------------------ last error (per thread) */
+static __thread int t_status = FMMFFT_OK;
+static __thread char t_msg[256];
+
+static int set_err(int status, const char *msg) {
+  t_status = status;
+  snprintf(t_msg, sizeof t_msg, "%s", msg ? msg : "");
+  if (status != FMMFFT_OK && msg && getenv("FMMFFT_QUIET") == NULL)
+    fprintf(stderr, "fmmfft: %s\n", msg);
+  return status;
+}
+
+int fmmfft_last_error(void) { return t_status; }
+const char *fmmfft_last_error_string(void) { return t_msg; }
+
+/* ------------------------------------------------------------------ native API */
+int fmmfft_plan_create(fmmfft_plan *out, long N, long P, long terms, long b, int precision) {
+  if (!out) return set_err(FMMFFT_ERR_INVALID, "plan_create: NULL output pointer");
+  *out = NULL;
+  if (precision < FMMFFT_F64 || precision > FMMFFT_F32_TC)
+    return set_err(FMMFFT_ERR_INVALID, "plan_create: unknown precision");
+  if (P < 2 || N <= 0 || N % P)
+    return set_err(FMMFFT_ERR_INVALID, "plan_create: N must be a positive multiple of P >= 2");
+  long M = N / P;
+  if (!fmm_validate(M, P, terms, b)) {
+    char m[200];
+    snprintf(m, sizeof m,
+             "plan_create: unsupported (N=%ld, P=%ld, terms=%ld, b=%ld): need powers of two, "
+             "2<=P<=1024, b>=2, M/b>=4, 2<=terms<=64, M<=2^26", N, P, terms, b);
+    return set_err(FMMFFT_ERR_INVALID, m);
+  }
+  fmm_ops64 ops;
+  int rc = fmm_ops64_build(M, P, terms, b, &ops);
+  if (rc) return set_err(FMMFFT_ERR_NOMEM, "plan_create: host allocation failed");
+  struct fmmfft_plan_s *pl = (struct fmmfft_plan_s *)calloc(1, sizeof *pl);
+  if (!pl) {
+    fmm_ops64_free(&ops);
+    return set_err(FMMFFT_ERR_NOMEM, "plan_create: host allocation failed");
+  }
+  char err[256] = {0};
+  rc = fmmk_create(&ops, precision, &pl->dev, &pl->device_bytes, err, sizeof err);
+  fmm_ops64_free(&ops);
+  if (rc) {
+    free(pl);
+    return set_err(rc, err);
+  }
+  pl->N = N, pl->P = P, pl->M = M, pl->T = terms, pl->b = b, pl->precision = precision;
+  *out = pl;
+  return set_err(FMMFFT_OK, NULL);
+}
+
+int fmmfft_plan_destroy(fmmfft_plan plan) {
+  if (!plan) return FMMFFT_OK;
+  fmmk_destroy(plan->dev);
+  free(plan);
+  return FMMFFT_OK;
+}
+
+int fmmfft_plan_device_bytes(fmmfft_plan plan, size_t *bytes) {
+  if (!plan || !bytes) return set_err(FMMFFT_ERR_INVALID, "plan_device_bytes: NULL argument");
+  *bytes = plan->device_bytes;
+  return FMMFFT_OK;
+}
+
+static int exec_common(fmmfft_plan plan, const void *d_in, void *d_out, void *stream, int inv) {
+  if (!plan || !d_in || !d_out) return set_err(FMMFFT_ERR_INVALID, "execute: NULL argument");
+  char err[256] = {0};
+  int rc = fmmk_execute(plan->dev, d_in, d_out, stream, inv, err, sizeof err);
+  return rc ? set_err(rc, err) : FMMFFT_OK;
+}
+
+int fmmfft_execute(fmmfft_plan plan, const void *d_in, void *d_out, void *stream) {
+  return exec_common(plan, d_in, d_out, stream, 0);
+}
+
+int fmmfft_execute_inverse(fmmfft_plan plan, const void *d_in, void *d_out, void *stream) {
+  return exec_common(plan, d_in, d_out, stream, 1);
+}
+
+int fmmfft_execute_host(fmmfft_plan plan, const void *h_in, void *h_out, void *stream) {
+  if (!plan || !h_in || !h_out) return set_err(FMMFFT_ERR_INVALID, "execute_host: NULL argument");
+  char err[256] = {0};
+  int rc = fmmk_execute_host(plan->dev, h_in, h_out, stream, err, sizeof err);
+  return rc ? set_err(rc, err) : FMMFFT_OK;
+}
+
+int fmmfft_debug_fetch(fmmfft_plan plan, double *u, double *z, double *phi, double *psi) {
+  if (!plan) return set_err(FMMFFT_ERR_INVALID, "debug_fetch: NULL plan");
+  int rc = fmmk_debug_fetch(plan->dev, u, z, phi, psi);
+  return rc ? set_err(FMMFFT_ERR_CUDA, "debug_fetch: copy failed") : FMMFFT_OK;
+}
+
+int fmmfft_profile_start(fmmfft_plan plan, int max_executes) {
+  if (!plan) return set_err(FMMFFT_ERR_INVALID, "profile_start: NULL plan");
+  int rc = fmmk_profile_start(plan->dev, max_executes);
+  return rc ? set_err(rc == 1 ? FMMFFT_ERR_INVALID : FMMFFT_ERR_CUDA, "profile_start failed")
+            : FMMFFT_OK;
+}
+
+int fmmfft_profile_stop(fmmfft_plan plan, double *stage_ms, int *stage_launches, int cap,
+                        int *nstages, int *nexecutes) {
+  if (!plan || !stage_ms || !stage_launches || !nstages)
+    return set_err(FMMFFT_ERR_INVALID, "profile_stop: NULL argument");
+  int n = fmmk_profile_stop(plan->dev, stage_ms, stage_launches, cap, nexecutes);
+  if (n < 0) return set_err(FMMFFT_ERR_INVALID, "profile_stop: profiling was not started");
+  *nstages = n;
+  return FMMFFT_OK;
+}
+
+const char *fmmfft_stage_name(int i) { return fmmk_stage_name(i); }
+
+/* ------------------------------------------------------------------ reference-compatible */
+
+/* Device plans made by mfti, keyed by (lq, p, terms, b), kept until process exit: mft finds
+ * the plan mfti made for the same parameters, as the reference's mft reuses mfti's w. */
+typedef struct compat_entry {
+  long lq, p, terms, b;
+  fmmfft_plan plan;
+  struct compat_entry *next;
+} compat_entry;
+static compat_entry *g_compat = NULL;
+static pthread_mutex_t g_compat_mu = PTHREAD_MUTEX_INITIALIZER;
+
+static fmmfft_plan compat_plan(long lq, long p, long terms, long b, int *status) {
+  pthread_mutex_lock(&g_compat_mu);
+  for (compat_entry *e = g_compat; e; e = e->next)
+    if (e->lq == lq && e->p == p && e->terms == terms && e->b == b) {
+      pthread_mutex_unlock(&g_compat_mu);
+      *status = FMMFFT_OK;
+      return e->plan;
+    }
+  fmmfft_plan pl = NULL;
+  *status = fmmfft_plan_create(&pl, lq * p, p, terms, b, FMMFFT_F64);
+  if (*status == FMMFFT_OK) {
+    compat_entry *e = (compat_entry *)calloc(1, sizeof *e);
+    if (!e) {
+      fmmfft_plan_destroy(pl);
+      pthread_mutex_unlock(&g_compat_mu);
+      *status = set_err(FMMFFT_ERR_NOMEM, "compat plan cache: allocation failed");
+      return NULL;
+    }
+    *e = (compat_entry){lq, p, terms, b, pl, g_compat};
+    g_compat = e;
+  }
+  pthread_mutex_unlock(&g_compat_mu);
+  return pl;
+}
+
+long getwlen2(long lq, long terms, long p, long b) {
+  long v = fmm_getwlen2(lq, terms, p, b);
+  set_err(v < 0 ? FMMFFT_ERR_INVALID : FMMFFT_OK, v < 0 ? "getwlen2: unsupported parameters" : NULL);
+  return v;
+}
+
+long getvlen(long lq, long terms, long p, long b) {
+  long v = fmm_getvlen(lq, terms, p, b);
+  set_err(v < 0 ? FMMFFT_ERR_INVALID : FMMFFT_OK, v < 0 ? "getvlen: unsupported parameters" : NULL);
+  return v;
+}
+
+void mfti(long lq, long p, long terms, long b, double *w, double *v, long szkeep, long sztemp) {
+  (void)v, (void)szkeep, (void)sztemp;
+  if (!fmm_validate(lq, p, terms, b)) {
+    set_err(FMMFFT_ERR_INVALID, "mfti: unsupported parameters");
+    return;
+  }
+  if (w) {
+    fmm_ops64 ops;
+    if (fmm_ops64_build(lq, p, terms, b, &ops)) {
+      set_err(FMMFFT_ERR_NOMEM, "mfti: host allocation failed");
+      return;
+    }
+    fmm_ops64_to_reference_w(&ops, w);
+    fmm_ops64_free(&ops);
+  }
+  int st;
+  compat_plan(lq, p, terms, b, &st);
+  if (st == FMMFFT_OK) set_err(FMMFFT_OK, NULL);
+}
+
+void mft(long lq, void *qr, long dir, long p, long myid, long terms, long b, double *w, double *v,
+         long sz1, long szwk, void *forward_plan) {
+  (void)myid, (void)w, (void)v, (void)sz1, (void)szwk, (void)forward_plan;
+  if (!qr) {
+    set_err(FMMFFT_ERR_INVALID, "mft: NULL qr");
+    return;
+  }
+  if (dir < 0) {
+    set_err(FMMFFT_ERR_UNSUPPORTED,
+            "mft: dir < 0 is not served (the reference's inverse conjugates before its local "
+            "FFT, src/fmmfft.c:976-977 vs :1080); use fmmfft_execute_inverse");
+    return;
+  }
+  if (!fmm_validate(lq, p, terms, b)) {
+    set_err(FMMFFT_ERR_INVALID, "mft: unsupported parameters");
+    return;
+  }
+  int st;
+  fmmfft_plan pl = compat_plan(lq, p, terms, b, &st);
+  if (!pl) return;
+  st = fmmfft_execute_host(pl, qr, qr, NULL);
+  if (st == FMMFFT_OK) set_err(FMMFFT_OK, NULL);
+}

@@ -1,0 +1,58 @@
+/*
+ * Internal interface between the C host layer (fmmfft_ops.c, fmmfft_api.c) and the CUDA layer
+ * (fmmfft_kernels.cu).  Not part of the public C-ABI.
+ */
+#ifndef FMMFFT_INTERNAL_H
+#define FMMFFT_INTERNAL_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Operator indices inside one level's block of fmm_ops64.levops, in the order the reference
+ * builds them (src/fmmfft.c:282-289). */
+enum { FMM_SHFTFN = 0, FMM_SHFTFP, FMM_FLIP2N, FMM_FLIP2P, FMM_FLIP3N, FMM_FLIP3P, FMM_SHFTLN,
+       FMM_SHFTLP, FMM_NLEVOPS };
+
+/* Every FMM operator of one (M, P, terms, b), built in FP64 on the host. */
+typedef struct fmm_ops64 {
+  long M, P, T, b, s, n;
+  double *chnods; /* [T]                        src/fmmfft.c:273-275 */
+  double *initch; /* [b][T]      S2M            :242-259 */
+  double *topflp; /* [T][T]      level-2 M2L    :279 */
+  double *levops; /* [n-2][8][T][T]  per level  :281-290 (index 0 = level 3) */
+  double *evalm;  /* [b][P-1][T] L2T weights    :295-298 */
+  double *evalmh; /* [P/2][T]    half-shifted   :300-304 */
+  double *cot;    /* [P-1][4b]   cot(pi(d + sc/P)/M), index d + 2b, d in [-2b, 2b) :306-318 */
+  double *fo;     /* [P][P-1] complex (re, im)  :325-331 */
+} fmm_ops64;
+
+int fmm_validate(long M, long P, long T, long b);
+int fmm_ops64_build(long M, long P, long T, long b, fmm_ops64 *o);
+void fmm_ops64_free(fmm_ops64 *o);
+/* Lays the operators out as the reference's mfti does (src/fmmfft.c:343-374). */
+void fmm_ops64_to_reference_w(const fmm_ops64 *o, double *w);
+long fmm_getwlen2(long lq, long terms, long p, long b);
+long fmm_getvlen(long lq, long terms, long p, long b);
+
+/* ---- CUDA layer (fmmfft_kernels.cu) ---- */
+typedef struct fmmk_state fmmk_state;
+int fmmk_create(const fmm_ops64 *ops, int precision, fmmk_state **out, size_t *device_bytes,
+                char *err, size_t errlen);
+void fmmk_destroy(fmmk_state *st);
+int fmmk_execute(fmmk_state *st, const void *d_in, void *d_out, void *stream, int inverse,
+                 char *err, size_t errlen);
+int fmmk_execute_host(fmmk_state *st, const void *h_in, void *h_out, void *stream, char *err,
+                      size_t errlen);
+int fmmk_debug_fetch(fmmk_state *st, double *u, double *z, double *phi, double *psi);
+int fmmk_device_ok(char *err, size_t errlen);
+int fmmk_profile_start(fmmk_state *st, int cap);
+int fmmk_profile_stop(fmmk_state *st, double *stage_ms, int *stage_launches, int cap, int *nexec);
+const char *fmmk_stage_name(int i);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

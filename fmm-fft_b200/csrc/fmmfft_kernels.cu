@@ -1,0 +1,1051 @@
+/*
+ * CUDA layer of the B200-native FMM-FFT (sm_100a).
+ *
+ * One forward transform of N = P*M points runs as these device stages (reference call stack
+ * src/fmmfft.c mft -> mftint, :384-1081):
+ *
+ *   1  k_sections      x[M][P] -> xt[2P][M] planar sections + per-tile section sums
+ *                      (deinterleave :419-439, section sums :441-457)
+ *   2  k_sum_sections  tiles -> Sigma_m x_sc[m] (the MPI_Reduce/Bcast of :452-453)
+ *   3  S2M             rowgemm: phi_n = xt . initch                      (:199-211, :465)
+ *   4  M2M             rowgemm per level: phi_L = [phi_L+1 pair] . [S_L;S_R]  (:476-515)
+ *   5  top flip        rowgemm: psi_2[c] = topflp . phi_2[c+2]          (:620-639)
+ *   6  M2L + L2L       rowgemm per level over parent boxes, both children at once
+ *                      (:643-749)
+ *   7  leaf            rowgemm per section: u = [psi_n | x window] . [E_sc ; cot Toeplitz]
+ *                      + k_leaf_fix for the half-shifted first point (:751-954)
+ *   8  k_combine       pre-twiddle and length-P DFT over sections, transposed store
+ *                      (:956-968 and the MPI_Alltoall of :970)
+ *   9  k_fft_pass      size-M Stockham FFTs, one or two passes (FFTW at :1080)
+ *
+ * All tree operators are shared by every section and box, so each tree stage is one dense
+ * contraction over "rows" (section, re/im plane, box) with a small operator; rowgemm is the
+ * CUDA-core form of that contraction.  Real type R = float (complex64 plans) or double
+ * (complex128 plans).  Expansions are stored planar: phi_l[(sc-1)*2 + ri][box][T].
+ */
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <new>
+
+#include "fmmfft_internal.h"
+
+#define FMM_CUDA_TRY(call)                                                              \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess) {                                                            \
+      if (err) snprintf(err, errlen, "%s failed: %s", #call, cudaGetErrorString(e_));   \
+      return 3;                                                                         \
+    }                                                                                   \
+  } while (0)
+
+template <typename R> struct cplx;
+template <> struct cplx<float> { using T = float2; };
+template <> struct cplx<double> { using T = double2; };
+
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  C r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) {
+  a.x += b.x, a.y += b.y;
+  return a;
+}
+template <typename C> __device__ __forceinline__ C csub(C a, C b) {
+  a.x -= b.x, a.y -= b.y;
+  return a;
+}
+
+/* ======================================================================== device plan */
+
+/* Stages of one execute, for per-stage CUDA-event timing (fmmfft_profile_*). */
+enum { ST_SECTIONS = 0, ST_SUMS, ST_S2M, ST_M2M, ST_TOP, ST_M2L, ST_LEAF, ST_LEAFFIX, ST_COMBINE,
+       ST_FFT1, ST_FFT2, ST_DC, ST_COUNT };
+static const char *const kStageNames[ST_COUNT] = {
+    "sections", "section_sums", "s2m", "m2m", "topflip", "m2l_l2l", "leaf_l2t_near",
+    "leaf_halfshift", "combine_dftP", "fft_pass1", "fft_pass2", "block_dc"};
+
+struct Prof {
+  int on, cap, count;
+  cudaEvent_t *ev; /* cap x (ST_COUNT + 1) */
+  int launches[ST_COUNT];
+};
+
+
+template <typename R> struct Dev {
+  using C = typename cplx<R>::T;
+  long M, P, T, b, s, n, N, S1;
+  int precision;
+  /* operators */
+  R *initch;  /* [b][T] */
+  R *btop;    /* [T][T]       btop[k][t] = topflp[t][k] */
+  R *bm2m;    /* [n-2][2T][T] index L-2 for parent level L = 2..n-1 */
+  R *bm2l;    /* [n-2][5T][2T] index l-3 for child level l = 3..n */
+  R *evalmT;  /* [P-1][T][b]  evalmT[sc-1][k][j] = evalm[j][sc-1][k] */
+  R *evalmh;  /* [P-1][T]     row sc-1 used for sc >= P/2 */
+  R *cot;     /* [P-1][4b] */
+  C *pretw;   /* [P]  c_sc = -exp(-i pi sc/P) sin(pi sc/P) */
+  C *twP;     /* [P]  exp(-2 pi i k / P) */
+  C *twM;     /* [M]  exp(-2 pi i k / M) */
+  /* workspace */
+  R *xt;      /* [2P][M] */
+  C *part;    /* [ntile][P] */
+  C *ssum;    /* [P] */
+  R *phi, *psi;
+  R *u;       /* [2(P-1)][M] */
+  C *z;       /* [P][M] */
+  C *tmp;     /* [P][M] */
+  long ntile, tileM;
+  long M1, M2; /* size-M FFT split (M2 = 1 when one pass) */
+  size_t bytes;
+  void *pool;
+  Prof prof;
+};
+
+struct fmmk_state {
+  int precision;
+  void *dev; /* Dev<float> or Dev<double> */
+};
+
+__host__ __device__ __forceinline__ long lvl_off(long l, long S1, long T) {
+  return 2 * S1 * T * ((1L << l) - 4);
+}
+
+/* ======================================================================== stage 1-2 */
+
+/* Deinterleave a tile of TMt points x all P sections into planar sections and write the
+ * tile's per-section sums.  x[m*P + sc] -> xt[(2 sc + ri) * M + m]. */
+template <typename R>
+__global__ void k_sections(const typename cplx<R>::T *__restrict__ x, R *__restrict__ xt,
+                           typename cplx<R>::T *__restrict__ part, long M, int P, int TMt,
+                           int conj_in) {
+  using C = typename cplx<R>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *tile = reinterpret_cast<C *>(smem_raw); /* [TMt][P] */
+  const long m0 = (long)blockIdx.x * TMt;
+  const int E = TMt * P;
+  for (int e = threadIdx.x; e < E; e += blockDim.x) {
+    C v = x[m0 * P + e];
+    if (conj_in) v.y = -v.y;
+    tile[e] = v;
+  }
+  __syncthreads();
+  /* planar store: plane (2sc+ri), TMt contiguous points */
+  for (int e = threadIdx.x; e < 2 * E; e += blockDim.x) {
+    int mm = e % TMt, q = e / TMt, sc = q >> 1, ri = q & 1;
+    C v = tile[mm * P + sc];
+    xt[(long)q * M + m0 + mm] = ri ? v.y : v.x;
+  }
+  /* tile sums per section, fixed order */
+  for (int sc = threadIdx.x; sc < P; sc += blockDim.x) {
+    C acc;
+    acc.x = 0, acc.y = 0;
+    for (int mm = 0; mm < TMt; ++mm) acc = cadd(acc, tile[mm * P + sc]);
+    part[(long)blockIdx.x * P + sc] = acc;
+  }
+}
+
+/* ssum[sc] = sum over tiles of part[tile][sc]: fixed-shape tree, so results do not depend on
+ * scheduling. */
+template <typename R>
+__global__ void k_sum_sections(const typename cplx<R>::T *__restrict__ part, long ntile, int P,
+                               typename cplx<R>::T *__restrict__ ssum) {
+  using C = typename cplx<R>::T;
+  __shared__ C red[256];
+  const int sc = blockIdx.x;
+  C acc;
+  acc.x = 0, acc.y = 0;
+  for (long t = threadIdx.x; t < ntile; t += blockDim.x) acc = cadd(acc, part[t * P + sc]);
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] = cadd(red[threadIdx.x], red[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) ssum[sc] = red[0];
+}
+
+/* ======================================================================== rowgemm */
+/* D[r][n] = sum_k A(r,k) B(k,n) for rows r < rows, n < N.  A rows are gathered from the
+ * stage's arrays by the problem object; B is a dense operator in global memory or generated
+ * (leaf).  Tile BM x BN x BK; each thread owns a TM x TN block of outputs. */
+
+template <typename R> struct ProbS2M {
+  const R *xt, *B;
+  R *out;
+  long rows, M;
+  int K, N;
+  __device__ void begin(int) {}
+  __device__ R a(long r, int k) const { return xt[2 * M + r * K + k]; }
+  __device__ R bv(int k, int n) const { return B[k * N + n]; }
+  __device__ R *d(long r) const { return out + r * N; }
+};
+
+template <typename R> struct ProbM2M { /* parent level L: A row = children pair of level L+1 */
+  const R *child, *B;
+  R *out;
+  long rows;
+  int K, N;
+  __device__ void begin(int) {}
+  __device__ R a(long r, int k) const { return child[r * K + k]; }
+  __device__ R bv(int k, int n) const { return B[k * N + n]; }
+  __device__ R *d(long r) const { return out + r * N; }
+};
+
+template <typename R> struct ProbTop { /* level 2: psi[c] = topflp . phi[c+2 mod 4] */
+  const R *phi2, *B;
+  R *out;
+  long rows;
+  int K, N;
+  __device__ void begin(int) {}
+  __device__ R a(long r, int k) const {
+    long pl = r >> 2, c = r & 3;
+    return phi2[(pl * 4 + ((c + 2) & 3)) * K + k];
+  }
+  __device__ R bv(int k, int n) const { return B[k * N + n]; }
+  __device__ R *d(long r) const { return out + r * N; }
+};
+
+/* Child level l, one row per parent box B (plane pl): A = [psi_{l-1}[B] | phi_l[2B-2, 2B-1] |
+ * phi_l[2B+2, 2B+3]] (K = 5T), output = psi_l[2B], psi_l[2B+1] (N = 2T). */
+template <typename R> struct ProbM2L {
+  const R *psi_par, *phi, *B;
+  R *out;
+  long rows;
+  int K, N, T, lpar; /* lpar = l - 1 */
+  __device__ void begin(int) {}
+  __device__ R a(long r, int k) const {
+    if (k < T) return psi_par[r * T + k];
+    long pl = r >> lpar, Bx = r & ((1L << lpar) - 1), mask = (2L << lpar) - 1;
+    long base = pl << (lpar + 1);
+    if (k < 3 * T) return phi[(base + ((2 * Bx - 2) & mask)) * T + (k - T)];
+    return phi[(base + ((2 * Bx + 2) & mask)) * T + (k - 3 * T)];
+  }
+  __device__ R bv(int k, int n) const { return B[k * N + n]; }
+  __device__ R *d(long r) const { return out + r * N; }
+};
+
+/* Leaf stage for one section (batch z = sc - 1): rows (ri, box), A = [psi_n[box] | x_sc over
+ * boxes box-1..box+1] (K = T + 3b), B = [E_sc ; Toeplitz cot], output u[plane][box*b + j]. */
+template <typename R> struct ProbLeaf {
+  const R *psi_n, *xt, *evalmT, *cot;
+  R *u;
+  long rows, M, s;
+  int K, N, T, b;
+  /* per batch */
+  const R *ps, *xs, *E, *ct;
+  R *us;
+  __device__ void begin(int z) {
+    long pl0 = 2L * z;
+    ps = psi_n + pl0 * s * T;
+    xs = xt + (pl0 + 2) * M;
+    E = evalmT + (long)z * T * b;
+    ct = cot + (long)z * 4 * b;
+    us = u + pl0 * M;
+  }
+  __device__ R a(long r, int k) const {
+    if (k < T) return ps[r * T + k];
+    long ri = r / s, bx = r - ri * s;
+    long m = (bx * b - b + (k - T)) & (M - 1);
+    return xs[ri * M + m];
+  }
+  __device__ R bv(int k, int n) const {
+    if (k < T) return E[k * b + n];
+    return ct[(k - T) + b - n];
+  }
+  __device__ R *d(long r) const {
+    long ri = r / s, bx = r - ri * s;
+    return us + ri * M + bx * b;
+  }
+};
+
+template <typename R, int BM, int BN, int BK, int TM, int TN, class Prob>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_rowgemm(Prob pb) {
+  constexpr int NTX = BN / TN;
+  constexpr int NT = (BM / TM) * NTX;
+  __shared__ R As[BK][BM + 1];
+  __shared__ R Bs[BK][BN + 1];
+  const int tid = threadIdx.x;
+  const int tn = tid % NTX, tm = tid / NTX;
+  const long row0 = (long)blockIdx.x * BM;
+  const int n0 = blockIdx.y * BN;
+  pb.begin(blockIdx.z);
+  R acc[TM][TN];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) acc[i][j] = R(0);
+  for (int k0 = 0; k0 < pb.K; k0 += BK) {
+    for (int e = tid; e < BM * BK; e += NT) {
+      int m = e / BK, kk = e - m * BK;
+      long r = row0 + m;
+      int k = k0 + kk;
+      As[kk][m] = (r < pb.rows && k < pb.K) ? pb.a(r, k) : R(0);
+    }
+    for (int e = tid; e < BK * BN; e += NT) {
+      int kk = e / BN, nn = e - kk * BN;
+      int k = k0 + kk, nc = n0 + nn;
+      Bs[kk][nn] = (k < pb.K && nc < pb.N) ? pb.bv(k, nc) : R(0);
+    }
+    __syncthreads();
+    /* Each BK slice is summed into its own partial before it joins the running total, so
+     * FP32 rounding grows like sqrt(BK) + sqrt(K/BK) instead of sqrt(K) for long K (the
+     * 3b-point near-field windows reach K = 6160 at b = 2048). */
+    R part[TM][TN];
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TN; ++j) part[i][j] = R(0);
+#pragma unroll 4
+    for (int kk = 0; kk < BK; ++kk) {
+      R av[TM], bw[TN];
+#pragma unroll
+      for (int i = 0; i < TM; ++i) av[i] = As[kk][tm * TM + i];
+#pragma unroll
+      for (int j = 0; j < TN; ++j) bw[j] = Bs[kk][tn * TN + j];
+#pragma unroll
+      for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) part[i][j] = fma(av[i], bw[j], part[i][j]);
+    }
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TN; ++j) acc[i][j] += part[i][j];
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < TM; ++i) {
+    long r = row0 + tm * TM + i;
+    if (r >= pb.rows) continue;
+    R *dst = pb.d(r);
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      int nc = n0 + tn * TN + j;
+      if (nc < pb.N) dst[nc] = acc[i][j];
+    }
+  }
+}
+
+template <typename R, class Prob>
+static void launch_rowgemm(const Prob &pb, long rows_per_batch, int N, int batches,
+                           cudaStream_t st) {
+  if (rows_per_batch <= 32 && N > 64) {
+    dim3 g((unsigned)((rows_per_batch + 15) / 16), (unsigned)((N + 63) / 64), batches);
+    k_rowgemm<R, 16, 64, 16, 2, 2, Prob><<<g, 256, 0, st>>>(pb);
+  } else if (N <= 32) {
+    dim3 g((unsigned)((rows_per_batch + 127) / 128), 1, batches);
+    k_rowgemm<R, 128, 32, 16, 8, 4, Prob><<<g, 128, 0, st>>>(pb);
+  } else {
+    dim3 g((unsigned)((rows_per_batch + 63) / 64), (unsigned)((N + 63) / 64), batches);
+    k_rowgemm<R, 64, 64, 16, 4, 4, Prob><<<g, 256, 0, st>>>(pb);
+  }
+}
+
+/* First point of each leaf box for the sections whose shifted target leaves its box
+ * (sc >= P/2): reference fmmfft.c:771-803 (far) and :839-954 (near).  For sc > P/2 the value
+ * comes from box-1 (local expansion evalmh, window box-2..box with the cotsh offsets); for
+ * sc = P/2 it is the mean of that and the in-box value the rowgemm stored. */
+template <typename R>
+__global__ void k_leaf_fix(const R *__restrict__ psi_n, const R *__restrict__ xt,
+                           const R *__restrict__ evalmh, const R *__restrict__ cot,
+                           R *__restrict__ u, long M, long s, int T, int b, int P) {
+  const int sc = P / 2 + blockIdx.y; /* sc in [P/2, P-1] */
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= 2 * s) return;
+  const long ri = idx / s, bx = idx - ri * s;
+  const long pl = 2L * (sc - 1) + ri;
+  const R *pp = psi_n + (pl * s + ((bx - 1) & (s - 1))) * T;
+  const R *eh = evalmh + (long)(sc - 1) * T;
+  R far = 0;
+  for (int k = 0; k < T; ++k) far = fma(pp[k], eh[k], far);
+  const R *xs = xt + (pl + 2) * M;
+  const R *ct = cot + (long)(sc - 1) * 4 * b;
+  R near = 0;
+  for (int q = 0; q < 3 * b; ++q) near = fma(xs[(bx * b - 2 * b + q) & (M - 1)], ct[q], near);
+  R v = far + near;
+  R *dst = u + pl * M + bx * b;
+  if (2 * sc > P)
+    *dst = v;
+  else
+    *dst = R(0.5) * (*dst + v);
+}
+
+/* ======================================================================== shared-memory FFT */
+
+/* W independent forward DFTs of length L held in shared memory as buf[i*W + w].  Stockham
+ * radix-4 stages (one radix-2 stage first when log2 L is odd), ping-ponging between buf and
+ * alt; returns the buffer that holds the result.  Twiddle exp(-2 pi i t / L) = tw[t * tws]. */
+template <typename C>
+__device__ C *smem_fft(C *buf, C *alt, int L, int W, const C *__restrict__ tw, long tws) {
+  int Ns = 1;
+  if (__ffs(L) & 1) { /* log2 L even: all radix-4 */
+  } else { /* odd: one radix-2 stage */
+    const int half = L / 2;
+    for (int e = threadIdx.x; e < half * W; e += blockDim.x) {
+      int j = e / W, w = e - j * W;
+      C v0 = buf[j * W + w], v1 = buf[(j + half) * W + w];
+      C a = cadd(v0, v1), c = csub(v0, v1);
+      alt[(2 * j) * W + w] = a;
+      alt[(2 * j + 1) * W + w] = c;
+    }
+    __syncthreads();
+    C *t = buf;
+    buf = alt, alt = t;
+    Ns = 2;
+  }
+  const int q4 = L / 4;
+  for (; Ns < L; Ns *= 4) {
+    for (int e = threadIdx.x; e < q4 * W; e += blockDim.x) {
+      int j = e / W, w = e - j * W;
+      int k = j % Ns;
+      C v0 = buf[j * W + w], v1 = buf[(j + q4) * W + w], v2 = buf[(j + 2 * q4) * W + w],
+        v3 = buf[(j + 3 * q4) * W + w];
+      if (Ns > 1) {
+        long ts = (long)k * (L / (Ns * 4)) * tws;
+        v1 = cmul(v1, tw[ts]);
+        v2 = cmul(v2, tw[2 * ts]);
+        v3 = cmul(v3, tw[3 * ts]);
+      }
+      C a = cadd(v0, v2), bq = csub(v0, v2), c = cadd(v1, v3), d = csub(v1, v3);
+      C dd;
+      dd.x = d.y, dd.y = -d.x; /* -i * d */
+      int o = (j / Ns) * Ns * 4 + k;
+      alt[(o)*W + w] = cadd(a, c);
+      alt[(o + Ns) * W + w] = cadd(bq, dd);
+      alt[(o + 2 * Ns) * W + w] = csub(a, c);
+      alt[(o + 3 * Ns) * W + w] = csub(bq, dd);
+    }
+    __syncthreads();
+    C *t = buf;
+    buf = alt, alt = t;
+  }
+  return buf;
+}
+
+/* One FFT pass over `nseq` sequences of length L:
+ *   element i of sequence g (g = batch*per + w) is read from in[ibase(g) + i*istride],
+ *   transformed, optionally multiplied by exp(-2 pi i * post(g) * kout / M) (4-step twiddle),
+ *   and written to out[obase(g) + kout*ostride].
+ * Sequences come in groups of W per block; `per` sequences per batch row (row = block of M). */
+struct FftPass {
+  int L, W, per;     /* per: sequences per row */
+  long M;            /* row length */
+  long iseq, istr;   /* input: seq stride, element stride (within a row) */
+  long oseq, ostr;   /* output */
+  int twiddle_post;  /* apply exp(-2 pi i * w_global * k / M) */
+  long tws;          /* twiddle stride into twM for length-L DFTs: M / L */
+  int conj_out;
+};
+
+template <typename R>
+__global__ void k_fft_pass(const typename cplx<R>::T *__restrict__ in,
+                           typename cplx<R>::T *__restrict__ out,
+                           const typename cplx<R>::T *__restrict__ twM, FftPass fp) {
+  using C = typename cplx<R>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *buf = reinterpret_cast<C *>(smem_raw);
+  C *alt = buf + (long)fp.L * fp.W;
+  const long row = blockIdx.y;
+  const long g0 = (long)blockIdx.x * fp.W; /* first sequence of this block within the row */
+  const C *src = in + row * fp.M;
+  C *dst = out + row * fp.M;
+  const int LW = fp.L * fp.W;
+  if (fp.istr == 1) {
+    for (int e = threadIdx.x; e < LW; e += blockDim.x) {
+      int i = e % fp.L, w = e / fp.L;
+      buf[i * fp.W + w] = src[(g0 + w) * fp.iseq + i];
+    }
+  } else {
+    for (int e = threadIdx.x; e < LW; e += blockDim.x) {
+      int w = e % fp.W, i = e / fp.W;
+      buf[i * fp.W + w] = src[(g0 + w) * fp.iseq + (long)i * fp.istr];
+    }
+  }
+  __syncthreads();
+  C *res = smem_fft<C>(buf, alt, fp.L, fp.W, twM, fp.tws);
+  if (fp.ostr == 1) {
+    for (int e = threadIdx.x; e < LW; e += blockDim.x) {
+      int i = e % fp.L, w = e / fp.L;
+      C v = res[i * fp.W + w];
+      if (fp.twiddle_post) v = cmul(v, twM[((g0 + w) * i) & (fp.M - 1)]);
+      if (fp.conj_out) v.y = -v.y;
+      dst[(g0 + w) * fp.oseq + i] = v;
+    }
+  } else {
+    for (int e = threadIdx.x; e < LW; e += blockDim.x) {
+      int w = e % fp.W, i = e / fp.W;
+      C v = res[i * fp.W + w];
+      if (fp.twiddle_post) v = cmul(v, twM[((g0 + w) * i) & (fp.M - 1)]);
+      if (fp.conj_out) v.y = -v.y;
+      dst[(g0 + w) * fp.oseq + (long)i * fp.ostr] = v;
+    }
+  }
+}
+
+/* ======================================================================== combine */
+
+/* For TMc points m and every section: w_0 = x_0[m], w_sc = c_sc (u_sc[m] - (i/M) Ssum_sc),
+ * z_r[m] = sum_sc exp(-2 pi i sc r / P) w_sc[m] (a length-P DFT), written to z[r][m]. */
+template <typename R>
+__global__ void k_combine(const R *__restrict__ xt, const R *__restrict__ u,
+                          const typename cplx<R>::T *__restrict__ ssum,
+                          const typename cplx<R>::T *__restrict__ pretw,
+                          const typename cplx<R>::T *__restrict__ twP,
+                          typename cplx<R>::T *__restrict__ z, long M, int P, int TMc) {
+  using C = typename cplx<R>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *buf = reinterpret_cast<C *>(smem_raw); /* [P][TMc] */
+  C *alt = buf + (long)P * TMc;
+  const long m0 = (long)blockIdx.x * TMc;
+  const R invM = R(1) / R(M);
+  for (int e = threadIdx.x; e < P * TMc; e += blockDim.x) {
+    int mm = e % TMc, sc = e / TMc;
+    C w;
+    if (sc == 0) {
+      w.x = xt[m0 + mm];
+      w.y = xt[M + m0 + mm];
+    } else {
+      C v;
+      C S = ssum[sc];
+      v.x = u[(2L * (sc - 1)) * M + m0 + mm] + S.y * invM; /* u - i S / M */
+      v.y = u[(2L * (sc - 1) + 1) * M + m0 + mm] - S.x * invM;
+      w = cmul(pretw[sc], v);
+    }
+    buf[sc * TMc + mm] = w;
+  }
+  __syncthreads();
+  C *res = smem_fft<C>(buf, alt, P, TMc, twP, 1);
+  for (int e = threadIdx.x; e < P * TMc; e += blockDim.x) {
+    int mm = e % TMc, r = e / TMc;
+    z[(long)r * M + m0 + mm] = res[r * TMc + mm];
+  }
+}
+
+/* Bin 0 of every output block, y[r M], equals sum_n x[n] exp(-2 pi i n r / P), i.e. the
+ * length-P DFT of the section sums that stage 2 already holds.  Through the FMM that bin is
+ * reached via the cot kernel's zero-frequency eigenvalue -cot(pi sc / P) (about 20 for
+ * sc = 1, P = 64), which the pre-twiddle c_sc then cancels; in FP32 the amplified rounding
+ * makes these P bins the least accurate of the transform.  FP32 plans with >= 10 terms
+ * therefore evaluate them from this identity, in FP64. */
+template <typename R>
+__global__ void k_block_dc(const typename cplx<R>::T *__restrict__ ssum,
+                           typename cplx<R>::T *__restrict__ y, long M, int P, int conj_out) {
+  using C = typename cplx<R>::T;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= P) return;
+  double re = 0, im = 0;
+  for (int sc = 0; sc < P; ++sc) {
+    double sn, cs;
+    sincospi(-2.0 * (double)((long)sc * r % P) / (double)P, &sn, &cs);
+    C v = ssum[sc];
+    re += (double)v.x * cs - (double)v.y * sn;
+    im += (double)v.x * sn + (double)v.y * cs;
+  }
+  C out;
+  out.x = (R)re;
+  out.y = (R)(conj_out ? -im : im);
+  y[(long)r * M] = out;
+}
+
+/* ======================================================================== host orchestration */
+
+template <typename R> static int upload(R **dst, const double *src, size_t n, char *err, size_t errlen) {
+  R *h = (R *)malloc(sizeof(R) * (n ? n : 1));
+  if (!h) return 2;
+  for (size_t i = 0; i < n; ++i) h[i] = (R)src[i];
+  cudaError_t e = cudaMemcpy(*dst, h, sizeof(R) * n, cudaMemcpyHostToDevice);
+  free(h);
+  if (e != cudaSuccess) {
+    snprintf(err, errlen, "cudaMemcpy: %s", cudaGetErrorString(e));
+    return 3;
+  }
+  return 0;
+}
+
+static inline size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
+static inline long pow2_floor(long v) {
+  long p = 1;
+  while (p * 2 <= v) p *= 2;
+  return p;
+}
+
+template <typename R>
+static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err, size_t errlen) {
+  using C = typename cplx<R>::T;
+  Dev<R> *d = new (std::nothrow) Dev<R>();
+  if (!d) return 2;
+  memset((void *)d, 0, sizeof(*d));
+  const long M = o->M, P = o->P, T = o->T, b = o->b, s = o->s, n = o->n, S1 = P - 1;
+  d->M = M, d->P = P, d->T = T, d->b = b, d->s = s, d->n = n, d->N = M * P, d->S1 = S1;
+  d->precision = precision;
+  d->tileM = P >= 2048 ? 1 : 2048 / P;
+  if (d->tileM > M) d->tileM = M;
+  d->ntile = M / d->tileM;
+  /* size-M FFT split */
+  const long LMAX = sizeof(R) == 4 ? 4096 : 2048;
+  if (M <= LMAX) {
+    d->M1 = M, d->M2 = 1;
+  } else {
+    long lg = 0;
+    while ((1L << lg) < M) ++lg;
+    d->M2 = 1L << ((lg + 1) / 2);
+    d->M1 = M / d->M2;
+  }
+  const long nlev = n - 2 > 0 ? n - 2 : 0;
+  const long lvtot = 2 * S1 * T * ((2L << n) - 4);
+  size_t off = 0;
+#define CARVE(field, count, type)          \
+  size_t off_##field = off;                \
+  off = align_up(off + sizeof(type) * (size_t)(count));
+  CARVE(initch, b * T, R)
+  CARVE(btop, T * T, R)
+  CARVE(bm2m, (nlev ? nlev : 1) * 2 * T * T, R)
+  CARVE(bm2l, (nlev ? nlev : 1) * 10 * T * T, R)
+  CARVE(evalmT, S1 * T * b, R)
+  CARVE(evalmh, S1 * T, R)
+  CARVE(cot, S1 * 4 * b, R)
+  CARVE(pretw, P, C)
+  CARVE(twP, P, C)
+  CARVE(twM, M, C)
+  CARVE(xt, 2 * P * M, R)
+  CARVE(part, d->ntile * P, C)
+  CARVE(ssum, P, C)
+  CARVE(phi, lvtot, R)
+  CARVE(psi, lvtot, R)
+  CARVE(u, 2 * S1 * M, R)
+  CARVE(z, P * M, C)
+  CARVE(tmp, P * M, C)
+#undef CARVE
+  void *pool = NULL;
+  cudaError_t ce = cudaMalloc(&pool, off);
+  if (ce != cudaSuccess) {
+    snprintf(err, errlen, "cudaMalloc(%zu): %s", off, cudaGetErrorString(ce));
+    delete d;
+    return 2;
+  }
+  d->pool = pool;
+  d->bytes = off;
+  char *base = (char *)pool;
+  d->initch = (R *)(base + off_initch);
+  d->btop = (R *)(base + off_btop);
+  d->bm2m = (R *)(base + off_bm2m);
+  d->bm2l = (R *)(base + off_bm2l);
+  d->evalmT = (R *)(base + off_evalmT);
+  d->evalmh = (R *)(base + off_evalmh);
+  d->cot = (R *)(base + off_cot);
+  d->pretw = (C *)(base + off_pretw);
+  d->twP = (C *)(base + off_twP);
+  d->twM = (C *)(base + off_twM);
+  d->xt = (R *)(base + off_xt);
+  d->part = (C *)(base + off_part);
+  d->ssum = (C *)(base + off_ssum);
+  d->phi = (R *)(base + off_phi);
+  d->psi = (R *)(base + off_psi);
+  d->z = (C *)(base + off_z);
+  d->tmp = (C *)(base + off_tmp);
+  d->u = (R *)(base + off_u);
+
+  /* ---- operator layouts (FP64 on the host, rounded once to R) ---- */
+  int rc = 0;
+  size_t hn = (size_t)(10 * T * T);
+  if ((size_t)(S1 * T * b) > hn) hn = (size_t)(S1 * T * b);
+  if ((size_t)(2 * P) > hn) hn = (size_t)(2 * P);
+  double *h = (double *)malloc(sizeof(double) * (hn + 16));
+  if (!h) return 2;
+  rc |= upload<R>(&d->initch, o->initch, b * T, err, errlen);
+  for (long k = 0; k < T; ++k)
+    for (long t = 0; t < T; ++t) h[k * T + t] = o->topflp[t * T + k];
+  rc |= upload<R>(&d->btop, h, T * T, err, errlen);
+  for (long L = 2; L <= n - 1; ++L) { /* M2M parent level L uses shftfn/fp index L-2 */
+    const double *ops = o->levops + (L - 2) * FMM_NLEVOPS * T * T;
+    for (long k = 0; k < T; ++k)
+      for (long t = 0; t < T; ++t) {
+        h[k * T + t] = ops[FMM_SHFTFN * T * T + t * T + k];
+        h[(T + k) * T + t] = ops[FMM_SHFTFP * T * T + t * T + k];
+      }
+    R *dst = d->bm2m + (L - 2) * 2 * T * T;
+    rc |= upload<R>(&dst, h, 2 * T * T, err, errlen);
+  }
+  for (long l = 3; l <= n; ++l) { /* M2L+L2L child level l uses index l-3 */
+    const double *ops = o->levops + (l - 3) * FMM_NLEVOPS * T * T;
+#define OPT(which, t, k) ops[(which) * T * T + (t) * T + (k)]
+    const long N2 = 2 * T;
+    for (long i = 0; i < 10 * T * T; ++i) h[i] = 0;
+    for (long k = 0; k < T; ++k)
+      for (long t = 0; t < T; ++t) {
+        h[(0 * T + k) * N2 + t] = OPT(FMM_SHFTLP, t, k);     /* psi parent -> left */
+        h[(0 * T + k) * N2 + T + t] = OPT(FMM_SHFTLN, t, k); /* psi parent -> right */
+        h[(1 * T + k) * N2 + t] = OPT(FMM_FLIP2P, t, k);     /* phi[2B-2] -> left  (c-2) */
+        h[(1 * T + k) * N2 + T + t] = OPT(FMM_FLIP3P, t, k); /* phi[2B-2] -> right (c-3) */
+        h[(2 * T + k) * N2 + T + t] = OPT(FMM_FLIP2P, t, k); /* phi[2B-1] -> right (c-2) */
+        h[(3 * T + k) * N2 + t] = OPT(FMM_FLIP2N, t, k);     /* phi[2B+2] -> left  (c+2) */
+        h[(4 * T + k) * N2 + t] = OPT(FMM_FLIP3N, t, k);     /* phi[2B+3] -> left  (c+3) */
+        h[(4 * T + k) * N2 + T + t] = OPT(FMM_FLIP2N, t, k); /* phi[2B+3] -> right (c+2) */
+      }
+#undef OPT
+    R *dst = d->bm2l + (l - 3) * 10 * T * T;
+    rc |= upload<R>(&dst, h, 10 * T * T, err, errlen);
+  }
+  for (long sc = 1; sc < P; ++sc)
+    for (long k = 0; k < T; ++k)
+      for (long j = 0; j < b; ++j) h[((sc - 1) * T + k) * b + j] = o->evalm[(j * S1 + (sc - 1)) * T + k];
+  rc |= upload<R>(&d->evalmT, h, S1 * T * b, err, errlen);
+  for (long i = 0; i < S1 * T; ++i) h[i] = 0;
+  for (long sc = P / 2; sc < P; ++sc)
+    for (long k = 0; k < T; ++k) h[(sc - 1) * T + k] = o->evalmh[(sc - P / 2) * T + k];
+  rc |= upload<R>(&d->evalmh, h, S1 * T, err, errlen);
+  rc |= upload<R>(&d->cot, o->cot, S1 * 4 * b, err, errlen);
+  const double PI = 3.14159265358979323846264338327950288;
+  h[0] = 0, h[1] = 0;
+  for (long sc = 1; sc < P; ++sc) {
+    h[2 * sc] = -cos(PI * sc / P) * sin(PI * sc / P);
+    h[2 * sc + 1] = sin(PI * sc / P) * sin(PI * sc / P);
+  }
+  rc |= upload<R>((R **)&d->pretw, h, 2 * P, err, errlen);
+  for (long k = 0; k < P; ++k) h[2 * k] = cos(2 * PI * k / P), h[2 * k + 1] = -sin(2 * PI * k / P);
+  rc |= upload<R>((R **)&d->twP, h, 2 * P, err, errlen);
+  free(h);
+  double *hm = (double *)malloc(sizeof(double) * 2 * (size_t)M);
+  if (!hm) return 2;
+  for (long k = 0; k < M; ++k) {
+    double a = 2 * PI * (double)k / (double)M;
+    hm[2 * k] = cos(a), hm[2 * k + 1] = -sin(a);
+  }
+  rc |= upload<R>((R **)&d->twM, hm, 2 * M, err, errlen);
+  free(hm);
+  if (rc) {
+    cudaFree(pool);
+    delete d;
+    return rc;
+  }
+  *out = d;
+  return 0;
+}
+
+template <typename R>
+static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, int inverse,
+                       char *err, size_t errlen) {
+  using C = typename cplx<R>::T;
+  const long M = d->M, P = d->P, T = d->T, b = d->b, s = d->s, n = d->n, S1 = d->S1;
+  const C *x = (const C *)vin;
+  C *y = (C *)vout;
+  Prof &pf = d->prof;
+  const int slot = (pf.on && pf.count < pf.cap) ? pf.count++ : -1;
+  int cur = -1;
+  auto stage = [&](int id) {
+    if (slot >= 0)
+      for (int k = cur + 1; k <= id; ++k) cudaEventRecord(pf.ev[slot * (ST_COUNT + 1) + k], st);
+    cur = id;
+  };
+  for (int k = 0; k < ST_COUNT; ++k) pf.launches[k] = 0;
+  /* 1-2: sections and their sums */
+  stage(ST_SECTIONS);
+  {
+    int TMt = (int)d->tileM;
+    size_t sm = sizeof(C) * TMt * P;
+    k_sections<R><<<(unsigned)d->ntile, 256, sm, st>>>(x, d->xt, d->part, M, (int)P, TMt, inverse);
+    pf.launches[ST_SECTIONS]++;
+    stage(ST_SUMS);
+    k_sum_sections<R><<<(unsigned)P, 256, 0, st>>>(d->part, d->ntile, (int)P, d->ssum);
+    pf.launches[ST_SUMS]++;
+  }
+  /* 3: S2M at level n */
+  stage(ST_S2M);
+  {
+    ProbS2M<R> pb{d->xt, d->initch, d->phi + lvl_off(n, S1, T), 2 * S1 * s, M, (int)b, (int)T};
+    launch_rowgemm<R>(pb, pb.rows, (int)T, 1, st);
+    pf.launches[ST_S2M]++;
+  }
+  /* 4: M2M, parent level L = n-1 .. 2 */
+  stage(ST_M2M);
+  for (long L = n - 1; L >= 2; --L) {
+    ProbM2M<R> pb{d->phi + lvl_off(L + 1, S1, T), d->bm2m + (L - 2) * 2 * T * T,
+                  d->phi + lvl_off(L, S1, T), 2 * S1 * (1L << L), (int)(2 * T), (int)T};
+    launch_rowgemm<R>(pb, pb.rows, (int)T, 1, st);
+    pf.launches[ST_M2M]++;
+  }
+  /* 5: top flip */
+  stage(ST_TOP);
+  {
+    ProbTop<R> pb{d->phi + lvl_off(2, S1, T), d->btop, d->psi + lvl_off(2, S1, T), 2 * S1 * 4,
+                  (int)T, (int)T};
+    launch_rowgemm<R>(pb, pb.rows, (int)T, 1, st);
+    pf.launches[ST_TOP]++;
+  }
+  /* 6: M2L + L2L, child level l = 3..n (rows = parent boxes) */
+  stage(ST_M2L);
+  for (long l = 3; l <= n; ++l) {
+    ProbM2L<R> pb{d->psi + lvl_off(l - 1, S1, T), d->phi + lvl_off(l, S1, T),
+                  d->bm2l + (l - 3) * 10 * T * T, d->psi + lvl_off(l, S1, T),
+                  2 * S1 * (1L << (l - 1)), (int)(5 * T), (int)(2 * T), (int)T, (int)(l - 1)};
+    launch_rowgemm<R>(pb, pb.rows, (int)(2 * T), 1, st);
+    pf.launches[ST_M2L]++;
+  }
+  /* 7: leaf far + near field per section, then the half-shifted first points */
+  stage(ST_LEAF);
+  {
+    ProbLeaf<R> pb{};
+    pb.psi_n = d->psi + lvl_off(n, S1, T);
+    pb.xt = d->xt;
+    pb.evalmT = d->evalmT;
+    pb.cot = d->cot;
+    pb.u = d->u;
+    pb.rows = 2 * s, pb.M = M, pb.s = s;
+    pb.K = (int)(T + 3 * b), pb.N = (int)b, pb.T = (int)T, pb.b = (int)b;
+    launch_rowgemm<R>(pb, pb.rows, (int)b, (int)S1, st);
+    pf.launches[ST_LEAF]++;
+    stage(ST_LEAFFIX);
+    pf.launches[ST_LEAFFIX]++;
+    dim3 g((unsigned)((2 * s + 127) / 128), (unsigned)(P - P / 2));
+    k_leaf_fix<R><<<g, 128, 0, st>>>(pb.psi_n, d->xt, d->evalmh, d->cot, d->u, M, s, (int)T,
+                                     (int)b, (int)P);
+  }
+  /* 8: combine -> z[P][M] */
+  stage(ST_COMBINE);
+  pf.launches[ST_COMBINE]++;
+  {
+    int TMc = (int)(P >= 1024 ? 1 : (1024 / P < 32 ? 1024 / P : 32));
+    if (TMc > M) TMc = (int)M;
+    size_t sm = 2 * sizeof(C) * (size_t)P * TMc;
+    k_combine<R><<<(unsigned)(M / TMc), 256, sm, st>>>(d->xt, d->u, d->ssum, d->pretw, d->twP,
+                                                        d->z, M, (int)P, TMc);
+  }
+  /* 9: size-M FFTs, z -> y */
+  stage(ST_FFT1);
+  {
+    const long SMEM = 96 * 1024;
+    if (d->M2 == 1) {
+      int W = (int)pow2_floor(SMEM / (long)(2 * sizeof(C) * M));
+      if (W > P) W = (int)P;
+      FftPass fp{(int)M, 1, 1, M, M, 1, M, 1, 0, 1, inverse};
+      /* W rows per block: treat W consecutive rows as one "row" of W sequences */
+      fp.W = W, fp.per = W, fp.M = M * W, fp.iseq = M, fp.oseq = M;
+      dim3 g(1, (unsigned)(P / W));
+      size_t sm = 2 * sizeof(C) * (size_t)M * W;
+      k_fft_pass<R><<<g, 256, sm, st>>>(d->z, y, d->twM, fp);
+      pf.launches[ST_FFT1]++;
+    } else {
+      const long M1 = d->M1, M2 = d->M2;
+      /* pass 1: for each m1, DFT over m2 (stride M1), twiddle, store tmp[k2*M1 + m1] */
+      int W1 = (int)pow2_floor(SMEM / (long)(2 * sizeof(C) * M2));
+      if (W1 > 16) W1 = 16;
+      if (W1 > M1) W1 = (int)M1;
+      FftPass f1{(int)M2, W1, (int)M1, M, 1, M1, 1, M1, 1, M / M2, 0};
+      dim3 g1((unsigned)(M1 / W1), (unsigned)P);
+      k_fft_pass<R><<<g1, 256, 2 * sizeof(C) * (size_t)M2 * W1, st>>>(d->z, d->tmp, d->twM, f1);
+      pf.launches[ST_FFT1]++;
+      stage(ST_FFT2);
+      /* pass 2: for each k2, DFT over m1 (contiguous), store y[k2 + M2*k1] */
+      int W2 = (int)pow2_floor(SMEM / (long)(2 * sizeof(C) * M1));
+      if (W2 > 16) W2 = 16;
+      if (W2 > M2) W2 = (int)M2;
+      FftPass f2{(int)M1, W2, (int)M2, M, M1, 1, 1, M2, 0, M / M1, inverse};
+      dim3 g2((unsigned)(M2 / W2), (unsigned)P);
+      k_fft_pass<R><<<g2, 256, 2 * sizeof(C) * (size_t)M1 * W2, st>>>(d->tmp, y, d->twM, f2);
+      pf.launches[ST_FFT2]++;
+    }
+  }
+  stage(ST_DC);
+  /* below 10 terms the FMM's own truncation at these bins exceeds FP32 resolution (3e-8 at
+   * 10 terms, 5e-6 at 8), and the reference's value is the FMM one, so it is kept */
+  if (sizeof(R) == 4 && T >= 10) {
+    k_block_dc<R><<<(unsigned)((P + 127) / 128), 128, 0, st>>>(d->ssum, y, M, (int)P, inverse);
+    pf.launches[ST_DC]++;
+  }
+  if (slot >= 0) cudaEventRecord(pf.ev[slot * (ST_COUNT + 1) + ST_COUNT], st);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    snprintf(err, errlen, "kernel launch: %s", cudaGetErrorString(e));
+    return 3;
+  }
+  return 0;
+}
+
+/* ======================================================================== C interface */
+
+static int set_smem_limits(void) {
+  static int done = 0;
+  if (done) return 0;
+  int maxopt = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  int lim = maxopt > 0 ? maxopt : 48 * 1024;
+  cudaFuncSetAttribute(k_fft_pass<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_pass<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_combine<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_combine<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_sections<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_sections<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  done = 1;
+  return 0;
+}
+
+extern "C" int fmmk_device_ok(char *err, size_t errlen) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    snprintf(err, errlen, "no CUDA device: %s", cudaGetErrorString(e));
+    return 4;
+  }
+  int dev = 0, major = 0, minor = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+  if (major != 10 || minor != 0) {
+    snprintf(err, errlen, "device is sm_%d%d; this library is built for sm_100a only", major, minor);
+    return 4;
+  }
+  return 0;
+}
+
+extern "C" int fmmk_create(const fmm_ops64 *ops, int precision, fmmk_state **out,
+                           size_t *device_bytes, char *err, size_t errlen) {
+  int rc = fmmk_device_ok(err, errlen);
+  if (rc) return rc;
+  set_smem_limits();
+  fmmk_state *st = (fmmk_state *)calloc(1, sizeof(fmmk_state));
+  if (!st) return 2;
+  st->precision = precision;
+  if (precision == 0) {
+    Dev<double> *d = NULL;
+    rc = dev_create<double>(ops, precision, &d, err, errlen);
+    st->dev = d;
+    if (!rc && device_bytes) *device_bytes = d->bytes;
+  } else {
+    Dev<float> *d = NULL;
+    rc = dev_create<float>(ops, precision, &d, err, errlen);
+    st->dev = d;
+    if (!rc && device_bytes) *device_bytes = d->bytes;
+  }
+  if (rc) {
+    free(st);
+    return rc;
+  }
+  *out = st;
+  return 0;
+}
+
+extern "C" void fmmk_destroy(fmmk_state *st) {
+  if (!st) return;
+  if (st->precision == 0) {
+    Dev<double> *d = (Dev<double> *)st->dev;
+    if (d) cudaFree(d->pool), delete d;
+  } else {
+    Dev<float> *d = (Dev<float> *)st->dev;
+    if (d) cudaFree(d->pool), delete d;
+  }
+  free(st);
+}
+
+extern "C" int fmmk_execute(fmmk_state *st, const void *d_in, void *d_out, void *stream,
+                            int inverse, char *err, size_t errlen) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (st->precision == 0) return dev_execute<double>((Dev<double> *)st->dev, d_in, d_out, s, inverse, err, errlen);
+  return dev_execute<float>((Dev<float> *)st->dev, d_in, d_out, s, inverse, err, errlen);
+}
+
+extern "C" int fmmk_execute_host(fmmk_state *st, const void *h_in, void *h_out, void *stream,
+                                 char *err, size_t errlen) {
+  cudaStream_t s = (cudaStream_t)stream;
+  long N;
+  size_t esz;
+  void *work;
+  if (st->precision == 0) {
+    Dev<double> *d = (Dev<double> *)st->dev;
+    N = d->N, esz = sizeof(double2), work = d->z;
+  } else {
+    Dev<float> *d = (Dev<float> *)st->dev;
+    N = d->N, esz = sizeof(float2), work = d->z;
+  }
+  /* the input lands in z (dead until the combine), the output is produced in tmp's place by
+   * the FFT and copied back; z and tmp are both [P][M] complex */
+  void *outbuf = NULL;
+  if (st->precision == 0)
+    outbuf = ((Dev<double> *)st->dev)->tmp;
+  else
+    outbuf = ((Dev<float> *)st->dev)->tmp;
+  (void)outbuf;
+  FMM_CUDA_TRY(cudaMemcpyAsync(work, h_in, esz * (size_t)N, cudaMemcpyHostToDevice, s));
+  /* in-place execute on the staged copy: stage 1 consumes z before z is rewritten */
+  int rc = fmmk_execute(st, work, work, stream, 0, err, errlen);
+  if (rc) return rc;
+  FMM_CUDA_TRY(cudaMemcpyAsync(h_out, work, esz * (size_t)N, cudaMemcpyDeviceToHost, s));
+  FMM_CUDA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
+template <typename R>
+static int fetch(Dev<R> *d, double *u, double *z, double *phi, double *psi) {
+  const long M = d->M, P = d->P, T = d->T, n = d->n, S1 = d->S1;
+  cudaDeviceSynchronize();
+  auto grab = [](const void *src, size_t count, double *dst) -> int {
+    R *h = (R *)malloc(sizeof(R) * count);
+    if (!h) return 2;
+    if (cudaMemcpy(h, src, sizeof(R) * count, cudaMemcpyDeviceToHost) != cudaSuccess) {
+      free(h);
+      return 3;
+    }
+    for (size_t i = 0; i < count; ++i) dst[i] = (double)h[i];
+    free(h);
+    return 0;
+  };
+  int rc = 0;
+  if (u) rc |= grab(d->u, (size_t)(2 * S1 * M), u);
+  if (z) rc |= grab(d->z, (size_t)(2 * P * M), z);
+  size_t lv = (size_t)(2 * S1 * T * ((2L << n) - 4));
+  if (phi) rc |= grab(d->phi, lv, phi);
+  if (psi) rc |= grab(d->psi, lv, psi);
+  return rc;
+}
+
+extern "C" int fmmk_debug_fetch(fmmk_state *st, double *u, double *z, double *phi, double *psi) {
+  if (st->precision == 0) return fetch<double>((Dev<double> *)st->dev, u, z, phi, psi);
+  return fetch<float>((Dev<float> *)st->dev, u, z, phi, psi);
+}
+
+/* ======================================================================== profiling */
+
+template <typename R> static Prof *prof_of(fmmk_state *st) { return &((Dev<R> *)st->dev)->prof; }
+
+extern "C" int fmmk_profile_start(fmmk_state *st, int cap) {
+  Prof *pf = st->precision == 0 ? prof_of<double>(st) : prof_of<float>(st);
+  if (pf->ev) return 1;
+  if (cap < 1) cap = 1;
+  pf->ev = (cudaEvent_t *)calloc((size_t)cap * (ST_COUNT + 1), sizeof(cudaEvent_t));
+  if (!pf->ev) return 2;
+  for (int i = 0; i < cap * (ST_COUNT + 1); ++i)
+    if (cudaEventCreate(&pf->ev[i]) != cudaSuccess) return 3;
+  pf->cap = cap, pf->count = 0, pf->on = 1;
+  return 0;
+}
+
+/* Sums, over the executes recorded since start, the device time of each stage (ms) and reports
+ * the kernel launches per execute of each stage; frees the events.  Returns the stage count. */
+extern "C" int fmmk_profile_stop(fmmk_state *st, double *stage_ms, int *stage_launches, int cap,
+                                 int *nexec) {
+  Prof *pf = st->precision == 0 ? prof_of<double>(st) : prof_of<float>(st);
+  if (!pf->ev) return -1;
+  int n = cap < ST_COUNT ? cap : ST_COUNT;
+  for (int k = 0; k < n; ++k) stage_ms[k] = 0, stage_launches[k] = pf->launches[k];
+  if (pf->count > 0) cudaEventSynchronize(pf->ev[(pf->count - 1) * (ST_COUNT + 1) + ST_COUNT]);
+  for (int e = 0; e < pf->count; ++e)
+    for (int k = 0; k < n; ++k) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, pf->ev[e * (ST_COUNT + 1) + k], pf->ev[e * (ST_COUNT + 1) + k + 1]);
+      stage_ms[k] += ms;
+    }
+  if (nexec) *nexec = pf->count;
+  for (int i = 0; i < pf->cap * (ST_COUNT + 1); ++i) cudaEventDestroy(pf->ev[i]);
+  free(pf->ev);
+  pf->ev = NULL, pf->on = 0, pf->count = 0, pf->cap = 0;
+  return ST_COUNT;
+}
+
+extern "C" const char *fmmk_stage_name(int i) { return (i >= 0 && i < ST_COUNT) ? kStageNames[i] : ""; }

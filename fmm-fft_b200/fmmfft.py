@@ -1,0 +1,216 @@
+"""Python mirror of the FMM-FFT C-ABI (include/fmmfft.h), over ctypes.
+
+Reference-compatible functions keep the reference's names and argument order
+(97amarnathk/fmm-fft src/fmmfft.c): getwlen2 (:1160), getvlen (:1110), mfti (:337), mft (:980).
+`mft` transforms the full N = p*lq vector (the P MPI ranks of the reference are P blocks of one
+GPU).  `Plan` is the native API: operators resident on the GPU, execution on device buffers.
+
+The library is loaded from this directory (libfmmfft_b200.so, built by build_lib.py).  There is no
+CPU fallback: if the library or a CUDA device is missing, calls raise FmmFftError.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfmmfft_b200.so")
+
+F64, F32, F32_TC = 0, 1, 2
+PRECISIONS = {"f64": F64, "f32": F32, "f32_tc": F32_TC}
+STATUS = {0: "OK", 1: "ERR_INVALID", 2: "ERR_NOMEM", 3: "ERR_CUDA", 4: "ERR_NO_DEVICE",
+          5: "ERR_UNSUPPORTED", 6: "ERR_TIMEOUT", 7: "ERR_BUSY"}
+
+# Every symbol include/fmmfft.h declares.
+EXPORTS = ["getwlen2", "getvlen", "mfti", "mft", "fmmfft_last_error", "fmmfft_last_error_string",
+           "fmmfft_plan_create", "fmmfft_plan_destroy", "fmmfft_plan_device_bytes",
+           "fmmfft_execute", "fmmfft_execute_inverse", "fmmfft_execute_host",
+           "fmmfft_debug_fetch", "fmmfft_profile_start", "fmmfft_profile_stop",
+           "fmmfft_stage_name"]
+
+
+class FmmFftError(RuntimeError):
+    def __init__(self, status, msg=""):
+        self.status = status
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+
+
+_lib = None
+_L, _VP, _I = ctypes.c_long, ctypes.c_void_p, ctypes.c_int
+
+
+def load(path=LIB_PATH):
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FmmFftError(4, f"{path} is missing: run `python fmm-fft_b200/build_lib.py`")
+    lib = ctypes.CDLL(path)
+    lib.getwlen2.argtypes = [_L] * 4
+    lib.getwlen2.restype = _L
+    lib.getvlen.argtypes = [_L] * 4
+    lib.getvlen.restype = _L
+    lib.mfti.argtypes = [_L, _L, _L, _L, _VP, _VP, _L, _L]
+    lib.mfti.restype = None
+    lib.mft.argtypes = [_L, _VP, _L, _L, _L, _L, _L, _VP, _VP, _L, _L, _VP]
+    lib.mft.restype = None
+    lib.fmmfft_last_error.restype = _I
+    lib.fmmfft_last_error_string.restype = ctypes.c_char_p
+    lib.fmmfft_plan_create.argtypes = [ctypes.POINTER(_VP), _L, _L, _L, _L, _I]
+    lib.fmmfft_plan_destroy.argtypes = [_VP]
+    lib.fmmfft_plan_device_bytes.argtypes = [_VP, ctypes.POINTER(ctypes.c_size_t)]
+    for f in ("fmmfft_execute", "fmmfft_execute_inverse", "fmmfft_execute_host"):
+        getattr(lib, f).argtypes = [_VP, _VP, _VP, _VP]
+        getattr(lib, f).restype = _I
+    lib.fmmfft_debug_fetch.argtypes = [_VP, _VP, _VP, _VP, _VP]
+    lib.fmmfft_profile_start.argtypes = [_VP, _I]
+    lib.fmmfft_profile_stop.argtypes = [_VP, _VP, _VP, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)]
+    lib.fmmfft_stage_name.argtypes = [_I]
+    lib.fmmfft_stage_name.restype = ctypes.c_char_p
+    _lib = lib
+    return lib
+
+
+def last_error():
+    lib = load()
+    return lib.fmmfft_last_error(), lib.fmmfft_last_error_string().decode()
+
+
+def _check(rc):
+    if rc != 0:
+        raise FmmFftError(rc, load().fmmfft_last_error_string().decode())
+
+
+# ---------------------------------------------------------------- reference-compatible
+def getwlen2(lq, terms, p, b):
+    return load().getwlen2(lq, terms, p, b)
+
+
+def getvlen(lq, terms, p, b):
+    return load().getvlen(lq, terms, p, b)
+
+
+def mfti(lq, p, terms, b, w, v=None, szkeep=0, sztemp=0):
+    """Fills w (float64, getwlen2 entries) with the operators, reference layout; makes the
+    device plan for (lq, p, terms, b) resident.  Raises on error."""
+    assert w.dtype == np.float64 and w.flags.c_contiguous
+    load().mfti(lq, p, terms, b, w.ctypes.data, None if v is None else v.ctypes.data, szkeep,
+                sztemp)
+    st, msg = last_error()
+    if st:
+        raise FmmFftError(st, msg)
+
+
+def mft(lq, qr, dir, p, myid=0, terms=None, b=None, w=None, v=None, sz1=0, szwk=0, plan=None):
+    """In-place forward FMM-FFT of the full vector qr (complex128, p*lq values, host)."""
+    assert qr.dtype == np.complex128 and qr.flags.c_contiguous and qr.size == p * lq
+    load().mft(lq, qr.ctypes.data, dir, p, myid, terms, b,
+               None if w is None else w.ctypes.data, None if v is None else v.ctypes.data,
+               sz1, szwk, plan)
+    st, msg = last_error()
+    if st:
+        raise FmmFftError(st, msg)
+
+
+# ---------------------------------------------------------------- native plans
+class Plan:
+    """One resident FMM-FFT plan: N points in P blocks, `terms` Chebyshev terms, b points per
+    leaf box.  precision: 'f64' (complex128), 'f32' (complex64, CUDA cores) or 'f32_tc'."""
+
+    def __init__(self, N, P, terms, b, precision="f32"):
+        self.N, self.P, self.terms, self.b = int(N), int(P), int(terms), int(b)
+        self.M = self.N // self.P
+        self.precision = precision
+        self._p = PRECISIONS[precision]
+        h = _VP()
+        _check(load().fmmfft_plan_create(ctypes.byref(h), self.N, self.P, self.terms, self.b,
+                                         self._p))
+        self._h = h
+
+    @property
+    def complex_dtype(self):
+        return np.complex128 if self._p == F64 else np.complex64
+
+    @property
+    def device_bytes(self):
+        v = ctypes.c_size_t()
+        _check(load().fmmfft_plan_device_bytes(self._h, ctypes.byref(v)))
+        return v.value
+
+    def execute_ptr(self, d_in, d_out, stream=0, inverse=False):
+        f = load().fmmfft_execute_inverse if inverse else load().fmmfft_execute
+        _check(f(self._h, d_in, d_out, stream or None))
+
+    def execute_host(self, x):
+        x = np.ascontiguousarray(x, dtype=self.complex_dtype)
+        assert x.size == self.N
+        y = np.empty_like(x)
+        _check(load().fmmfft_execute_host(self._h, x.ctypes.data, y.ctypes.data, None))
+        return y
+
+    def execute_host_ptr(self, h_in, h_out, stream=0):
+        """Host-memory transform (pointers, e.g. pinned buffers): H2D copy, execute, D2H copy,
+        synchronise, all on `stream`."""
+        _check(load().fmmfft_execute_host(self._h, h_in, h_out, stream or None))
+
+    def __call__(self, x, out=None, inverse=False, stream=None):
+        """x: torch complex tensor on the GPU with N elements (complex128 for 'f64', complex64
+        otherwise).  Runs on `stream` (torch.cuda.Stream) or the current stream."""
+        import torch
+        assert x.is_cuda and x.numel() == self.N and x.is_contiguous()
+        want = torch.complex128 if self._p == F64 else torch.complex64
+        assert x.dtype == want, f"plan expects {want}"
+        if out is None:
+            out = torch.empty_like(x)
+        s = stream if stream is not None else torch.cuda.current_stream(x.device)
+        self.execute_ptr(x.data_ptr(), out.data_ptr(), s.cuda_stream, inverse)
+        return out
+
+    def debug_fetch(self):
+        """Intermediates of the last execute (float64): u [P-1,2,M], z [P,M] complex,
+        phi/psi flat (levels 2..n, planar)."""
+        P, M, T = self.P, self.M, self.terms
+        s = M // self.b
+        n = s.bit_length() - 1
+        lv = 2 * (P - 1) * T * ((2 << n) - 4)
+        u = np.zeros((P - 1, 2, M))
+        z = np.zeros((P, M, 2))
+        phi = np.zeros(lv)
+        psi = np.zeros(lv)
+        _check(load().fmmfft_debug_fetch(self._h, u.ctypes.data, z.ctypes.data, phi.ctypes.data,
+                                         psi.ctypes.data))
+        return dict(u=u[:, 0] + 1j * u[:, 1], z=z[..., 0] + 1j * z[..., 1], phi=phi, psi=psi)
+
+    def profile_start(self, max_executes):
+        _check(load().fmmfft_profile_start(self._h, int(max_executes)))
+
+    def profile_stop(self):
+        """-> (nexecutes, {stage: (total_ms, launches_per_execute)})"""
+        cap = 32
+        ms = (ctypes.c_double * cap)()
+        ln = (_I * cap)()
+        ns, ne = _I(), _I()
+        _check(load().fmmfft_profile_stop(self._h, ms, ln, cap, ctypes.byref(ns), ctypes.byref(ne)))
+        lib = load()
+        out = {}
+        for i in range(ns.value):
+            out[lib.fmmfft_stage_name(i).decode()] = (ms[i], ln[i])
+        return ne.value, out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().fmmfft_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def level_planar(flat, P, T, n, level):
+    """View of level `level` of a planar expansion array as [P-1, 2, 2^level, T]."""
+    off = 2 * (P - 1) * T * ((1 << level) - 4)
+    cnt = 2 * (P - 1) * T * (1 << level)
+    return flat[off:off + cnt].reshape(P - 1, 2, 1 << level, T)

@@ -1,0 +1,134 @@
+/*
+ * fmmfft.h — C-ABI of the B200-native FMM-accelerated FFT (libfmmfft_b200.so).
+ *
+ * Drop-in boundary for the forward FMM-FFT of 97amarnathk/fmm-fft (src/fmmfft.c).  The
+ * reference ships no header (README.md:38-39 lists it as a TODO); the four compatibility entry
+ * points below keep its names, argument order and argument meaning:
+ *
+ *   getwlen2  src/fmmfft.c:1160   size (doubles) of the operator buffer w
+ *   getvlen   src/fmmfft.c:1110   size (doubles) of the scratch buffer v
+ *   mfti      src/fmmfft.c:337    build the operators for (lq, p, terms, b) into w
+ *   mft       src/fmmfft.c:980    run the transform
+ *
+ * What changes at the boundary: the reference runs as P MPI ranks that each pass their own
+ * lq = N/P block; here the P ranks are P blocks of one GPU, so `mft` takes the FULL vector of
+ * N = p*lq complex128 values (rank r's block at offset r*lq, i.e. natural order) on the host,
+ * transforms it on the GPU and writes the result back in place, natural order.  `myid` is
+ * ignored.  The FFTW plan argument is ignored (it may be NULL): the size-lq FFTs run on the GPU.
+ * The reference does no validation (bad sizes are undefined behaviour there); these functions
+ * validate, leave the buffers untouched on error and record a status that
+ * fmmfft_last_error() returns.
+ *
+ * The native API (fmmfft_plan_*) keeps operators and workspace resident on the device and runs
+ * on caller-provided device buffers and a CUDA stream.  Every function returns an fmmfft_status.
+ * No function takes or returns framework (torch) types: plain pointers and sizes only.
+ */
+#ifndef FMMFFT_B200_H
+#define FMMFFT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status codes */
+typedef enum {
+  FMMFFT_OK = 0,
+  FMMFFT_ERR_INVALID = 1,     /* parameter outside the supported set */
+  FMMFFT_ERR_NOMEM = 2,       /* host or device allocation failed */
+  FMMFFT_ERR_CUDA = 3,        /* a CUDA call failed (message in fmmfft_last_error_string) */
+  FMMFFT_ERR_NO_DEVICE = 4,   /* no CUDA device, or the kernels were not built for it */
+  FMMFFT_ERR_UNSUPPORTED = 5, /* valid request this build does not serve (e.g. dir < 0 in mft) */
+  FMMFFT_ERR_TIMEOUT = 6,     /* a bounded device-side wait gave up */
+  FMMFFT_ERR_BUSY = 7         /* admission refused (serving queue / HBM budget) */
+} fmmfft_status;
+
+/* Arithmetic of a plan.  Input/output element type follows: complex128 for F64, complex64 for
+ * the others (interleaved re, im). */
+typedef enum {
+  FMMFFT_F64 = 0,     /* FP64 everywhere (the reference's precision) */
+  FMMFFT_F32 = 1,     /* FP32 on CUDA cores: the plain GPU FMM-FFT */
+  FMMFFT_F32_TC = 2   /* operator contractions on tcgen05 tensor cores in 3xTF32, rest FP32 */
+} fmmfft_precision;
+
+/* ------------------------------------------------------------------ reference-compatible */
+
+/* src/fmmfft.c:1160.  Number of doubles the caller allocates for w.  Returns -1 for sizes the
+ * library rejects. */
+long getwlen2(long lq, long terms, long p, long b);
+
+/* src/fmmfft.c:1110.  Number of doubles the caller allocates for v (kept identical to the
+ * reference so callers allocate the same; this library does not use v).  -1 if invalid. */
+long getvlen(long lq, long terms, long p, long b);
+
+/* src/fmmfft.c:337.  Builds every FMM operator for lq points per block, p blocks, `terms`
+ * Chebyshev terms and b points per leaf box into w, in the reference's layout and bit for bit
+ * equal to it, and makes the device plan for (lq, p, terms, b) resident.  szkeep / sztemp are
+ * ignored, as in the reference. */
+void mfti(long lq, long p, long terms, long b, double *w, double *v, long szkeep, long sztemp);
+
+/* src/fmmfft.c:980.  Forward FMM-FFT of the full vector qr (p*lq complex128, host memory) in
+ * place.  dir must be +1 (the reference's dir < 0 path is not a correct inverse,
+ * fmmfft.c:976-977 vs :1080; use fmmfft_execute_inverse).  myid, w, v, sz1, szwk and
+ * forward_plan are accepted for signature compatibility and not used (w may be NULL). */
+void mft(long lq, void *qr, long dir, long p, long myid, long terms, long b, double *w, double *v,
+         long sz1, long szwk, void *forward_plan);
+
+/* Status of the calling thread's last compatibility call (FMMFFT_OK after success). */
+int fmmfft_last_error(void);
+const char *fmmfft_last_error_string(void);
+
+/* ------------------------------------------------------------------ native plan API */
+typedef struct fmmfft_plan_s *fmmfft_plan;
+
+/* Plan for one forward transform of length N = P*M split into P blocks, with `terms`
+ * Chebyshev terms and b points per leaf box (tree depth n = log2(M/b)).  Requirements: P, M, b
+ * powers of two; 2 <= P <= 1024; 2 <= b; M/b >= 4; 2 <= terms <= 64; M <= 2^26.  Operators are
+ * built in FP64 on the host and kept resident on the current device; the workspace is
+ * plan-owned. */
+int fmmfft_plan_create(fmmfft_plan *out, long N, long P, long terms, long b, int precision);
+int fmmfft_plan_destroy(fmmfft_plan plan);
+/* Device bytes the plan holds (operators + workspace). */
+int fmmfft_plan_device_bytes(fmmfft_plan plan, size_t *bytes);
+
+/* Forward transform: d_in, d_out = N interleaved complex values in device memory (complex128
+ * for FMMFFT_F64, complex64 otherwise), natural order; d_in is not modified; d_in == d_out is
+ * allowed.  Enqueued on `stream` (a cudaStream_t, NULL = legacy default stream); returns once
+ * enqueued.  Calls on one plan must not overlap in time (the workspace is shared). */
+int fmmfft_execute(fmmfft_plan plan, const void *d_in, void *d_out, void *stream);
+
+/* Inverse transform (unnormalised: returns N * IDFT), computed as conj(F(conj(x))) with the
+ * conjugations around the whole forward transform. */
+int fmmfft_execute_inverse(fmmfft_plan plan, const void *d_in, void *d_out, void *stream);
+
+/* Same transform from and to HOST memory: copies in, executes, copies out, synchronises. */
+int fmmfft_execute_host(fmmfft_plan plan, const void *h_in, void *h_out, void *stream);
+
+/* Stage-level access for parity tests: copies the plan's intermediate arrays after the last
+ * execute into host memory as float64 (NULL to skip):
+ *   u   [P-1][2][M]  far+near field per section, planar re/im
+ *   z   [P][M] complex  (interleaved) combined blocks before the local FFTs
+ *   phi, psi [levels 2..n][P-1][2][2^l][terms] planar expansions (level l at offset
+ *        (2^l - 4) * (P-1) * 2 * terms) */
+int fmmfft_debug_fetch(fmmfft_plan plan, double *u, double *z, double *phi, double *psi);
+
+/* ------------------------------------------------------------------ stage timing */
+/* Records CUDA events around every stage of the next `max_executes` executes of this plan (on
+ * the stream each execute runs on).  No counterpart in the reference, which only times the
+ * whole mft call (src/fmmfft.c:1259-1263). */
+int fmmfft_profile_start(fmmfft_plan plan, int max_executes);
+/* Synchronises on the last recorded execute and returns, per stage, the summed device time in
+ * ms over the recorded executes (stage_ms) and the kernel launches one execute makes in that
+ * stage (stage_launches); *nstages = number of stages (<= cap filled), *nexecutes = executes
+ * recorded.  Stops profiling. */
+int fmmfft_profile_stop(fmmfft_plan plan, double *stage_ms, int *stage_launches, int cap,
+                        int *nstages, int *nexecutes);
+/* Name of stage i ("sections", "s2m", "m2l_l2l", "fft_pass1", ...), "" when out of range. */
+const char *fmmfft_stage_name(int i);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FMMFFT_B200_H */
