@@ -129,6 +129,39 @@ int fmmfft_profile_stop(fmmfft_plan plan, double *stage_ms, int *stage_launches,
 
 const char *fmmfft_stage_name(int i) { return fmmk_stage_name(i); }
 
+/* ------------------------------------------------------------------ allocation-free entry */
+
+/* FP64 operator tables for fmmfft_execute_noalloc, built in this file-scope store (no heap):
+ * 2^21 doubles (16 MiB) of host memory, enough for every size the 32 MiB device array holds. */
+#define FMMFFT_NOALLOC_OPS_DOUBLES (1L << 21)
+static double g_na_store[FMMFFT_NOALLOC_OPS_DOUBLES];
+static fmm_ops64 g_na_ops;
+static long g_na_key[4];
+static pthread_mutex_t g_na_mu = PTHREAD_MUTEX_INITIALIZER;
+
+int fmmfft_execute_noalloc(long N, long P, long terms, long b, const void *d_in, void *d_out,
+                           void *stream) {
+  if (!d_in || !d_out) return set_err(FMMFFT_ERR_INVALID, "execute_noalloc: NULL argument");
+  if (P < 2 || N <= 0 || N % P || !fmm_validate(N / P, P, terms, b))
+    return set_err(FMMFFT_ERR_INVALID, "execute_noalloc: unsupported parameters");
+  long M = N / P, key[4] = {M, P, terms, b};
+  char err[256] = {0};
+  pthread_mutex_lock(&g_na_mu);
+  if (memcmp(key, g_na_key, sizeof key) != 0) {
+    memset(g_na_key, 0, sizeof g_na_key);
+    int rc = fmm_ops64_build_in(M, P, terms, b, &g_na_ops, g_na_store, FMMFFT_NOALLOC_OPS_DOUBLES);
+    if (rc) {
+      pthread_mutex_unlock(&g_na_mu);
+      return set_err(FMMFFT_ERR_INVALID,
+                     "execute_noalloc: operator tables exceed the allocation-free limit");
+    }
+    memcpy(g_na_key, key, sizeof key);
+  }
+  int rc = fmmk_execute_noalloc(&g_na_ops, 1, d_in, d_out, stream, err, sizeof err);
+  pthread_mutex_unlock(&g_na_mu);
+  return rc ? set_err(rc == 1 ? FMMFFT_ERR_INVALID : rc, err) : set_err(FMMFFT_OK, NULL);
+}
+
 /* ------------------------------------------------------------------ reference-compatible */
 
 /* Device plans made by mfti, keyed by (lq, p, terms, b), kept until process exit: mft finds

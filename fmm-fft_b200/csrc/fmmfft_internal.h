@@ -35,6 +35,8 @@ void fmm_ops64_free(fmm_ops64 *o);
 /* Lays the operators out as the reference's mfti does (src/fmmfft.c:343-374). */
 void fmm_ops64_to_reference_w(const fmm_ops64 *o, double *w);
 long fmm_getwlen2(long lq, long terms, long p, long b);
+long fmm_ops64_doubles(long M, long P, long T, long b);
+int fmm_ops64_build_in(long M, long P, long T, long b, fmm_ops64 *o, double *store, long cap);
 long fmm_getvlen(long lq, long terms, long p, long b);
 
 /* ---- CUDA layer (fmmfft_kernels.cu) ---- */
@@ -51,6 +53,8 @@ int fmmk_device_ok(char *err, size_t errlen);
 int fmmk_profile_start(fmmk_state *st, int cap);
 int fmmk_profile_stop(fmmk_state *st, double *stage_ms, int *stage_launches, int cap, int *nexec);
 const char *fmmk_stage_name(int i);
+int fmmk_execute_noalloc(const fmm_ops64 *ops, int reuse_ops, const void *d_in, void *d_out,
+                         void *stream, char *err, size_t errlen);
 
 #ifdef __cplusplus
 }

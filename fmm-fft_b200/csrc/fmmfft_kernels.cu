@@ -1049,3 +1049,193 @@ extern "C" int fmmk_profile_stop(fmmk_state *st, double *stage_ms, int *stage_la
 }
 
 extern "C" const char *fmmk_stage_name(int i) { return (i >= 0 && i < ST_COUNT) ? kStageNames[i] : ""; }
+
+/* ======================================================================== allocation-free entry */
+/* fmmfft_execute_noalloc runs the complex64 FP32 transform with its operator tables and its
+ * workspace in this file-scope device array instead of plan memory from cudaMalloc.  Every GPU
+ * that loads the library holds the array until process exit.  Its device address is taken once
+ * per device with cudaGetSymbolAddress (host code cannot use the symbol itself as a device
+ * pointer).  Calls share the array: the tables of the last (N, P, terms, b) stay in it and are
+ * reused, and two calls whose kernels overlap on the GPU race on it. */
+#define FMMK_NOALLOC_BYTES ((size_t)32 << 20)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[FMMK_NOALLOC_BYTES];
+
+#define FMMK_NOALLOC_MAXDEV 64
+#define FMMK_NOALLOC_STAGE_FLOATS ((size_t)2 << 20) /* host staging for the FP32 tables, 8 MiB */
+static void *g_noalloc_base[FMMK_NOALLOC_MAXDEV];
+static long g_noalloc_key[FMMK_NOALLOC_MAXDEV][4];
+static float g_noalloc_stage[FMMK_NOALLOC_STAGE_FLOATS];
+
+/* Operator and workspace layout inside the array: the same arrays, order and rounding as a
+ * complex64 plan (dev_create), offsets relative to the array base. */
+struct NoallocLayout {
+  size_t initch, btop, bm2m, bm2l, evalmT, evalmh, cot, pretw, twP, twM, xt, part, ssum, phi, psi,
+      u, z, tmp, end;
+};
+
+static NoallocLayout noalloc_layout(const fmm_ops64 *o, long ntile) {
+  const long M = o->M, P = o->P, T = o->T, b = o->b, n = o->n, S1 = P - 1;
+  const long nlev = n - 2 > 0 ? n - 2 : 0;
+  const long lvtot = 2 * S1 * T * ((2L << n) - 4);
+  NoallocLayout L;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t at = off;
+    off = align_up(off + bytes);
+    return at;
+  };
+  L.initch = take(sizeof(float) * b * T);
+  L.btop = take(sizeof(float) * T * T);
+  L.bm2m = take(sizeof(float) * (nlev ? nlev : 1) * 2 * T * T);
+  L.bm2l = take(sizeof(float) * (nlev ? nlev : 1) * 10 * T * T);
+  L.evalmT = take(sizeof(float) * S1 * T * b);
+  L.evalmh = take(sizeof(float) * S1 * T);
+  L.cot = take(sizeof(float) * S1 * 4 * b);
+  L.pretw = take(sizeof(float2) * P);
+  L.twP = take(sizeof(float2) * P);
+  L.twM = take(sizeof(float2) * M);
+  L.xt = take(sizeof(float) * 2 * P * M);
+  L.part = take(sizeof(float2) * ntile * P);
+  L.ssum = take(sizeof(float2) * P);
+  L.phi = take(sizeof(float) * lvtot);
+  L.psi = take(sizeof(float) * lvtot);
+  L.u = take(sizeof(float) * 2 * S1 * M);
+  L.z = take(sizeof(float2) * P * M);
+  L.tmp = take(sizeof(float2) * P * M);
+  L.end = off;
+  return L;
+}
+
+/* FP32 operator tables into g_noalloc_stage at the layout's offsets (same transposes and
+ * stacking as dev_create). */
+static void noalloc_stage_ops(const fmm_ops64 *o, const NoallocLayout &L) {
+  const long M = o->M, P = o->P, T = o->T, b = o->b, n = o->n, S1 = P - 1;
+  float *st = g_noalloc_stage;
+  memset(st, 0, L.xt);
+  float *f;
+  f = st + L.initch / 4;
+  for (long i = 0; i < b * T; ++i) f[i] = (float)o->initch[i];
+  f = st + L.btop / 4;
+  for (long k = 0; k < T; ++k)
+    for (long t = 0; t < T; ++t) f[k * T + t] = (float)o->topflp[t * T + k];
+  for (long Lv = 2; Lv <= n - 1; ++Lv) {
+    const double *ops = o->levops + (Lv - 2) * FMM_NLEVOPS * T * T;
+    f = st + L.bm2m / 4 + (Lv - 2) * 2 * T * T;
+    for (long k = 0; k < T; ++k)
+      for (long t = 0; t < T; ++t) {
+        f[k * T + t] = (float)ops[FMM_SHFTFN * T * T + t * T + k];
+        f[(T + k) * T + t] = (float)ops[FMM_SHFTFP * T * T + t * T + k];
+      }
+  }
+  for (long l = 3; l <= n; ++l) {
+    const double *ops = o->levops + (l - 3) * FMM_NLEVOPS * T * T;
+    f = st + L.bm2l / 4 + (l - 3) * 10 * T * T;
+    const long N2 = 2 * T;
+    for (long k = 0; k < T; ++k)
+      for (long t = 0; t < T; ++t) {
+        f[(0 * T + k) * N2 + t] = (float)ops[FMM_SHFTLP * T * T + t * T + k];
+        f[(0 * T + k) * N2 + T + t] = (float)ops[FMM_SHFTLN * T * T + t * T + k];
+        f[(1 * T + k) * N2 + t] = (float)ops[FMM_FLIP2P * T * T + t * T + k];
+        f[(1 * T + k) * N2 + T + t] = (float)ops[FMM_FLIP3P * T * T + t * T + k];
+        f[(2 * T + k) * N2 + T + t] = (float)ops[FMM_FLIP2P * T * T + t * T + k];
+        f[(3 * T + k) * N2 + t] = (float)ops[FMM_FLIP2N * T * T + t * T + k];
+        f[(4 * T + k) * N2 + t] = (float)ops[FMM_FLIP3N * T * T + t * T + k];
+        f[(4 * T + k) * N2 + T + t] = (float)ops[FMM_FLIP2N * T * T + t * T + k];
+      }
+  }
+  f = st + L.evalmT / 4;
+  for (long sc = 1; sc < P; ++sc)
+    for (long k = 0; k < T; ++k)
+      for (long j = 0; j < b; ++j) f[((sc - 1) * T + k) * b + j] = (float)o->evalm[(j * S1 + (sc - 1)) * T + k];
+  f = st + L.evalmh / 4;
+  for (long sc = P / 2; sc < P; ++sc)
+    for (long k = 0; k < T; ++k) f[(sc - 1) * T + k] = (float)o->evalmh[(sc - P / 2) * T + k];
+  f = st + L.cot / 4;
+  for (long i = 0; i < S1 * 4 * b; ++i) f[i] = (float)o->cot[i];
+  const double PI = 3.14159265358979323846264338327950288;
+  f = st + L.pretw / 4;
+  for (long sc = 1; sc < P; ++sc) {
+    f[2 * sc] = (float)(-cos(PI * sc / P) * sin(PI * sc / P));
+    f[2 * sc + 1] = (float)(sin(PI * sc / P) * sin(PI * sc / P));
+  }
+  f = st + L.twP / 4;
+  for (long k = 0; k < P; ++k) f[2 * k] = (float)cos(2 * PI * k / P), f[2 * k + 1] = (float)-sin(2 * PI * k / P);
+  f = st + L.twM / 4;
+  for (long k = 0; k < M; ++k) {
+    double a = 2 * PI * (double)k / (double)M;
+    f[2 * k] = (float)cos(a), f[2 * k + 1] = (float)-sin(a);
+  }
+}
+
+/* reuse_ops: the caller knows the tables in the array are for these parameters already. */
+extern "C" int fmmk_execute_noalloc(const fmm_ops64 *o, int reuse_ops, const void *d_in,
+                                    void *d_out, void *stream, char *err, size_t errlen) {
+  int dev = 0;
+  FMM_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= FMMK_NOALLOC_MAXDEV) {
+    snprintf(err, errlen, "device %d outside the %d devices the no-alloc entry tracks", dev,
+             FMMK_NOALLOC_MAXDEV);
+    return 1;
+  }
+  if (!g_noalloc_base[dev]) { /* set-up, once per device, with that device current */
+    void *p = NULL;
+    FMM_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_base[dev] = p;
+    set_smem_limits();
+  }
+  Dev<float> d;
+  memset((void *)&d, 0, sizeof(d));
+  d.M = o->M, d.P = o->P, d.T = o->T, d.b = o->b, d.s = o->s, d.n = o->n;
+  d.N = o->M * o->P, d.S1 = o->P - 1, d.precision = 1;
+  d.tileM = d.P >= 2048 ? 1 : 2048 / d.P;
+  if (d.tileM > d.M) d.tileM = d.M;
+  d.ntile = d.M / d.tileM;
+  if (d.M <= 4096) {
+    d.M1 = d.M, d.M2 = 1;
+  } else {
+    long lg = 0;
+    while ((1L << lg) < d.M) ++lg;
+    d.M2 = 1L << ((lg + 1) / 2);
+    d.M1 = d.M / d.M2;
+  }
+  NoallocLayout L = noalloc_layout(o, d.ntile);
+  if (L.end > FMMK_NOALLOC_BYTES || L.xt / sizeof(float) > FMMK_NOALLOC_STAGE_FLOATS) {
+    snprintf(err, errlen,
+             "N=%ld P=%ld terms=%ld b=%ld needs %zu bytes of device scratch; the allocation-free "
+             "entry point holds at most %zu",
+             d.N, d.P, d.T, d.b, L.end, (size_t)FMMK_NOALLOC_BYTES);
+    return 1;
+  }
+  char *base = (char *)g_noalloc_base[dev];
+  cudaStream_t st = (cudaStream_t)stream;
+  const long key[4] = {o->M, o->P, o->T, o->b};
+  int same = reuse_ops && memcmp(key, g_noalloc_key[dev], sizeof key) == 0;
+  if (!same) {
+    noalloc_stage_ops(o, L);
+    FMM_CUDA_TRY(cudaMemcpyAsync(base, g_noalloc_stage, L.xt, cudaMemcpyHostToDevice, st));
+    /* no workspace array is read before it is written; zeroing it anyway keeps a fresh
+     * configuration independent of what an earlier one left behind */
+    FMM_CUDA_TRY(cudaMemsetAsync(base + L.xt, 0, L.end - L.xt, st));
+    FMM_CUDA_TRY(cudaStreamSynchronize(st)); /* the host staging array is reused next call */
+    memcpy(g_noalloc_key[dev], key, sizeof key);
+  }
+  d.initch = (float *)(base + L.initch);
+  d.btop = (float *)(base + L.btop);
+  d.bm2m = (float *)(base + L.bm2m);
+  d.bm2l = (float *)(base + L.bm2l);
+  d.evalmT = (float *)(base + L.evalmT);
+  d.evalmh = (float *)(base + L.evalmh);
+  d.cot = (float *)(base + L.cot);
+  d.pretw = (float2 *)(base + L.pretw);
+  d.twP = (float2 *)(base + L.twP);
+  d.twM = (float2 *)(base + L.twM);
+  d.xt = (float *)(base + L.xt);
+  d.part = (float2 *)(base + L.part);
+  d.ssum = (float2 *)(base + L.ssum);
+  d.phi = (float *)(base + L.phi);
+  d.psi = (float *)(base + L.psi);
+  d.u = (float *)(base + L.u);
+  d.z = (float2 *)(base + L.z);
+  d.tmp = (float2 *)(base + L.tmp);
+  return dev_execute<float>(&d, d_in, d_out, st, 0, err, errlen);
+}

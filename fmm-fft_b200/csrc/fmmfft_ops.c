@@ -256,3 +256,81 @@ void fmm_ops64_to_reference_w(const fmm_ops64 *o, double *w) {
   memcpy(w + at, o->chnods, sizeof(double) * T), at += T;
   memcpy(w + at, o->fo, sizeof(double) * 2 * P * (P - 1));
 }
+
+/* ------------------------------------------------------------------ build into given storage */
+
+/* Doubles fmm_ops64_build_in needs for (M, P, T, b): the operator tables plus the builder's
+ * scratch.  -1 for unsupported parameters. */
+long fmm_ops64_doubles(long M, long P, long T, long b) {
+  if (!fmm_validate(M, P, T, b)) return -1;
+  long s = M / b, n = lg2(s), nlev = n - 2 > 0 ? n - 2 : 1;
+  return T + b * T + T * T + nlev * FMM_NLEVOPS * T * T + b * (P - 1) * T + (P / 2) * T +
+         (P - 1) * 4 * b + 2 * P * (P - 1) + T + (T > b ? T : b) + T;
+}
+
+/* The same operators as fmm_ops64_build, written into `store` (cap doubles) instead of the
+ * heap; o's arrays point into store and must not be passed to fmm_ops64_free. */
+int fmm_ops64_build_in(long M, long P, long T, long b, fmm_ops64 *o, double *store, long cap) {
+  memset(o, 0, sizeof(*o));
+  long need = fmm_ops64_doubles(M, P, T, b);
+  if (need < 0) return 1;
+  if (need > cap) return 2;
+  long s = M / b, n = lg2(s), nlev = n - 2 > 0 ? n - 2 : 1;
+  o->M = M, o->P = P, o->T = T, o->b = b, o->s = s, o->n = n;
+  double *at = store;
+  o->chnods = at, at += T;
+  o->initch = at, at += b * T;
+  o->topflp = at, at += T * T;
+  o->levops = at, at += nlev * FMM_NLEVOPS * T * T;
+  o->evalm = at, at += b * (P - 1) * T;
+  o->evalmh = at, at += (P / 2) * T;
+  o->cot = at, at += (P - 1) * 4 * b;
+  o->fo = at, at += 2 * P * (P - 1);
+  op_scratch S = {T, o->chnods, NULL, NULL, NULL};
+  S.e = at, at += T;
+  S.x = at, at += (T > b ? T : b);
+  S.wgt = at;
+  for (long j = 0; j < T; ++j) o->chnods[j] = cheb(j, T);
+  {
+    double a = FMM_PI / (2.0 * s), ta3 = 3 * tan(a);
+    for (long j = 0; j < b; ++j) S.x[j] = tan(((double)(2 * (j + 1) - b - 1)) / (double)b * a);
+    for (long j = 0; j < b; ++j)
+      for (long k = 0; k < T; ++k)
+        o->initch[j * T + k] = (o->chnods[k] + ta3 * S.x[j]) / (ta3 - o->chnods[k] * S.x[j]);
+  }
+  op_flip(&S, 2, 2, o->topflp);
+  for (long lev = 1; lev <= n - 2; ++lev) {
+    double *L = o->levops + (lev - 1) * FMM_NLEVOPS * T * T;
+    op_shift_up(&S, lev + 2, -1, L + FMM_SHFTFN * T * T);
+    op_shift_up(&S, lev + 2, +1, L + FMM_SHFTFP * T * T);
+    op_flip(&S, lev + 2, -2, L + FMM_FLIP2N * T * T);
+    op_flip(&S, lev + 2, +2, L + FMM_FLIP2P * T * T);
+    op_flip(&S, lev + 2, -3, L + FMM_FLIP3N * T * T);
+    op_flip(&S, lev + 2, +3, L + FMM_FLIP3P * T * T);
+    op_shift_down(&S, lev + 1, -1, L + FMM_SHFTLN * T * T);
+    op_shift_down(&S, lev + 1, +1, L + FMM_SHFTLP * T * T);
+  }
+  double dlq = (double)M;
+  for (long sc = 1; sc <= P - 1; ++sc) {
+    double gfrac = ((double)sc) / P;
+    for (long j = 1; j <= b; ++j) {
+      double ffr = ((double)(2 * j - 1) - (((double)(2 * sc)) / P)) / b - 1;
+      op_eval_point(&S, ffr, s, M, o->evalm + ((j - 1) * (P - 1) + (sc - 1)) * T);
+    }
+    if (sc >= P / 2) {
+      double ffr = (((double)2 * b + 1) - ((double)2 * sc) / (P)) / (b)-1;
+      op_eval_point(&S, ffr, s, M, o->evalmh + (sc - P / 2) * T);
+    }
+    for (long d = -2 * b; d < 2 * b; ++d)
+      o->cot[(sc - 1) * 4 * b + d + 2 * b] = -1 / tan(FMM_PI / dlq * ((double)d + gfrac)) / dlq;
+  }
+  for (long sc = 1; sc <= P - 1; ++sc) {
+    double ang = FMM_PI * ((double)sc) / P;
+    for (long j = 1; j <= P; ++j) {
+      double complex v = -cexp((ang * (1 - 2 * j)) * I) * sin(ang);
+      o->fo[2 * ((j - 1) * (P - 1) + (sc - 1))] = creal(v);
+      o->fo[2 * ((j - 1) * (P - 1) + (sc - 1)) + 1] = cimag(v);
+    }
+  }
+  return 0;
+}

@@ -26,7 +26,7 @@ EXPORTS = ["getwlen2", "getvlen", "mfti", "mft", "fmmfft_last_error", "fmmfft_la
            "fmmfft_plan_create", "fmmfft_plan_destroy", "fmmfft_plan_device_bytes",
            "fmmfft_execute", "fmmfft_execute_inverse", "fmmfft_execute_host",
            "fmmfft_debug_fetch", "fmmfft_profile_start", "fmmfft_profile_stop",
-           "fmmfft_stage_name"]
+           "fmmfft_stage_name", "fmmfft_execute_noalloc"]
 
 
 class FmmFftError(RuntimeError):
@@ -67,6 +67,8 @@ def load(path=LIB_PATH):
     lib.fmmfft_profile_stop.argtypes = [_VP, _VP, _VP, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)]
     lib.fmmfft_stage_name.argtypes = [_I]
     lib.fmmfft_stage_name.restype = ctypes.c_char_p
+    lib.fmmfft_execute_noalloc.argtypes = [_L, _L, _L, _L, _VP, _VP, _VP]
+    lib.fmmfft_execute_noalloc.restype = _I
     _lib = lib
     return lib
 
@@ -110,6 +112,13 @@ def mft(lq, qr, dir, p, myid=0, terms=None, b=None, w=None, v=None, sz1=0, szwk=
     st, msg = last_error()
     if st:
         raise FmmFftError(st, msg)
+
+
+def execute_noalloc(N, P, terms, b, d_in, d_out, stream=0):
+    """complex64 forward transform between caller-owned device buffers (pointers) without any
+    allocation: tables and workspace live in the library's static 32 MiB device array."""
+    _check(load().fmmfft_execute_noalloc(int(N), int(P), int(terms), int(b), d_in, d_out,
+                                         stream or None))
 
 
 # ---------------------------------------------------------------- native plans

@@ -128,6 +128,24 @@ int fmmfft_profile_stop(fmmfft_plan plan, double *stage_ms, int *stage_launches,
 /* Name of stage i ("sections", "s2m", "m2l_l2l", "fft_pass1", ...), "" when out of range. */
 const char *fmmfft_stage_name(int i);
 
+/* ------------------------------------------------------------------ allocation-free entry */
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc: code that runs
+ * under a device-memory budget owned by someone else (a pool or arena it may not grow), or in a
+ * phase where it must not allocate at all.  Forward transform of N complex64 values (FP32, the
+ * FMMFFT_F32 arithmetic, same result as fmmfft_execute on an FMMFFT_F32 plan) from d_in to
+ * d_out, both caller-owned device buffers, enqueued on `stream`.  Nothing is allocated: the
+ * operator tables and the workspace live in one file-scope device array of 32 MiB that every
+ * GPU which loads this library holds until process exit (the FP64 operator build uses a
+ * file-scope 16 MiB host array).  Sizes whose tables plus workspace exceed 32 MiB (about
+ * N = 2^18 complex64 at 24 terms, b = 32) return FMMFFT_ERR_INVALID.
+ * The first call on a device sets that device up (it looks up the array's device address) and
+ * the first call for new (N, P, terms, b) uploads the tables and synchronises `stream`; make
+ * those calls before any stream capture.  All calls share the one array, which keeps the last
+ * call's tables: calls whose work overlaps on the GPU (other streams, other threads) race on
+ * it and must be serialised by the caller. */
+int fmmfft_execute_noalloc(long N, long P, long terms, long b, const void *d_in, void *d_out,
+                           void *stream);
+
 #ifdef __cplusplus
 }
 #endif
