@@ -129,6 +129,14 @@ int fmmfft_profile_stop(fmmfft_plan plan, double *stage_ms, int *stage_launches,
 
 const char *fmmfft_stage_name(int i) { return fmmk_stage_name(i); }
 
+int fmmfft_plan_check(fmmfft_plan plan) {
+  if (!plan) return set_err(FMMFFT_ERR_INVALID, "plan_check: NULL plan");
+  int rc = fmmk_check(plan->dev);
+  if (rc == FMMFFT_ERR_TIMEOUT)
+    return set_err(rc, "plan_check: a bounded wait in a tensor-core kernel gave up");
+  return rc ? set_err(rc, "plan_check: CUDA error") : FMMFFT_OK;
+}
+
 /* ------------------------------------------------------------------ allocation-free entry */
 
 /* FP64 operator tables for fmmfft_execute_noalloc, built in this file-scope store (no heap):

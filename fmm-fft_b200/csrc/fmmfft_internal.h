@@ -53,6 +53,7 @@ int fmmk_device_ok(char *err, size_t errlen);
 int fmmk_profile_start(fmmk_state *st, int cap);
 int fmmk_profile_stop(fmmk_state *st, double *stage_ms, int *stage_launches, int cap, int *nexec);
 const char *fmmk_stage_name(int i);
+int fmmk_check(fmmk_state *st);
 int fmmk_execute_noalloc(const fmm_ops64 *ops, int reuse_ops, const void *d_in, void *d_out,
                          void *stream, char *err, size_t errlen);
 

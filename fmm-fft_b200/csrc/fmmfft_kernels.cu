@@ -33,6 +33,7 @@
 #include <new>
 
 #include "fmmfft_internal.h"
+#include "fmmfft_tc.cuh"
 
 #define FMM_CUDA_TRY(call)                                                              \
   do {                                                                                  \
@@ -106,6 +107,17 @@ template <typename R> struct Dev {
   size_t bytes;
   void *pool;
   Prof prof;
+  /* tensor-core (FMMFFT_F32_TC) operators: pre-split TF32 hi/lo, [npad][kpad] K-major */
+  int tc, num_sms;
+  int *status;          /* device word: non-zero after a bounded device wait gave up */
+  float *tc_s2m[2];     /* hi, lo */
+  float *tc_m2m[2];     /* per parent level L = 2..n-1, stride tc_m2m_stride */
+  float *tc_m2l[2];     /* per child level l = 3..n, stride tc_m2l_stride */
+  float *tc_leaf[2];    /* per section, stride tc_leaf_stride */
+  long tc_m2m_stride, tc_m2l_stride, tc_leaf_stride;
+  int kp_s2m, np_s2m, kp_m2m, np_m2m, kp_m2l, np_m2l, kp_leaf, np_leaf;
+  int ok_s2m, ok_m2m, ok_m2l, ok_leaf;
+  long tc_min_rows; /* stages with fewer rows use the CUDA-core kernel */
 };
 
 struct fmmk_state {
@@ -265,6 +277,62 @@ template <typename R> struct ProbLeaf {
   }
 };
 
+/* ---- the same four contractions for the tcgen05 kernel (fmmfft_tc.cuh) ---- */
+struct TcBase {
+  long rows;
+  int batches, nchunks, clen[4], coff[4], kpad, npad, nout;
+  const float *bhi, *blo;
+  long bstride;
+};
+
+struct TcS2M : TcBase {
+  const float *xt;
+  float *out;
+  long M;
+  int b, T;
+  __device__ const float *src(int, long r, int) const { return xt + 2 * M + r * b; }
+  __device__ float *dst(long r, int) const { return out + r * T; }
+};
+
+struct TcM2M : TcBase {
+  const float *child;
+  float *out;
+  int T;
+  __device__ const float *src(int, long r, int) const { return child + r * 2 * T; }
+  __device__ float *dst(long r, int) const { return out + r * T; }
+};
+
+struct TcM2L : TcBase {
+  const float *psi_par, *phi;
+  float *out;
+  int T, lpar;
+  __device__ const float *src(int c, long r, int) const {
+    if (c == 0) return psi_par + r * T;
+    long pl = r >> lpar, Bx = r & ((1L << lpar) - 1), mask = (2L << lpar) - 1;
+    long base = pl << (lpar + 1);
+    long box = (c == 1) ? ((2 * Bx - 2) & mask) : ((2 * Bx + 2) & mask);
+    return phi + (base + box) * T;
+  }
+  __device__ float *dst(long r, int) const { return out + r * 2 * T; }
+};
+
+struct TcLeaf : TcBase { /* batch z = section - 1; s is a power of two (log2s) */
+  const float *psi_n, *xt;
+  float *u;
+  long M, s;
+  int T, b, log2s;
+  __device__ const float *src(int c, long r, int z) const {
+    const long pl0 = 2L * z;
+    if (c == 0) return psi_n + pl0 * s * T + r * T;
+    long ri = r >> log2s, bx = r & (s - 1);
+    return xt + (pl0 + 2 + ri) * M + (((bx - 2 + c) * b) & (M - 1));
+  }
+  __device__ float *dst(long r, int z) const {
+    long ri = r >> log2s, bx = r & (s - 1);
+    return u + (2L * z + ri) * M + bx * b;
+  }
+};
+
 template <typename R, int BM, int BN, int BK, int TM, int TN, class Prob>
 __global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_rowgemm(Prob pb) {
   constexpr int NTX = BN / TN;
@@ -346,6 +414,19 @@ static void launch_rowgemm(const Prob &pb, long rows_per_batch, int N, int batch
     dim3 g((unsigned)((rows_per_batch + 63) / 64), (unsigned)((N + 63) / 64), batches);
     k_rowgemm<R, 64, 64, 16, 4, 4, Prob><<<g, 256, 0, st>>>(pb);
   }
+}
+
+constexpr long kTcMinRows = 8192; /* default: below this a stage runs on the CUDA-core kernel */
+
+template <class Prob> static size_t tc_smem_bytes(const Prob &pb) {
+  return tc::smem_bytes(pb.kpad, pb.npad);
+}
+
+template <class Prob> static void launch_tc(const Prob &pb, int num_sms, int *status, cudaStream_t st) {
+  long tiles = (pb.rows + tc::kRows - 1) / tc::kRows * pb.batches;
+  long cap = 2L * num_sms; /* two CTAs per SM */
+  int grid = (int)(tiles < cap ? tiles : cap);
+  tc::k_tc_rowgemm<Prob><<<grid, 256, tc_smem_bytes(pb), st>>>(pb, status);
 }
 
 /* First point of each leaf box for the sections whose shifted target leaves its box
@@ -576,6 +657,106 @@ static inline long pow2_floor(long v) {
   return p;
 }
 
+/* Round to TF32 (nearest, ties away from zero), as cvt.rna.tf32.f32 does. */
+static float tf32_rna_host(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  if ((u & 0x7f800000u) != 0x7f800000u) {
+    u += 0x1000u;
+    u &= 0xffffe000u;
+  }
+  float r;
+  memcpy(&r, &u, 4);
+  return r;
+}
+
+/* Uploads one operator, given as FP64 [npad][kpad] K-major values, split into TF32 hi and lo. */
+static int tc_put(float *dhi, float *dlo, const double *v, long cnt, char *err, size_t errlen) {
+  float *h = (float *)malloc(sizeof(float) * 2 * (cnt ? cnt : 1));
+  if (!h) return 2;
+  for (long i = 0; i < cnt; ++i) {
+    float f = (float)v[i];
+    float hi = tf32_rna_host(f);
+    h[i] = hi;
+    h[cnt + i] = tf32_rna_host(f - hi);
+  }
+  cudaError_t e = cudaMemcpy(dhi, h, sizeof(float) * cnt, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dlo, h + cnt, sizeof(float) * cnt, cudaMemcpyHostToDevice);
+  free(h);
+  if (e != cudaSuccess) {
+    snprintf(err, errlen, "cudaMemcpy: %s", cudaGetErrorString(e));
+    return 3;
+  }
+  return 0;
+}
+
+/* B operands of the tensor-core stages, K-major: B[n][k] multiplies A column k into output n. */
+template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, char *err, size_t errlen) {
+  const long T = o->T, b = o->b, P = o->P, n = o->n, S1 = P - 1;
+  long cap = (long)d->kp_s2m * d->np_s2m;
+  if (d->tc_m2m_stride > cap) cap = d->tc_m2m_stride;
+  if (d->tc_m2l_stride > cap) cap = d->tc_m2l_stride;
+  if (d->tc_leaf_stride > cap) cap = d->tc_leaf_stride;
+  double *v = (double *)malloc(sizeof(double) * cap);
+  if (!v) return 2;
+  int rc = 0;
+  if (d->ok_s2m) {
+    const int kp = d->kp_s2m, np = d->np_s2m;
+    for (long i = 0; i < (long)kp * np; ++i) v[i] = 0;
+    for (long nn = 0; nn < T; ++nn)
+      for (long k = 0; k < b; ++k) v[nn * kp + k] = o->initch[k * T + nn];
+    rc |= tc_put(d->tc_s2m[0], d->tc_s2m[1], v, (long)kp * np, err, errlen);
+  }
+  if (d->ok_m2m)
+    for (long L = 2; L <= n - 1; ++L) {
+      const int kp = d->kp_m2m, np = d->np_m2m;
+      const double *ops = o->levops + (L - 2) * FMM_NLEVOPS * T * T;
+      for (long i = 0; i < (long)kp * np; ++i) v[i] = 0;
+      for (long t = 0; t < T; ++t)
+        for (long k = 0; k < T; ++k) {
+          v[t * kp + k] = ops[FMM_SHFTFN * T * T + t * T + k];
+          v[t * kp + T + k] = ops[FMM_SHFTFP * T * T + t * T + k];
+        }
+      rc |= tc_put(d->tc_m2m[0] + (L - 2) * d->tc_m2m_stride, d->tc_m2m[1] + (L - 2) * d->tc_m2m_stride,
+                   v, (long)kp * np, err, errlen);
+    }
+  if (d->ok_m2l)
+    for (long l = 3; l <= n; ++l) {
+      const int kp = d->kp_m2l, np = d->np_m2l;
+      const double *ops = o->levops + (l - 3) * FMM_NLEVOPS * T * T;
+      for (long i = 0; i < (long)kp * np; ++i) v[i] = 0;
+#define OPT(which, t, k) ops[(which) * T * T + (t) * T + (k)]
+      for (long t = 0; t < T; ++t)
+        for (long k = 0; k < T; ++k) {
+          v[t * kp + 0 * T + k] = OPT(FMM_SHFTLP, t, k);       /* left child  <- psi parent */
+          v[(T + t) * kp + 0 * T + k] = OPT(FMM_SHFTLN, t, k); /* right child <- psi parent */
+          v[t * kp + 1 * T + k] = OPT(FMM_FLIP2P, t, k);       /* left  <- phi[2B-2] */
+          v[(T + t) * kp + 1 * T + k] = OPT(FMM_FLIP3P, t, k); /* right <- phi[2B-2] */
+          v[(T + t) * kp + 2 * T + k] = OPT(FMM_FLIP2P, t, k); /* right <- phi[2B-1] */
+          v[t * kp + 3 * T + k] = OPT(FMM_FLIP2N, t, k);       /* left  <- phi[2B+2] */
+          v[t * kp + 4 * T + k] = OPT(FMM_FLIP3N, t, k);       /* left  <- phi[2B+3] */
+          v[(T + t) * kp + 4 * T + k] = OPT(FMM_FLIP2N, t, k); /* right <- phi[2B+3] */
+        }
+#undef OPT
+      rc |= tc_put(d->tc_m2l[0] + (l - 3) * d->tc_m2l_stride, d->tc_m2l[1] + (l - 3) * d->tc_m2l_stride,
+                   v, (long)kp * np, err, errlen);
+    }
+  if (d->ok_leaf)
+    for (long sc = 1; sc < P; ++sc) {
+      const int kp = d->kp_leaf, np = d->np_leaf;
+      const double *ct = o->cot + (sc - 1) * 4 * b;
+      for (long i = 0; i < (long)kp * np; ++i) v[i] = 0;
+      for (long j = 0; j < b; ++j) {
+        for (long k = 0; k < T; ++k) v[j * kp + k] = o->evalm[(j * S1 + (sc - 1)) * T + k];
+        for (long q = 0; q < 3 * b; ++q) v[j * kp + T + q] = ct[q + b - j];
+      }
+      rc |= tc_put(d->tc_leaf[0] + (sc - 1) * d->tc_leaf_stride, d->tc_leaf[1] + (sc - 1) * d->tc_leaf_stride,
+                   v, (long)kp * np, err, errlen);
+    }
+  free(v);
+  return rc;
+}
+
 template <typename R>
 static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err, size_t errlen) {
   using C = typename cplx<R>::T;
@@ -600,6 +781,42 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   }
   const long nlev = n - 2 > 0 ? n - 2 : 0;
   const long lvtot = 2 * S1 * T * ((2L << n) - 4);
+  /* tensor-core operator shapes (precision FMMFFT_F32_TC only) */
+  const int tc = (precision == 2 && sizeof(R) == 4);
+  auto up8 = [](long v) { return (int)((v + 7) / 8 * 8); };
+  auto up16 = [](long v) { return (int)((v + 15) / 16 * 16); };
+  d->tc = tc;
+  d->kp_s2m = up8(b), d->np_s2m = up16(T);
+  d->kp_m2m = up8(2 * T), d->np_m2m = up16(T);
+  d->kp_m2l = up8(5 * T), d->np_m2l = up16(2 * T);
+  d->kp_leaf = up8(T + 3 * b), d->np_leaf = up16(b);
+  auto fits = [&](int kp, int np) {
+    return tc && (T % 4 == 0) && (b % 4 == 0) && np <= 256 && kp <= 256 &&
+           tc::smem_bytes(kp, np) <= (size_t)110 * 1024 && tc::tmem_cols(kp, np) <= 256;
+  };
+  d->ok_s2m = fits(d->kp_s2m, d->np_s2m);
+  d->ok_m2m = fits(d->kp_m2m, d->np_m2m) && nlev > 0;
+  d->ok_m2l = fits(d->kp_m2l, d->np_m2l) && nlev > 0;
+  /* The leaf contraction multiplies inputs by near-singular cot weights (|w| ~ P/pi), and the
+   * 2^-22 split error of 3xTF32 there lifts the transform's rel-L2 from 2e-7 to 1.3e-6 at
+   * N = 2^24, P = 64, against 2e-7 when it runs in FP32; it stays on the CUDA cores unless
+   * FMMFFT_TC_STAGES asks for it.  The tree stages on the tensor cores keep 2.4e-7. */
+  d->ok_leaf = fits(d->kp_leaf, d->np_leaf) && getenv("FMMFFT_TC_STAGES") != NULL;
+  d->tc_min_rows = kTcMinRows;
+  if (const char *ev = getenv("FMMFFT_TC_MIN_ROWS")) d->tc_min_rows = atol(ev);
+  /* FMMFFT_TC_STAGES: bit mask of the stages routed to the tensor cores (1 S2M, 2 M2M, 4 M2L,
+   * 8 leaf); default all */
+  if (const char *ev = getenv("FMMFFT_TC_STAGES")) {
+    long m = atol(ev);
+    d->ok_s2m &= (m & 1) != 0, d->ok_m2m &= (m & 2) != 0, d->ok_m2l &= (m & 4) != 0, d->ok_leaf &= (m & 8) != 0;
+  }
+  const long sz_s2m = d->ok_s2m ? (long)d->kp_s2m * d->np_s2m : 0;
+  d->tc_m2m_stride = (long)d->kp_m2m * d->np_m2m;
+  d->tc_m2l_stride = (long)d->kp_m2l * d->np_m2l;
+  d->tc_leaf_stride = (long)d->kp_leaf * d->np_leaf;
+  const long sz_m2m = d->ok_m2m ? nlev * d->tc_m2m_stride : 0;
+  const long sz_m2l = d->ok_m2l ? nlev * d->tc_m2l_stride : 0;
+  const long sz_leaf = d->ok_leaf ? S1 * d->tc_leaf_stride : 0;
   size_t off = 0;
 #define CARVE(field, count, type)          \
   size_t off_##field = off;                \
@@ -622,6 +839,11 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   CARVE(u, 2 * S1 * M, R)
   CARVE(z, P * M, C)
   CARVE(tmp, P * M, C)
+  CARVE(status, 1, int)
+  CARVE(tcs2m, 2 * sz_s2m, float)
+  CARVE(tcm2m, 2 * sz_m2m, float)
+  CARVE(tcm2l, 2 * sz_m2l, float)
+  CARVE(tcleaf, 2 * sz_leaf, float)
 #undef CARVE
   void *pool = NULL;
   cudaError_t ce = cudaMalloc(&pool, off);
@@ -651,6 +873,17 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   d->z = (C *)(base + off_z);
   d->tmp = (C *)(base + off_tmp);
   d->u = (R *)(base + off_u);
+  d->status = (int *)(base + off_status);
+  d->tc_s2m[0] = (float *)(base + off_tcs2m), d->tc_s2m[1] = d->tc_s2m[0] + sz_s2m;
+  d->tc_m2m[0] = (float *)(base + off_tcm2m), d->tc_m2m[1] = d->tc_m2m[0] + sz_m2m;
+  d->tc_m2l[0] = (float *)(base + off_tcm2l), d->tc_m2l[1] = d->tc_m2l[0] + sz_m2l;
+  d->tc_leaf[0] = (float *)(base + off_tcleaf), d->tc_leaf[1] = d->tc_leaf[0] + sz_leaf;
+  cudaMemset(d->status, 0, sizeof(int));
+  {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&d->num_sms, cudaDevAttrMultiProcessorCount, dev);
+  }
 
   /* ---- operator layouts (FP64 on the host, rounded once to R) ---- */
   int rc = 0;
@@ -720,6 +953,7 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   }
   rc |= upload<R>((R **)&d->twM, hm, 2 * M, err, errlen);
   free(hm);
+  if (tc && !rc) rc = tc_upload_ops(d, o, err, errlen);
   if (rc) {
     cudaFree(pool);
     delete d;
@@ -759,16 +993,45 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   /* 3: S2M at level n */
   stage(ST_S2M);
   {
-    ProbS2M<R> pb{d->xt, d->initch, d->phi + lvl_off(n, S1, T), 2 * S1 * s, M, (int)b, (int)T};
-    launch_rowgemm<R>(pb, pb.rows, (int)T, 1, st);
+    bool done = false;
+    if constexpr (sizeof(R) == 4) {
+      if (d->tc && d->ok_s2m && 2 * S1 * s >= d->tc_min_rows) {
+        TcS2M q{};
+        q.rows = 2 * S1 * s, q.batches = 1, q.nchunks = 1, q.clen[0] = (int)b, q.coff[0] = 0;
+        q.kpad = d->kp_s2m, q.npad = d->np_s2m, q.nout = (int)T;
+        q.bhi = d->tc_s2m[0], q.blo = d->tc_s2m[1], q.bstride = 0;
+        q.xt = d->xt, q.out = d->phi + lvl_off(n, S1, T), q.M = M, q.b = (int)b, q.T = (int)T;
+        launch_tc(q, d->num_sms, d->status, st);
+        done = true;
+      }
+    }
+    if (!done) {
+      ProbS2M<R> pb{d->xt, d->initch, d->phi + lvl_off(n, S1, T), 2 * S1 * s, M, (int)b, (int)T};
+      launch_rowgemm<R>(pb, pb.rows, (int)T, 1, st);
+    }
     pf.launches[ST_S2M]++;
   }
   /* 4: M2M, parent level L = n-1 .. 2 */
   stage(ST_M2M);
   for (long L = n - 1; L >= 2; --L) {
-    ProbM2M<R> pb{d->phi + lvl_off(L + 1, S1, T), d->bm2m + (L - 2) * 2 * T * T,
-                  d->phi + lvl_off(L, S1, T), 2 * S1 * (1L << L), (int)(2 * T), (int)T};
-    launch_rowgemm<R>(pb, pb.rows, (int)T, 1, st);
+    bool done = false;
+    if constexpr (sizeof(R) == 4) {
+      if (d->tc && d->ok_m2m && 2 * S1 * (1L << L) >= d->tc_min_rows) {
+        TcM2M q{};
+        q.rows = 2 * S1 * (1L << L), q.batches = 1, q.nchunks = 1, q.clen[0] = (int)(2 * T), q.coff[0] = 0;
+        q.kpad = d->kp_m2m, q.npad = d->np_m2m, q.nout = (int)T;
+        q.bhi = d->tc_m2m[0] + (L - 2) * d->tc_m2m_stride, q.blo = d->tc_m2m[1] + (L - 2) * d->tc_m2m_stride;
+        q.bstride = 0;
+        q.child = d->phi + lvl_off(L + 1, S1, T), q.out = d->phi + lvl_off(L, S1, T), q.T = (int)T;
+        launch_tc(q, d->num_sms, d->status, st);
+        done = true;
+      }
+    }
+    if (!done) {
+      ProbM2M<R> pb{d->phi + lvl_off(L + 1, S1, T), d->bm2m + (L - 2) * 2 * T * T,
+                    d->phi + lvl_off(L, S1, T), 2 * S1 * (1L << L), (int)(2 * T), (int)T};
+      launch_rowgemm<R>(pb, pb.rows, (int)T, 1, st);
+    }
     pf.launches[ST_M2M]++;
   }
   /* 5: top flip */
@@ -782,10 +1045,28 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   /* 6: M2L + L2L, child level l = 3..n (rows = parent boxes) */
   stage(ST_M2L);
   for (long l = 3; l <= n; ++l) {
-    ProbM2L<R> pb{d->psi + lvl_off(l - 1, S1, T), d->phi + lvl_off(l, S1, T),
-                  d->bm2l + (l - 3) * 10 * T * T, d->psi + lvl_off(l, S1, T),
-                  2 * S1 * (1L << (l - 1)), (int)(5 * T), (int)(2 * T), (int)T, (int)(l - 1)};
-    launch_rowgemm<R>(pb, pb.rows, (int)(2 * T), 1, st);
+    bool done = false;
+    if constexpr (sizeof(R) == 4) {
+      if (d->tc && d->ok_m2l && 2 * S1 * (1L << (l - 1)) >= d->tc_min_rows) {
+        TcM2L q{};
+        q.rows = 2 * S1 * (1L << (l - 1)), q.batches = 1, q.nchunks = 3;
+        q.clen[0] = (int)T, q.clen[1] = (int)(2 * T), q.clen[2] = (int)(2 * T);
+        q.coff[0] = 0, q.coff[1] = (int)T, q.coff[2] = (int)(3 * T);
+        q.kpad = d->kp_m2l, q.npad = d->np_m2l, q.nout = (int)(2 * T);
+        q.bhi = d->tc_m2l[0] + (l - 3) * d->tc_m2l_stride, q.blo = d->tc_m2l[1] + (l - 3) * d->tc_m2l_stride;
+        q.bstride = 0;
+        q.psi_par = d->psi + lvl_off(l - 1, S1, T), q.phi = d->phi + lvl_off(l, S1, T);
+        q.out = d->psi + lvl_off(l, S1, T), q.T = (int)T, q.lpar = (int)(l - 1);
+        launch_tc(q, d->num_sms, d->status, st);
+        done = true;
+      }
+    }
+    if (!done) {
+      ProbM2L<R> pb{d->psi + lvl_off(l - 1, S1, T), d->phi + lvl_off(l, S1, T),
+                    d->bm2l + (l - 3) * 10 * T * T, d->psi + lvl_off(l, S1, T),
+                    2 * S1 * (1L << (l - 1)), (int)(5 * T), (int)(2 * T), (int)T, (int)(l - 1)};
+      launch_rowgemm<R>(pb, pb.rows, (int)(2 * T), 1, st);
+    }
     pf.launches[ST_M2L]++;
   }
   /* 7: leaf far + near field per section, then the half-shifted first points */
@@ -799,7 +1080,22 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
     pb.u = d->u;
     pb.rows = 2 * s, pb.M = M, pb.s = s;
     pb.K = (int)(T + 3 * b), pb.N = (int)b, pb.T = (int)T, pb.b = (int)b;
-    launch_rowgemm<R>(pb, pb.rows, (int)b, (int)S1, st);
+    bool done = false;
+    if constexpr (sizeof(R) == 4) {
+      if (d->tc && d->ok_leaf && 2 * s >= (d->tc_min_rows < 256 ? d->tc_min_rows : 256)) {
+        TcLeaf q{};
+        q.rows = 2 * s, q.batches = (int)S1, q.nchunks = 4;
+        q.clen[0] = (int)T, q.clen[1] = q.clen[2] = q.clen[3] = (int)b;
+        q.coff[0] = 0, q.coff[1] = (int)T, q.coff[2] = (int)(T + b), q.coff[3] = (int)(T + 2 * b);
+        q.kpad = d->kp_leaf, q.npad = d->np_leaf, q.nout = (int)b;
+        q.bhi = d->tc_leaf[0], q.blo = d->tc_leaf[1], q.bstride = d->tc_leaf_stride;
+        q.psi_n = pb.psi_n, q.xt = d->xt, q.u = d->u, q.M = M, q.s = s, q.T = (int)T, q.b = (int)b;
+        q.log2s = (int)n;
+        launch_tc(q, d->num_sms, d->status, st);
+        done = true;
+      }
+    }
+    if (!done) launch_rowgemm<R>(pb, pb.rows, (int)b, (int)S1, st);
     pf.launches[ST_LEAF]++;
     stage(ST_LEAFFIX);
     pf.launches[ST_LEAFFIX]++;
@@ -870,6 +1166,15 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
 
 /* ======================================================================== C interface */
 
+/* Opt a kernel in to the largest dynamic shared memory the device allows next to its static
+ * shared memory. */
+template <typename K> static void allow_dyn_smem(K *kernel, int maxopt) {
+  cudaFuncAttributes a;
+  if (cudaFuncGetAttributes(&a, kernel) != cudaSuccess) return;
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       maxopt - (int)a.sharedSizeBytes);
+}
+
 static int set_smem_limits(void) {
   static int done = 0;
   if (done) return 0;
@@ -883,6 +1188,10 @@ static int set_smem_limits(void) {
   cudaFuncSetAttribute(k_combine<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_sections<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_sections<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  allow_dyn_smem(tc::k_tc_rowgemm<TcS2M>, lim);
+  allow_dyn_smem(tc::k_tc_rowgemm<TcM2M>, lim);
+  allow_dyn_smem(tc::k_tc_rowgemm<TcM2L>, lim);
+  allow_dyn_smem(tc::k_tc_rowgemm<TcLeaf>, lim);
   done = 1;
   return 0;
 }
@@ -1238,4 +1547,14 @@ extern "C" int fmmk_execute_noalloc(const fmm_ops64 *o, int reuse_ops, const voi
   d.z = (float2 *)(base + L.z);
   d.tmp = (float2 *)(base + L.tmp);
   return dev_execute<float>(&d, d_in, d_out, st, 0, err, errlen);
+}
+
+/* Reads (and clears) the plan's device status word; synchronises the device. */
+extern "C" int fmmk_check(fmmk_state *st) {
+  int *status = st->precision == 0 ? ((Dev<double> *)st->dev)->status : ((Dev<float> *)st->dev)->status;
+  int h = 0;
+  if (cudaDeviceSynchronize() != cudaSuccess) return 3;
+  if (cudaMemcpy(&h, status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return 3;
+  if (h) cudaMemset(status, 0, sizeof(int));
+  return h ? 6 : 0;
 }

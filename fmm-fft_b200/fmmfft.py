@@ -26,7 +26,7 @@ EXPORTS = ["getwlen2", "getvlen", "mfti", "mft", "fmmfft_last_error", "fmmfft_la
            "fmmfft_plan_create", "fmmfft_plan_destroy", "fmmfft_plan_device_bytes",
            "fmmfft_execute", "fmmfft_execute_inverse", "fmmfft_execute_host",
            "fmmfft_debug_fetch", "fmmfft_profile_start", "fmmfft_profile_stop",
-           "fmmfft_stage_name", "fmmfft_execute_noalloc"]
+           "fmmfft_stage_name", "fmmfft_execute_noalloc", "fmmfft_plan_check"]
 
 
 class FmmFftError(RuntimeError):
@@ -69,6 +69,8 @@ def load(path=LIB_PATH):
     lib.fmmfft_stage_name.restype = ctypes.c_char_p
     lib.fmmfft_execute_noalloc.argtypes = [_L, _L, _L, _L, _VP, _VP, _VP]
     lib.fmmfft_execute_noalloc.restype = _I
+    lib.fmmfft_plan_check.argtypes = [_VP]
+    lib.fmmfft_plan_check.restype = _I
     _lib = lib
     return lib
 
@@ -189,6 +191,10 @@ class Plan:
         _check(load().fmmfft_debug_fetch(self._h, u.ctypes.data, z.ctypes.data, phi.ctypes.data,
                                          psi.ctypes.data))
         return dict(u=u[:, 0] + 1j * u[:, 1], z=z[..., 0] + 1j * z[..., 1], phi=phi, psi=psi)
+
+    def check(self):
+        """Synchronise; raise FmmFftError(ERR_TIMEOUT) if a bounded device wait gave up."""
+        _check(load().fmmfft_plan_check(self._h))
 
     def profile_start(self, max_executes):
         _check(load().fmmfft_profile_start(self._h, int(max_executes)))

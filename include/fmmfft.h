@@ -114,6 +114,11 @@ int fmmfft_execute_host(fmmfft_plan plan, const void *h_in, void *h_out, void *s
  *        (2^l - 4) * (P-1) * 2 * terms) */
 int fmmfft_debug_fetch(fmmfft_plan plan, double *u, double *z, double *phi, double *psi);
 
+/* Synchronises the device and reports FMMFFT_ERR_TIMEOUT if, since the last check, a bounded
+ * device-side wait (the tensor-core kernels' mbarrier waits) gave up instead of completing;
+ * FMMFFT_OK otherwise.  Clears the recorded status. */
+int fmmfft_plan_check(fmmfft_plan plan);
+
 /* ------------------------------------------------------------------ stage timing */
 /* Records CUDA events around every stage of the next `max_executes` executes of this plan (on
  * the stream each execute runs on).  No counterpart in the reference, which only times the

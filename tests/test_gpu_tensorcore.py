@@ -1,0 +1,84 @@
+"""The 3xTF32 tcgen05 path (FMMFFT_F32_TC) against the FP64 oracle, stage by stage.
+
+FMMFFT_TC_MIN_ROWS=1 (set before the plans are made) sends every eligible stage, however small,
+through the tensor-core kernel so that small cases cover it; the default threshold only routes
+stages with >= 8192 rows there.  Tolerance: rel-L2 <= 1e-6 against FP64, as for FP32 plans.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+from gpu_util import run_device
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-6          # the transform's output and z, against FP64
+TOL_STAGE = 1e-4    # intermediate expansions: 3xTF32 leaves ~2^-22 per product, and with few
+                    # terms and wide boxes (S2M with K = b = 128) cancellation magnifies it
+
+CASES = [(4096, 4, 8, 16), (16384, 8, 12, 32), (65536, 16, 16, 32), (65536, 64, 24, 32),
+         (1 << 18, 4, 20, 64), (1 << 18, 32, 24, 16), (1 << 18, 2, 8, 128)]
+
+
+@pytest.fixture(scope="module")
+def fm():
+    import fmmfft
+    fmmfft.load()
+    return fmmfft
+
+
+@pytest.fixture()
+def force_tc():
+    old = os.environ.get("FMMFFT_TC_MIN_ROWS")
+    os.environ["FMMFFT_TC_MIN_ROWS"] = "1"
+    yield
+    if old is None:
+        del os.environ["FMMFFT_TC_MIN_ROWS"]
+    else:
+        os.environ["FMMFFT_TC_MIN_ROWS"] = old
+
+
+@pytest.mark.parametrize("N,P,T,b", CASES)
+def test_tc_stagewise_vs_oracle(fm, force_tc, N, P, T, b):
+    x = ol.seeded_input(N, 17 + N % 97)
+    o = ol.forward_ex(x, P, T, b)
+    plan = fm.Plan(N, P, T, b, "f32_tc")
+    y = run_device(plan, x)
+    plan.check()
+    d = plan.debug_fetch()
+    M = N // P
+    s = M // b
+    n = s.bit_length() - 1
+    for lev in range(2, n + 1):
+        gp = fm.level_planar(d["phi"], P, T, n, lev)
+        gs = fm.level_planar(d["psi"], P, T, n, lev)
+        gp = (gp[:, 0] + 1j * gp[:, 1]).transpose(1, 0, 2)
+        gs = (gs[:, 0] + 1j * gs[:, 1]).transpose(1, 0, 2)
+        assert ol.rel_l2(gp, o["phi"][ol.level_slice(lev)]) < TOL_STAGE, ("phi", lev)
+        assert ol.rel_l2(gs, o["psi"][ol.level_slice(lev)]) < TOL_STAGE, ("psi", lev)
+    assert ol.rel_l2(d["u"], o["u"]) < TOL_STAGE
+    assert ol.rel_l2(d["z"], o["z"]) < TOL
+    assert ol.rel_l2(y, o["y"]) < TOL
+
+
+def test_tc_config2_full_size(fm):
+    """N = 2^24 complex64, P = 64, p = 24, b = 32 with the default routing."""
+    N, P, T, b = 1 << 24, 64, 24, 32
+    x = ol.seeded_input(N, 0)
+    plan = fm.Plan(N, P, T, b, "f32_tc")
+    y = run_device(plan, x)
+    plan.check()
+    ref = np.fft.fft(x)
+    assert ol.rel_l2(y, ref) < TOL
+    assert np.max(np.abs(y - ref)) / np.max(np.abs(ref)) < 1e-5
+
+
+def test_tc_matches_plain_f32(fm):
+    N, P, T, b = 1 << 20, 64, 16, 32
+    x = ol.seeded_input(N, 4)
+    y1 = run_device(fm.Plan(N, P, T, b, "f32"), x)
+    plan = fm.Plan(N, P, T, b, "f32_tc")
+    y2 = run_device(plan, x)
+    plan.check()
+    assert ol.rel_l2(y2, y1) < TOL
