@@ -139,26 +139,27 @@ __global__ void k_sections(const typename cplx<R>::T *__restrict__ x, R *__restr
                            int conj_in) {
   using C = typename cplx<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *tile = reinterpret_cast<C *>(smem_raw); /* [TMt][P] */
+  C *tile = reinterpret_cast<C *>(smem_raw); /* [TMt][P + 1]: the pad spreads a column over banks */
+  const int PP = P + 1, lp = __ffs(P) - 1, lt = __ffs(TMt) - 1;
   const long m0 = (long)blockIdx.x * TMt;
   const int E = TMt * P;
   for (int e = threadIdx.x; e < E; e += blockDim.x) {
     C v = x[m0 * P + e];
     if (conj_in) v.y = -v.y;
-    tile[e] = v;
+    tile[(e >> lp) * PP + (e & (P - 1))] = v;
   }
   __syncthreads();
   /* planar store: plane (2sc+ri), TMt contiguous points */
   for (int e = threadIdx.x; e < 2 * E; e += blockDim.x) {
-    int mm = e % TMt, q = e / TMt, sc = q >> 1, ri = q & 1;
-    C v = tile[mm * P + sc];
+    int mm = e & (TMt - 1), q = e >> lt, sc = q >> 1, ri = q & 1;
+    C v = tile[mm * PP + sc];
     xt[(long)q * M + m0 + mm] = ri ? v.y : v.x;
   }
   /* tile sums per section, fixed order */
   for (int sc = threadIdx.x; sc < P; sc += blockDim.x) {
     C acc;
     acc.x = 0, acc.y = 0;
-    for (int mm = 0; mm < TMt; ++mm) acc = cadd(acc, tile[mm * P + sc]);
+    for (int mm = 0; mm < TMt; ++mm) acc = cadd(acc, tile[mm * PP + sc]);
     part[(long)blockIdx.x * P + sc] = acc;
   }
 }
@@ -458,50 +459,206 @@ __global__ void k_leaf_fix(const R *__restrict__ psi_n, const R *__restrict__ xt
     *dst = R(0.5) * (*dst + v);
 }
 
+/* Leaf stage, direct form (b a multiple of 8): far field (L2T) plus near field of one re/im
+ * plane of one section for NB consecutive leaf boxes (reference fmmfft.c:751-954).
+ *
+ * Each thread computes 8 consecutive targets j0..j0+7 of one box:
+ *   u[j] = sum_k psi[box][k] E_sc[k][j] + sum_{q < 3b} x[(box-1) b + q] cot_sc[q + b - j],
+ * the near-field coefficients of the 8 targets are a sliding window of the Toeplitz row, so
+ * per 8 window points the thread loads 8 x values and 16 cot values (vector loads from shared
+ * memory) for 64 FMAs.  The first point of each box for sc >= P/2 (target shifted into the
+ * previous box) is evaluated from box-1's local expansion (evalmh) and the window box-2..box,
+ * and for sc = P/2 averaged with the in-box value, as the reference does (:771-803, :839-954).
+ * Block: 256 threads, grid (boxes / NB, 2 (P-1) planes). */
+template <typename R> __device__ __forceinline__ void ld8(const R *p, R *o) {
+#pragma unroll
+  for (int i = 0; i < 8; ++i) o[i] = p[i];
+}
+template <> __device__ __forceinline__ void ld8<float>(const float *p, float *o) {
+  float4 a = *reinterpret_cast<const float4 *>(p), c = *reinterpret_cast<const float4 *>(p + 4);
+  o[0] = a.x, o[1] = a.y, o[2] = a.z, o[3] = a.w, o[4] = c.x, o[5] = c.y, o[6] = c.z, o[7] = c.w;
+}
+template <> __device__ __forceinline__ void ld8<double>(const double *p, double *o) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    double2 a = *reinterpret_cast<const double2 *>(p + 2 * i);
+    o[2 * i] = a.x, o[2 * i + 1] = a.y;
+  }
+}
+
+/* Shared-memory row pitch for n values: a multiple of 4 whose quarter is odd, so that rows of
+ * consecutive boxes start in different 16-byte bank groups. */
+__host__ __device__ __forceinline__ long skew_pitch(long n) {
+  long p = (n + 3) & ~3L;
+  return ((p >> 2) & 1) ? p : p + 4;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_leaf(const R *__restrict__ psi_n, const R *__restrict__ xt,
+                                              const R *__restrict__ evalmT, const R *__restrict__ evalmh,
+                                              const R *__restrict__ cot, R *__restrict__ u, long M,
+                                              long s, int T, int b, int P, int NB, int e_in_smem) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const long xp = skew_pitch(b), tp = skew_pitch(T);
+  R *xw = reinterpret_cast<R *>(smem_raw); /* boxes B0-2 .. B0+NB, one row of pitch xp each */
+  R *ps = xw + (long)(NB + 3) * xp;        /* psi of boxes B0-1 .. B0+NB-1, pitch tp */
+  R *ct = ps + (((long)(NB + 1) * tp + 7) & ~7L); /* 4b */
+  R *eh = ct + 4 * b;                      /* T (rounded up to 8) */
+  R *Es = eh + ((T + 7) & ~7);             /* T b when e_in_smem */
+  const int pl = blockIdx.y, sc = pl / 2 + 1;
+  const long B0 = (long)blockIdx.x * NB;
+  const R *xs = xt + (long)(pl + 2) * M;
+  const R *pp = psi_n + (long)pl * s * T;
+  const R *E = evalmT + (long)(sc - 1) * T * b;
+  const bool shifted = 2 * sc >= P;
+  const int lb = __ffs(b) - 1; /* b is a power of two */
+  for (int e = threadIdx.x; e < (NB + 3) * b; e += blockDim.x)
+    xw[(long)(e >> lb) * xp + (e & (b - 1))] = xs[((B0 - 2) * b + e) & (M - 1)];
+  for (int e = threadIdx.x; e < (NB + 1) * T; e += blockDim.x) {
+    const int bx = e / T, k = e - bx * T; /* 32-bit division */
+    ps[(long)bx * tp + k] = pp[((B0 - 1 + bx) & (s - 1)) * T + k];
+  }
+  for (int e = threadIdx.x; e < 4 * b; e += blockDim.x) ct[e] = cot[(long)(sc - 1) * 4 * b + e];
+  if (shifted)
+    for (int e = threadIdx.x; e < T; e += blockDim.x) eh[e] = evalmh[(long)(sc - 1) * T + e];
+  if (e_in_smem)
+    for (long e = threadIdx.x; e < (long)T * b; e += blockDim.x) Es[e] = E[e];
+  __syncthreads();
+  const R *Eu = e_in_smem ? Es : E;
+  const int G = b >> 3; /* threads per box */
+  for (int w = threadIdx.x; w < NB * G; w += blockDim.x) {
+    const int bi = w / G, j0 = (w - bi * G) * 8;
+    R acc[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) acc[t] = R(0);
+    /* far field */
+    const R *pr = ps + (long)(bi + 1) * tp;
+    for (int k = 0; k < T; ++k) {
+      R e8[8];
+      ld8<R>(Eu + (long)k * b + j0, e8);
+      const R a = pr[k];
+#pragma unroll
+      for (int t = 0; t < 8; ++t) acc[t] = fma(a, e8[t], acc[t]);
+    }
+    /* near field over boxes box-1 .. box+1; each box's part is summed separately before it
+     * joins the total (long windows, b up to 2048, keep their FP32 rounding small) */
+#pragma unroll 1
+    for (int seg = 0; seg < 3; ++seg) {
+      const R *xr = xw + (long)(bi + 1 + seg) * xp; /* xw row i holds box B0 - 2 + i */
+      R part[8];
+#pragma unroll
+      for (int t = 0; t < 8; ++t) part[t] = R(0);
+      for (int q = 0; q < b; q += 8) {
+        R x8[8], w16[16];
+        const int cq = seg * b + q + b - j0; /* cot index of (point q, target j0) */
+        ld8<R>(xr + q, x8);
+        ld8<R>(ct + (cq - 8), w16);
+        ld8<R>(ct + cq, w16 + 8);
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+          for (int t = 0; t < 8; ++t) part[t] = fma(x8[i], w16[i - t + 8], part[t]);
+      }
+#pragma unroll
+      for (int t = 0; t < 8; ++t) acc[t] += part[t];
+    }
+    if (j0 == 0 && shifted) {
+      R far = R(0), near = R(0);
+      const R *pq = ps + (long)bi * tp; /* box - 1 */
+      for (int k = 0; k < T; ++k) far = fma(pq[k], eh[k], far);
+      for (int seg = 0; seg < 3; ++seg) { /* window box-2 .. box */
+        const R *xq = xw + (long)(bi + seg) * xp;
+        R part = R(0);
+        for (int q = 0; q < b; ++q) part = fma(xq[q], ct[seg * b + q], part);
+        near += part;
+      }
+      const R v = far + near;
+      acc[0] = (2 * sc > P) ? v : R(0.5) * (acc[0] + v);
+    }
+    R *dst = u + (long)pl * M + (B0 + bi) * b + j0;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) dst[t] = acc[t];
+  }
+}
+
 /* ======================================================================== shared-memory FFT */
 
+/* Forward DFT of 8 values in registers (split into two 4-point DFTs). */
+template <typename C> __device__ __forceinline__ void dft4(C &a, C &b, C &c, C &d) {
+  C t0 = cadd(a, c), t1 = csub(a, c), t2 = cadd(b, d), u = csub(b, d), t3;
+  t3.x = u.y, t3.y = -u.x; /* -i (b - d) */
+  a = cadd(t0, t2), b = cadd(t1, t3), c = csub(t0, t2), d = csub(t1, t3);
+}
+template <typename C> __device__ __forceinline__ void dft8(C *v) {
+  using R = decltype(v[0].x);
+  const R h = R(0.70710678118654752440084436210484904);
+  dft4(v[0], v[2], v[4], v[6]);
+  dft4(v[1], v[3], v[5], v[7]);
+  C o1 = v[3], o2 = v[5], o3 = v[7], w;
+  /* o_k * exp(-2 pi i k / 8), k = 1, 2, 3 */
+  w.x = h * (o1.x + o1.y), w.y = h * (o1.y - o1.x), o1 = w;
+  w.x = o2.y, w.y = -o2.x, o2 = w;
+  w.x = h * (o3.y - o3.x), w.y = -h * (o3.x + o3.y), o3 = w;
+  C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6], o0 = v[1];
+  v[0] = cadd(e0, o0), v[4] = csub(e0, o0);
+  v[1] = cadd(e1, o1), v[5] = csub(e1, o1);
+  v[2] = cadd(e2, o2), v[6] = csub(e2, o2);
+  v[3] = cadd(e3, o3), v[7] = csub(e3, o3);
+}
+
 /* W independent forward DFTs of length L held in shared memory as buf[i*W + w].  Stockham
- * radix-4 stages (one radix-2 stage first when log2 L is odd), ping-ponging between buf and
- * alt; returns the buffer that holds the result.  Twiddle exp(-2 pi i t / L) = tw[t * tws]. */
+ * stages of radix 8 (each thread: 8 values, twiddles, an 8-point DFT in registers), after one
+ * radix-2 or radix-4 stage when log2 L is not a multiple of 3; ping-pongs between buf and alt
+ * and returns the buffer that holds the result.  Twiddle exp(-2 pi i t / L) = tw[t * tws]. */
 template <typename C>
 __device__ C *smem_fft(C *buf, C *alt, int L, int W, const C *__restrict__ tw, long tws) {
-  int Ns = 1;
-  if (__ffs(L) & 1) { /* log2 L even: all radix-4 */
-  } else { /* odd: one radix-2 stage */
+  int lg = __ffs(L) - 1, Ns = 1;
+  if (lg % 3 == 1) { /* one radix-2 stage */
     const int half = L / 2;
     for (int e = threadIdx.x; e < half * W; e += blockDim.x) {
       int j = e / W, w = e - j * W;
       C v0 = buf[j * W + w], v1 = buf[(j + half) * W + w];
-      C a = cadd(v0, v1), c = csub(v0, v1);
-      alt[(2 * j) * W + w] = a;
-      alt[(2 * j + 1) * W + w] = c;
+      alt[(2 * j) * W + w] = cadd(v0, v1);
+      alt[(2 * j + 1) * W + w] = csub(v0, v1);
     }
     __syncthreads();
     C *t = buf;
     buf = alt, alt = t;
     Ns = 2;
-  }
-  const int q4 = L / 4;
-  for (; Ns < L; Ns *= 4) {
+  } else if (lg % 3 == 2) { /* one radix-4 stage */
+    const int q4 = L / 4;
     for (int e = threadIdx.x; e < q4 * W; e += blockDim.x) {
       int j = e / W, w = e - j * W;
+      C a = buf[j * W + w], b = buf[(j + q4) * W + w], c = buf[(j + 2 * q4) * W + w],
+        d = buf[(j + 3 * q4) * W + w];
+      dft4(a, b, c, d);
+      alt[(4 * j) * W + w] = a;
+      alt[(4 * j + 1) * W + w] = b;
+      alt[(4 * j + 2) * W + w] = c;
+      alt[(4 * j + 3) * W + w] = d;
+    }
+    __syncthreads();
+    C *t = buf;
+    buf = alt, alt = t;
+    Ns = 4;
+  }
+  const int q8 = L / 8;
+  for (; Ns < L; Ns *= 8) {
+    for (int e = threadIdx.x; e < q8 * W; e += blockDim.x) {
+      int j = e / W, w = e - j * W;
       int k = j % Ns;
-      C v0 = buf[j * W + w], v1 = buf[(j + q4) * W + w], v2 = buf[(j + 2 * q4) * W + w],
-        v3 = buf[(j + 3 * q4) * W + w];
+      C v[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) v[r] = buf[(j + r * q8) * W + w];
       if (Ns > 1) {
-        long ts = (long)k * (L / (Ns * 4)) * tws;
-        v1 = cmul(v1, tw[ts]);
-        v2 = cmul(v2, tw[2 * ts]);
-        v3 = cmul(v3, tw[3 * ts]);
+        const long ts = (long)k * (L / (Ns * 8)) * tws;
+#pragma unroll
+        for (int r = 1; r < 8; ++r) v[r] = cmul(v[r], tw[r * ts]);
       }
-      C a = cadd(v0, v2), bq = csub(v0, v2), c = cadd(v1, v3), d = csub(v1, v3);
-      C dd;
-      dd.x = d.y, dd.y = -d.x; /* -i * d */
-      int o = (j / Ns) * Ns * 4 + k;
-      alt[(o)*W + w] = cadd(a, c);
-      alt[(o + Ns) * W + w] = cadd(bq, dd);
-      alt[(o + 2 * Ns) * W + w] = csub(a, c);
-      alt[(o + 3 * Ns) * W + w] = csub(bq, dd);
+      dft8(v);
+      const int o = (j / Ns) * Ns * 8 + k;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) alt[(o + r * Ns) * W + w] = v[r];
     }
     __syncthreads();
     C *t = buf;
@@ -983,7 +1140,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   stage(ST_SECTIONS);
   {
     int TMt = (int)d->tileM;
-    size_t sm = sizeof(C) * TMt * P;
+    size_t sm = sizeof(C) * TMt * (P + 1);
     k_sections<R><<<(unsigned)d->ntile, 256, sm, st>>>(x, d->xt, d->part, M, (int)P, TMt, inverse);
     pf.launches[ST_SECTIONS]++;
     stage(ST_SUMS);
@@ -1095,13 +1252,28 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         done = true;
       }
     }
-    if (!done) launch_rowgemm<R>(pb, pb.rows, (int)b, (int)S1, st);
-    pf.launches[ST_LEAF]++;
-    stage(ST_LEAFFIX);
-    pf.launches[ST_LEAFFIX]++;
-    dim3 g((unsigned)((2 * s + 127) / 128), (unsigned)(P - P / 2));
-    k_leaf_fix<R><<<g, 128, 0, st>>>(pb.psi_n, d->xt, d->evalmh, d->cot, d->u, M, s, (int)T,
-                                     (int)b, (int)P);
+    if (!done && b % 8 == 0) {
+      /* direct form; it also evaluates the half-shifted first points */
+      int NB = (int)(256 / (b / 8));
+      if (NB < 1) NB = 1;
+      if (NB > s) NB = (int)s;
+      const int e_in_smem = (size_t)T * b * sizeof(R) <= 16384;
+      size_t sm = sizeof(R) * ((size_t)(NB + 3) * skew_pitch(b) +
+                               (((size_t)(NB + 1) * skew_pitch(T) + 7) & ~(size_t)7) + 4 * b +
+                               ((T + 7) & ~7) + (e_in_smem ? (size_t)T * b : 0));
+      dim3 g((unsigned)(s / NB), (unsigned)(2 * S1));
+      k_leaf<R><<<g, 256, sm, st>>>(pb.psi_n, d->xt, d->evalmT, d->evalmh, d->cot, d->u, M, s,
+                                    (int)T, (int)b, (int)P, NB, e_in_smem);
+      pf.launches[ST_LEAF]++;
+    } else {
+      if (!done) launch_rowgemm<R>(pb, pb.rows, (int)b, (int)S1, st);
+      pf.launches[ST_LEAF]++;
+      stage(ST_LEAFFIX);
+      pf.launches[ST_LEAFFIX]++;
+      dim3 g((unsigned)((2 * s + 127) / 128), (unsigned)(P - P / 2));
+      k_leaf_fix<R><<<g, 128, 0, st>>>(pb.psi_n, d->xt, d->evalmh, d->cot, d->u, M, s, (int)T,
+                                       (int)b, (int)P);
+    }
   }
   /* 8: combine -> z[P][M] */
   stage(ST_COMBINE);
@@ -1188,6 +1360,8 @@ static int set_smem_limits(void) {
   cudaFuncSetAttribute(k_combine<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_sections<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_sections<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_leaf<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_leaf<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   allow_dyn_smem(tc::k_tc_rowgemm<TcS2M>, lim);
   allow_dyn_smem(tc::k_tc_rowgemm<TcM2M>, lim);
   allow_dyn_smem(tc::k_tc_rowgemm<TcM2L>, lim);
