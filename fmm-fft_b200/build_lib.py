@@ -19,8 +19,8 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
 CU_SOURCES = ["fmmfft_kernels.cu"]
-C_SOURCES = ["fmmfft_ops.c", "fmmfft_api.c"]
-HEADERS = ["fmmfft_internal.h", os.path.join("..", "..", "include", "fmmfft.h")]
+C_SOURCES = ["fmmfft_ops.c", "fmmfft_api.c", "fmmfft_serve.c"]
+HEADERS = ["fmmfft_internal.h", "fmmfft_tc.cuh", os.path.join("..", "..", "include", "fmmfft.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

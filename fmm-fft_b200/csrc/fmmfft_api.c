@@ -137,6 +137,76 @@ int fmmfft_plan_check(fmmfft_plan plan) {
   return rc ? set_err(rc, "plan_check: CUDA error") : FMMFFT_OK;
 }
 
+int fmmfft_execute_graph(fmmfft_plan plan, const void *d_in, void *d_out, void *stream) {
+  if (!plan || !d_in || !d_out) return set_err(FMMFFT_ERR_INVALID, "execute_graph: NULL argument");
+  char err[256] = {0};
+  int rc = fmmk_execute_graph(plan->dev, d_in, d_out, stream, 0, err, sizeof err);
+  return rc ? set_err(rc, err) : FMMFFT_OK;
+}
+
+/* ------------------------------------------------------------------ batches */
+struct fmmfft_batch_s {
+  void *exec;
+  int n, nbranch;
+};
+
+int fmmfft_batch_create(fmmfft_batch *out, const fmmfft_plan *plans, const void *const *d_in,
+                        void *const *d_out, int n, int nbranch) {
+  if (!out || !plans || !d_in || !d_out || n < 1 || nbranch < 1 || nbranch > 64)
+    return set_err(FMMFFT_ERR_INVALID, "batch_create: bad arguments");
+  *out = NULL;
+  fmmk_state **sts = (fmmk_state **)calloc((size_t)n, sizeof(fmmk_state *));
+  int *branch = (int *)calloc((size_t)n, sizeof(int));
+  double *load = (double *)calloc((size_t)nbranch, sizeof(double));
+  struct fmmfft_batch_s *b = (struct fmmfft_batch_s *)calloc(1, sizeof *b);
+  if (!sts || !branch || !load || !b) {
+    free(sts), free(branch), free(load), free(b);
+    return set_err(FMMFFT_ERR_NOMEM, "batch_create: allocation failed");
+  }
+  /* every transform of one plan goes to the branch its plan first went to (shared workspace);
+   * a new plan goes to the branch with the least work so far */
+  for (int i = 0; i < n; ++i) {
+    if (!plans[i]) {
+      free(sts), free(branch), free(load), free(b);
+      return set_err(FMMFFT_ERR_INVALID, "batch_create: NULL plan");
+    }
+    sts[i] = plans[i]->dev;
+    int br = -1;
+    for (int j = 0; j < i && br < 0; ++j)
+      if (plans[j] == plans[i]) br = branch[j];
+    if (br < 0) {
+      br = 0;
+      for (int k = 1; k < nbranch; ++k)
+        if (load[k] < load[br]) br = k;
+    }
+    branch[i] = br;
+    load[br] += (double)plans[i]->N;
+  }
+  char err[256] = {0};
+  int rc = fmmk_batch_capture(sts, d_in, d_out, NULL, branch, n, nbranch, &b->exec, err, sizeof err);
+  free(sts), free(branch), free(load);
+  if (rc) {
+    free(b);
+    return set_err(rc, err);
+  }
+  b->n = n, b->nbranch = nbranch;
+  *out = b;
+  return set_err(FMMFFT_OK, NULL);
+}
+
+int fmmfft_batch_launch(fmmfft_batch batch, void *stream) {
+  if (!batch) return set_err(FMMFFT_ERR_INVALID, "batch_launch: NULL batch");
+  return fmmk_batch_launch(batch->exec, stream) ? set_err(FMMFFT_ERR_CUDA, "batch_launch failed")
+                                                : FMMFFT_OK;
+}
+
+int fmmfft_batch_destroy(fmmfft_batch batch) {
+  if (!batch) return FMMFFT_OK;
+  fmmk_batch_free(batch->exec);
+  free(batch);
+  return FMMFFT_OK;
+}
+
 /* ------------------------------------------------------------------ allocation-free entry */
 
 /* FP64 operator tables for fmmfft_execute_noalloc, built in this file-scope store (no heap):

@@ -54,6 +54,13 @@ int fmmk_profile_start(fmmk_state *st, int cap);
 int fmmk_profile_stop(fmmk_state *st, double *stage_ms, int *stage_launches, int cap, int *nexec);
 const char *fmmk_stage_name(int i);
 int fmmk_check(fmmk_state *st);
+int fmmk_execute_graph(fmmk_state *st, const void *d_in, void *d_out, void *stream, int inverse,
+                       char *err, size_t errlen);
+int fmmk_batch_capture(fmmk_state *const *sts, const void *const *ins, void *const *outs,
+                       const int *inverse, const int *branch, int n, int nbranch, void **exec_out,
+                       char *err, size_t errlen);
+int fmmk_batch_launch(void *exec, void *stream);
+void fmmk_batch_free(void *exec);
 int fmmk_execute_noalloc(const fmm_ops64 *ops, int reuse_ops, const void *d_in, void *d_out,
                          void *stream, char *err, size_t errlen);
 

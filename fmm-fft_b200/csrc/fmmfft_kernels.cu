@@ -120,9 +120,22 @@ template <typename R> struct Dev {
   long tc_min_rows; /* stages with fewer rows use the CUDA-core kernel */
 };
 
+/* Instantiated CUDA graphs of one plan's execute, keyed by (input, output, direction): the
+ * ~35 kernel launches of a transform become one graph launch. */
+#define FMMK_GRAPHS 8
+struct GraphSlot {
+  const void *in;
+  void *out;
+  int inverse;
+  unsigned long long last_use;
+  cudaGraphExec_t exec;
+};
+
 struct fmmk_state {
   int precision;
   void *dev; /* Dev<float> or Dev<double> */
+  GraphSlot graphs[FMMK_GRAPHS];
+  unsigned long long graph_clock;
 };
 
 __host__ __device__ __forceinline__ long lvl_off(long l, long S1, long T) {
@@ -690,6 +703,8 @@ __global__ void k_fft_pass(const typename cplx<R>::T *__restrict__ in,
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *buf = reinterpret_cast<C *>(smem_raw);
   C *alt = buf + (long)fp.L * fp.W;
+  C *twl = alt + (long)fp.L * fp.W; /* exp(-2 pi i t / L), t < L: the DFT twiddles, in shared memory */
+  for (int t = threadIdx.x; t < fp.L; t += blockDim.x) twl[t] = twM[(long)t * fp.tws];
   const long row = blockIdx.y;
   const long g0 = (long)blockIdx.x * fp.W; /* first sequence of this block within the row */
   const C *src = in + row * fp.M;
@@ -707,7 +722,7 @@ __global__ void k_fft_pass(const typename cplx<R>::T *__restrict__ in,
     }
   }
   __syncthreads();
-  C *res = smem_fft<C>(buf, alt, fp.L, fp.W, twM, fp.tws);
+  C *res = smem_fft<C>(buf, alt, fp.L, fp.W, twl, 1);
   if (fp.ostr == 1) {
     for (int e = threadIdx.x; e < LW; e += blockDim.x) {
       int i = e % fp.L, w = e / fp.L;
@@ -1296,7 +1311,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
       /* W rows per block: treat W consecutive rows as one "row" of W sequences */
       fp.W = W, fp.per = W, fp.M = M * W, fp.iseq = M, fp.oseq = M;
       dim3 g(1, (unsigned)(P / W));
-      size_t sm = 2 * sizeof(C) * (size_t)M * W;
+      size_t sm = sizeof(C) * (size_t)M * (2 * W + 1);
       k_fft_pass<R><<<g, 256, sm, st>>>(d->z, y, d->twM, fp);
       pf.launches[ST_FFT1]++;
     } else {
@@ -1307,7 +1322,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
       if (W1 > M1) W1 = (int)M1;
       FftPass f1{(int)M2, W1, (int)M1, M, 1, M1, 1, M1, 1, M / M2, 0};
       dim3 g1((unsigned)(M1 / W1), (unsigned)P);
-      k_fft_pass<R><<<g1, 256, 2 * sizeof(C) * (size_t)M2 * W1, st>>>(d->z, d->tmp, d->twM, f1);
+      k_fft_pass<R><<<g1, 256, sizeof(C) * (size_t)M2 * (2 * W1 + 1), st>>>(d->z, d->tmp, d->twM, f1);
       pf.launches[ST_FFT1]++;
       stage(ST_FFT2);
       /* pass 2: for each k2, DFT over m1 (contiguous), store y[k2 + M2*k1] */
@@ -1316,7 +1331,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
       if (W2 > M2) W2 = (int)M2;
       FftPass f2{(int)M1, W2, (int)M2, M, M1, 1, 1, M2, 0, M / M1, inverse};
       dim3 g2((unsigned)(M2 / W2), (unsigned)P);
-      k_fft_pass<R><<<g2, 256, 2 * sizeof(C) * (size_t)M1 * W2, st>>>(d->tmp, y, d->twM, f2);
+      k_fft_pass<R><<<g2, 256, sizeof(C) * (size_t)M1 * (2 * W2 + 1), st>>>(d->tmp, y, d->twM, f2);
       pf.launches[ST_FFT2]++;
     }
   }
@@ -1417,6 +1432,8 @@ extern "C" int fmmk_create(const fmm_ops64 *ops, int precision, fmmk_state **out
 
 extern "C" void fmmk_destroy(fmmk_state *st) {
   if (!st) return;
+  for (int i = 0; i < FMMK_GRAPHS; ++i)
+    if (st->graphs[i].exec) cudaGraphExecDestroy(st->graphs[i].exec);
   if (st->precision == 0) {
     Dev<double> *d = (Dev<double> *)st->dev;
     if (d) cudaFree(d->pool), delete d;
@@ -1731,4 +1748,117 @@ extern "C" int fmmk_check(fmmk_state *st) {
   if (cudaMemcpy(&h, status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return 3;
   if (h) cudaMemset(status, 0, sizeof(int));
   return h ? 6 : 0;
+}
+
+/* ======================================================================== CUDA graphs */
+
+/* Execute through a cached graph: the first call for a given (in, out, direction) captures the
+ * plan's launch sequence on a private stream and instantiates it; later calls launch the graph
+ * on `stream`.  The least recently used of FMMK_GRAPHS graphs is replaced when full. */
+extern "C" int fmmk_execute_graph(fmmk_state *st, const void *d_in, void *d_out, void *stream,
+                                  int inverse, char *err, size_t errlen) {
+  GraphSlot *hit = NULL, *victim = &st->graphs[0];
+  for (int i = 0; i < FMMK_GRAPHS; ++i) {
+    GraphSlot *g = &st->graphs[i];
+    if (g->exec && g->in == d_in && g->out == d_out && g->inverse == inverse) hit = g;
+    if (!g->exec || (victim->exec && g->last_use < victim->last_use)) victim = g;
+  }
+  if (!hit) {
+    cudaStream_t cap;
+    FMM_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+      cudaStreamDestroy(cap);
+      snprintf(err, errlen, "cudaStreamBeginCapture: %s", cudaGetErrorString(e));
+      return 3;
+    }
+    int rc = fmmk_execute(st, d_in, d_out, cap, inverse, err, errlen);
+    cudaGraph_t graph = NULL;
+    e = cudaStreamEndCapture(cap, &graph);
+    cudaStreamDestroy(cap);
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if (e != cudaSuccess) {
+      snprintf(err, errlen, "cudaStreamEndCapture: %s", cudaGetErrorString(e));
+      return 3;
+    }
+    cudaGraphExec_t exec = NULL;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      snprintf(err, errlen, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+      return 3;
+    }
+    if (victim->exec) cudaGraphExecDestroy(victim->exec);
+    victim->in = d_in, victim->out = d_out, victim->inverse = inverse, victim->exec = exec;
+    hit = victim;
+  }
+  hit->last_use = ++st->graph_clock;
+  FMM_CUDA_TRY(cudaGraphLaunch(hit->exec, (cudaStream_t)stream));
+  return 0;
+}
+
+/* ======================================================================== batches */
+
+/* Captures n transforms into one graph: a fork from the capturing stream into nbranch
+ * streams, transform i enqueued on branch[i] (all transforms of one plan must share a branch:
+ * they share its workspace), and a join.  One cudaGraphLaunch then runs the whole batch, the
+ * branches overlapping on the device. */
+extern "C" int fmmk_batch_capture(fmmk_state *const *sts, const void *const *ins, void *const *outs,
+                                  const int *inverse, const int *branch, int n, int nbranch,
+                                  void **exec_out, char *err, size_t errlen) {
+  cudaStream_t root;
+  FMM_CUDA_TRY(cudaStreamCreateWithFlags(&root, cudaStreamNonBlocking));
+  cudaStream_t *br = (cudaStream_t *)calloc((size_t)nbranch, sizeof(cudaStream_t));
+  cudaEvent_t *ev = (cudaEvent_t *)calloc((size_t)nbranch + 1, sizeof(cudaEvent_t));
+  if (!br || !ev) return 2;
+  int rc = 0;
+  for (int i = 0; i < nbranch && !rc; ++i)
+    if (cudaStreamCreateWithFlags(&br[i], cudaStreamNonBlocking) != cudaSuccess) rc = 3;
+  for (int i = 0; i <= nbranch && !rc; ++i)
+    if (cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess) rc = 3;
+  cudaGraph_t graph = NULL;
+  if (!rc && cudaStreamBeginCapture(root, cudaStreamCaptureModeThreadLocal) != cudaSuccess) rc = 3;
+  if (!rc) {
+    cudaEventRecord(ev[nbranch], root);
+    for (int b = 0; b < nbranch; ++b) cudaStreamWaitEvent(br[b], ev[nbranch], 0);
+    for (int i = 0; i < n && !rc; ++i)
+      rc = fmmk_execute(sts[i], ins[i], outs[i], br[branch[i]], inverse ? inverse[i] : 0, err, errlen);
+    for (int b = 0; b < nbranch; ++b) {
+      cudaEventRecord(ev[b], br[b]);
+      cudaStreamWaitEvent(root, ev[b], 0);
+    }
+    cudaError_t e = cudaStreamEndCapture(root, &graph);
+    if (!rc && e != cudaSuccess) {
+      snprintf(err, errlen, "batch capture: %s", cudaGetErrorString(e));
+      rc = 3;
+    }
+  }
+  if (!rc) {
+    cudaGraphExec_t exec = NULL;
+    cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) {
+      snprintf(err, errlen, "batch instantiate: %s", cudaGetErrorString(e));
+      rc = 3;
+    } else {
+      *exec_out = (void *)exec;
+    }
+  }
+  if (graph) cudaGraphDestroy(graph);
+  for (int i = 0; i <= nbranch; ++i)
+    if (ev[i]) cudaEventDestroy(ev[i]);
+  for (int i = 0; i < nbranch; ++i)
+    if (br[i]) cudaStreamDestroy(br[i]);
+  cudaStreamDestroy(root);
+  free(br), free(ev);
+  return rc;
+}
+
+extern "C" int fmmk_batch_launch(void *exec, void *stream) {
+  return cudaGraphLaunch((cudaGraphExec_t)exec, (cudaStream_t)stream) == cudaSuccess ? 0 : 3;
+}
+extern "C" void fmmk_batch_free(void *exec) {
+  if (exec) cudaGraphExecDestroy((cudaGraphExec_t)exec);
 }

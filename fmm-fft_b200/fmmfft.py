@@ -26,7 +26,11 @@ EXPORTS = ["getwlen2", "getvlen", "mfti", "mft", "fmmfft_last_error", "fmmfft_la
            "fmmfft_plan_create", "fmmfft_plan_destroy", "fmmfft_plan_device_bytes",
            "fmmfft_execute", "fmmfft_execute_inverse", "fmmfft_execute_host",
            "fmmfft_debug_fetch", "fmmfft_profile_start", "fmmfft_profile_stop",
-           "fmmfft_stage_name", "fmmfft_execute_noalloc", "fmmfft_plan_check"]
+           "fmmfft_stage_name", "fmmfft_execute_noalloc", "fmmfft_plan_check",
+           "fmmfft_execute_graph", "fmmfft_batch_create", "fmmfft_batch_launch",
+           "fmmfft_batch_destroy", "fmmfft_server_create", "fmmfft_server_destroy",
+           "fmmfft_server_submit", "fmmfft_server_query", "fmmfft_server_wait",
+           "fmmfft_server_stats"]
 
 
 class FmmFftError(RuntimeError):
@@ -71,6 +75,26 @@ def load(path=LIB_PATH):
     lib.fmmfft_execute_noalloc.restype = _I
     lib.fmmfft_plan_check.argtypes = [_VP]
     lib.fmmfft_plan_check.restype = _I
+    lib.fmmfft_execute_graph.argtypes = [_VP, _VP, _VP, _VP]
+    lib.fmmfft_execute_graph.restype = _I
+    lib.fmmfft_batch_create.argtypes = [ctypes.POINTER(_VP), _VP, _VP, _VP, _I, _I]
+    lib.fmmfft_batch_create.restype = _I
+    lib.fmmfft_batch_launch.argtypes = [_VP, _VP]
+    lib.fmmfft_batch_launch.restype = _I
+    lib.fmmfft_batch_destroy.argtypes = [_VP]
+    lib.fmmfft_server_create.argtypes = [ctypes.POINTER(_VP), ctypes.c_size_t, _I]
+    lib.fmmfft_server_create.restype = _I
+    lib.fmmfft_server_destroy.argtypes = [_VP]
+    lib.fmmfft_server_submit.argtypes = [_VP, _L, _L, _L, _L, _I, _VP, _VP,
+                                         ctypes.POINTER(ctypes.c_uint64)]
+    lib.fmmfft_server_submit.restype = _I
+    lib.fmmfft_server_query.argtypes = [_VP, ctypes.c_uint64]
+    lib.fmmfft_server_query.restype = _I
+    lib.fmmfft_server_wait.argtypes = [_VP, ctypes.c_uint64, _L]
+    lib.fmmfft_server_wait.restype = _I
+    lib.fmmfft_server_stats.argtypes = [_VP, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(_I),
+                                        ctypes.POINTER(_I)]
+    lib.fmmfft_server_stats.restype = _I
     _lib = lib
     return lib
 
@@ -159,6 +183,10 @@ class Plan:
         _check(load().fmmfft_execute_host(self._h, x.ctypes.data, y.ctypes.data, None))
         return y
 
+    def execute_graph_ptr(self, d_in, d_out, stream=0):
+        """Forward transform through the plan's cached CUDA graph for (d_in, d_out)."""
+        _check(load().fmmfft_execute_graph(self._h, d_in, d_out, stream or None))
+
     def execute_host_ptr(self, h_in, h_out, stream=0):
         """Host-memory transform (pointers, e.g. pinned buffers): H2D copy, execute, D2H copy,
         synchronise, all on `stream`."""
@@ -215,6 +243,80 @@ class Plan:
     def close(self):
         if getattr(self, "_h", None):
             load().fmmfft_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Transforms plans[i]: d_in[i] -> d_out[i] (device pointers) as one CUDA graph with
+    `nbranch` parallel branches; launch() runs them all."""
+
+    def __init__(self, plans, d_in, d_out, nbranch=8):
+        n = len(plans)
+        self._plans = list(plans)  # keep the plans alive
+        ph = (_VP * n)(*[p._h for p in plans])
+        ins = (_VP * n)(*d_in)
+        outs = (_VP * n)(*d_out)
+        h = _VP()
+        _check(load().fmmfft_batch_create(ctypes.byref(h), ph, ins, outs, n, int(nbranch)))
+        self._h = h
+
+    def launch(self, stream=0):
+        _check(load().fmmfft_batch_launch(self._h, stream or None))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().fmmfft_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Request server (fmmfft_server_*): submit() admits a transform onto one of `nstreams`
+    streams under an HBM budget for resident plans; returns a ticket, or raises FmmFftError
+    with status ERR_BUSY (7) when the request cannot be admitted now."""
+
+    def __init__(self, hbm_budget_bytes, nstreams=8):
+        h = _VP()
+        _check(load().fmmfft_server_create(ctypes.byref(h), int(hbm_budget_bytes), int(nstreams)))
+        self._h = h
+
+    def submit(self, N, P, terms, b, precision, d_in, d_out):
+        t = ctypes.c_uint64()
+        rc = load().fmmfft_server_submit(self._h, int(N), int(P), int(terms), int(b),
+                                         PRECISIONS[precision], d_in, d_out, ctypes.byref(t))
+        if rc:
+            raise FmmFftError(rc, "submit refused" if rc == 7 else "submit failed")
+        return t.value
+
+    def done(self, ticket):
+        rc = load().fmmfft_server_query(self._h, ticket)
+        if rc not in (0, 7):
+            raise FmmFftError(rc, "query failed")
+        return rc == 0
+
+    def wait(self, ticket, timeout_ms=60000):
+        _check(load().fmmfft_server_wait(self._h, ticket, int(timeout_ms)))
+
+    def stats(self):
+        used, plans, streams = ctypes.c_size_t(), _I(), _I()
+        _check(load().fmmfft_server_stats(self._h, ctypes.byref(used), ctypes.byref(plans),
+                                          ctypes.byref(streams)))
+        return {"hbm_used": used.value, "plans": plans.value, "streams": streams.value}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().fmmfft_server_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -119,6 +119,44 @@ int fmmfft_debug_fetch(fmmfft_plan plan, double *u, double *z, double *phi, doub
  * FMMFFT_OK otherwise.  Clears the recorded status. */
 int fmmfft_plan_check(fmmfft_plan plan);
 
+/* Same transform as fmmfft_execute through a CUDA graph: the first call for a given
+ * (d_in, d_out) captures the plan's launch sequence and instantiates it (make that call outside
+ * any stream capture); later calls are a single graph launch on `stream`.  Up to 8 buffer pairs
+ * per plan stay cached. */
+int fmmfft_execute_graph(fmmfft_plan plan, const void *d_in, void *d_out, void *stream);
+
+/* ------------------------------------------------------------------ batches */
+/* Many transforms, of uneven sizes, as one graph: transform i runs plans[i] from d_in[i] to
+ * d_out[i] (device buffers).  The transforms are spread over `nbranch` parallel branches of the
+ * graph; all transforms that use the same plan share its workspace, so they are placed in the
+ * same branch and run one after another there.  fmmfft_batch_launch runs the whole batch with
+ * one graph launch on `stream`.  The plans and buffers must outlive the batch. */
+typedef struct fmmfft_batch_s *fmmfft_batch;
+int fmmfft_batch_create(fmmfft_batch *out, const fmmfft_plan *plans, const void *const *d_in,
+                        void *const *d_out, int n, int nbranch);
+int fmmfft_batch_launch(fmmfft_batch batch, void *stream);
+int fmmfft_batch_destroy(fmmfft_batch batch);
+
+/* ------------------------------------------------------------------ serving */
+/* A request server: transforms of mixed sizes and precisions submitted one at a time are
+ * admitted onto `nstreams` CUDA streams, so that requests arriving while others run overlap on
+ * the device.  Plans stay resident per (N, P, terms, b, precision) and per stream; the device
+ * memory they hold is capped by hbm_budget_bytes: a request that needs a new plan evicts idle
+ * plans least-recently-used, and is refused with FMMFFT_ERR_BUSY (retry later) when the plans
+ * in use leave no room.  d_in / d_out are caller-owned device buffers that must stay valid
+ * until the request completes.  Results do not depend on what else is in flight. */
+typedef struct fmmfft_server_s *fmmfft_server;
+typedef uint64_t fmmfft_ticket;
+int fmmfft_server_create(fmmfft_server *out, size_t hbm_budget_bytes, int nstreams);
+int fmmfft_server_destroy(fmmfft_server server); /* waits for every request in flight */
+int fmmfft_server_submit(fmmfft_server server, long N, long P, long terms, long b, int precision,
+                         const void *d_in, void *d_out, fmmfft_ticket *ticket);
+/* FMMFFT_OK when the request is complete, FMMFFT_ERR_BUSY while it runs. */
+int fmmfft_server_query(fmmfft_server server, fmmfft_ticket ticket);
+/* Waits up to timeout_ms; FMMFFT_OK or FMMFFT_ERR_TIMEOUT. */
+int fmmfft_server_wait(fmmfft_server server, fmmfft_ticket ticket, long timeout_ms);
+int fmmfft_server_stats(fmmfft_server server, size_t *hbm_used, int *plans, int *streams);
+
 /* ------------------------------------------------------------------ stage timing */
 /* Records CUDA events around every stage of the next `max_executes` executes of this plan (on
  * the stream each execute runs on).  No counterpart in the reference, which only times the

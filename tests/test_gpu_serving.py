@@ -1,0 +1,132 @@
+"""Graphs, batches and the request server (north-star batching and serving) on the GPU.
+
+Each transform is checked against the plain per-call execute of the same plan (bitwise: the
+graph replays the same kernels) and against an FP64 FFT (rel-L2 <= 1e-6 for FP32 plans)."""
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-6
+
+
+@pytest.fixture(scope="module")
+def fm():
+    import fmmfft
+    fmmfft.load()
+    return fmmfft
+
+
+def _dev(x, dt):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x)).to(dt).cuda()
+
+
+def test_graph_execute_equals_plain_execute(fm):
+    import torch
+    for N, P, T, b, prec in [(1 << 16, 16, 16, 32, "f32"), (1 << 18, 64, 24, 32, "f32_tc"),
+                             (1 << 14, 4, 16, 256, "f64")]:
+        x = ol.seeded_input(N, N)
+        dt = torch.complex128 if prec == "f64" else torch.complex64
+        d = _dev(x, dt)
+        y1, y2 = torch.empty_like(d), torch.empty_like(d)
+        plan = fm.Plan(N, P, T, b, prec)
+        s = torch.cuda.current_stream().cuda_stream
+        plan.execute_ptr(d.data_ptr(), y1.data_ptr(), s)
+        for _ in range(3):  # first call captures, the rest replay
+            y2.zero_()
+            plan.execute_graph_ptr(d.data_ptr(), y2.data_ptr(), s)
+        torch.cuda.synchronize()
+        assert torch.equal(y1, y2)
+
+
+def _uneven_jobs(n, seed):
+    """Sizes as in the uneven-batch workload: N log-uniform over powers of two 2^12..2^22, P from
+    {8, 16, 32, 64} with M >= 256, p = 16 (scaled down in count for a test)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    jobs = []
+    while len(jobs) < n:
+        lg = int(rng.integers(12, 19))
+        P = int(rng.choice([8, 16, 32, 64]))
+        N = 1 << lg
+        if N // P < 256:
+            continue
+        b = 32 if N // P >= 128 else 8
+        jobs.append((N, P, 16, b))
+    return jobs
+
+
+def test_uneven_batch_one_graph(fm):
+    import torch
+    jobs = _uneven_jobs(40, 3)
+    plans = {}
+    for N, P, T, b in jobs:
+        plans.setdefault((N, P, T, b), fm.Plan(N, P, T, b, "f32"))
+    xs = [ol.seeded_input(N, 100 + i) for i, (N, P, T, b) in enumerate(jobs)]
+    din = [_dev(x, torch.complex64) for x in xs]
+    dout = [torch.empty_like(d) for d in din]
+    batch = fm.Batch([plans[j] for j in jobs], [d.data_ptr() for d in din],
+                     [d.data_ptr() for d in dout], nbranch=6)
+    batch.launch(torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    s = torch.cuda.current_stream().cuda_stream
+    for i, (job, x) in enumerate(zip(jobs, xs)):
+        alone = torch.empty_like(din[i])
+        plans[job].execute_ptr(din[i].data_ptr(), alone.data_ptr(), s)
+        torch.cuda.synchronize()
+        assert torch.equal(alone, dout[i]), job
+        assert ol.rel_l2(dout[i].cpu().numpy(), np.fft.fft(x)) < TOL, job
+    batch.close()
+
+
+def test_server_mix_equals_alone(fm):
+    """Requests submitted back to back overlap on 4 streams; each result must be bitwise the
+    result of the same request run alone."""
+    import torch
+    jobs = _uneven_jobs(24, 5) + [(1 << 20, 64, 20, 32), (1 << 16, 8, 8, 32)]
+    precs = ["f32_tc" if i % 3 == 0 else "f32" for i in range(len(jobs))]
+    xs = [ol.seeded_input(N, 900 + i) for i, (N, P, T, b) in enumerate(jobs)]
+    din = [_dev(x, torch.complex64) for x in xs]
+    mixed = [torch.empty_like(d) for d in din]
+    srv = fm.Server(8 << 30, nstreams=4)
+    tickets = [srv.submit(N, P, T, b, pr, din[i].data_ptr(), mixed[i].data_ptr())
+               for i, ((N, P, T, b), pr) in enumerate(zip(jobs, precs))]
+    for t in tickets:
+        srv.wait(t)
+    st = srv.stats()
+    assert st["plans"] >= 1 and st["hbm_used"] <= 8 << 30
+    srv.close()
+    s = torch.cuda.current_stream().cuda_stream
+    for i, ((N, P, T, b), pr) in enumerate(zip(jobs, precs)):
+        plan = fm.Plan(N, P, T, b, pr)
+        alone = torch.empty_like(din[i])
+        plan.execute_ptr(din[i].data_ptr(), alone.data_ptr(), s)
+        torch.cuda.synchronize()
+        assert torch.equal(alone, mixed[i]), (N, P, T, b, pr)
+        assert ol.rel_l2(mixed[i].cpu().numpy(), np.fft.fft(xs[i])) < TOL
+
+
+def test_server_admission_by_budget(fm):
+    import torch
+    N, P, T, b = 1 << 20, 64, 16, 32
+    probe = fm.Plan(N, P, T, b, "f32")
+    one = probe.device_bytes
+    probe.close()
+    x = _dev(ol.seeded_input(N, 1), torch.complex64)
+    y = torch.empty_like(x)
+    srv = fm.Server(int(one * 1.5), nstreams=2)  # room for one resident plan of this size
+    t = srv.submit(N, P, T, b, "f32", x.data_ptr(), y.data_ptr())
+    srv.wait(t)
+    # a different shape needs a new plan: the idle one is evicted to make room
+    x2 = _dev(ol.seeded_input(N // 2, 2), torch.complex64)
+    y2 = torch.empty_like(x2)
+    t2 = srv.submit(N // 2, P, T, b, "f32", x2.data_ptr(), y2.data_ptr())
+    srv.wait(t2)
+    assert srv.stats()["plans"] == 1
+    assert ol.rel_l2(y2.cpu().numpy(), np.fft.fft(x2.cpu().numpy())) < TOL
+    # a plan larger than the whole budget is refused, not run
+    with pytest.raises(fm.FmmFftError) as ei:
+        srv.submit(4 * N, P, T, b, "f32", x.data_ptr(), y.data_ptr())
+    assert ei.value.status == 7
+    srv.close()
