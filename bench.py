@@ -42,6 +42,12 @@ def parse():
     ap.add_argument("--precision", default=None, help="f32 | f32_tc | f64 (default: fastest)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--workload", choices=["single", "uneven-batch", "serving"], default="single",
+                    help="single: the headline transform (default); uneven-batch: 512 transforms "
+                         "of mixed N and P as one graph; serving: Poisson arrivals through the "
+                         "request server")
+    ap.add_argument("--rate", type=float, default=2000.0, help="serving: arrivals per second")
+    ap.add_argument("--duration", type=float, default=2.0, help="serving: seconds of arrivals")
     return ap.parse_args()
 
 
@@ -192,8 +198,217 @@ def reference_cpu(N, P, T, b, steps, warmup, budget_s=150.0):
                 seconds_per_transform=med, runs=len(times))
 
 
+# ------------------------------------------------------------------------ uneven batch
+def uneven_jobs(n, seed, lo=12, hi=22, terms=16):
+    """N log-uniform over powers of two 2^lo..2^hi, P from {8,16,32,64} subject to M >= 256."""
+    import numpy as np
+    rng = np.random.Generator(np.random.PCG64(seed))
+    jobs = []
+    while len(jobs) < n:
+        N = 1 << int(rng.integers(lo, hi + 1))
+        P = int(rng.choice([8, 16, 32, 64]))
+        if N // P < 256:
+            continue
+        jobs.append((N, P, terms, 32))
+    return jobs
+
+
+def run_uneven_batch(a):
+    import numpy as np
+    import torch
+    import fmmfft
+    torch.cuda.set_device(0)
+    jobs = uneven_jobs(512, 4)
+    prec = a.precision or "f32"
+    copies = 4  # plan instances per shape, so that equal shapes can run in parallel branches
+    plans, inst_of = {}, []
+    for i, job in enumerate(jobs):
+        lst = plans.setdefault(job, [])
+        k = sum(1 for j in jobs[:i] if j == job) % copies
+        while len(lst) <= k:
+            lst.append(fmmfft.Plan(*job, prec))
+        inst_of.append(lst[k])
+    dt = torch.complex64 if prec != "f64" else torch.complex128
+    xs = [torch.randn(N, dtype=dt, device="cuda") for (N, P, T, b) in jobs]
+    ys = [torch.empty_like(x) for x in xs]
+    total = sum(N for (N, P, T, b) in jobs)
+    stream = torch.cuda.current_stream()
+    t0 = time.time()
+    batch = fmmfft.Batch(inst_of, [x.data_ptr() for x in xs], [y.data_ptr() for y in ys], nbranch=16)
+    build_s = time.time() - t0
+    for _ in range(max(3, a.warmup)):
+        batch.launch(stream.cuda_stream)
+    torch.cuda.synchronize()
+    K = a.steps
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(K):
+        batch.launch(stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / K
+    # plain comparator: the same transforms one after another, no graph, one stream
+    for i, job in enumerate(jobs):
+        plans[job][0].execute_ptr(xs[i].data_ptr(), ys[i].data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(max(1, K // 2)):
+        for i, job in enumerate(jobs):
+            plans[job][0].execute_ptr(xs[i].data_ptr(), ys[i].data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_plain = e0.elapsed_time(e1) / max(1, K // 2)
+    worst = 0.0
+    for i in range(0, len(jobs), 64):  # accuracy of a sample against FP64
+        x = xs[i].cpu().numpy().astype(np.complex128)
+        inst_of[i].execute_ptr(xs[i].data_ptr(), ys[i].data_ptr(), stream.cuda_stream)
+        torch.cuda.synchronize()
+        y = ys[i].cpu().numpy().astype(np.complex128)
+        ref = np.fft.fft(x)
+        worst = max(worst, float(np.linalg.norm(y - ref) / np.linalg.norm(ref)))
+    line = {"metric": "Msamples/s, uneven batch of 512 transforms as one graph", "value": total / (ms / 1e3) / 1e6,
+            "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": max(3, a.warmup), "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"f32": "fp32", "f32_tc": "fp32 (3xTF32 tcgen05)", "f64": "fp64"}[prec],
+            "data": "synthetic", "impl": "ours",
+            "config": {"workload": "uneven batch", "transforms": len(jobs), "N": "2^12..2^22 log-uniform",
+                       "P": "{8,16,32,64}, M >= 256", "terms": 16, "b": 32, "graph_branches": 16,
+                       "plan_copies_per_shape": copies, "distinct_shapes": len(plans),
+                       "samples_per_step": total, "graph_build_s": build_s},
+            "plain_per_transform": {"value": total / (ms_plain / 1e3) / 1e6, "unit": UNIT,
+                                    "ms_per_step": ms_plain, "how": "fmmfft_execute per transform, one stream"},
+            "accuracy": {"worst_rel_l2_vs_fp64_sampled": worst}}
+    batch.close()
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------------ serving
+def serving_requests(rate, duration, seed):
+    """Poisson arrivals; N log-uniform over powers of two 2^10..2^24; two accuracy classes
+    (rel-L2 1e-4 -> p = 8 on FP32 CUDA cores, 1e-6 -> p = 20 with the tensor-core tree)."""
+    import numpy as np
+    rng = np.random.Generator(np.random.PCG64(seed))
+    t, reqs = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > duration:
+            break
+        N = 1 << int(rng.integers(10, 25))
+        cls = int(rng.integers(0, 2))
+        P = max(2, min(64, N // 512))
+        terms, prec = (8, "f32") if cls == 0 else (20, "f32_tc")
+        reqs.append((t, N, P, terms, 32, prec))
+    return reqs
+
+
+def run_serving(a):
+    import numpy as np
+    import torch
+    import fmmfft
+    torch.cuda.set_device(0)
+    reqs = serving_requests(a.rate, a.duration, 7)
+    nbuf = 4
+    bufs = {}
+    for (_, N, P, T, b, prec) in reqs:
+        if N not in bufs:
+            bufs[N] = [(torch.randn(N, dtype=torch.complex64, device="cuda"),
+                        torch.empty(N, dtype=torch.complex64, device="cuda")) for _ in range(nbuf)]
+    total = sum(r[1] for r in reqs)
+    budget = 120 << 30
+    srv = fmmfft.Server(budget, nstreams=8)
+    # warm: make every shape's plans and graphs resident (plan build is not a request cost)
+    seen = {}
+    for (_, N, P, T, b, prec) in reqs:
+        key = (N, P, T, b, prec)
+        if key in seen:
+            continue
+        seen[key] = 1
+        for k in range(nbuf):
+            x, y = bufs[N][k]
+            srv.wait(srv.submit(N, P, T, b, prec, x.data_ptr(), y.data_ptr()))
+    torch.cuda.synchronize()
+
+    def drive(submit, poll):
+        lat, pend, counter = [], [], {}
+        t0 = time.perf_counter()
+        i = 0
+        while i < len(reqs) or pend:
+            now = time.perf_counter() - t0
+            while i < len(reqs) and reqs[i][0] <= now:
+                arr, N, P, T, b, prec = reqs[i]
+                k = counter.get(N, 0)
+                counter[N] = k + 1
+                x, y = bufs[N][k % nbuf]
+                h = submit(N, P, T, b, prec, x, y)
+                if h is None:  # refused: retry on the next pass
+                    break
+                pend.append((h, arr))
+                i += 1
+            now = time.perf_counter() - t0
+            keep = []
+            for h, arr in pend:
+                if poll(h):
+                    lat.append(now - arr)
+                else:
+                    keep.append((h, arr))
+            pend = keep
+        return time.perf_counter() - t0, lat
+
+    def srv_submit(N, P, T, b, prec, x, y):
+        try:
+            return srv.submit(N, P, T, b, prec, x.data_ptr(), y.data_ptr())
+        except fmmfft.FmmFftError as e:
+            if e.status == 7:
+                return None
+            raise
+
+    span_s, lat_s = drive(srv_submit, srv.done)
+    st = srv.stats()
+    srv.close()
+
+    # plain per-request comparator: resident plans, one request at a time, no graphs
+    plans = {}
+    stream = torch.cuda.current_stream()
+    for (_, N, P, T, b, prec) in reqs:
+        if (N, P, T, b, prec) not in plans:
+            plans[(N, P, T, b, prec)] = fmmfft.Plan(N, P, T, b, prec)
+
+    def plain_submit(N, P, T, b, prec, x, y):
+        plans[(N, P, T, b, prec)].execute_ptr(x.data_ptr(), y.data_ptr(), stream.cuda_stream)
+        torch.cuda.synchronize()
+        return True
+
+    span_p, lat_p = drive(plain_submit, lambda h: True)
+
+    def pct(v, q):
+        v = sorted(v)
+        return v[min(len(v) - 1, int(q * len(v)))] * 1e3 if v else None
+
+    line = {"metric": "Msamples/s and p99 latency, served vs plain FMM-FFT (Poisson arrivals)",
+            "value": total / span_s / 1e6, "unit": UNIT, "n_gpus": 1, "steps": len(reqs),
+            "warmup": 1, "ms_per_step": span_s * 1e3 / max(1, len(reqs)), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32 / fp32 (3xTF32)",
+            "data": "synthetic", "impl": "ours",
+            "config": {"workload": "serving", "rate_per_s": a.rate, "duration_s": a.duration,
+                       "requests": len(reqs), "N": "2^10..2^24 log-uniform",
+                       "classes": {"1e-4": "p=8 fp32", "1e-6": "p=20 tensor-core tree"},
+                       "hbm_budget_bytes": budget, "streams": 8, "resident_plans": st["plans"],
+                       "resident_plan_bytes": st["hbm_used"]},
+            "latency_ms": {"p50": pct(lat_s, 0.5), "p99": pct(lat_s, 0.99)},
+            "plain_per_request": {"value": total / span_p / 1e6, "unit": UNIT,
+                                  "latency_ms": {"p50": pct(lat_p, 0.5), "p99": pct(lat_p, 0.99)},
+                                  "how": "resident plans, fmmfft_execute + synchronise per request"}}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     a = parse()
+    if a.workload == "uneven-batch":
+        return run_uneven_batch(a)
+    if a.workload == "serving":
+        return run_serving(a)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -226,7 +441,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
-    prec = a.precision or "f32"
+    prec = a.precision or "f32_tc"
     plan = fmmfft.Plan(N, P, T, b, prec)
     cdt = torch.complex128 if prec == "f64" else torch.complex64
     esz = 16 if prec == "f64" else 8
@@ -277,6 +492,26 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         tot = float(t.item())
     clocks = clk.summary()
+
+    # in-run comparator: the plain FP32 CUDA-core FMM-FFT on the same input, same timing rule
+    plain = {}
+    if prec != "f32":
+        pplan = fmmfft.Plan(N, P, T, b, "f32")
+        for _ in range(3):
+            pplan.execute_ptr(x.data_ptr(), y.data_ptr(), sp)
+        pms = []
+        for i in range(max(3, K // 2)):
+            flush.fill_(float(i))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            pplan.execute_ptr(x.data_ptr(), y.data_ptr(), sp)
+            e1.record(stream)
+            pms.append((e0, e1))
+        torch.cuda.synchronize()
+        pm = sum(e0.elapsed_time(e1) for e0, e1 in pms) / len(pms)
+        plain = {"value": N * world / (pm / 1e3) / 1e6, "unit": UNIT, "ms_per_step": pm,
+                 "how": "FMMFFT_F32 plan: every contraction on CUDA cores"}
+        pplan.close()
 
     # e2e through the C-ABI from pinned host memory
     hin = torch.from_numpy(xh).to(cdt).pin_memory()
@@ -339,6 +574,7 @@ def main():
                          "traffic": None, "peak_kind": peak_kind,
                          "alg_bytes_per_launch": d.get("alg_bytes_per_execute", 0) / d["launches_per_execute"]},
             "stages": stage_tab,
+            "plain_fp32_comparator": plain,
             "gpu_launches": launches_per_exec * K,
             "clocks": clocks,
         }
