@@ -118,6 +118,7 @@ template <typename R> struct Dev {
   int kp_s2m, np_s2m, kp_m2m, np_m2m, kp_m2l, np_m2l, kp_leaf, np_leaf;
   int ok_s2m, ok_m2m, ok_m2l, ok_leaf;
   long tc_min_rows; /* stages with fewer rows use the CUDA-core kernel */
+  int fft_threads;  /* threads per block of the register FFT pass (power of two, <= 512) */
 };
 
 /* Instantiated CUDA graphs of one plan's execute, keyed by (input, output, direction): the
@@ -742,6 +743,179 @@ __global__ void k_fft_pass(const typename cplx<R>::T *__restrict__ in,
   }
 }
 
+/* Register-resident Stockham pass: one thread per radix-8 butterfly column (L/8 threads per
+ * sequence, W sequences per block) keeps its 8 values in registers through every stage; the
+ * stages exchange through ONE shared buffer laid out per sequence, buf[w*LP + i + i/8] with
+ * LP = L + L/8 + 1, which keeps both thread orders below free of bank conflicts.  The first
+ * stage reads global memory directly and the last stage writes it directly.  Thread order:
+ * along the sequence (TIN) when the input is contiguous in i, across sequences otherwise, so
+ * that a warp's loads are coalesced either way; when the output wants the other order
+ * (TOUT != TIN) the result goes once through the shared buffer.  The 4-step twiddle of output
+ * i = t + r L/8 of sequence g factors as exp(-2 pi i g t / M) exp(-2 pi i g (L/8) r / M): one
+ * gather per thread and 8 W steps in shared memory.  Shared: W*LP + L + L/16 + 1 + 8 W
+ * elements; needs 16 <= L and W*L/8 <= 512; offsets within a row fit 32 bits (M <= 2^26). */
+template <typename R, bool TIN, bool TOUT>
+__global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1) k_fft_reg(const typename cplx<R>::T *__restrict__ in,
+                                                 typename cplx<R>::T *__restrict__ out,
+                                                 const typename cplx<R>::T *__restrict__ twM,
+                                                 FftPass fp) {
+  using C = typename cplx<R>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int L = fp.L, W = fp.W, q = L >> 3;
+  const int lq = __ffs(q) - 1, lW = __ffs(W) - 1;
+  const int LP = L + q + 1;
+  C *buf = reinterpret_cast<C *>(smem_raw);
+  C *twl = buf + W * LP;    /* exp(-2 pi i m / L) at m + m/16 */
+  C *twq = twl + L + L / 16 + 1; /* 4-step twiddle steps exp(-2 pi i g q r / M), [w][r] */
+  const int tid = threadIdx.x;
+  const unsigned Mmask = (unsigned)fp.M - 1;
+  const unsigned g0 = blockIdx.x * (unsigned)W;
+  for (int m = tid; m < L; m += blockDim.x) twl[m + (m >> 4)] = twM[(long)m * fp.tws];
+  if (fp.twiddle_post)
+    for (int m = tid; m < 8 * W; m += blockDim.x)
+      twq[m] = twM[((g0 + (m >> 3)) * (unsigned)q * (unsigned)(m & 7)) & Mmask];
+  int t, w;
+  if (TIN) t = tid & (q - 1), w = tid >> lq;
+  else w = tid & (W - 1), t = tid >> lW;
+  const unsigned istr = (unsigned)fp.istr, ostr = (unsigned)fp.ostr;
+  const long row = blockIdx.y;
+  C v[8];
+  {
+    const C *sp = in + row * fp.M + (g0 + w) * fp.iseq + t * istr;
+    const unsigned qs = (unsigned)q * istr;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) v[r] = sp[r * qs];
+  }
+  C *bw = buf + w * LP;
+  const int lg = __ffs(L) - 1;
+  int Ns, lNs;
+  if (lg % 3 == 0) { /* radix-8 first stage: outputs 8t + r */
+    dft8(v);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int i = 8 * t + r;
+      bw[i + (i >> 3)] = v[r];
+    }
+    Ns = 8, lNs = 3;
+  } else if (lg % 3 == 2) { /* radix 4: butterflies t (v0,2,4,6) and t+q (v1,3,5,7) */
+    dft4(v[0], v[2], v[4], v[6]);
+    dft4(v[1], v[3], v[5], v[7]);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int i0 = 4 * t + r, i1 = 4 * (t + q) + r;
+      bw[i0 + (i0 >> 3)] = v[2 * r];
+      bw[i1 + (i1 >> 3)] = v[2 * r + 1];
+    }
+    Ns = 4, lNs = 2;
+  } else { /* radix 2: butterflies t + m q, inputs v[m], v[m+4] */
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      const int i = 2 * (t + m * q);
+      bw[i + (i >> 3)] = cadd(v[m], v[m + 4]);
+      bw[i + 1 + ((i + 1) >> 3)] = csub(v[m], v[m + 4]);
+    }
+    Ns = 2, lNs = 1;
+  }
+  for (;;) {
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int i = t + r * q;
+      v[r] = bw[i + (i >> 3)];
+    }
+    const int k = t & (Ns - 1);
+    const int ts = k << (lg - 3 - lNs); /* k L / (8 Ns) */
+#pragma unroll
+    for (int r = 1; r < 8; ++r) {
+      const int m = r * ts;
+      v[r] = cmul(v[r], twl[m + (m >> 4)]);
+    }
+    dft8(v);
+    if (lNs + 3 == lg) break; /* v[r] = output t + r q */
+    __syncthreads();
+    const int o = ((t >> lNs) << (lNs + 3)) + k;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int i = o + (r << lNs);
+      bw[i + (i >> 3)] = v[r];
+    }
+    Ns <<= 3, lNs += 3;
+  }
+  C *dp = out + row * fp.M;
+  if (TOUT == TIN) {
+    const unsigned g = g0 + w;
+    C *op = dp + g * fp.oseq + t * ostr;
+    const unsigned qs = (unsigned)q * ostr;
+    C a;
+    if (fp.twiddle_post) a = twM[(g * (unsigned)t) & Mmask];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      C x = v[r];
+      if (fp.twiddle_post) x = cmul(x, cmul(a, twq[w * 8 + r]));
+      if (fp.conj_out) x.y = -x.y;
+      op[r * qs] = x;
+    }
+  } else {
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int i = t + r * q;
+      bw[i + (i >> 3)] = v[r];
+    }
+    __syncthreads();
+    int t2, w2;
+    if (TOUT) t2 = tid & (q - 1), w2 = tid >> lq;
+    else w2 = tid & (W - 1), t2 = tid >> lW;
+    const unsigned g = g0 + w2;
+    const C *b2 = buf + w2 * LP;
+    C *op = dp + g * fp.oseq + t2 * ostr;
+    const unsigned qs = (unsigned)q * ostr;
+    C a;
+    if (fp.twiddle_post) a = twM[(g * (unsigned)t2) & Mmask];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int i = t2 + r * q;
+      C x = b2[i + (i >> 3)];
+      if (fp.twiddle_post) x = cmul(x, cmul(a, twq[w2 * 8 + r]));
+      if (fp.conj_out) x.y = -x.y;
+      op[r * qs] = x;
+    }
+  }
+}
+
+/* Launch one FFT pass: the register kernel when the shape allows it, else the shared-memory
+ * pass.  per = sequences per row; W_old = sequences per block of the shared-memory pass. */
+template <typename R>
+static void launch_fft_pass(const typename cplx<R>::T *in, typename cplx<R>::T *out,
+                            const typename cplx<R>::T *twM, FftPass fp, long per, long rows,
+                            int W_old, int reg_threads, cudaStream_t st) {
+  using C = typename cplx<R>::T;
+  const int L = fp.L;
+  const bool tin = fp.istr == 1, tout = fp.ostr == 1;
+  if (L >= 16 && L <= 8 * reg_threads && !(tout && !tin)) {
+    int W = reg_threads / (L / 8);
+    if (W > 16) W = 16;
+    if (W > per) W = (int)per;
+    if (W < 1) W = 1;
+    if (tin || W >= 4) {
+      fp.W = W;
+      const int thr = W * (L / 8);
+      const size_t sm = sizeof(C) * ((size_t)W * (L + L / 8 + 1) + L + L / 16 + 1 + 8 * W);
+      dim3 g((unsigned)(per / W), (unsigned)rows);
+      if (tin && tout)
+        k_fft_reg<R, true, true><<<g, thr, sm, st>>>(in, out, twM, fp);
+      else if (tin)
+        k_fft_reg<R, true, false><<<g, thr, sm, st>>>(in, out, twM, fp);
+      else
+        k_fft_reg<R, false, false><<<g, thr, sm, st>>>(in, out, twM, fp);
+      return;
+    }
+  }
+  fp.W = W_old;
+  dim3 g((unsigned)(per / W_old), (unsigned)rows);
+  k_fft_pass<R><<<g, 256, sizeof(C) * (size_t)L * (2 * W_old + 1), st>>>(in, out, twM, fp);
+}
+
 /* ======================================================================== combine */
 
 /* For TMc points m and every section: w_0 = x_0[m], w_sc = c_sc (u_sc[m] - (i/M) Ssum_sc),
@@ -976,6 +1150,11 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   d->ok_leaf = fits(d->kp_leaf, d->np_leaf) && getenv("FMMFFT_TC_STAGES") != NULL;
   d->tc_min_rows = kTcMinRows;
   if (const char *ev = getenv("FMMFFT_TC_MIN_ROWS")) d->tc_min_rows = atol(ev);
+  d->fft_threads = 512;
+  if (const char *ev = getenv("FMMFFT_FFT_THREADS")) {
+    const int v = atoi(ev);
+    if (v >= 32 && v <= 512 && (v & (v - 1)) == 0) d->fft_threads = v;
+  }
   /* FMMFFT_TC_STAGES: bit mask of the stages routed to the tensor cores (1 S2M, 2 M2M, 4 M2L,
    * 8 leaf); default all */
   if (const char *ev = getenv("FMMFFT_TC_STAGES")) {
@@ -1307,12 +1486,18 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
     if (d->M2 == 1) {
       int W = (int)pow2_floor(SMEM / (long)(2 * sizeof(C) * M));
       if (W > P) W = (int)P;
-      FftPass fp{(int)M, 1, 1, M, M, 1, M, 1, 0, 1, inverse};
-      /* W rows per block: treat W consecutive rows as one "row" of W sequences */
-      fp.W = W, fp.per = W, fp.M = M * W, fp.iseq = M, fp.oseq = M;
-      dim3 g(1, (unsigned)(P / W));
-      size_t sm = sizeof(C) * (size_t)M * (2 * W + 1);
-      k_fft_pass<R><<<g, 256, sm, st>>>(d->z, y, d->twM, fp);
+      /* W rows of one sequence each: treat them as one "row" of W sequences */
+      FftPass fp{(int)M, W, W, M * W, M, 1, M, 1, 0, 1, inverse};
+      if (M >= 16 && M <= 8L * d->fft_threads) { /* register kernel: its own W, rows = P / W */
+        int Wr = d->fft_threads / (int)(M / 8);
+        if (Wr > 16) Wr = 16;
+        if (Wr > P) Wr = (int)P;
+        if (Wr < 1) Wr = 1;
+        fp.M = M * Wr;
+        launch_fft_pass<R>(d->z, y, d->twM, fp, Wr, P / Wr, W, d->fft_threads, st);
+      } else {
+        launch_fft_pass<R>(d->z, y, d->twM, fp, W, P / W, W, d->fft_threads, st);
+      }
       pf.launches[ST_FFT1]++;
     } else {
       const long M1 = d->M1, M2 = d->M2;
@@ -1321,8 +1506,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
       if (W1 > 16) W1 = 16;
       if (W1 > M1) W1 = (int)M1;
       FftPass f1{(int)M2, W1, (int)M1, M, 1, M1, 1, M1, 1, M / M2, 0};
-      dim3 g1((unsigned)(M1 / W1), (unsigned)P);
-      k_fft_pass<R><<<g1, 256, sizeof(C) * (size_t)M2 * (2 * W1 + 1), st>>>(d->z, d->tmp, d->twM, f1);
+      launch_fft_pass<R>(d->z, d->tmp, d->twM, f1, M1, P, W1, d->fft_threads, st);
       pf.launches[ST_FFT1]++;
       stage(ST_FFT2);
       /* pass 2: for each k2, DFT over m1 (contiguous), store y[k2 + M2*k1] */
@@ -1330,8 +1514,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
       if (W2 > 16) W2 = 16;
       if (W2 > M2) W2 = (int)M2;
       FftPass f2{(int)M1, W2, (int)M2, M, M1, 1, 1, M2, 0, M / M1, inverse};
-      dim3 g2((unsigned)(M2 / W2), (unsigned)P);
-      k_fft_pass<R><<<g2, 256, sizeof(C) * (size_t)M1 * (2 * W2 + 1), st>>>(d->tmp, y, d->twM, f2);
+      launch_fft_pass<R>(d->tmp, y, d->twM, f2, M2, P, W2, d->fft_threads, st);
       pf.launches[ST_FFT2]++;
     }
   }
@@ -1371,6 +1554,12 @@ static int set_smem_limits(void) {
   int lim = maxopt > 0 ? maxopt : 48 * 1024;
   cudaFuncSetAttribute(k_fft_pass<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_fft_pass<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<float, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<float, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<float, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_combine<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_combine<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_sections<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
@@ -1687,6 +1876,7 @@ extern "C" int fmmk_execute_noalloc(const fmm_ops64 *o, int reuse_ops, const voi
   memset((void *)&d, 0, sizeof(d));
   d.M = o->M, d.P = o->P, d.T = o->T, d.b = o->b, d.s = o->s, d.n = o->n;
   d.N = o->M * o->P, d.S1 = o->P - 1, d.precision = 1;
+  d.fft_threads = 512;
   d.tileM = d.P >= 2048 ? 1 : 2048 / d.P;
   if (d.tileM > d.M) d.tileM = d.M;
   d.ntile = d.M / d.tileM;
