@@ -409,9 +409,9 @@ def main():
         return run_uneven_batch(a)
     if a.workload == "serving":
         return run_serving(a)
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import replicas
+    info = replicas.rank_info()
+    world, rank, local = info.world, info.rank, info.local
     N, P, T, b = WORKLOAD["N"], WORKLOAD["P"], WORKLOAD["terms"], WORKLOAD["b"]
     cfg = dict(WORKLOAD)
 
@@ -435,17 +435,12 @@ def main():
     import fmmfft
 
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    dist = replicas.init_group(info, "nccl", device=torch.device("cuda", local))
     prec = a.precision or "f32_tc"
     plan = fmmfft.Plan(N, P, T, b, prec)
     cdt = torch.complex128 if prec == "f64" else torch.complex64
     esz = 16 if prec == "f64" else 8
-    xh = seeded(N, rank, np.complex128)
+    xh = seeded(N, replicas.replica_seed(0, rank), np.complex128)
     x = torch.from_numpy(xh).to(cdt).cuda()
     y = torch.empty_like(x)
     stream = torch.cuda.current_stream()
@@ -471,8 +466,7 @@ def main():
     ev_s = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     ev_e = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     plan.profile_start(K)
-    if dist:
-        dist.barrier()
+    replicas.barrier(dist)
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         for i in range(K):
@@ -481,16 +475,11 @@ def main():
             plan.execute_ptr(x.data_ptr(), y.data_ptr(), sp)
             ev_e[i].record(stream)
         torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    replicas.barrier(dist)
     torch.cuda.synchronize()
     nexec, stages = plan.profile_stop()
     per = [s.elapsed_time(e) for s, e in zip(ev_s, ev_e)]
-    tot = sum(per)
-    if dist:
-        t = torch.tensor([tot], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot = float(t.item())
+    tot = replicas.max_over_ranks(sum(per), dist, "cuda")
     clocks = clk.summary()
 
     # in-run comparator: the plain FP32 CUDA-core FMM-FFT on the same input, same timing rule
@@ -527,15 +516,11 @@ def main():
         s1.record(stream)
         s1.synchronize()
         e2e_ms.append(s0.elapsed_time(s1))
-    e2e_tot = sum(e2e_ms)
-    if dist:
-        t = torch.tensor([e2e_tot], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_tot = float(t.item())
+    e2e_tot = replicas.max_over_ranks(sum(e2e_ms), dist, "cuda")
 
     if rank == 0:
         ms_step = tot / K
-        value = N * K * world / (tot / 1e3) / 1e6
+        value = replicas.whole_job_rate(N, K, world, tot) / 1e6
         byts = stage_bytes(N, P, T, b, esz)
         hbm, peak_kind = peaks()
         stage_tab = {}
@@ -566,7 +551,7 @@ def main():
             "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
                            "min": lat[0], "max": lat[-1]},
             "accuracy": acc,
-            "e2e": {"value": N * E * world / (e2e_tot / 1e3) / 1e6, "unit": UNIT,
+            "e2e": {"value": replicas.whole_job_rate(N, E, world, e2e_tot) / 1e6, "unit": UNIT,
                     "h2d_bytes_per_step": N * esz, "d2h_bytes_per_step": N * esz,
                     "ms_per_step": e2e_tot / E, "path": "fmmfft_execute_host, pinned buffers"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
@@ -583,9 +568,7 @@ def main():
             line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         print(json.dumps(line))
     plan.close()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(dist)
     return 0
 
 
