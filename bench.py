@@ -502,6 +502,34 @@ def main():
                  "how": "FMMFFT_F32 plan: every contraction on CUDA cores"}
         pplan.close()
 
+    # a conventional FFT of the same N on the same GPU: the project's plain Stockham FFT (where
+    # the reference's FFTW comparator programs stand) and, as library context only, cuFFT
+    def timed(fn, reps):
+        for _ in range(3):
+            fn()
+        evs = []
+        for i in range(reps):
+            flush.fill_(float(i))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+        return sum(e0.elapsed_time(e1) for e0, e1 in evs) / reps
+
+    fft_cmp = {}
+    pfft = fmmfft.PlainFFT(N, "f64" if prec == "f64" else "f32")
+    ms_pf = timed(lambda: pfft.execute_ptr(x.data_ptr(), y.data_ptr(), sp), max(3, K // 2))
+    fft_cmp["plain_stockham"] = {"value": N * world / (ms_pf / 1e3) / 1e6, "unit": UNIT,
+                                 "ms_per_step": ms_pf,
+                                 "how": "fmmfft_fft_execute: project-written size-N FFT, "
+                                        "register Stockham passes"}
+    pfft.close()
+    ms_cu = timed(lambda: torch.fft.fft(x), max(3, K // 2))
+    fft_cmp["cufft_library"] = {"value": N * world / (ms_cu / 1e3) / 1e6, "unit": UNIT,
+                                "ms_per_step": ms_cu, "how": "torch.fft.fft (cuFFT), context only"}
+
     # e2e through the C-ABI from pinned host memory
     hin = torch.from_numpy(xh).to(cdt).pin_memory()
     hout = torch.empty_like(hin).pin_memory()
@@ -560,6 +588,7 @@ def main():
                          "alg_bytes_per_launch": d.get("alg_bytes_per_execute", 0) / d["launches_per_execute"]},
             "stages": stage_tab,
             "plain_fp32_comparator": plain,
+            "plain_fft_comparator": fft_cmp,
             "gpu_launches": launches_per_exec * K,
             "clocks": clocks,
         }

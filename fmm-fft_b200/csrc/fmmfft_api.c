@@ -332,3 +332,47 @@ void mft(long lq, void *qr, long dir, long p, long myid, long terms, long b, dou
   st = fmmfft_execute_host(pl, qr, qr, NULL);
   if (st == FMMFFT_OK) set_err(FMMFFT_OK, NULL);
 }
+
+/* ------------------------------------------------------------------ plain FFT comparator */
+
+struct fmmfft_fft_s {
+  fmmk_fft *dev;
+  size_t bytes;
+};
+
+int fmmfft_fft_create(fmmfft_fft *out, long N, int precision) {
+  if (!out) return set_err(FMMFFT_ERR_INVALID, "fft_create: NULL output pointer");
+  *out = NULL;
+  if (precision < FMMFFT_F64 || precision > FMMFFT_F32_TC)
+    return set_err(FMMFFT_ERR_INVALID, "fft_create: unknown precision");
+  struct fmmfft_fft_s *f = (struct fmmfft_fft_s *)calloc(1, sizeof *f);
+  if (!f) return set_err(FMMFFT_ERR_NOMEM, "fft_create: host allocation failed");
+  char err[256] = {0};
+  int rc = fmmk_fft_create(N, precision == FMMFFT_F64, &f->dev, &f->bytes, err, sizeof err);
+  if (rc) {
+    free(f);
+    return set_err(rc, err);
+  }
+  *out = f;
+  return set_err(FMMFFT_OK, NULL);
+}
+
+int fmmfft_fft_execute(fmmfft_fft f, const void *d_in, void *d_out, void *stream) {
+  if (!f || !d_in || !d_out) return set_err(FMMFFT_ERR_INVALID, "fft_execute: NULL argument");
+  char err[256] = {0};
+  int rc = fmmk_fft_execute(f->dev, d_in, d_out, stream, err, sizeof err);
+  return rc ? set_err(rc, err) : FMMFFT_OK;
+}
+
+int fmmfft_fft_device_bytes(fmmfft_fft f, size_t *bytes) {
+  if (!f || !bytes) return set_err(FMMFFT_ERR_INVALID, "fft_device_bytes: NULL argument");
+  *bytes = f->bytes;
+  return FMMFFT_OK;
+}
+
+int fmmfft_fft_destroy(fmmfft_fft f) {
+  if (!f) return FMMFFT_OK;
+  fmmk_fft_destroy(f->dev);
+  free(f);
+  return FMMFFT_OK;
+}

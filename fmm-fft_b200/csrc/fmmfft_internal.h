@@ -64,6 +64,12 @@ void fmmk_batch_free(void *exec);
 int fmmk_execute_noalloc(const fmm_ops64 *ops, int reuse_ops, const void *d_in, void *d_out,
                          void *stream, char *err, size_t errlen);
 
+typedef struct fmmk_fft fmmk_fft;
+int fmmk_fft_create(long N, int dbl, fmmk_fft **out, size_t *device_bytes, char *err, size_t errlen);
+int fmmk_fft_execute(fmmk_fft *f, const void *in, void *out, void *stream, char *err, size_t errlen);
+size_t fmmk_fft_bytes(const fmmk_fft *f);
+void fmmk_fft_destroy(fmmk_fft *f);
+
 #ifdef __cplusplus
 }
 #endif

@@ -694,7 +694,20 @@ struct FftPass {
   int twiddle_post;  /* apply exp(-2 pi i * w_global * k / M) */
   long tws;          /* twiddle stride into twM for length-L DFTs: M / L */
   int conj_out;
+  /* register pass only (k_fft_reg): row strides of input and output, and the post-twiddle
+   * exp(-2 pi i e / T) of exponent e = (g i twmul) & twmask, T = twmask + 1, read from twP as
+   * twP[e] (twbits = 0) or as twP[e & lo] * twP[lo + 1 + (e >> twbits)], lo = 2^twbits - 1 */
+  long irow, orow;
+  unsigned twmul, twmask;
+  int twbits;
 };
+
+/* FMM-FFT passes: rows of M (or of W rows of M), post-twiddle table exp(-2 pi i t / M). */
+static FftPass fmm_pass(FftPass fp) {
+  fp.irow = fp.orow = fp.M;
+  fp.twmul = 1, fp.twmask = (unsigned)(fp.M - 1), fp.twbits = 0;
+  return fp;
+}
 
 template <typename R>
 __global__ void k_fft_pass(const typename cplx<R>::T *__restrict__ in,
@@ -755,10 +768,10 @@ __global__ void k_fft_pass(const typename cplx<R>::T *__restrict__ in,
  * gather per thread and 8 W steps in shared memory.  Shared: W*LP + L + L/16 + 1 + 8 W
  * elements; needs 16 <= L and W*L/8 <= 512; offsets within a row fit 32 bits (M <= 2^26). */
 template <typename R, bool TIN, bool TOUT>
-__global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1) k_fft_reg(const typename cplx<R>::T *__restrict__ in,
-                                                 typename cplx<R>::T *__restrict__ out,
-                                                 const typename cplx<R>::T *__restrict__ twM,
-                                                 FftPass fp) {
+__global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
+    k_fft_reg(const typename cplx<R>::T *__restrict__ in, typename cplx<R>::T *__restrict__ out,
+              const typename cplx<R>::T *__restrict__ twD, const typename cplx<R>::T *__restrict__ twP,
+              FftPass fp) {
   using C = typename cplx<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int L = fp.L, W = fp.W, q = L >> 3;
@@ -768,12 +781,18 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1) k_fft_reg(const t
   C *twl = buf + W * LP;    /* exp(-2 pi i m / L) at m + m/16 */
   C *twq = twl + L + L / 16 + 1; /* 4-step twiddle steps exp(-2 pi i g q r / M), [w][r] */
   const int tid = threadIdx.x;
-  const unsigned Mmask = (unsigned)fp.M - 1;
   const unsigned g0 = blockIdx.x * (unsigned)W;
-  for (int m = tid; m < L; m += blockDim.x) twl[m + (m >> 4)] = twM[(long)m * fp.tws];
+  /* post-twiddle exp(-2 pi i e / T) for e = g * i */
+  auto post = [&](unsigned gi) -> C {
+    const unsigned e = (gi * fp.twmul) & fp.twmask;
+    if (fp.twbits == 0) return twP[e];
+    const unsigned lo = (1u << fp.twbits) - 1;
+    return cmul(twP[lo + 1 + (e >> fp.twbits)], twP[e & lo]);
+  };
+  for (int m = tid; m < L; m += blockDim.x) twl[m + (m >> 4)] = twD[(long)m * fp.tws];
   if (fp.twiddle_post)
     for (int m = tid; m < 8 * W; m += blockDim.x)
-      twq[m] = twM[((g0 + (m >> 3)) * (unsigned)q * (unsigned)(m & 7)) & Mmask];
+      twq[m] = post((g0 + (m >> 3)) * (unsigned)q * (unsigned)(m & 7));
   int t, w;
   if (TIN) t = tid & (q - 1), w = tid >> lq;
   else w = tid & (W - 1), t = tid >> lW;
@@ -781,7 +800,7 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1) k_fft_reg(const t
   const long row = blockIdx.y;
   C v[8];
   {
-    const C *sp = in + row * fp.M + (g0 + w) * fp.iseq + t * istr;
+    const C *sp = in + row * fp.irow + (g0 + w) * fp.iseq + t * istr;
     const unsigned qs = (unsigned)q * istr;
 #pragma unroll
     for (int r = 0; r < 8; ++r) v[r] = sp[r * qs];
@@ -841,13 +860,13 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1) k_fft_reg(const t
     }
     Ns <<= 3, lNs += 3;
   }
-  C *dp = out + row * fp.M;
+  C *dp = out + row * fp.orow;
   if (TOUT == TIN) {
     const unsigned g = g0 + w;
     C *op = dp + g * fp.oseq + t * ostr;
     const unsigned qs = (unsigned)q * ostr;
     C a;
-    if (fp.twiddle_post) a = twM[(g * (unsigned)t) & Mmask];
+    if (fp.twiddle_post) a = post(g * (unsigned)t);
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
       C x = v[r];
@@ -871,7 +890,7 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1) k_fft_reg(const t
     C *op = dp + g * fp.oseq + t2 * ostr;
     const unsigned qs = (unsigned)q * ostr;
     C a;
-    if (fp.twiddle_post) a = twM[(g * (unsigned)t2) & Mmask];
+    if (fp.twiddle_post) a = post(g * (unsigned)t2);
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
       const int i = t2 + r * q;
@@ -903,11 +922,11 @@ static void launch_fft_pass(const typename cplx<R>::T *in, typename cplx<R>::T *
       const size_t sm = sizeof(C) * ((size_t)W * (L + L / 8 + 1) + L + L / 16 + 1 + 8 * W);
       dim3 g((unsigned)(per / W), (unsigned)rows);
       if (tin && tout)
-        k_fft_reg<R, true, true><<<g, thr, sm, st>>>(in, out, twM, fp);
+        k_fft_reg<R, true, true><<<g, thr, sm, st>>>(in, out, twM, twM, fmm_pass(fp));
       else if (tin)
-        k_fft_reg<R, true, false><<<g, thr, sm, st>>>(in, out, twM, fp);
+        k_fft_reg<R, true, false><<<g, thr, sm, st>>>(in, out, twM, twM, fmm_pass(fp));
       else
-        k_fft_reg<R, false, false><<<g, thr, sm, st>>>(in, out, twM, fp);
+        k_fft_reg<R, false, false><<<g, thr, sm, st>>>(in, out, twM, twM, fmm_pass(fp));
       return;
     }
   }
@@ -2051,4 +2070,169 @@ extern "C" int fmmk_batch_launch(void *exec, void *stream) {
 }
 extern "C" void fmmk_batch_free(void *exec) {
   if (exec) cudaGraphExecDestroy((cudaGraphExec_t)exec);
+}
+
+/* ======================================================================== plain size-N FFT */
+
+/* A conventional FFT of the whole N-vector on the GPU, the same register Stockham passes as the
+ * FMM-FFT's size-M FFTs: one pass (N <= 4096), a 4-step of two passes (N <= 2^21) or a 4-step
+ * whose second factor is itself a 4-step (three passes, N <= 2^30).  It stands where the
+ * reference's plain FFTW comparators stand (src/fftw_serial.c:53-58, src/fftw_mpi.c:54-58):
+ * FMM-FFT against an ordinary FFT of the same length on the same machine.  Forward,
+ * unnormalised, out of place (in != out). */
+struct fmmk_fft {
+  long N;
+  int dbl;
+  int npass;
+  FftPass pass[3];
+  long per[3], rows[3];
+  int tin[3], tout[3];
+  int src[3], dst[3]; /* 0 in, 1 out, 2 tmp */
+  void *tmp, *twD, *twP;
+  size_t bytes;
+};
+
+static FftPass plain_pass(int L, long per, long irow, long iseq, long istr, long orow, long oseq,
+                          long ostr, int post, unsigned twmul, long N) {
+  FftPass f{};
+  f.L = L;
+  int W = 512 / (L / 8);
+  if (W > 16) W = 16;
+  if (W > per) W = (int)per;
+  if (W < 1) W = 1;
+  f.W = W, f.per = (int)per, f.M = N;
+  f.irow = irow, f.iseq = iseq, f.istr = istr;
+  f.orow = orow, f.oseq = oseq, f.ostr = ostr;
+  f.twiddle_post = post, f.tws = 4096 / L, f.conj_out = 0;
+  f.twmul = twmul, f.twmask = (unsigned)(N - 1), f.twbits = N > 4096 ? 12 : 0;
+  return f;
+}
+
+extern "C" int fmmk_fft_create(long N, int dbl, fmmk_fft **out, size_t *device_bytes, char *err,
+                               size_t errlen) {
+  int rc = fmmk_device_ok(err, errlen);
+  if (rc) return rc;
+  int lg = 0;
+  while (lg < 62 && (1L << lg) < N) ++lg;
+  if (N < 16 || (1L << lg) != N || lg > 30) {
+    snprintf(err, errlen, "plain FFT length %ld: a power of two in [16, 2^30] is required", N);
+    return 1;
+  }
+  set_smem_limits();
+  fmmk_fft *f = (fmmk_fft *)calloc(1, sizeof(fmmk_fft));
+  if (!f) return 2;
+  f->N = N, f->dbl = dbl;
+  if (lg <= 12) {
+    f->npass = 1;
+    f->pass[0] = plain_pass((int)N, 1, N, N, 1, N, N, 1, 0, 1, N);
+    f->per[0] = 1, f->rows[0] = 1, f->tin[0] = 1, f->tout[0] = 1, f->src[0] = 0, f->dst[0] = 1;
+  } else if (lg <= 21) {
+    int a = lg / 2 > 9 ? 9 : lg / 2;
+    if (a < lg - 12) a = lg - 12;
+    const long N2 = 1L << a, N1 = N / N2;
+    f->npass = 2;
+    /* for each n1: DFT over n2 (stride N1), times exp(-2 pi i n1 k2 / N) -> tmp[k2 N1 + n1] */
+    f->pass[0] = plain_pass((int)N2, N1, 0, 1, N1, 0, 1, N1, 1, 1, N);
+    f->per[0] = N1, f->rows[0] = 1, f->tin[0] = 0, f->tout[0] = 0, f->src[0] = 0, f->dst[0] = 2;
+    /* for each k2: DFT over n1 (contiguous) -> out[k2 + N2 k1] */
+    f->pass[1] = plain_pass((int)N1, N2, 0, N1, 1, 0, 1, N2, 0, 1, N);
+    f->per[1] = N2, f->rows[1] = 1, f->tin[1] = 1, f->tout[1] = 0, f->src[1] = 2, f->dst[1] = 1;
+  } else {
+    const int a = lg / 3 > 9 ? 9 : lg / 3;
+    const int rest = lg - a;
+    const int bb = rest / 2 > 9 ? 9 : rest / 2;
+    const long N2 = 1L << a, N1 = N / N2, B = 1L << bb, A = N1 / B;
+    f->npass = 3;
+    /* pass 1 as in the two-pass case, into out (used as scratch) */
+    f->pass[0] = plain_pass((int)N2, N1, 0, 1, N1, 0, 1, N1, 1, 1, N);
+    f->per[0] = N1, f->rows[0] = 1, f->tin[0] = 0, f->tout[0] = 0, f->src[0] = 0, f->dst[0] = 1;
+    /* row k2 (length N1, n1 = a + A b): for each a, DFT over b (stride A), times
+     * exp(-2 pi i a kb / N1) = exp(-2 pi i a kb N2 / N) -> tmp[k2 N1 + kb A + a] */
+    f->pass[1] = plain_pass((int)B, A, N1, 1, A, N1, 1, A, 1, (unsigned)N2, N);
+    f->per[1] = A, f->rows[1] = N2, f->tin[1] = 0, f->tout[1] = 0, f->src[1] = 1, f->dst[1] = 2;
+    /* for each (k2, kb): DFT over a (contiguous) -> out[k2 + N2 (kb + B ka)] */
+    f->pass[2] = plain_pass((int)A, B, N1, A, 1, 1, N2, N2 * B, 0, 1, N);
+    f->per[2] = B, f->rows[2] = N2, f->tin[2] = 1, f->tout[2] = 0, f->src[2] = 2, f->dst[2] = 1;
+  }
+  const size_t esz = dbl ? 16 : 8;
+  const long nlo = N > 4096 ? 4096 : N, nP = N > 4096 ? 4096 + N / 4096 : N;
+  const size_t bt = align_up(esz * (size_t)N), bD = align_up(esz * 4096), bP = align_up(esz * (size_t)nP);
+  char *base = NULL;
+  if (cudaMalloc((void **)&base, bt + bD + bP) != cudaSuccess) {
+    free(f);
+    snprintf(err, errlen, "cudaMalloc of %zu bytes failed", bt + bD + bP);
+    return 2;
+  }
+  f->tmp = base, f->twD = base + bt, f->twP = base + bt + bD;
+  f->bytes = bt + bD + bP;
+  double *h = (double *)malloc(sizeof(double) * 2 * (size_t)(nP > 4096 ? nP : 4096));
+  if (!h) {
+    cudaFree(base), free(f);
+    return 2;
+  }
+  const double PI = 3.14159265358979323846264338327950288;
+  for (long t = 0; t < 4096; ++t) h[2 * t] = cos(2 * PI * t / 4096), h[2 * t + 1] = -sin(2 * PI * t / 4096);
+  if (dbl) rc = upload<double>((double **)&f->twD, h, 2 * 4096, err, errlen);
+  else rc = upload<float>((float **)&f->twD, h, 2 * 4096, err, errlen);
+  for (long t = 0; t < nlo; ++t) h[2 * t] = cos(2 * PI * t / N), h[2 * t + 1] = -sin(2 * PI * t / N);
+  for (long t = 0; t < nP - nlo; ++t) {
+    const double ang = 2 * PI * (double)(t * nlo) / (double)N;
+    h[2 * (nlo + t)] = cos(ang), h[2 * (nlo + t) + 1] = -sin(ang);
+  }
+  if (!rc) {
+    if (dbl) rc = upload<double>((double **)&f->twP, h, 2 * nP, err, errlen);
+    else rc = upload<float>((float **)&f->twP, h, 2 * nP, err, errlen);
+  }
+  free(h);
+  if (rc) {
+    cudaFree(base), free(f);
+    return rc;
+  }
+  if (device_bytes) *device_bytes = f->bytes;
+  *out = f;
+  return 0;
+}
+
+template <typename R>
+static int fft_run(fmmk_fft *f, const void *in, void *out, cudaStream_t st, char *err, size_t errlen) {
+  using C = typename cplx<R>::T;
+  const C *twD = (const C *)f->twD, *twP = (const C *)f->twP;
+  for (int k = 0; k < f->npass; ++k) {
+    const FftPass &fp = f->pass[k];
+    const C *src = (const C *)(f->src[k] == 0 ? in : (f->src[k] == 1 ? out : f->tmp));
+    C *dst = (C *)(f->dst[k] == 1 ? out : f->tmp);
+    const int thr = fp.W * (fp.L / 8);
+    const size_t sm = sizeof(C) * ((size_t)fp.W * (fp.L + fp.L / 8 + 1) + fp.L + fp.L / 16 + 1 + 8 * fp.W);
+    dim3 g((unsigned)(f->per[k] / fp.W), (unsigned)f->rows[k]);
+    if (f->tin[k] && f->tout[k])
+      k_fft_reg<R, true, true><<<g, thr, sm, st>>>(src, dst, twD, twP, fp);
+    else if (f->tin[k])
+      k_fft_reg<R, true, false><<<g, thr, sm, st>>>(src, dst, twD, twP, fp);
+    else
+      k_fft_reg<R, false, false><<<g, thr, sm, st>>>(src, dst, twD, twP, fp);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    snprintf(err, errlen, "plain FFT launch: %s", cudaGetErrorString(e));
+    return 3;
+  }
+  return 0;
+}
+
+extern "C" int fmmk_fft_execute(fmmk_fft *f, const void *in, void *out, void *stream, char *err,
+                                size_t errlen) {
+  if (in == out) {
+    snprintf(err, errlen, "the plain FFT is out of place: input and output must differ");
+    return 1;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  return f->dbl ? fft_run<double>(f, in, out, st, err, errlen) : fft_run<float>(f, in, out, st, err, errlen);
+}
+
+extern "C" size_t fmmk_fft_bytes(const fmmk_fft *f) { return f->bytes; }
+
+extern "C" void fmmk_fft_destroy(fmmk_fft *f) {
+  if (!f) return;
+  cudaFree(f->tmp);
+  free(f);
 }

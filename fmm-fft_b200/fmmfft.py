@@ -30,7 +30,8 @@ EXPORTS = ["getwlen2", "getvlen", "mfti", "mft", "fmmfft_last_error", "fmmfft_la
            "fmmfft_execute_graph", "fmmfft_batch_create", "fmmfft_batch_launch",
            "fmmfft_batch_destroy", "fmmfft_server_create", "fmmfft_server_destroy",
            "fmmfft_server_submit", "fmmfft_server_query", "fmmfft_server_wait",
-           "fmmfft_server_stats"]
+           "fmmfft_server_stats", "fmmfft_fft_create", "fmmfft_fft_execute",
+           "fmmfft_fft_device_bytes", "fmmfft_fft_destroy"]
 
 
 class FmmFftError(RuntimeError):
@@ -95,6 +96,14 @@ def load(path=LIB_PATH):
     lib.fmmfft_server_stats.argtypes = [_VP, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(_I),
                                         ctypes.POINTER(_I)]
     lib.fmmfft_server_stats.restype = _I
+    lib.fmmfft_fft_create.argtypes = [ctypes.POINTER(_VP), _L, _I]
+    lib.fmmfft_fft_create.restype = _I
+    lib.fmmfft_fft_execute.argtypes = [_VP, _VP, _VP, _VP]
+    lib.fmmfft_fft_execute.restype = _I
+    lib.fmmfft_fft_device_bytes.argtypes = [_VP, ctypes.POINTER(ctypes.c_size_t)]
+    lib.fmmfft_fft_device_bytes.restype = _I
+    lib.fmmfft_fft_destroy.argtypes = [_VP]
+    lib.fmmfft_fft_destroy.restype = _I
     _lib = lib
     return lib
 
@@ -317,6 +326,38 @@ class Server:
     def close(self):
         if getattr(self, "_h", None):
             load().fmmfft_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PlainFFT:
+    """Conventional forward FFT of length N on the GPU (fmmfft_fft_*), the counterpart of the
+    reference's FFTW comparators (src/fftw_serial.c:53-58, src/fftw_mpi.c:54-58).
+    precision "f64" (complex128) or "f32" / "f32_tc" (complex64)."""
+
+    def __init__(self, N, precision="f32"):
+        h = _VP()
+        _check(load().fmmfft_fft_create(ctypes.byref(h), int(N), PRECISIONS[precision]))
+        self._h = h
+        self.N = int(N)
+        self.precision = precision
+
+    def execute_ptr(self, d_in, d_out, stream=0):
+        _check(load().fmmfft_fft_execute(self._h, d_in, d_out, stream or None))
+
+    def device_bytes(self):
+        v = ctypes.c_size_t()
+        _check(load().fmmfft_fft_device_bytes(self._h, ctypes.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().fmmfft_fft_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -189,6 +189,20 @@ const char *fmmfft_stage_name(int i);
 int fmmfft_execute_noalloc(long N, long P, long terms, long b, const void *d_in, void *d_out,
                            void *stream);
 
+/* ------------------------------------------------------------------ plain FFT comparator */
+/* A conventional (non-FMM) forward FFT of length N on the GPU: the reference's plain FFTW
+ * comparators, src/fftw_serial.c:53-58 (fftw_plan_dft + fftw_execute, FFTW_FORWARD) and
+ * src/fftw_mpi.c:54-58, which the reference times beside mft.  Same sign and scaling as
+ * fmmfft_execute (y[k] = sum_n x[n] exp(-2 pi i n k / N), unnormalised); out of place, unlike
+ * FFTW's in-place x -> x there (d_in != d_out).  N a power of two in [16, 2^30]; precision
+ * FMMFFT_F64 (complex128) or FMMFFT_F32 / FMMFFT_F32_TC (complex64: both the same FP32 FFT).
+ * The handle owns one N-element workspace and the twiddle tables. */
+typedef struct fmmfft_fft_s *fmmfft_fft;
+int fmmfft_fft_create(fmmfft_fft *out, long N, int precision);
+int fmmfft_fft_execute(fmmfft_fft f, const void *d_in, void *d_out, void *stream);
+int fmmfft_fft_device_bytes(fmmfft_fft f, size_t *bytes);
+int fmmfft_fft_destroy(fmmfft_fft f);
+
 #ifdef __cplusplus
 }
 #endif
