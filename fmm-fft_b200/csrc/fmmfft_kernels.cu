@@ -119,6 +119,7 @@ template <typename R> struct Dev {
   int ok_s2m, ok_m2m, ok_m2l, ok_leaf;
   long tc_min_rows; /* stages with fewer rows use the CUDA-core kernel */
   int fft_threads;  /* threads per block of the register FFT pass (power of two, <= 512) */
+  int tc_pipelined; /* tree stages on the pipelined tensor-core kernel where it fits */
 };
 
 /* Instantiated CUDA graphs of one plan's execute, keyed by (input, output, direction): the
@@ -437,7 +438,21 @@ template <class Prob> static size_t tc_smem_bytes(const Prob &pb) {
   return tc::smem_bytes(pb.kpad, pb.npad);
 }
 
-template <class Prob> static void launch_tc(const Prob &pb, int num_sms, int *status, cudaStream_t st) {
+/* The pipelined form (tc::k_tc_rowgemm_t) takes one operator of at most 64 outputs for all
+ * rows and K <= 256 within 220 KB of shared memory; everything else runs the row form. */
+template <class Prob> static bool tc_pipelined_fits(const Prob &pb) {
+  return pb.batches == 1 && pb.npad <= 64 && pb.nout <= 64 && pb.kpad % 8 == 0 &&
+         pb.kpad <= tc::kTKs * tc::kTMaxSteps && tc::t_smem_bytes(pb.kpad) <= (size_t)220 * 1024;
+}
+
+template <class Prob>
+static void launch_tc(const Prob &pb, int num_sms, int *status, cudaStream_t st, int pipelined) {
+  if (pipelined && tc_pipelined_fits(pb)) {
+    const long tiles = (pb.rows + tc::kTRows - 1) / tc::kTRows;
+    const int grid = (int)(tiles < num_sms ? tiles : num_sms); /* one CTA per SM: all of TMEM */
+    tc::k_tc_rowgemm_t<Prob><<<grid, tc::kTThreads, tc::t_smem_bytes(pb.kpad), st>>>(pb, status);
+    return;
+  }
   long tiles = (pb.rows + tc::kRows - 1) / tc::kRows * pb.batches;
   long cap = 2L * num_sms; /* two CTAs per SM */
   int grid = (int)(tiles < cap ? tiles : cap);
@@ -1169,6 +1184,11 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   d->ok_leaf = fits(d->kp_leaf, d->np_leaf) && getenv("FMMFFT_TC_STAGES") != NULL;
   d->tc_min_rows = kTcMinRows;
   if (const char *ev = getenv("FMMFFT_TC_MIN_ROWS")) d->tc_min_rows = atol(ev);
+  /* FMMFFT_TC_FORM=pipelined routes the tree stages that fit to the warp-specialised kernel
+   * (4xTF32, rel-L2 2.4e-7 at N = 2^24, P = 64, 24 terms, against 2.7e-7); the row form stays
+   * the default because it is faster there (M2L 0.47 ms against 0.58 ms on a B200) */
+  d->tc_pipelined = 0;
+  if (const char *ev = getenv("FMMFFT_TC_FORM")) d->tc_pipelined = strcmp(ev, "pipelined") == 0;
   d->fft_threads = 512;
   if (const char *ev = getenv("FMMFFT_FFT_THREADS")) {
     const int v = atoi(ev);
@@ -1371,7 +1391,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.kpad = d->kp_s2m, q.npad = d->np_s2m, q.nout = (int)T;
         q.bhi = d->tc_s2m[0], q.blo = d->tc_s2m[1], q.bstride = 0;
         q.xt = d->xt, q.out = d->phi + lvl_off(n, S1, T), q.M = M, q.b = (int)b, q.T = (int)T;
-        launch_tc(q, d->num_sms, d->status, st);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_pipelined);
         done = true;
       }
     }
@@ -1393,7 +1413,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.bhi = d->tc_m2m[0] + (L - 2) * d->tc_m2m_stride, q.blo = d->tc_m2m[1] + (L - 2) * d->tc_m2m_stride;
         q.bstride = 0;
         q.child = d->phi + lvl_off(L + 1, S1, T), q.out = d->phi + lvl_off(L, S1, T), q.T = (int)T;
-        launch_tc(q, d->num_sms, d->status, st);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_pipelined);
         done = true;
       }
     }
@@ -1427,7 +1447,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.bstride = 0;
         q.psi_par = d->psi + lvl_off(l - 1, S1, T), q.phi = d->phi + lvl_off(l, S1, T);
         q.out = d->psi + lvl_off(l, S1, T), q.T = (int)T, q.lpar = (int)(l - 1);
-        launch_tc(q, d->num_sms, d->status, st);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_pipelined);
         done = true;
       }
     }
@@ -1461,7 +1481,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.bhi = d->tc_leaf[0], q.blo = d->tc_leaf[1], q.bstride = d->tc_leaf_stride;
         q.psi_n = pb.psi_n, q.xt = d->xt, q.u = d->u, q.M = M, q.s = s, q.T = (int)T, q.b = (int)b;
         q.log2s = (int)n;
-        launch_tc(q, d->num_sms, d->status, st);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_pipelined);
         done = true;
       }
     }
@@ -1589,6 +1609,9 @@ static int set_smem_limits(void) {
   allow_dyn_smem(tc::k_tc_rowgemm<TcM2M>, lim);
   allow_dyn_smem(tc::k_tc_rowgemm<TcM2L>, lim);
   allow_dyn_smem(tc::k_tc_rowgemm<TcLeaf>, lim);
+  allow_dyn_smem(tc::k_tc_rowgemm_t<TcS2M>, lim);
+  allow_dyn_smem(tc::k_tc_rowgemm_t<TcM2M>, lim);
+  allow_dyn_smem(tc::k_tc_rowgemm_t<TcM2L>, lim);
   done = 1;
   return 0;
 }

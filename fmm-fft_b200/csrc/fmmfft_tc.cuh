@@ -370,4 +370,357 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
   if (warp == 0) tmem_dealloc(tmem, ncols);
 }
 
+
+/* ======================================================================== pipelined form */
+
+/* The same contraction with the roles of the operands exchanged, for operators of at most 64
+ * outputs shared by all rows (one batch): the tensor core computes D = Op X^T with
+ *   Op (MMA M = 128): rows 0..63 the operator's TF32 hi part, rows 64..127 its lo part;
+ *   X  (MMA N = 256): 256 data rows of the tile, as TF32 hi or lo (two MMAs per K step);
+ * so that D[n][c] + D[64 + n][c] = sum over the four hi/lo products of output n of data row c
+ * (the lo*lo product too: 4xTF32).  Each MMA is M = 128, N = 256, K = 8, five times the work of
+ * the row form's M = 128, N = 48 instruction.  One CTA per SM, warp-specialised:
+ *   warps 0-7  producers: thread p loads data row p of the tile from HBM (16 K columns per
+ *              stage, four stages of loads in flight), splits it into TF32 hi / lo and writes
+ *              both into a shared-memory stage in the K-major no-swizzle layout; kTStages
+ *              stages in a ring (mbarriers full / empty);
+ *   warps 8-15 epilogue: two per TMEM lane quarter q = warp & 3; per 32 rows the hi quarters
+ *              0-1 and the lo quarters 2-3 write their columns into two staging blocks in
+ *              shared memory, which all eight warps add and store with float4 (Prob::dst(r)
+ *              must be dst(0) + r * nout: rows stored back to back, as every tree stage
+ *              stores them);
+ *   warp 16    one thread issues the MMAs into one of two TMEM accumulators of 256 columns
+ *              (mbarriers dfull / dempty), so the epilogue of a tile overlaps the next tile.
+ * Every wait is bounded by the global timer; on expiry the CTA records kErrWaitTimeout, every
+ * role leaves its loop, the MMA thread waits (bounded) for its MMAs in flight, and TMEM is
+ * freed. */
+constexpr int kTRows = 256;     /* data rows per tile: MMA N */
+constexpr int kTKs = 16;        /* K columns per stage */
+constexpr int kTStages = 4;     /* shared-memory stages in the ring */
+constexpr int kTProd = 8;       /* producer warps: one thread per data row */
+constexpr int kTEpi = 8;        /* epilogue warps: two per TMEM lane quarter */
+constexpr int kTThreads = (kTProd + kTEpi + 1) * 32;
+constexpr int kTMaxSteps = 16;  /* K <= 256 */
+constexpr unsigned long long kWaitNs = 2000000000ull; /* 2 s per wait */
+
+__host__ __device__ constexpr size_t t_smem_bytes(int kpad) {
+  return (size_t)128 * kpad * 4 + (size_t)kTStages * 2 * kTRows * kTKs * 4 + (size_t)2 * 32 * 64 * 4;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" : : "r"(smem_addr(bar)) : "memory");
+}
+
+/* Waits for phase `parity` of `bar`; false when the CTA aborted or 2 s passed (then the abort
+ * flag and the status word are set).  The clock is read only after 4096 unsuccessful polls. */
+__device__ __forceinline__ bool t_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag,
+                                       int *status) {
+  unsigned long long t0 = 0;
+  for (unsigned it = 0;; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 63) == 63 && *abort_flag) return false;
+    if ((it & 4095) == 4095) {
+      const unsigned long long now = global_ns();
+      if (t0 == 0) {
+        t0 = now;
+      } else if (now - t0 > kWaitNs) {
+        atomicExch(status, kErrWaitTimeout);
+        *abort_flag = 1;
+        return false;
+      }
+    }
+  }
+}
+
+/* Waits for phase `parity` of `bar` for at most about 2 s, whatever the abort flag says. */
+__device__ __forceinline__ bool t_wait_time(uint64_t *bar, uint32_t parity) {
+  unsigned long long t0 = 0;
+  for (unsigned it = 0;; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 4095) == 4095) {
+      const unsigned long long now = global_ns();
+      if (t0 == 0) t0 = now;
+      else if (now - t0 > kWaitNs) return false;
+    }
+  }
+}
+
+__device__ __forceinline__ void named_bar(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" : : "r"(id), "r"(nthreads) : "memory");
+}
+
+/* Barrier `id` over `nthreads` threads that also ANDs a flag across them: every participant
+ * gets the same answer, so they all take the same branch afterwards. */
+__device__ __forceinline__ bool named_bar_and(int id, int nthreads, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(id), "r"(nthreads)
+      : "memory");
+  return r != 0;
+}
+
+/* 16 consecutive TMEM columns of this thread's lane (two x8 loads, one wait). */
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
+  uint32_t r[16];
+#pragma unroll
+  for (int q = 0; q < 2; ++q)
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(r[8 * q]), "=r"(r[8 * q + 1]), "=r"(r[8 * q + 2]), "=r"(r[8 * q + 3]),
+          "=r"(r[8 * q + 4]), "=r"(r[8 * q + 5]), "=r"(r[8 * q + 6]), "=r"(r[8 * q + 7])
+        : "r"(taddr + 8 * q)
+        : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+/* 32 consecutive TMEM columns of this thread's lane (four x8 loads, one wait). */
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
+  uint32_t r[32];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(r[8 * q]), "=r"(r[8 * q + 1]), "=r"(r[8 * q + 2]), "=r"(r[8 * q + 3]),
+          "=r"(r[8 * q + 4]), "=r"(r[8 * q + 5]), "=r"(r[8 * q + 6]), "=r"(r[8 * q + 7])
+        : "r"(taddr + 8 * q)
+        : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+/* Optional per-role cycle counters: empty unless a build defines them. */
+#ifndef TC_PHASE
+#define TC_CLOCK(tp)
+#define TC_PHASE(slot, tp)
+#endif
+
+template <class Prob>
+__global__ void __launch_bounds__(kTThreads, 1) k_tc_rowgemm_t(const __grid_constant__ Prob pb, int *status) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ uint64_t full[kTStages], empty[kTStages], dfull[2], dempty[2], fin;
+  __shared__ uint32_t tmem_slot;
+  __shared__ volatile int abort_flag;
+  __shared__ int lmap[kTMaxSteps][4]; /* per step and float4: chunk (low byte, 0xFF none), offset */
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int kpad = pb.kpad, nsteps = (kpad + kTKs - 1) / kTKs;
+  float *Op = reinterpret_cast<float *>(smem_raw);
+  float *Xs = Op + 128 * kpad;                    /* stage s: hi, then lo */
+  float *xch = Xs + kTStages * 2 * kTRows * kTKs; /* epilogue staging: hi, lo [32 rows][nout] */
+  const int mma_warp = kTProd + kTEpi;
+  if (warp == mma_warp) tmem_alloc(&tmem_slot, 512);
+  if (tid == 0) {
+    for (int i = 0; i < kTStages; ++i) mbar_init(&full[i], kTProd), mbar_init(&empty[i], 1);
+    for (int i = 0; i < 2; ++i) mbar_init(&dfull[i], 1), mbar_init(&dempty[i], kTEpi);
+    mbar_init(&fin, 1);
+    fence_mbar_init();
+    abort_flag = 0;
+  }
+  if (tid < kTMaxSteps * 4) {
+    const int st = tid >> 2, i = tid & 3, k = st * kTKs + 4 * i;
+    int e = 0xFF;
+    if (k < kpad)
+      for (int c = 0; c < pb.nchunks; ++c)
+        if (k >= pb.coff[c] && k < pb.coff[c] + pb.clen[c]) e = c | ((k - pb.coff[c]) << 8);
+    lmap[st][i] = e;
+  }
+  /* operator: hi in rows 0..npad-1, lo in rows 64..64+npad-1, zero elsewhere */
+  for (int e = tid; e < 128 * kpad; e += blockDim.x) {
+    const int m = e / kpad, k = e - m * kpad;
+    float v = 0.f;
+    if (m < pb.npad) v = pb.bhi[(long)m * kpad + k];
+    else if (m >= 64 && m - 64 < pb.npad) v = pb.blo[(long)(m - 64) * kpad + k];
+    Op[core_off(m, k, kpad) >> 2] = v;
+  }
+  fence_smem_to_async();
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = tmem_slot;
+  const long ntiles = (pb.rows + kTRows - 1) / kTRows;
+
+  if (warp < kTProd) {
+    /* ------------------------------------------------------------ producers */
+    /* thread p fills data row p of the tile: 16 K columns (4 float4) per stage, with four
+     * stages of loads in flight (a register ring, the loop unrolled by four so that its
+     * indices stay static) */
+    const int p = tid;
+    const uint32_t xs0 = smem_addr(Xs);
+    long ltile = blockIdx.x; /* load cursor, four stages ahead of the store cursor */
+    int lst = 0;
+    const float *rowp[4] = {nullptr, nullptr, nullptr, nullptr};
+    auto set_rows = [&]() {
+      const long r = ltile * kTRows + p;
+      const bool live = r < pb.rows;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) rowp[c] = (live && c < pb.nchunks) ? pb.src(c, r, 0) : nullptr;
+    };
+    auto load = [&](float4 (&v)[4]) {
+      if (ltile >= ntiles) return;
+      if (lst == 0) set_rows();
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int e = lmap[lst][i], c = e & 0xFF;
+        v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (c != 0xFF) {
+          const float *rp = c == 0 ? rowp[0] : (c == 1 ? rowp[1] : (c == 2 ? rowp[2] : rowp[3]));
+          if (rp) v[i] = __ldg(reinterpret_cast<const float4 *>(rp + (e >> 8)));
+        }
+      }
+      if (++lst == nsteps) lst = 0, ltile += gridDim.x;
+    };
+    long tile = blockIdx.x;
+    int st = 0;
+    unsigned it = 0;
+    bool go = tile < ntiles;
+    /* one stage: wait for the ring slot, split the registers loaded four stages ago into
+     * TF32 hi / lo straight into it, refill them with the stage four ahead, signal */
+    auto step = [&](float4 (&v)[4]) {
+      if (!go) return;
+      TC_CLOCK(tp);
+      const int s = (int)(it % kTStages);
+      bool ok = true;
+      if (lane == 0) ok = t_wait(&empty[s], ((it / kTStages) & 1) ^ 1, &abort_flag, status);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) {
+        go = false;
+        return;
+      }
+      TC_PHASE(2, tp);
+      const uint32_t hb = xs0 + (uint32_t)(s * 2 * kTRows * kTKs * 4), lb = hb + kTRows * kTKs * 4;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const uint32_t o = core_off(p, 4 * j, kTKs);
+        const float a0 = v[j].x, a1 = v[j].y, a2 = v[j].z, a3 = v[j].w;
+        const float h0 = tf32_rna(a0), h1 = tf32_rna(a1), h2 = tf32_rna(a2), h3 = tf32_rna(a3);
+        asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" : : "r"(hb + o), "f"(h0), "f"(h1),
+                     "f"(h2), "f"(h3) : "memory");
+        asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" : : "r"(lb + o), "f"(tf32_rna(a0 - h0)),
+                     "f"(tf32_rna(a1 - h1)), "f"(tf32_rna(a2 - h2)), "f"(tf32_rna(a3 - h3)) : "memory");
+      }
+      TC_PHASE(0, tp);
+      load(v);
+      TC_PHASE(1, tp);
+      fence_smem_to_async();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&full[s]);
+      TC_PHASE(3, tp);
+      ++it;
+      if (++st == nsteps) st = 0, tile += gridDim.x;
+      go = tile < ntiles;
+    };
+    float4 v0[4], v1[4], v2[4], v3[4];
+    load(v0), load(v1), load(v2), load(v3);
+    while (go) {
+      step(v0), step(v1), step(v2), step(v3);
+    }
+  } else if (warp < kTProd + kTEpi) {
+    /* ------------------------------------------------------------ epilogue */
+    /* per 32 rows: warp (q, h) reads lane quarter q, columns [16 h, 16 h + 16) of the chunk and
+     * writes them into staging block q / 2 (hi or lo) as [row][nout]; then all epilogue
+     * threads add the two blocks and store the rows' contiguous output with float4 */
+    const int q = warp & 3, h = (warp - kTProd) >> 2, et = tid - kTProd * 32;
+    const uint32_t lane_addr = (uint32_t)(q * 32) << 16;
+    const int nout = pb.nout;
+    const int n = (q & 1) * 32 + lane; /* output index of this lane (hi and lo quarters) */
+    float *stg = xch + (q >> 1) * 32 * 64;
+    unsigned tc = 0;
+    for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++tc) {
+      TC_CLOCK(tp);
+      const int b = (int)(tc & 1);
+      bool ok = true;
+      if (lane == 0) ok = t_wait(&dfull[b], (tc >> 1) & 1, &abort_flag, status);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      /* all epilogue warps continue, or all leave (they meet at named barriers below) */
+      if (!named_bar_and(3, kTEpi * 32, ok)) break;
+      fence_after_sync();
+      TC_PHASE(4, tp);
+      for (int ch = 0; ch < kTRows / 32; ++ch) {
+        float t[16];
+        tmem_ld16(tmem + lane_addr + (uint32_t)(b * 256 + ch * 32 + h * 16), t);
+        if (n < nout) {
+#pragma unroll
+          for (int c = 0; c < 16; ++c) stg[(h * 16 + c) * nout + n] = t[c];
+        }
+        named_bar(1, kTEpi * 32);
+        const long rb = tile * kTRows + ch * 32;
+        const long nr = pb.rows - rb < 32 ? pb.rows - rb : 32;
+        if (nr > 0) {
+          float4 *g = reinterpret_cast<float4 *>(pb.dst(rb, 0));
+          const float4 *sh = reinterpret_cast<const float4 *>(xch);
+          const float4 *sl = reinterpret_cast<const float4 *>(xch + 32 * 64);
+          const int n4 = (int)nr * nout / 4;
+          for (int i = et; i < n4; i += kTEpi * 32) {
+            const float4 x = sh[i], y = sl[i];
+            g[i] = make_float4(x.x + y.x, x.y + y.y, x.z + y.z, x.w + y.w);
+          }
+        }
+        named_bar(1, kTEpi * 32);
+      }
+      fence_before_sync();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&dempty[b]);
+      TC_PHASE(5, tp);
+    }
+  } else {
+    if (lane == 0) {
+      /* ---------------------------------------------------------- MMA issue */
+      const uint32_t idesc = make_idesc_tf32(kTRows);
+      const uint32_t op = smem_addr(Op), xs0 = smem_addr(Xs);
+      const uint32_t op_sbo = (uint32_t)kpad * 32, x_sbo = (uint32_t)kTKs * 32;
+      unsigned it = 0, tc = 0;
+      bool ok = true;
+      for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++tc) {
+        TC_CLOCK(tp);
+        const int b = (int)(tc & 1);
+        ok = t_wait(&dempty[b], ((tc >> 1) & 1) ^ 1, &abort_flag, status);
+        if (!ok) break;
+        fence_after_sync();
+        TC_PHASE(6, tp);
+        const uint32_t d = tmem + (uint32_t)(b * 256);
+        for (int st = 0; st < nsteps; ++st, ++it) {
+          const int s = (int)(it % kTStages);
+          ok = t_wait(&full[s], (it / kTStages) & 1, &abort_flag, status);
+          if (!ok) break;
+          fence_after_sync();
+          TC_PHASE(7, tp);
+          const int k0 = st * kTKs;
+          const int ksteps = ((kpad - k0) < kTKs ? (kpad - k0) : kTKs) >> 3;
+          const uint32_t hb = xs0 + (uint32_t)(s * 2 * kTRows * kTKs * 4), lb = hb + kTRows * kTKs * 4;
+          for (int kk = 0; kk < ksteps; ++kk) {
+            const uint64_t da = make_desc(op + 256u * (uint32_t)((k0 >> 3) + kk), 128, op_sbo);
+            mma_tf32(d, da, make_desc(hb + 256u * kk, 128, x_sbo), idesc, (st | kk) != 0);
+            mma_tf32(d, da, make_desc(lb + 256u * kk, 128, x_sbo), idesc, 1);
+          }
+          mma_commit(&empty[s]);
+          TC_PHASE(8, tp);
+        }
+        if (!ok) break;
+        mma_commit(&dfull[b]);
+      }
+      /* every MMA issued has completed before TMEM is freed */
+      mma_commit(&fin);
+      if (!t_wait_time(&fin, 0)) atomicExch(status, kErrWaitTimeout);
+    }
+    __syncwarp();
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  if (warp == mma_warp) tmem_dealloc(tmem, 512);
+}
+
 }  // namespace tc

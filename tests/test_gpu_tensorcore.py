@@ -2,7 +2,8 @@
 
 FMMFFT_TC_MIN_ROWS=1 (set before the plans are made) sends every eligible stage, however small,
 through the tensor-core kernel so that small cases cover it; the default threshold only routes
-stages with >= 8192 rows there.  Tolerance: rel-L2 <= 1e-6 against FP64, as for FP32 plans.
+stages with >= 8192 rows there.  Each test runs for both kernel forms (FMMFFT_TC_FORM row and
+pipelined).  Tolerance: rel-L2 <= 1e-6 against FP64, as for FP32 plans.
 """
 import os
 
@@ -28,15 +29,19 @@ def fm():
     return fmmfft
 
 
-@pytest.fixture()
-def force_tc():
-    old = os.environ.get("FMMFFT_TC_MIN_ROWS")
+@pytest.fixture(params=["row", "pipelined"])
+def force_tc(request):
+    """Every eligible stage on the tensor cores, in the row form (default) or the pipelined,
+    warp-specialised form (FMMFFT_TC_FORM=pipelined)."""
+    saved = {k: os.environ.get(k) for k in ("FMMFFT_TC_MIN_ROWS", "FMMFFT_TC_FORM")}
     os.environ["FMMFFT_TC_MIN_ROWS"] = "1"
-    yield
-    if old is None:
-        del os.environ["FMMFFT_TC_MIN_ROWS"]
-    else:
-        os.environ["FMMFFT_TC_MIN_ROWS"] = old
+    os.environ["FMMFFT_TC_FORM"] = request.param
+    yield request.param
+    for k, v in saved.items():
+        if v is None:
+            os.environ.pop(k, None)
+        else:
+            os.environ[k] = v
 
 
 @pytest.mark.parametrize("N,P,T,b", CASES)
@@ -62,7 +67,19 @@ def test_tc_stagewise_vs_oracle(fm, force_tc, N, P, T, b):
     assert ol.rel_l2(y, o["y"]) < TOL
 
 
-def test_tc_config2_full_size(fm):
+@pytest.fixture(params=["row", "pipelined"])
+def tc_form(request):
+    """Default routing (stages of >= 8192 rows on the tensor cores) in either kernel form."""
+    saved = os.environ.get("FMMFFT_TC_FORM")
+    os.environ["FMMFFT_TC_FORM"] = request.param
+    yield request.param
+    if saved is None:
+        os.environ.pop("FMMFFT_TC_FORM", None)
+    else:
+        os.environ["FMMFFT_TC_FORM"] = saved
+
+
+def test_tc_config2_full_size(fm, tc_form):
     """N = 2^24 complex64, P = 64, p = 24, b = 32 with the default routing."""
     N, P, T, b = 1 << 24, 64, 24, 32
     x = ol.seeded_input(N, 0)
