@@ -130,12 +130,19 @@ def stage_bytes(N, P, T, b, esz):
     xt_all = 2 * P * M * R
     xt_sec = 2 * S1 * M * R
     u = 2 * S1 * M * R
+    # levels of fewer than 4096 rows (2 (P-1) boxes each) run in the coarse-tree launch
+    coarse = lambda rows: rows < 4096
+    m2m = [l for l in range(2, n)]
+    m2l = [l for l in range(3, n + 1)]
+    m2m_c = [l for l in m2m if coarse(2 * S1 * (1 << l))]
+    m2l_c = [l for l in m2l if coarse(2 * S1 * (1 << (l - 1)))]
     return {
         "sections": N * esz + xt_all,
         "s2m": xt_sec + lv(n),
-        "m2m": sum(lv(l + 1) + lv(l) for l in range(2, n)),
-        "topflip": 2 * lv(2),
-        "m2l_l2l": sum(lv(l - 1) + lv(l) + lv(l) for l in range(3, n + 1)),
+        "m2m": sum(lv(l + 1) + lv(l) for l in m2m if l not in m2m_c),
+        "coarse_tree": sum(lv(l + 1) + lv(l) for l in m2m_c) + 2 * lv(2) +
+                       sum(lv(l - 1) + lv(l) + lv(l) for l in m2l_c),
+        "m2l_l2l": sum(lv(l - 1) + lv(l) + lv(l) for l in m2l if l not in m2l_c),
         "leaf_l2t_near": lv(n) + xt_sec + u,
         "combine_dftP": 2 * M * R + u + N * esz,
         "fft_pass1": 2 * N * esz,

@@ -69,7 +69,7 @@ template <typename C> __device__ __forceinline__ C csub(C a, C b) {
 enum { ST_SECTIONS = 0, ST_SUMS, ST_S2M, ST_M2M, ST_TOP, ST_M2L, ST_LEAF, ST_LEAFFIX, ST_COMBINE,
        ST_FFT1, ST_FFT2, ST_DC, ST_COUNT };
 static const char *const kStageNames[ST_COUNT] = {
-    "sections", "section_sums", "s2m", "m2m", "topflip", "m2l_l2l", "leaf_l2t_near",
+    "sections", "section_sums", "s2m", "m2m", "coarse_tree", "m2l_l2l", "leaf_l2t_near",
     "leaf_halfshift", "combine_dftP", "fft_pass1", "fft_pass2", "block_dc"};
 
 struct Prof {
@@ -120,6 +120,9 @@ template <typename R> struct Dev {
   long tc_min_rows; /* stages with fewer rows use the CUDA-core kernel */
   int fft_threads;  /* threads per block of the register FFT pass (power of two, <= 512) */
   int tc_pipelined; /* tree stages on the pipelined tensor-core kernel where it fits */
+  unsigned *sync;   /* grid barrier of the coarse-tree kernel: [0] arrivals, [32] generation */
+  long coarse_rows; /* levels with fewer rows go to the coarse-tree kernel (0: none) */
+  int coarse_grid;  /* its cooperative grid (blocks of 256) */
 };
 
 /* Instantiated CUDA graphs of one plan's execute, keyed by (input, output, direction): the
@@ -998,21 +1001,158 @@ __global__ void k_combine(const R *__restrict__ xt, const R *__restrict__ u,
 template <typename R>
 __global__ void k_block_dc(const typename cplx<R>::T *__restrict__ ssum,
                            typename cplx<R>::T *__restrict__ y, long M, int P, int conj_out) {
+  /* one warp per output bin r; lane l sums sc = l, l + 32, ...; FP64 warp reduction */
   using C = typename cplx<R>::T;
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (r >= P) return;
   double re = 0, im = 0;
-  for (int sc = 0; sc < P; ++sc) {
+  for (int sc = lane; sc < P; sc += 32) {
     double sn, cs;
     sincospi(-2.0 * (double)((long)sc * r % P) / (double)P, &sn, &cs);
     C v = ssum[sc];
     re += (double)v.x * cs - (double)v.y * sn;
     im += (double)v.x * sn + (double)v.y * cs;
   }
-  C out;
-  out.x = (R)re;
-  out.y = (R)(conj_out ? -im : im);
-  y[(long)r * M] = out;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    re += __shfl_xor_sync(0xffffffffu, re, o);
+    im += __shfl_xor_sync(0xffffffffu, im, o);
+  }
+  if (lane == 0) {
+    C out;
+    out.x = (R)re;
+    out.y = (R)(conj_out ? -im : im);
+    y[(long)r * M] = out;
+  }
+}
+
+/* ======================================================================== coarse tree */
+
+/* The coarse levels of the tree (few boxes: every level whose row count is below a threshold)
+ * in one cooperative launch instead of one launch per level: the upward M2M for parent levels
+ * Lm .. 2, the top flip, and the downward M2L + L2L for child levels 3 .. Ll, with a grid-wide
+ * barrier between levels.  Same operators, layouts and outputs (every level's phi / psi) as the
+ * per-level launches (reference fmmfft.c:476-515 upward, :620-749 top and downward).  Each
+ * level's operator is first staged in shared memory by the whole block; then one warp per
+ * output row, lane = output column (N / 32 columns per lane), the row's A values broadcast from
+ * the lanes that loaded them; the K sum accumulates per 32-column block, then into the total
+ * (two-level FP32 accumulation, as in the row kernels). */
+template <typename R> struct CoarseArgs {
+  R *phi, *psi;
+  const R *bm2m, *btop, *bm2l;
+  long S1;
+  int T, Lm, Ll; /* coarse M2M parent levels Lm..2 (none when Lm < 2); M2L child levels 3..Ll */
+  unsigned *sync; /* [0] arrivals, [32] generation: separate 128-byte lines; [0] zeroed first */
+  int *status;
+};
+
+constexpr unsigned long long kGridWaitNs = 1000000000ull; /* 1 s per barrier */
+
+/* Grid-wide barrier of a cooperative launch; false when a block waited 1 s (status set). */
+__device__ __forceinline__ bool grid_barrier(unsigned *sync, int *status) {
+  __shared__ int gb_fail;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    gb_fail = 0;
+    volatile unsigned *gen = sync + 32;
+    const unsigned g = *gen;
+    __threadfence();
+    if (atomicAdd(sync, 1u) == gridDim.x - 1) {
+      atomicExch(sync, 0u);
+      __threadfence();
+      atomicAdd(sync + 32, 1u);
+    } else {
+      unsigned long long t0 = 0;
+      for (unsigned it = 0; *gen == g; ++it) {
+        __nanosleep(32);
+        if ((it & 255) == 255) {
+          unsigned long long now;
+          asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+          if (t0 == 0) {
+            t0 = now;
+          } else if (now - t0 > kGridWaitNs) {
+            atomicExch(status, 1);
+            gb_fail = 1;
+            break;
+          }
+        }
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return gb_fail == 0;
+}
+
+/* out[r][n] = sum_k A(r, k) Bs[k][n] for the rows of one level; B (K x N) is copied into the
+ * shared array Bs first; arow(r, k) is the address of element k of row r's A. */
+template <typename R, class Arow>
+__device__ __forceinline__ void coarse_rows(long rows, int K, int N, const R *__restrict__ B,
+                                            R *__restrict__ Bs, R *__restrict__ out, Arow arow) {
+  __syncthreads(); /* the previous level's reads of Bs are done */
+  for (int e = threadIdx.x; e < K * N; e += blockDim.x) Bs[e] = B[e];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const long w0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long nw = ((long)gridDim.x * blockDim.x) >> 5;
+  for (long r = w0; r < rows; r += nw) {
+    R acc[4] = {0, 0, 0, 0};
+    for (int k0 = 0; k0 < K; k0 += 32) {
+      const R av = (k0 + lane < K) ? *arow(r, k0 + lane) : R(0);
+      R part[4] = {0, 0, 0, 0};
+      const int kn = K - k0 < 32 ? K - k0 : 32;
+#pragma unroll 8
+      for (int kk = 0; kk < kn; ++kk) {
+        const R a = __shfl_sync(0xffffffffu, av, kk);
+        const R *bk = Bs + (k0 + kk) * N;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (lane + 32 * j < N) part[j] = fma(a, bk[lane + 32 * j], part[j]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[j] += part[j];
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (lane + 32 * j < N) out[r * N + lane + 32 * j] = acc[j];
+  }
+}
+
+/* Shared memory of the coarse kernel: the largest operator, the M2L one (5T x 2T). */
+template <typename R> static size_t coarse_smem(long T) { return sizeof(R) * 10 * (size_t)T * T; }
+
+template <typename R> __global__ void __launch_bounds__(256, 1) k_coarse(CoarseArgs<R> a) {
+  extern __shared__ __align__(16) unsigned char coarse_raw[];
+  R *Bs = reinterpret_cast<R *>(coarse_raw);
+  const long S1 = a.S1;
+  const int T = a.T;
+  for (int L = a.Lm; L >= 2; --L) { /* M2M: parent L from child pairs of L+1 */
+    const R *child = a.phi + lvl_off(L + 1, S1, T);
+    coarse_rows<R>(2 * S1 * (1L << L), 2 * T, T, a.bm2m + (long)(L - 2) * 2 * T * T, Bs,
+                   a.phi + lvl_off(L, S1, T),
+                   [=](long r, int k) { return child + r * 2 * T + k; });
+    if (!grid_barrier(a.sync, a.status)) return;
+  }
+  { /* top flip: psi_2[c] = topflp . phi_2[(c + 2) mod 4] */
+    const R *phi2 = a.phi + lvl_off(2, S1, T);
+    coarse_rows<R>(2 * S1 * 4, T, T, a.btop, Bs, a.psi + lvl_off(2, S1, T), [=](long r, int k) {
+      const long pl = r >> 2, c = r & 3;
+      return phi2 + (pl * 4 + ((c + 2) & 3)) * T + k;
+    });
+  }
+  for (int l = 3; l <= a.Ll; ++l) { /* M2L + L2L: child level l, one row per parent box */
+    if (!grid_barrier(a.sync, a.status)) return;
+    const R *psi_par = a.psi + lvl_off(l - 1, S1, T), *phi = a.phi + lvl_off(l, S1, T);
+    const int lpar = l - 1;
+    coarse_rows<R>(2 * S1 * (1L << lpar), 5 * T, 2 * T, a.bm2l + (long)(l - 3) * 10 * T * T, Bs,
+                   a.psi + lvl_off(l, S1, T), [=](long r, int k) {
+                     if (k < T) return psi_par + r * T + k;
+                     const long pl = r >> lpar, Bx = r & ((1L << lpar) - 1), mask = (2L << lpar) - 1;
+                     const long base = pl << (lpar + 1);
+                     if (k < 3 * T) return phi + (base + ((2 * Bx - 2) & mask)) * T + (k - T);
+                     return phi + (base + ((2 * Bx + 2) & mask)) * T + (k - 3 * T);
+                   });
+  }
 }
 
 /* ======================================================================== host orchestration */
@@ -1137,6 +1277,25 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
   return rc;
 }
 
+constexpr long kCoarseRows = 4096; /* default: tree levels with fewer rows form the coarse tree */
+
+/* Coarse-tree settings of a plan: threshold (FMMFFT_COARSE_ROWS overrides, 0 turns the fused
+ * kernel off) and the cooperative grid, at most two blocks per SM. */
+template <typename R> static void coarse_setup(Dev<R> *d) {
+  d->coarse_rows = kCoarseRows;
+  if (const char *ev = getenv("FMMFFT_COARSE_ROWS")) d->coarse_rows = atol(ev);
+  const size_t sm = coarse_smem<R>(d->T);
+  int dev = 0, nsm = 0, nb = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (sm <= (size_t)200 * 1024) {
+    cudaFuncSetAttribute(k_coarse<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_coarse<R>, 256, sm);
+  }
+  d->coarse_grid = nsm * (nb < 2 ? nb : 2);
+  if (d->coarse_grid < 1) d->coarse_rows = 0; /* operator too large for shared memory */
+}
+
 template <typename R>
 static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err, size_t errlen) {
   using C = typename cplx<R>::T;
@@ -1189,6 +1348,7 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
    * the default because it is faster there (M2L 0.47 ms against 0.58 ms on a B200) */
   d->tc_pipelined = 0;
   if (const char *ev = getenv("FMMFFT_TC_FORM")) d->tc_pipelined = strcmp(ev, "pipelined") == 0;
+  coarse_setup(d);
   d->fft_threads = 512;
   if (const char *ev = getenv("FMMFFT_FFT_THREADS")) {
     const int v = atoi(ev);
@@ -1230,6 +1390,7 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   CARVE(z, P * M, C)
   CARVE(tmp, P * M, C)
   CARVE(status, 1, int)
+  CARVE(sync, 64, unsigned)
   CARVE(tcs2m, 2 * sz_s2m, float)
   CARVE(tcm2m, 2 * sz_m2m, float)
   CARVE(tcm2l, 2 * sz_m2l, float)
@@ -1264,6 +1425,7 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   d->tmp = (C *)(base + off_tmp);
   d->u = (R *)(base + off_u);
   d->status = (int *)(base + off_status);
+  d->sync = (unsigned *)(base + off_sync);
   d->tc_s2m[0] = (float *)(base + off_tcs2m), d->tc_s2m[1] = d->tc_s2m[0] + sz_s2m;
   d->tc_m2m[0] = (float *)(base + off_tcm2m), d->tc_m2m[1] = d->tc_m2m[0] + sz_m2m;
   d->tc_m2l[0] = (float *)(base + off_tcm2l), d->tc_m2l[1] = d->tc_m2l[0] + sz_m2l;
@@ -1401,9 +1563,20 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
     }
     pf.launches[ST_S2M]++;
   }
-  /* 4: M2M, parent level L = n-1 .. 2 */
+  /* coarse tree: levels below the row threshold run in one cooperative launch (stage 5) */
+  long thr = d->coarse_rows;
+  if (d->tc && d->tc_min_rows < thr) thr = d->tc_min_rows; /* never take a level off the TCs */
+  const bool coarse = d->sync != nullptr && thr > 2 * S1 * 4;
+  long Lm = 1, Ll = 2;
+  if (coarse) {
+    for (long L = 2; L <= n - 1; ++L)
+      if (2 * S1 * (1L << L) < thr) Lm = L;
+    for (long l = 3; l <= n; ++l)
+      if (2 * S1 * (1L << (l - 1)) < thr) Ll = l;
+  }
+  /* 4: M2M, parent level L = n-1 .. 2 (.. Lm+1 with the coarse tree) */
   stage(ST_M2M);
-  for (long L = n - 1; L >= 2; --L) {
+  for (long L = n - 1; L >= (coarse ? Lm + 1 : 2); --L) {
     bool done = false;
     if constexpr (sizeof(R) == 4) {
       if (d->tc && d->ok_m2m && 2 * S1 * (1L << L) >= d->tc_min_rows) {
@@ -1424,17 +1597,30 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
     }
     pf.launches[ST_M2M]++;
   }
-  /* 5: top flip */
+  /* 5: top flip, or the whole coarse tree (M2M Lm..2, top flip, M2L 3..Ll) */
   stage(ST_TOP);
-  {
+  if (coarse) {
+    CoarseArgs<R> ca{d->phi, d->psi, d->bm2m, d->btop, d->bm2l, S1, (int)T, (int)Lm, (int)Ll,
+                     d->sync, d->status};
+    cudaMemsetAsync(d->sync, 0, sizeof(unsigned), st);
+    void *args[] = {(void *)&ca};
+    const cudaError_t ce = cudaLaunchCooperativeKernel((const void *)k_coarse<R>,
+                                                       dim3((unsigned)d->coarse_grid), dim3(256), args,
+                                                       coarse_smem<R>(T), st);
+    if (ce != cudaSuccess) {
+      snprintf(err, errlen, "coarse-tree launch: %s", cudaGetErrorString(ce));
+      return 3;
+    }
+    pf.launches[ST_TOP]++;
+  } else {
     ProbTop<R> pb{d->phi + lvl_off(2, S1, T), d->btop, d->psi + lvl_off(2, S1, T), 2 * S1 * 4,
                   (int)T, (int)T};
     launch_rowgemm<R>(pb, pb.rows, (int)T, 1, st);
     pf.launches[ST_TOP]++;
   }
-  /* 6: M2L + L2L, child level l = 3..n (rows = parent boxes) */
+  /* 6: M2L + L2L, child level l = 3..n (Ll+1..n with the coarse tree; rows = parent boxes) */
   stage(ST_M2L);
-  for (long l = 3; l <= n; ++l) {
+  for (long l = coarse ? Ll + 1 : 3; l <= n; ++l) {
     bool done = false;
     if constexpr (sizeof(R) == 4) {
       if (d->tc && d->ok_m2l && 2 * S1 * (1L << (l - 1)) >= d->tc_min_rows) {
@@ -1561,7 +1747,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   /* below 10 terms the FMM's own truncation at these bins exceeds FP32 resolution (3e-8 at
    * 10 terms, 5e-6 at 8), and the reference's value is the FMM one, so it is kept */
   if (sizeof(R) == 4 && T >= 10) {
-    k_block_dc<R><<<(unsigned)((P + 127) / 128), 128, 0, st>>>(d->ssum, y, M, (int)P, inverse);
+    k_block_dc<R><<<(unsigned)((P + 3) / 4), 128, 0, st>>>(d->ssum, y, M, (int)P, inverse);
     pf.launches[ST_DC]++;
   }
   if (slot >= 0) cudaEventRecord(pf.ev[slot * (ST_COUNT + 1) + ST_COUNT], st);
@@ -1801,7 +1987,7 @@ static float g_noalloc_stage[FMMK_NOALLOC_STAGE_FLOATS];
  * complex64 plan (dev_create), offsets relative to the array base. */
 struct NoallocLayout {
   size_t initch, btop, bm2m, bm2l, evalmT, evalmh, cot, pretw, twP, twM, xt, part, ssum, phi, psi,
-      u, z, tmp, end;
+      u, z, tmp, sync, end;
 };
 
 static NoallocLayout noalloc_layout(const fmm_ops64 *o, long ntile) {
@@ -1833,6 +2019,7 @@ static NoallocLayout noalloc_layout(const fmm_ops64 *o, long ntile) {
   L.u = take(sizeof(float) * 2 * S1 * M);
   L.z = take(sizeof(float2) * P * M);
   L.tmp = take(sizeof(float2) * P * M);
+  L.sync = take(64 * sizeof(unsigned));
   L.end = off;
   return L;
 }
@@ -1919,6 +2106,7 @@ extern "C" int fmmk_execute_noalloc(const fmm_ops64 *o, int reuse_ops, const voi
   d.M = o->M, d.P = o->P, d.T = o->T, d.b = o->b, d.s = o->s, d.n = o->n;
   d.N = o->M * o->P, d.S1 = o->P - 1, d.precision = 1;
   d.fft_threads = 512;
+  coarse_setup(&d);
   d.tileM = d.P >= 2048 ? 1 : 2048 / d.P;
   if (d.tileM > d.M) d.tileM = d.M;
   d.ntile = d.M / d.tileM;
@@ -1969,6 +2157,8 @@ extern "C" int fmmk_execute_noalloc(const fmm_ops64 *o, int reuse_ops, const voi
   d.u = (float *)(base + L.u);
   d.z = (float2 *)(base + L.z);
   d.tmp = (float2 *)(base + L.tmp);
+  d.sync = (unsigned *)(base + L.sync);
+  d.status = (int *)(d.sync + 48); /* the coarse-tree barrier records a timeout here */
   return dev_execute<float>(&d, d_in, d_out, st, 0, err, errlen);
 }
 
