@@ -518,6 +518,24 @@ template <> __device__ __forceinline__ void ld8<double>(const double *p, double 
   }
 }
 
+/* Two FP32 FMAs in one instruction (fma.rn.f32x2, sm_100): d = a * b + c per lane, each an
+ * IEEE fused multiply-add rounded to nearest, the same as fmaf. */
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+  float2 d;
+  asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+      "fma.rn.f32x2 rd, ra, rb, rc;\n\t"
+      "mov.b64 {%0, %1}, rd;\n\t}\n"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return d;
+}
+
+/* 16-byte vector of R (float4 / double2) for the shared-memory staging copies. */
+template <typename R> struct vec16;
+template <> struct vec16<float> { using T = float4; };
+template <> struct vec16<double> { using T = double2; };
+
 /* Shared-memory row pitch for n values: a multiple of 4 whose quarter is odd, so that rows of
  * consecutive boxes start in different 16-byte bank groups. */
 __host__ __device__ __forceinline__ long skew_pitch(long n) {
@@ -530,47 +548,84 @@ __global__ void __launch_bounds__(256) k_leaf(const R *__restrict__ psi_n, const
                                               const R *__restrict__ evalmT, const R *__restrict__ evalmh,
                                               const R *__restrict__ cot, R *__restrict__ u, long M,
                                               long s, int T, int b, int P, int NB, int e_in_smem) {
+  using V = typename vec16<R>::T;
+  constexpr int VW = 16 / sizeof(R); /* values per 16-byte vector */
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const long xp = skew_pitch(b), tp = skew_pitch(T);
   R *xw = reinterpret_cast<R *>(smem_raw); /* boxes B0-2 .. B0+NB, one row of pitch xp each */
   R *ps = xw + (long)(NB + 3) * xp;        /* psi of boxes B0-1 .. B0+NB-1, pitch tp */
   R *ct = ps + (((long)(NB + 1) * tp + 7) & ~7L); /* 4b */
-  R *eh = ct + 4 * b;                      /* T (rounded up to 8) */
+  R *cts = ct + 4 * b;                     /* 4b: cts[e] = ct[e + 1] (FP32 pairs of odd offset) */
+  R *eh = cts + 4 * b;                     /* T (rounded up to 8) */
   R *Es = eh + ((T + 7) & ~7);             /* T b when e_in_smem */
   const int pl = blockIdx.y, sc = pl / 2 + 1;
   const long B0 = (long)blockIdx.x * NB;
   const R *xs = xt + (long)(pl + 2) * M;
   const R *pp = psi_n + (long)pl * s * T;
   const R *E = evalmT + (long)(sc - 1) * T * b;
+  const R *cg = cot + (long)(sc - 1) * 4 * b;
   const bool shifted = 2 * sc >= P;
-  const int lb = __ffs(b) - 1; /* b is a power of two */
-  for (int e = threadIdx.x; e < (NB + 3) * b; e += blockDim.x)
-    xw[(long)(e >> lb) * xp + (e & (b - 1))] = xs[((B0 - 2) * b + e) & (M - 1)];
-  for (int e = threadIdx.x; e < (NB + 1) * T; e += blockDim.x) {
-    const int bx = e / T, k = e - bx * T; /* 32-bit division */
-    ps[(long)bx * tp + k] = pp[((B0 - 1 + bx) & (s - 1)) * T + k];
+  /* staging, 16 bytes per load where rows allow (b is a power of two >= 8) */
+  {
+    const int lv = __ffs(b / VW) - 1; /* vectors per x row = b / VW, a power of two */
+    for (int e = threadIdx.x; e < (NB + 3) * (b / VW); e += blockDim.x) {
+      const int row = e >> lv, c = e & ((b / VW) - 1);
+      *reinterpret_cast<V *>(xw + (long)row * xp + c * VW) =
+          *reinterpret_cast<const V *>(xs + ((B0 - 2 + row) & (s - 1)) * b + c * VW);
+    }
   }
-  for (int e = threadIdx.x; e < 4 * b; e += blockDim.x) ct[e] = cot[(long)(sc - 1) * 4 * b + e];
+  if (T % VW == 0) {
+    const int tv = T / VW;
+    for (int e = threadIdx.x; e < (NB + 1) * tv; e += blockDim.x) {
+      const int bx = e / tv, c = e - bx * tv;
+      *reinterpret_cast<V *>(ps + (long)bx * tp + c * VW) =
+          *reinterpret_cast<const V *>(pp + ((B0 - 1 + bx) & (s - 1)) * T + c * VW);
+    }
+  } else {
+    for (int e = threadIdx.x; e < (NB + 1) * T; e += blockDim.x) {
+      const int bx = e / T, k = e - bx * T; /* 32-bit division */
+      ps[(long)bx * tp + k] = pp[((B0 - 1 + bx) & (s - 1)) * T + k];
+    }
+  }
+  for (int e = threadIdx.x; e < 4 * b / VW; e += blockDim.x)
+    reinterpret_cast<V *>(ct)[e] = reinterpret_cast<const V *>(cg)[e];
+  for (int e = threadIdx.x; e < 4 * b; e += blockDim.x) cts[e] = e + 1 < 4 * b ? cg[e + 1] : R(0);
   if (shifted)
     for (int e = threadIdx.x; e < T; e += blockDim.x) eh[e] = evalmh[(long)(sc - 1) * T + e];
   if (e_in_smem)
-    for (long e = threadIdx.x; e < (long)T * b; e += blockDim.x) Es[e] = E[e];
+    for (long e = threadIdx.x; e < (long)T * b / VW; e += blockDim.x)
+      reinterpret_cast<V *>(Es)[e] = reinterpret_cast<const V *>(E)[e];
   __syncthreads();
   const R *Eu = e_in_smem ? Es : E;
   const int G = b >> 3; /* threads per box */
   for (int w = threadIdx.x; w < NB * G; w += blockDim.x) {
     const int bi = w / G, j0 = (w - bi * G) * 8;
     R acc[8];
-#pragma unroll
-    for (int t = 0; t < 8; ++t) acc[t] = R(0);
-    /* far field */
     const R *pr = ps + (long)(bi + 1) * tp;
-    for (int k = 0; k < T; ++k) {
-      R e8[8];
-      ld8<R>(Eu + (long)k * b + j0, e8);
-      const R a = pr[k];
+    if constexpr (sizeof(R) == 4) {
+      /* far field, targets paired: acc[2h], acc[2h+1] in one f32x2 FMA */
+      float2 a2[4];
 #pragma unroll
-      for (int t = 0; t < 8; ++t) acc[t] = fma(a, e8[t], acc[t]);
+      for (int h = 0; h < 4; ++h) a2[h] = make_float2(0.f, 0.f);
+      for (int k = 0; k < T; ++k) {
+        R e8[8];
+        ld8<R>(Eu + (long)k * b + j0, e8);
+        const float2 a = make_float2(pr[k], pr[k]);
+#pragma unroll
+        for (int h = 0; h < 4; ++h) a2[h] = ffma2(a, make_float2(e8[2 * h], e8[2 * h + 1]), a2[h]);
+      }
+#pragma unroll
+      for (int h = 0; h < 4; ++h) acc[2 * h] = a2[h].x, acc[2 * h + 1] = a2[h].y;
+    } else {
+#pragma unroll
+      for (int t = 0; t < 8; ++t) acc[t] = R(0);
+      for (int k = 0; k < T; ++k) {
+        R e8[8];
+        ld8<R>(Eu + (long)k * b + j0, e8);
+        const R a = pr[k];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) acc[t] = fma(a, e8[t], acc[t]);
+      }
     }
     /* near field over boxes box-1 .. box+1; each box's part is summed separately before it
      * joins the total (long windows, b up to 2048, keep their FP32 rounding small) */
@@ -578,18 +633,48 @@ __global__ void __launch_bounds__(256) k_leaf(const R *__restrict__ psi_n, const
     for (int seg = 0; seg < 3; ++seg) {
       const R *xr = xw + (long)(bi + 1 + seg) * xp; /* xw row i holds box B0 - 2 + i */
       R part[8];
+      if constexpr (sizeof(R) == 4) {
+        /* window points paired: even and odd points of target t accumulate in the two lanes
+         * of p2[t]; their weights (w[m], w[m+1]), m = 2p - t + 8, are an aligned pair of ct
+         * for even t and of the shifted copy cts for odd t */
+        float2 p2[8];
 #pragma unroll
-      for (int t = 0; t < 8; ++t) part[t] = R(0);
-      for (int q = 0; q < b; q += 8) {
-        R x8[8], w16[16];
-        const int cq = seg * b + q + b - j0; /* cot index of (point q, target j0) */
-        ld8<R>(xr + q, x8);
-        ld8<R>(ct + (cq - 8), w16);
-        ld8<R>(ct + cq, w16 + 8);
+        for (int t = 0; t < 8; ++t) p2[t] = make_float2(0.f, 0.f);
+        for (int q = 0; q < b; q += 8) {
+          R x8[8], w16[16], ws16[16];
+          const int cq = seg * b + q + b - j0; /* cot index of (point q, target j0) */
+          ld8<R>(xr + q, x8);
+          ld8<R>(ct + (cq - 8), w16);
+          ld8<R>(ct + cq, w16 + 8);
+          ld8<R>(cts + (cq - 8), ws16);
+          ld8<R>(cts + cq, ws16 + 8);
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
+          for (int pi = 0; pi < 4; ++pi) {
+            const float2 xv = make_float2(x8[2 * pi], x8[2 * pi + 1]);
 #pragma unroll
-          for (int t = 0; t < 8; ++t) part[t] = fma(x8[i], w16[i - t + 8], part[t]);
+            for (int t = 0; t < 8; ++t) {
+              const int m = 2 * pi - t + 8;
+              const float2 wv = (t & 1) ? make_float2(ws16[m - 1], ws16[m]) : make_float2(w16[m], w16[m + 1]);
+              p2[t] = ffma2(xv, wv, p2[t]);
+            }
+          }
+        }
+#pragma unroll
+        for (int t = 0; t < 8; ++t) part[t] = p2[t].x + p2[t].y;
+      } else {
+#pragma unroll
+        for (int t = 0; t < 8; ++t) part[t] = R(0);
+        for (int q = 0; q < b; q += 8) {
+          R x8[8], w16[16];
+          const int cq = seg * b + q + b - j0; /* cot index of (point q, target j0) */
+          ld8<R>(xr + q, x8);
+          ld8<R>(ct + (cq - 8), w16);
+          ld8<R>(ct + cq, w16 + 8);
+#pragma unroll
+          for (int i = 0; i < 8; ++i)
+#pragma unroll
+            for (int t = 0; t < 8; ++t) part[t] = fma(x8[i], w16[i - t + 8], part[t]);
+        }
       }
 #pragma unroll
       for (int t = 0; t < 8; ++t) acc[t] += part[t];
@@ -1678,7 +1763,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
       if (NB > s) NB = (int)s;
       const int e_in_smem = (size_t)T * b * sizeof(R) <= 16384;
       size_t sm = sizeof(R) * ((size_t)(NB + 3) * skew_pitch(b) +
-                               (((size_t)(NB + 1) * skew_pitch(T) + 7) & ~(size_t)7) + 4 * b +
+                               (((size_t)(NB + 1) * skew_pitch(T) + 7) & ~(size_t)7) + 8 * b +
                                ((T + 7) & ~7) + (e_in_smem ? (size_t)T * b : 0));
       dim3 g((unsigned)(s / NB), (unsigned)(2 * S1));
       k_leaf<R><<<g, 256, sm, st>>>(pb.psi_n, d->xt, d->evalmT, d->evalmh, d->cot, d->u, M, s,
