@@ -150,6 +150,17 @@ def stage_bytes(N, P, T, b, esz):
     }
 
 
+# DRAM bytes (read + write) per launch of the stage's kernel from one ncu capture of the bench
+# command (profiles/k_leaf_f32_N2p24_P64_T24_b32.txt, k_tc_rowgemm_TcM2L_N2p24_P64_T24_b32.txt:
+# the mean of the six tensor-core launches).  Only meaningful for the headline workload.
+TRAFFIC_PER_LAUNCH = {
+    "leaf_l2t_near": 231.463424e6 + 99.248640e6,
+    "m2l_l2l": (4.726528 + 9.371904 + 18.661632 + 37.348864 + 83.936256 + 207.177472) * 1e6 / 6,
+    "combine_dftP": 134.277376e6 + 97.344e6,
+    "sections": 134.224384e6 + 90.587648e6,
+}
+
+
 def peaks():
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
@@ -591,8 +602,11 @@ def main():
                     "ms_per_step": e2e_tot / E, "path": "fmmfft_execute_host, pinned buffers"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": (achieved / hbm) if achieved else None,
-                         "traffic": None, "peak_kind": peak_kind,
+                         "traffic": TRAFFIC_PER_LAUNCH.get(dom), "peak_kind": peak_kind,
                          "alg_bytes_per_launch": d.get("alg_bytes_per_execute", 0) / d["launches_per_execute"]},
+            # the transform as a whole against one read + one write of the vector (2 N e bytes)
+            "transform_roofline": {"alg_bytes": 2 * N * esz, "achieved_gbs": 2 * N * esz / (ms_step / 1e3) / 1e9,
+                                   "frac": 2 * N * esz / (ms_step / 1e3) / 1e9 / hbm},
             "stages": stage_tab,
             "plain_fp32_comparator": plain,
             "plain_fft_comparator": fft_cmp,
