@@ -870,9 +870,48 @@ __global__ void k_fft_pass(const typename cplx<R>::T *__restrict__ in,
  * i = t + r L/8 of sequence g factors as exp(-2 pi i g t / M) exp(-2 pi i g (L/8) r / M): one
  * gather per thread and 8 W steps in shared memory.  Shared: W*LP + L + L/16 + 1 + 8 W
  * elements; needs 16 <= L and W*L/8 <= 512; offsets within a row fit 32 bits (M <= 2^26). */
-template <typename R, bool TIN, bool TOUT>
+/* Input of a register pass: element t + r q (r < 8) of sequence g of row `row` into v[r]. */
+template <typename R> struct StridedLd { /* in + row irow + g iseq + i istr */
+  const typename cplx<R>::T *__restrict__ in;
+  long irow, iseq;
+  unsigned istr;
+  __device__ __forceinline__ void operator()(long row, unsigned g, int t, int q,
+                                             typename cplx<R>::T (&v)[8]) const {
+    const typename cplx<R>::T *sp = in + row * irow + g * iseq + t * istr;
+    const unsigned qs = (unsigned)q * istr;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) v[r] = sp[r * qs];
+  }
+};
+
+/* The combine's input: element sc of column m is x_0[m] for sc = 0, else
+ * c_sc (u_sc[m] - i S_sc / M) from the planar far+near field u (re, im planes per section). */
+template <typename R> struct CombineLd {
+  const R *__restrict__ xt, *__restrict__ u;
+  const typename cplx<R>::T *__restrict__ ssum, *__restrict__ pretw;
+  long M;
+  R invM;
+  __device__ __forceinline__ void operator()(long, unsigned m, int t, int q,
+                                             typename cplx<R>::T (&v)[8]) const {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int sc = t + r * q;
+      if (sc == 0) {
+        v[r].x = xt[m], v[r].y = xt[M + m];
+      } else {
+        const typename cplx<R>::T S = ssum[sc];
+        typename cplx<R>::T a;
+        a.x = u[(2L * (sc - 1)) * M + m] + S.y * invM;
+        a.y = u[(2L * (sc - 1) + 1) * M + m] - S.x * invM;
+        v[r] = cmul(pretw[sc], a);
+      }
+    }
+  }
+};
+
+template <typename R, bool TIN, bool TOUT, class Ld = StridedLd<R>>
 __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
-    k_fft_reg(const typename cplx<R>::T *__restrict__ in, typename cplx<R>::T *__restrict__ out,
+    k_fft_reg(const Ld ld, typename cplx<R>::T *__restrict__ out,
               const typename cplx<R>::T *__restrict__ twD, const typename cplx<R>::T *__restrict__ twP,
               FftPass fp) {
   using C = typename cplx<R>::T;
@@ -899,15 +938,10 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
   int t, w;
   if (TIN) t = tid & (q - 1), w = tid >> lq;
   else w = tid & (W - 1), t = tid >> lW;
-  const unsigned istr = (unsigned)fp.istr, ostr = (unsigned)fp.ostr;
+  const unsigned ostr = (unsigned)fp.ostr;
   const long row = blockIdx.y;
   C v[8];
-  {
-    const C *sp = in + row * fp.irow + (g0 + w) * fp.iseq + t * istr;
-    const unsigned qs = (unsigned)q * istr;
-#pragma unroll
-    for (int r = 0; r < 8; ++r) v[r] = sp[r * qs];
-  }
+  ld(row, g0 + w, t, q, v);
   C *bw = buf + w * LP;
   const int lg = __ffs(L) - 1;
   int Ns, lNs;
@@ -1021,15 +1055,16 @@ static void launch_fft_pass(const typename cplx<R>::T *in, typename cplx<R>::T *
     if (W < 1) W = 1;
     if (tin || W >= 4) {
       fp.W = W;
+      const StridedLd<R> sld{in, fp.M, fp.iseq, (unsigned)fp.istr};
       const int thr = W * (L / 8);
       const size_t sm = sizeof(C) * ((size_t)W * (L + L / 8 + 1) + L + L / 16 + 1 + 8 * W);
       dim3 g((unsigned)(per / W), (unsigned)rows);
       if (tin && tout)
-        k_fft_reg<R, true, true><<<g, thr, sm, st>>>(in, out, twM, twM, fmm_pass(fp));
+        k_fft_reg<R, true, true><<<g, thr, sm, st>>>(sld, out, twM, twM, fmm_pass(fp));
       else if (tin)
-        k_fft_reg<R, true, false><<<g, thr, sm, st>>>(in, out, twM, twM, fmm_pass(fp));
+        k_fft_reg<R, true, false><<<g, thr, sm, st>>>(sld, out, twM, twM, fmm_pass(fp));
       else
-        k_fft_reg<R, false, false><<<g, thr, sm, st>>>(in, out, twM, twM, fmm_pass(fp));
+        k_fft_reg<R, false, false><<<g, thr, sm, st>>>(sld, out, twM, twM, fmm_pass(fp));
       return;
     }
   }
@@ -1782,7 +1817,21 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   /* 8: combine -> z[P][M] */
   stage(ST_COMBINE);
   pf.launches[ST_COMBINE]++;
-  {
+  if (P >= 16 && P * M < (1L << 32)) {
+    /* register Stockham over sections, Wc columns per block, the pre-twiddle in the loader */
+    int Wc = 512 / (int)(P / 8);
+    if (Wc > 32) Wc = 32;
+    if (Wc > M) Wc = (int)M;
+    FftPass fp{};
+    fp.L = (int)P, fp.W = Wc, fp.per = (int)(M < (1L << 30) ? M : (1L << 30)), fp.M = M;
+    fp.irow = 0, fp.orow = 0, fp.oseq = 1, fp.ostr = M, fp.tws = 1;
+    fp.twiddle_post = 0, fp.conj_out = 0, fp.twmul = 1, fp.twmask = 0, fp.twbits = 0;
+    const CombineLd<R> cl{d->xt, d->u, d->ssum, d->pretw, M, R(1) / R(M)};
+    const int thr = Wc * (int)(P / 8);
+    const size_t sm = sizeof(C) * ((size_t)Wc * (P + P / 8 + 1) + P + P / 16 + 1 + 8 * (size_t)Wc);
+    k_fft_reg<R, false, false, CombineLd<R>><<<(unsigned)(M / Wc), thr, sm, st>>>(cl, d->z, d->twP,
+                                                                                  d->twP, fp);
+  } else {
     int TMc = (int)(P >= 1024 ? 1 : (1024 / P < 32 ? 1024 / P : 32));
     if (TMc > M) TMc = (int)M;
     size_t sm = 2 * sizeof(C) * (size_t)P * TMc;
@@ -1867,6 +1916,8 @@ static int set_smem_limits(void) {
   cudaFuncSetAttribute(k_fft_reg<float, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_fft_reg<float, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_fft_reg<float, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<float, false, false, CombineLd<float>>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<double, false, false, CombineLd<double>>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_fft_reg<double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_fft_reg<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_fft_reg<double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
@@ -2502,12 +2553,13 @@ static int fft_run(fmmk_fft *f, const void *in, void *out, cudaStream_t st, char
     const int thr = fp.W * (fp.L / 8);
     const size_t sm = sizeof(C) * ((size_t)fp.W * (fp.L + fp.L / 8 + 1) + fp.L + fp.L / 16 + 1 + 8 * fp.W);
     dim3 g((unsigned)(f->per[k] / fp.W), (unsigned)f->rows[k]);
+    const StridedLd<R> sld{src, fp.irow, fp.iseq, (unsigned)fp.istr};
     if (f->tin[k] && f->tout[k])
-      k_fft_reg<R, true, true><<<g, thr, sm, st>>>(src, dst, twD, twP, fp);
+      k_fft_reg<R, true, true><<<g, thr, sm, st>>>(sld, dst, twD, twP, fp);
     else if (f->tin[k])
-      k_fft_reg<R, true, false><<<g, thr, sm, st>>>(src, dst, twD, twP, fp);
+      k_fft_reg<R, true, false><<<g, thr, sm, st>>>(sld, dst, twD, twP, fp);
     else
-      k_fft_reg<R, false, false><<<g, thr, sm, st>>>(src, dst, twD, twP, fp);
+      k_fft_reg<R, false, false><<<g, thr, sm, st>>>(sld, dst, twD, twP, fp);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
