@@ -862,7 +862,7 @@ __global__ void k_fft_pass(const typename cplx<R>::T *__restrict__ in,
 /* Register-resident Stockham pass: one thread per radix-8 butterfly column (L/8 threads per
  * sequence, W sequences per block) keeps its 8 values in registers through every stage; the
  * stages exchange through ONE shared buffer laid out per sequence, buf[w*LP + i + i/8] with
- * LP = L + L/8 + 1, which keeps both thread orders below free of bank conflicts.  The first
+ * the pitch LP of fft_lp, which keeps both thread orders below free of bank conflicts.  The first
  * stage reads global memory directly and the last stage writes it directly.  Thread order:
  * along the sequence (TIN) when the input is contiguous in i, across sequences otherwise, so
  * that a warp's loads are coalesced either way; when the output wants the other order
@@ -870,6 +870,16 @@ __global__ void k_fft_pass(const typename cplx<R>::T *__restrict__ in,
  * i = t + r L/8 of sequence g factors as exp(-2 pi i g t / M) exp(-2 pi i g (L/8) r / M): one
  * gather per thread and 8 W steps in shared memory.  Shared: W*LP + L + L/16 + 1 + 8 W
  * elements; needs 16 <= L and W*L/8 <= 512; offsets within a row fit 32 bits (M <= 2^26). */
+/* Row pitch (in complex elements) of a sequence in the register pass's exchange buffer:
+ * >= L + L/8, and == 32/W (mod 16) so that a warp's W sequences x 32/W positions fall on
+ * distinct 8-byte bank slots in both thread orders (every slot hit twice: the minimum for a
+ * warp of 8-byte accesses). */
+__host__ __device__ __forceinline__ int fft_lp(int L, int W) {
+  const int base = L + L / 8;
+  const int a = W >= 2 ? (32 / W) & 15 : 1;
+  return base + ((a - base % 16) + 16) % 16;
+}
+
 /* Input of a register pass: element t + r q (r < 8) of sequence g of row `row` into v[r]. */
 template <typename R> struct StridedLd { /* in + row irow + g iseq + i istr */
   const typename cplx<R>::T *__restrict__ in;
@@ -918,7 +928,7 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int L = fp.L, W = fp.W, q = L >> 3;
   const int lq = __ffs(q) - 1, lW = __ffs(W) - 1;
-  const int LP = L + q + 1;
+  const int LP = fft_lp(L, W);
   C *buf = reinterpret_cast<C *>(smem_raw);
   C *twl = buf + W * LP;    /* exp(-2 pi i m / L) at m + m/16 */
   C *twq = twl + L + L / 16 + 1; /* 4-step twiddle steps exp(-2 pi i g q r / M), [w][r] */
@@ -1057,7 +1067,7 @@ static void launch_fft_pass(const typename cplx<R>::T *in, typename cplx<R>::T *
       fp.W = W;
       const StridedLd<R> sld{in, fp.M, fp.iseq, (unsigned)fp.istr};
       const int thr = W * (L / 8);
-      const size_t sm = sizeof(C) * ((size_t)W * (L + L / 8 + 1) + L + L / 16 + 1 + 8 * W);
+      const size_t sm = sizeof(C) * ((size_t)W * fft_lp(L, W) + L + L / 16 + 1 + 8 * W);
       dim3 g((unsigned)(per / W), (unsigned)rows);
       if (tin && tout)
         k_fft_reg<R, true, true><<<g, thr, sm, st>>>(sld, out, twM, twM, fmm_pass(fp));
@@ -1828,7 +1838,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
     fp.twiddle_post = 0, fp.conj_out = 0, fp.twmul = 1, fp.twmask = 0, fp.twbits = 0;
     const CombineLd<R> cl{d->xt, d->u, d->ssum, d->pretw, M, R(1) / R(M)};
     const int thr = Wc * (int)(P / 8);
-    const size_t sm = sizeof(C) * ((size_t)Wc * (P + P / 8 + 1) + P + P / 16 + 1 + 8 * (size_t)Wc);
+    const size_t sm = sizeof(C) * ((size_t)Wc * fft_lp((int)P, Wc) + P + P / 16 + 1 + 8 * (size_t)Wc);
     k_fft_reg<R, false, false, CombineLd<R>><<<(unsigned)(M / Wc), thr, sm, st>>>(cl, d->z, d->twP,
                                                                                   d->twP, fp);
   } else {
@@ -2551,7 +2561,7 @@ static int fft_run(fmmk_fft *f, const void *in, void *out, cudaStream_t st, char
     const C *src = (const C *)(f->src[k] == 0 ? in : (f->src[k] == 1 ? out : f->tmp));
     C *dst = (C *)(f->dst[k] == 1 ? out : f->tmp);
     const int thr = fp.W * (fp.L / 8);
-    const size_t sm = sizeof(C) * ((size_t)fp.W * (fp.L + fp.L / 8 + 1) + fp.L + fp.L / 16 + 1 + 8 * fp.W);
+    const size_t sm = sizeof(C) * ((size_t)fp.W * fft_lp(fp.L, fp.W) + fp.L + fp.L / 16 + 1 + 8 * fp.W);
     dim3 g((unsigned)(f->per[k] / fp.W), (unsigned)f->rows[k]);
     const StridedLd<R> sld{src, fp.irow, fp.iseq, (unsigned)fp.istr};
     if (f->tin[k] && f->tout[k])
