@@ -136,9 +136,11 @@ def stage_bytes(N, P, T, b, esz):
     m2l = [l for l in range(3, n + 1)]
     m2m_c = [l for l in m2m if coarse(2 * S1 * (1 << l))]
     m2l_c = [l for l in m2l if coarse(2 * S1 * (1 << (l - 1)))]
+    tile = max(1, 2048 // P)  # points per sections tile; S2M is fused there for whole boxes
+    fused = tile % b == 0 and T % 4 == 0
     return {
-        "sections": N * esz + xt_all,
-        "s2m": xt_sec + lv(n),
+        "sections": N * esz + xt_all + (lv(n) if fused else 0),
+        "s2m": 0 if fused else xt_sec + lv(n),
         "m2m": sum(lv(l + 1) + lv(l) for l in m2m if l not in m2m_c),
         "coarse_tree": sum(lv(l + 1) + lv(l) for l in m2m_c) + 2 * lv(2) +
                        sum(lv(l - 1) + lv(l) + lv(l) for l in m2l_c),

@@ -123,6 +123,7 @@ template <typename R> struct Dev {
   unsigned *sync;   /* grid barrier of the coarse-tree kernel: [0] arrivals, [32] generation */
   long coarse_rows; /* levels with fewer rows go to the coarse-tree kernel (0: none) */
   int coarse_grid;  /* its cooperative grid (blocks of 256) */
+  int fuse_s2m;     /* S2M inside the sections pass where tiles hold whole boxes */
 };
 
 /* Instantiated CUDA graphs of one plan's execute, keyed by (input, output, direction): the
@@ -149,15 +150,48 @@ __host__ __device__ __forceinline__ long lvl_off(long l, long S1, long T) {
 
 /* ======================================================================== stage 1-2 */
 
+/* Two FP32 FMAs in one instruction (fma.rn.f32x2, sm_100): d = a * b + c per lane, each an
+ * IEEE fused multiply-add rounded to nearest, the same as fmaf. */
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+  float2 d;
+  asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+      "fma.rn.f32x2 rd, ra, rb, rc;\n\t"
+      "mov.b64 {%0, %1}, rd;\n\t}\n"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return d;
+}
+
+/* 8 consecutive values into registers (16-byte loads; p 16-byte aligned). */
+template <typename R> __device__ __forceinline__ void ld8(const R *p, R *o) {
+#pragma unroll
+  for (int i = 0; i < 8; ++i) o[i] = p[i];
+}
+template <> __device__ __forceinline__ void ld8<float>(const float *p, float *o) {
+  float4 a = *reinterpret_cast<const float4 *>(p), c = *reinterpret_cast<const float4 *>(p + 4);
+  o[0] = a.x, o[1] = a.y, o[2] = a.z, o[3] = a.w, o[4] = c.x, o[5] = c.y, o[6] = c.z, o[7] = c.w;
+}
+template <> __device__ __forceinline__ void ld8<double>(const double *p, double *o) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    double2 a = *reinterpret_cast<const double2 *>(p + 2 * i);
+    o[2 * i] = a.x, o[2 * i + 1] = a.y;
+  }
+}
+
 /* Deinterleave a tile of TMt points x all P sections into planar sections and write the
- * tile's per-section sums.  x[m*P + sc] -> xt[(2 sc + ri) * M + m]. */
+ * tile's per-section sums (and, when fused, the S2M of its leaf boxes).
+ * x[m*P + sc] -> xt[(2 sc + ri) * M + m]. */
 template <typename R>
 __global__ void k_sections(const typename cplx<R>::T *__restrict__ x, R *__restrict__ xt,
                            typename cplx<R>::T *__restrict__ part, long M, int P, int TMt,
-                           int conj_in) {
+                           int conj_in, const R *__restrict__ initch, R *__restrict__ phi_n, int b,
+                           int T) {
   using C = typename cplx<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *tile = reinterpret_cast<C *>(smem_raw); /* [TMt][P + 1]: the pad spreads a column over banks */
+  R *ich = reinterpret_cast<R *>(tile + (long)TMt * (P + 1)); /* initch [b][T] when S2M is fused */
   const int PP = P + 1, lp = __ffs(P) - 1, lt = __ffs(TMt) - 1;
   const long m0 = (long)blockIdx.x * TMt;
   const int E = TMt * P;
@@ -166,6 +200,8 @@ __global__ void k_sections(const typename cplx<R>::T *__restrict__ x, R *__restr
     if (conj_in) v.y = -v.y;
     tile[(e >> lp) * PP + (e & (P - 1))] = v;
   }
+  if (phi_n != nullptr)
+    for (int e = threadIdx.x; e < b * T; e += blockDim.x) ich[e] = initch[e];
   __syncthreads();
   /* planar store: plane (2sc+ri), TMt contiguous points */
   for (int e = threadIdx.x; e < 2 * E; e += blockDim.x) {
@@ -173,12 +209,50 @@ __global__ void k_sections(const typename cplx<R>::T *__restrict__ x, R *__restr
     C v = tile[mm * PP + sc];
     xt[(long)q * M + m0 + mm] = ri ? v.y : v.x;
   }
-  /* tile sums per section, fixed order */
-  for (int sc = threadIdx.x; sc < P; sc += blockDim.x) {
-    C acc;
-    acc.x = 0, acc.y = 0;
-    for (int mm = 0; mm < TMt; ++mm) acc = cadd(acc, tile[mm * PP + sc]);
-    part[(long)blockIdx.x * P + sc] = acc;
+  /* S2M of the tile's leaf boxes (reference initmm, fmmfft.c:199-211), when the tile holds
+   * whole boxes (b | TMt) and T % 4 == 0: phi_n[(2(sc-1) + ri) s + box][k] =
+   * sum_j x_sc[box b + j] initch[j][k].  Work item: one section, 4 consecutive k, both planes;
+   * the P tile sums are extra work items, so no thread waits for another. */
+  const int T4 = T >> 2, nbox = phi_n != nullptr ? TMt / b : 0;
+  const int nitems = nbox * (P - 1) * T4;
+  for (int o = threadIdx.x; o < nitems + P; o += blockDim.x) {
+    if (o >= nitems) { /* tile sum of one section, fixed order */
+      const int sc = o - nitems;
+      C acc;
+      acc.x = 0, acc.y = 0;
+      for (int mm = 0; mm < TMt; ++mm) acc = cadd(acc, tile[mm * PP + sc]);
+      part[(long)blockIdx.x * P + sc] = acc;
+      continue;
+    }
+    const long s = M / b;
+    const int k0 = (o % T4) * 4, rest = o / T4, sc = rest % (P - 1) + 1, bx = rest / (P - 1);
+    R re[4] = {0, 0, 0, 0}, im[4] = {0, 0, 0, 0};
+    if constexpr (sizeof(R) == 4) { /* (re, im) of one point in one f32x2 FMA per weight */
+      float2 acc[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] = make_float2(0.f, 0.f);
+      for (int j = 0; j < b; ++j) {
+        const C v = tile[(bx * b + j) * PP + sc];
+        const float4 w = *reinterpret_cast<const float4 *>(ich + j * T + k0);
+        acc[0] = ffma2(v, make_float2(w.x, w.x), acc[0]);
+        acc[1] = ffma2(v, make_float2(w.y, w.y), acc[1]);
+        acc[2] = ffma2(v, make_float2(w.z, w.z), acc[2]);
+        acc[3] = ffma2(v, make_float2(w.w, w.w), acc[3]);
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) re[q] = acc[q].x, im[q] = acc[q].y;
+    } else {
+      for (int j = 0; j < b; ++j) {
+        const C v = tile[(bx * b + j) * PP + sc];
+        const R *w = ich + j * T + k0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) re[q] = fma(v.x, w[q], re[q]), im[q] = fma(v.y, w[q], im[q]);
+      }
+    }
+    const long box = m0 / b + bx;
+    R *pr = phi_n + ((2L * (sc - 1)) * s + box) * T + k0, *pi = pr + s * T;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) pr[q] = re[q], pi[q] = im[q];
   }
 }
 
@@ -502,34 +576,6 @@ __global__ void k_leaf_fix(const R *__restrict__ psi_n, const R *__restrict__ xt
  * previous box) is evaluated from box-1's local expansion (evalmh) and the window box-2..box,
  * and for sc = P/2 averaged with the in-box value, as the reference does (:771-803, :839-954).
  * Block: 256 threads, grid (boxes / NB, 2 (P-1) planes). */
-template <typename R> __device__ __forceinline__ void ld8(const R *p, R *o) {
-#pragma unroll
-  for (int i = 0; i < 8; ++i) o[i] = p[i];
-}
-template <> __device__ __forceinline__ void ld8<float>(const float *p, float *o) {
-  float4 a = *reinterpret_cast<const float4 *>(p), c = *reinterpret_cast<const float4 *>(p + 4);
-  o[0] = a.x, o[1] = a.y, o[2] = a.z, o[3] = a.w, o[4] = c.x, o[5] = c.y, o[6] = c.z, o[7] = c.w;
-}
-template <> __device__ __forceinline__ void ld8<double>(const double *p, double *o) {
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    double2 a = *reinterpret_cast<const double2 *>(p + 2 * i);
-    o[2 * i] = a.x, o[2 * i + 1] = a.y;
-  }
-}
-
-/* Two FP32 FMAs in one instruction (fma.rn.f32x2, sm_100): d = a * b + c per lane, each an
- * IEEE fused multiply-add rounded to nearest, the same as fmaf. */
-__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
-  float2 d;
-  asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
-      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
-      "fma.rn.f32x2 rd, ra, rb, rc;\n\t"
-      "mov.b64 {%0, %1}, rd;\n\t}\n"
-      : "=f"(d.x), "=f"(d.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
-  return d;
-}
 
 /* 16-byte vector of R (float4 / double2) for the shared-memory staging copies. */
 template <typename R> struct vec16;
@@ -1479,6 +1525,9 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   d->tc_pipelined = 0;
   if (const char *ev = getenv("FMMFFT_TC_FORM")) d->tc_pipelined = strcmp(ev, "pipelined") == 0;
   coarse_setup(d);
+  /* FMMFFT_FUSE_S2M=0 keeps S2M a separate stage (on the tensor cores for FP32 TC plans) */
+  d->fuse_s2m = 1;
+  if (const char *ev = getenv("FMMFFT_FUSE_S2M")) d->fuse_s2m = atoi(ev) != 0;
   d->fft_threads = 512;
   if (const char *ev = getenv("FMMFFT_FFT_THREADS")) {
     const int v = atoi(ev);
@@ -1663,18 +1712,23 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   for (int k = 0; k < ST_COUNT; ++k) pf.launches[k] = 0;
   /* 1-2: sections and their sums */
   stage(ST_SECTIONS);
+  /* S2M fused into the sections pass when tiles hold whole leaf boxes */
+  const bool s2m_fused = d->tileM % b == 0 && T % 4 == 0 && d->fuse_s2m;
   {
     int TMt = (int)d->tileM;
-    size_t sm = sizeof(C) * TMt * (P + 1);
-    k_sections<R><<<(unsigned)d->ntile, 256, sm, st>>>(x, d->xt, d->part, M, (int)P, TMt, inverse);
+    size_t sm = sizeof(C) * TMt * (P + 1) + (s2m_fused ? sizeof(R) * b * T : 0);
+    k_sections<R><<<(unsigned)d->ntile, 256, sm, st>>>(x, d->xt, d->part, M, (int)P, TMt, inverse,
+                                                        d->initch,
+                                                        s2m_fused ? d->phi + lvl_off(n, S1, T) : nullptr,
+                                                        (int)b, (int)T);
     pf.launches[ST_SECTIONS]++;
     stage(ST_SUMS);
     k_sum_sections<R><<<(unsigned)P, 256, 0, st>>>(d->part, d->ntile, (int)P, d->ssum);
     pf.launches[ST_SUMS]++;
   }
-  /* 3: S2M at level n */
+  /* 3: S2M at level n (done in stage 1 when fused) */
   stage(ST_S2M);
-  {
+  if (!s2m_fused) {
     bool done = false;
     if constexpr (sizeof(R) == 4) {
       if (d->tc && d->ok_s2m && 2 * S1 * s >= d->tc_min_rows) {

@@ -3,7 +3,7 @@
 FMMFFT_TC_MIN_ROWS=1 (set before the plans are made) sends every eligible stage, however small,
 through the tensor-core kernel so that small cases cover it; the default threshold only routes
 stages with >= 8192 rows there.  Each test runs for both kernel forms (FMMFFT_TC_FORM row and
-pipelined).  Tolerance: rel-L2 <= 1e-6 against FP64, as for FP32 plans.
+pipelined), with S2M as its own stage (FMMFFT_FUSE_S2M=0) so that it runs on the tensor cores.  Tolerance: rel-L2 <= 1e-6 against FP64, as for FP32 plans.
 """
 import os
 
@@ -33,9 +33,10 @@ def fm():
 def force_tc(request):
     """Every eligible stage on the tensor cores, in the row form (default) or the pipelined,
     warp-specialised form (FMMFFT_TC_FORM=pipelined)."""
-    saved = {k: os.environ.get(k) for k in ("FMMFFT_TC_MIN_ROWS", "FMMFFT_TC_FORM")}
+    saved = {k: os.environ.get(k) for k in ("FMMFFT_TC_MIN_ROWS", "FMMFFT_TC_FORM", "FMMFFT_FUSE_S2M")}
     os.environ["FMMFFT_TC_MIN_ROWS"] = "1"
     os.environ["FMMFFT_TC_FORM"] = request.param
+    os.environ["FMMFFT_FUSE_S2M"] = "0"  # S2M as its own tensor-core stage
     yield request.param
     for k, v in saved.items():
         if v is None:
