@@ -33,6 +33,7 @@
 #include <new>
 
 #include "fmmfft_internal.h"
+#include <cudaTypedefs.h>
 #include "fmmfft_tc.cuh"
 
 #define FMM_CUDA_TRY(call)                                                              \
@@ -119,7 +120,7 @@ template <typename R> struct Dev {
   int ok_s2m, ok_m2m, ok_m2l, ok_leaf;
   long tc_min_rows; /* stages with fewer rows use the CUDA-core kernel */
   int fft_threads;  /* threads per block of the register FFT pass (power of two, <= 512) */
-  int tc_pipelined; /* tree stages on the pipelined tensor-core kernel where it fits */
+  int tc_pipelined; /* tensor-core form of the tree stages: 0 row, 1 pipelined, 2 TMA-fed */
   unsigned *sync;   /* grid barrier of the coarse-tree kernel: [0] arrivals, [32] generation */
   long coarse_rows; /* levels with fewer rows go to the coarse-tree kernel (0: none) */
   int coarse_grid;  /* its cooperative grid (blocks of 256) */
@@ -376,6 +377,8 @@ struct TcBase {
   int batches, nchunks, clen[4], coff[4], kpad, npad, nout;
   const float *bhi, *blo;
   long bstride;
+  int yoff[4]; /* TMA-fed form: row offset of chunk c's 2-D block (chunk c of row r = row r + yoff[c]) */
+  __device__ bool wraps(int, long) const { return false; }
 };
 
 struct TcS2M : TcBase {
@@ -407,6 +410,12 @@ struct TcM2L : TcBase {
     return phi + (base + box) * T;
   }
   __device__ float *dst(long r, int) const { return out + r * 2 * T; }
+  /* chunks 1 and 2 (the neighbour pairs) wrap around within a section at its first / last
+   * parent; the TMA's 2-D block has the neighbouring section's pair there */
+  __device__ bool wraps(int c, long r) const {
+    const long Bx = r & ((1L << lpar) - 1);
+    return (c == 1 && Bx == 0) || (c == 2 && Bx == (1L << lpar) - 1);
+  }
 };
 
 struct TcLeaf : TcBase { /* batch z = section - 1; s is a power of two (log2s) */
@@ -515,6 +524,55 @@ template <class Prob> static size_t tc_smem_bytes(const Prob &pb) {
   return tc::smem_bytes(pb.kpad, pb.npad);
 }
 
+/* cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link). */
+static PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static int tried = 0;
+  if (!tried) {
+    tried = 1;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+/* 2-D FP32 tensor map: `rows` rows of `width` floats, `pitch` floats apart, read as boxes of
+ * the full width x tc::kMRows rows (no swizzle; rows outside the tensor read as zero). */
+static bool tma_map(CUtensorMap *m, const float *base, int width, long rows, long pitch) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tma_encoder();
+  if (!enc || width > 256 || (width * 4) % 16 != 0 || (pitch * 4) % 16 != 0 ||
+      ((uintptr_t)base & 15) != 0)
+    return false;
+  cuuint64_t dims[2] = {(cuuint64_t)width, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)pitch * 4};
+  cuuint32_t box[2] = {(cuuint32_t)width, (cuuint32_t)tc::kMRows};
+  cuuint32_t es[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)base, dims, strides, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+/* Tensor maps of each problem's A chunks (and their row offsets), for the TMA-fed form. */
+static bool tma_maps(TcS2M &q, tc::TmaMaps *m) {
+  q.yoff[0] = 0;
+  return tma_map(&m->m[0], q.xt + 2 * q.M, q.b, q.rows, q.b);
+}
+static bool tma_maps(TcM2M &q, tc::TmaMaps *m) {
+  q.yoff[0] = 0;
+  return tma_map(&m->m[0], q.child, 2 * q.T, q.rows, 2 * q.T);
+}
+static bool tma_maps(TcM2L &q, tc::TmaMaps *m) {
+  /* chunk 0: the parent's local expansion; chunks 1, 2: pairs of child boxes (2B-2, 2B-1) and
+   * (2B+2, 2B+3) = pair rows r - 1 and r + 1 of the child level read as pairs */
+  q.yoff[0] = 0, q.yoff[1] = -1, q.yoff[2] = 1;
+  return tma_map(&m->m[0], q.psi_par, q.T, q.rows, q.T) &&
+         tma_map(&m->m[1], q.phi, 2 * q.T, q.rows, 2 * q.T) && tma_map(&m->m[2], q.phi, 2 * q.T, q.rows, 2 * q.T);
+}
+static bool tma_maps(TcLeaf &, tc::TmaMaps *) { return false; }
+
 /* The pipelined form (tc::k_tc_rowgemm_t) takes one operator of at most 64 outputs for all
  * rows and K <= 256 within 220 KB of shared memory; everything else runs the row form. */
 template <class Prob> static bool tc_pipelined_fits(const Prob &pb) {
@@ -523,7 +581,22 @@ template <class Prob> static bool tc_pipelined_fits(const Prob &pb) {
 }
 
 template <class Prob>
-static void launch_tc(const Prob &pb, int num_sms, int *status, cudaStream_t st, int pipelined) {
+static void launch_tc(const Prob &pb0, int num_sms, int *status, cudaStream_t st, int form) {
+  Prob pb = pb0;
+  if (form == 2 && pb.batches == 1 && pb.npad <= 64 && pb.nout <= 64 && pb.kpad % 8 == 0 &&
+      pb.kpad <= 256) {
+    const int stages = tc::m_smem_bytes(pb.kpad, 4) <= (size_t)220 * 1024 ? 4 : 2;
+    tc::TmaMaps maps;
+    memset((void *)&maps, 0, sizeof maps);
+    if (tc::m_smem_bytes(pb.kpad, stages) <= (size_t)220 * 1024 && tma_maps(pb, &maps)) {
+      const long tiles = (pb.rows + tc::kMRows - 1) / tc::kMRows;
+      const int grid = (int)(tiles < num_sms ? tiles : num_sms); /* one CTA per SM: all of TMEM */
+      tc::k_tc_tma<Prob><<<grid, tc::kMThreads, tc::m_smem_bytes(pb.kpad, stages), st>>>(pb, maps, stages,
+                                                                                       status);
+      return;
+    }
+  }
+  const int pipelined = form == 1;
   if (pipelined && tc_pipelined_fits(pb)) {
     const long tiles = (pb.rows + tc::kTRows - 1) / tc::kTRows;
     const int grid = (int)(tiles < num_sms ? tiles : num_sms); /* one CTA per SM: all of TMEM */
@@ -1523,7 +1596,8 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
    * (4xTF32, rel-L2 2.4e-7 at N = 2^24, P = 64, 24 terms, against 2.7e-7); the row form stays
    * the default because it is faster there (M2L 0.47 ms against 0.58 ms on a B200) */
   d->tc_pipelined = 0;
-  if (const char *ev = getenv("FMMFFT_TC_FORM")) d->tc_pipelined = strcmp(ev, "pipelined") == 0;
+  if (const char *ev = getenv("FMMFFT_TC_FORM"))
+    d->tc_pipelined = strcmp(ev, "pipelined") == 0 ? 1 : (strcmp(ev, "tma") == 0 ? 2 : 0);
   coarse_setup(d);
   /* FMMFFT_FUSE_S2M=0 keeps S2M a separate stage (on the tensor cores for FP32 TC plans) */
   d->fuse_s2m = 1;
@@ -1998,6 +2072,9 @@ static int set_smem_limits(void) {
   allow_dyn_smem(tc::k_tc_rowgemm_t<TcS2M>, lim);
   allow_dyn_smem(tc::k_tc_rowgemm_t<TcM2M>, lim);
   allow_dyn_smem(tc::k_tc_rowgemm_t<TcM2L>, lim);
+  allow_dyn_smem(tc::k_tc_tma<TcS2M>, lim);
+  allow_dyn_smem(tc::k_tc_tma<TcM2M>, lim);
+  allow_dyn_smem(tc::k_tc_tma<TcM2L>, lim);
   done = 1;
   return 0;
 }

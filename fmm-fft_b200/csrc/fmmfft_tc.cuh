@@ -20,6 +20,7 @@
  * Waits on the mbarrier are bounded; on expiry the CTA records an error code and leaves.
  */
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -153,10 +154,12 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v) {
   for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+/* a rounded to TF32 (10 explicit mantissa bits), to nearest with ties away from zero, as FP32
+ * bits with the low 13 bits clear: half a TF32 ulp added to the magnitude bits, then the 13
+ * bits dropped (the carry moves into the exponent exactly as IEEE rounding does).  Two
+ * integer-pipe instructions instead of a conversion; finite inputs only. */
 __device__ __forceinline__ float tf32_rna(float a) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(a));
-  return __uint_as_float(r);
+  return __uint_as_float((__float_as_uint(a) + 0x1000u) & 0xFFFFE000u);
 }
 
 /* Byte offset of element (row m, column k) in a K-major no-swizzle tile whose K extent is
@@ -716,6 +719,289 @@ __global__ void __launch_bounds__(kTThreads, 1) k_tc_rowgemm_t(const __grid_cons
       if (!t_wait_time(&fin, 0)) atomicExch(status, kErrWaitTimeout);
     }
     __syncwarp();
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  if (warp == mma_warp) tmem_dealloc(tmem, 512);
+}
+
+
+/* ======================================================================== TMA-fed form */
+
+/* The pipelined form's operand arrangement (operator hi/lo stacked as M = 128, data rows as N)
+ * with the data rows brought into shared memory by the Tensor Memory Accelerator instead of
+ * per-thread loads.  Within a tile of 128 consecutive rows every A chunk is a strided 2-D block
+ * of global memory (a row of the chunk every `pitch` bytes), so one cp.async.bulk.tensor.2d per
+ * chunk per tile lands it densely in shared memory; rows outside the tensor (before the first
+ * or after the last) are zero-filled by the TMA and patched where the tree wraps around.  Roles
+ * (one CTA per SM, 17 warps):
+ *   warps 0-7  split: per 16-column slice, raw FP32 rows -> TF32 hi / lo in the K-major
+ *              no-swizzle core-matrix layout, into a ring of kMStages stages (mbarriers full /
+ *              empty); rows whose chunk wraps around within a section (Prob::wraps) are read
+ *              from global memory instead; warp 0 lane 0 also issues the TMA loads, two tiles
+ *              ahead, into two raw buffers (mbarrier rawfull with expected transaction bytes;
+ *              mbarrier rawempty, arrived by each split warp, frees a raw buffer);
+ *   warps 8-15 epilogue, as in the pipelined form (two TMEM accumulators of 128 columns);
+ *   warp 16    one thread issues the MMAs: A = the operator, resident in TMEM columns 256..
+ *              (written once per CTA), B = the data stage in shared memory, M = 128, N = 128,
+ *              K = 8, two MMAs (hi, lo data) per K step.
+ * Waits are bounded by the global timer as in the pipelined form. */
+constexpr int kMRows = 128;
+constexpr int kMKs = 16;
+constexpr int kMSplit = 8;
+constexpr int kMEpi = 8;
+constexpr int kMThreads = (kMSplit + kMEpi + 1) * 32;
+constexpr int kMMaxSteps = 16; /* K <= 256 */
+
+struct TmaMaps {
+  CUtensorMap m[4]; /* one per A chunk (64-byte aligned in the parameter space) */
+};
+
+__host__ __device__ constexpr size_t m_smem_bytes(int kpad, int stages) {
+  return (size_t)2 * kMRows * kpad * 4 + (size_t)stages * 2 * kMRows * kMKs * 4 + (size_t)2 * 32 * 64 * 4;
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;"
+               :
+               : "r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+      :
+      : "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+      : "memory");
+}
+
+template <class Prob>
+__global__ void __launch_bounds__(kMThreads, 1)
+    k_tc_tma(const __grid_constant__ Prob pb, const __grid_constant__ TmaMaps maps, int stages, int *status) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ uint64_t full[8], empty[8], dfull[2], dempty[2], rawfull[2], rawempty[2], fin;
+  __shared__ uint32_t tmem_slot;
+  __shared__ volatile int abort_flag;
+  __shared__ int lmap[kMMaxSteps][4]; /* per step and float4: chunk (low byte, 0xFF none), offset */
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int kpad = pb.kpad, nsteps = (kpad + kMKs - 1) / kMKs;
+  float *raw = reinterpret_cast<float *>(smem_raw);          /* 2 x [chunk c: 128 rows x clen] */
+  float *Xs = raw + 2 * kMRows * kpad;                        /* stage s: hi, then lo */
+  float *xch = Xs + stages * 2 * kMRows * kMKs;               /* epilogue staging */
+  const int mma_warp = kMSplit + kMEpi;
+  if (warp == mma_warp) tmem_alloc(&tmem_slot, 512);
+  if (tid == 0) {
+    for (int i = 0; i < stages; ++i) mbar_init(&full[i], kMSplit), mbar_init(&empty[i], 1);
+    for (int i = 0; i < 2; ++i)
+      mbar_init(&dfull[i], 1), mbar_init(&dempty[i], kMEpi), mbar_init(&rawfull[i], 1),
+          mbar_init(&rawempty[i], kMSplit);
+    mbar_init(&fin, 1);
+    fence_mbar_init();
+    abort_flag = 0;
+  }
+  if (tid < kMMaxSteps * 4) {
+    const int st = tid >> 2, i = tid & 3, k = st * kMKs + 4 * i;
+    int e = 0xFF;
+    if (k < kpad)
+      for (int c = 0; c < pb.nchunks; ++c)
+        if (k >= pb.coff[c] && k < pb.coff[c] + pb.clen[c]) e = c | ((k - pb.coff[c]) << 8);
+    lmap[st][i] = e;
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = tmem_slot;
+  /* the operator into TMEM columns 256 .. 256 + kpad: hi in lanes 0..npad-1, lo in 64.. */
+  if (warp >= kMSplit && warp < kMSplit + 4) {
+    const int q = warp & 3, m = q * 32 + lane;
+    const uint32_t lane_addr = (uint32_t)(q * 32) << 16;
+    for (int k = 0; k < kpad; k += 8) {
+      float v[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        float x = 0.f;
+        if (m < pb.npad) x = pb.bhi[(long)m * kpad + k + i];
+        else if (m >= 64 && m - 64 < pb.npad) x = pb.blo[(long)(m - 64) * kpad + k + i];
+        v[i] = x;
+      }
+      tmem_st8(tmem + lane_addr + 256u + (uint32_t)k, v);
+    }
+    tmem_st_wait();
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const long ntiles = (pb.rows + kMRows - 1) / kMRows;
+  uint32_t tx_bytes = 0;
+  for (int c = 0; c < pb.nchunks; ++c) tx_bytes += (uint32_t)(kMRows * pb.clen[c] * 4);
+
+  if (warp < kMSplit) {
+    /* ------------------------------------------------------------ split (+ TMA issue) */
+    const uint32_t raw0 = smem_addr(raw), xs0 = smem_addr(Xs);
+    auto issue = [&](long tile, int b) {
+      mbar_expect_tx(&rawfull[b], tx_bytes);
+      const uint32_t dst = raw0 + (uint32_t)(b * kMRows * kpad * 4);
+      for (int c = 0; c < pb.nchunks; ++c)
+        tma_load_2d(dst + (uint32_t)(kMRows * pb.coff[c] * 4), &maps.m[c], 0,
+                    (int)(tile * kMRows) + pb.yoff[c], &rawfull[b]);
+    };
+    if (tid == 0) {
+      if ((long)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+      if ((long)blockIdx.x + gridDim.x < ntiles) issue(blockIdx.x + gridDim.x, 1);
+    }
+    unsigned it = 0, tcount = 0;
+    bool ok = true;
+    for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++tcount) {
+      const int b = (int)(tcount & 1);
+      TC_CLOCK(tp);
+      if (lane == 0) ok = t_wait(&rawfull[b], (tcount >> 1) & 1, &abort_flag, status);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) break;
+      TC_PHASE(0, tp);
+      const float *rb = raw + b * kMRows * kpad;
+      for (int st = 0; st < nsteps; ++st, ++it) {
+        const int s = (int)(it % stages);
+        if (lane == 0) ok = t_wait(&empty[s], ((it / stages) & 1) ^ 1, &abort_flag, status);
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) break;
+        TC_PHASE(1, tp);
+        const uint32_t hb = xs0 + (uint32_t)(s * 2 * kMRows * kMKs * 4), lb = hb + kMRows * kMKs * 4;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const int i = tid + 256 * j, row = ((i >> 5) << 3) + ((i & 31) >> 2), k4 = i & 3;
+          const int e = lmap[st][k4], c = e & 0xFF, off = e >> 8;
+          float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (c != 0xFF) {
+            const long r = tile * kMRows + row;
+            if (r < pb.rows && pb.wraps(c, r))
+              v = __ldg(reinterpret_cast<const float4 *>(pb.src(c, r, 0) + off));
+            else
+              v = *reinterpret_cast<const float4 *>(rb + kMRows * pb.coff[c] + row * pb.clen[c] + off);
+          }
+          const float h0 = tf32_rna(v.x), h1 = tf32_rna(v.y), h2 = tf32_rna(v.z), h3 = tf32_rna(v.w);
+          const uint32_t o = core_off(row, 4 * k4, kMKs);
+          asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" : : "r"(hb + o), "f"(h0), "f"(h1),
+                       "f"(h2), "f"(h3) : "memory");
+          asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" : : "r"(lb + o), "f"(tf32_rna(v.x - h0)),
+                       "f"(tf32_rna(v.y - h1)), "f"(tf32_rna(v.z - h2)), "f"(tf32_rna(v.w - h3)) : "memory");
+        }
+        TC_PHASE(9, tp);
+        fence_smem_to_async();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&full[s]);
+        TC_PHASE(2, tp);
+      }
+      if (!ok) break;
+      /* this warp is done with raw buffer b; thread 0 refills it two tiles ahead once all
+       * eight split warps are (mbarrier rawempty, bounded wait) */
+      fence_smem_to_async();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&rawempty[b]);
+      if (tid == 0 && tile + 2L * gridDim.x < ntiles) {
+        ok = t_wait(&rawempty[b], (tcount >> 1) & 1, &abort_flag, status);
+        if (ok) issue(tile + 2L * gridDim.x, b);
+      }
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      TC_PHASE(3, tp);
+    }
+  } else if (warp < kMSplit + kMEpi) {
+    /* ------------------------------------------------------------ epilogue */
+    const int q = warp & 3, h = (warp - kMSplit) >> 2, et = tid - kMSplit * 32;
+    const uint32_t lane_addr = (uint32_t)(q * 32) << 16;
+    const int nout = pb.nout;
+    const int n = (q & 1) * 32 + lane;
+    float *stg = xch + (q >> 1) * 32 * 64;
+    unsigned tc = 0;
+    for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++tc) {
+      const int b = (int)(tc & 1);
+      bool ok = true;
+      TC_CLOCK(tp);
+      if (lane == 0) ok = t_wait(&dfull[b], (tc >> 1) & 1, &abort_flag, status);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!named_bar_and(3, kMEpi * 32, ok)) break;
+      fence_after_sync();
+      TC_PHASE(4, tp);
+      for (int ch = 0; ch < kMRows / 32; ++ch) {
+        float t[16];
+        tmem_ld16(tmem + lane_addr + (uint32_t)(b * 128 + ch * 32 + h * 16), t);
+        if (n < nout) {
+#pragma unroll
+          for (int c = 0; c < 16; ++c) stg[(h * 16 + c) * nout + n] = t[c];
+        }
+        named_bar(1, kMEpi * 32);
+        const long rb = tile * kMRows + ch * 32;
+        const long nr = pb.rows - rb < 32 ? pb.rows - rb : 32;
+        if (nr > 0) {
+          float4 *g = reinterpret_cast<float4 *>(pb.dst(rb, 0));
+          const float4 *sh = reinterpret_cast<const float4 *>(xch);
+          const float4 *sl = reinterpret_cast<const float4 *>(xch + 32 * 64);
+          const int n4 = (int)nr * nout / 4;
+          for (int i = et; i < n4; i += kMEpi * 32) {
+            const float4 x = sh[i], y = sl[i];
+            g[i] = make_float4(x.x + y.x, x.y + y.y, x.z + y.z, x.w + y.w);
+          }
+        }
+        named_bar(1, kMEpi * 32);
+      }
+      fence_before_sync();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&dempty[b]);
+      TC_PHASE(5, tp);
+    }
+  } else {
+    if (lane == 0) {
+      /* ---------------------------------------------------------- MMA issue */
+      const uint32_t idesc = make_idesc_tf32(kMRows);
+      const uint32_t xs0 = smem_addr(Xs), x_sbo = (uint32_t)kMKs * 32;
+      unsigned it = 0, tc = 0;
+      bool ok = true;
+      for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++tc) {
+        const int b = (int)(tc & 1);
+        TC_CLOCK(tp);
+        ok = t_wait(&dempty[b], ((tc >> 1) & 1) ^ 1, &abort_flag, status);
+        if (!ok) break;
+        fence_after_sync();
+        TC_PHASE(6, tp);
+        const uint32_t d = tmem + (uint32_t)(b * 128);
+        for (int st = 0; st < nsteps; ++st, ++it) {
+          const int s = (int)(it % stages);
+          ok = t_wait(&full[s], (it / stages) & 1, &abort_flag, status);
+          if (!ok) break;
+          fence_after_sync();
+          TC_PHASE(7, tp);
+          const int k0 = st * kMKs;
+          const int ksteps = ((kpad - k0) < kMKs ? (kpad - k0) : kMKs) >> 3;
+          const uint32_t hb = xs0 + (uint32_t)(s * 2 * kMRows * kMKs * 4), lb = hb + kMRows * kMKs * 4;
+          for (int kk = 0; kk < ksteps; ++kk) {
+            const uint32_t a = tmem + 256u + (uint32_t)(k0 + 8 * kk);
+            mma_tf32_ts(d, a, make_desc(hb + 256u * kk, 128, x_sbo), idesc, (st | kk) != 0);
+            mma_tf32_ts(d, a, make_desc(lb + 256u * kk, 128, x_sbo), idesc, 1);
+          }
+          mma_commit(&empty[s]);
+          TC_PHASE(8, tp);
+        }
+        if (!ok) break;
+        mma_commit(&dfull[b]);
+      }
+      mma_commit(&fin);
+      if (!t_wait_time(&fin, 0)) atomicExch(status, kErrWaitTimeout);
+    }
+    __syncwarp();
+  }
+  /* TMA loads still in flight (issued for tiles that an aborted CTA never consumed) must land
+   * before the CTA's shared memory goes away */
+  if (tid == 0) {
+    unsigned tcount = 0;
+    for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) ++tcount;
+    /* loads were issued for tiles 0 .. min(tcount, consumed + 2) - 1; wait for each buffer's
+     * last issued phase */
+    for (int b = 0; b < 2; ++b) {
+      const unsigned uses = tcount > (unsigned)b ? (tcount - 1 - b) / 2 + 1 : 0;
+      if (uses) t_wait_time(&rawfull[b], (uses - 1) & 1);
+    }
   }
   fence_before_sync();
   __syncthreads();

@@ -2,8 +2,8 @@
 
 FMMFFT_TC_MIN_ROWS=1 (set before the plans are made) sends every eligible stage, however small,
 through the tensor-core kernel so that small cases cover it; the default threshold only routes
-stages with >= 8192 rows there.  Each test runs for both kernel forms (FMMFFT_TC_FORM row and
-pipelined), with S2M as its own stage (FMMFFT_FUSE_S2M=0) so that it runs on the tensor cores.  Tolerance: rel-L2 <= 1e-6 against FP64, as for FP32 plans.
+stages with >= 8192 rows there.  Each test runs for the three kernel forms (FMMFFT_TC_FORM row,
+pipelined and tma), with S2M as its own stage (FMMFFT_FUSE_S2M=0) so that it runs on the tensor cores.  Tolerance: rel-L2 <= 1e-6 against FP64, as for FP32 plans.
 """
 import os
 
@@ -29,10 +29,10 @@ def fm():
     return fmmfft
 
 
-@pytest.fixture(params=["row", "pipelined"])
+@pytest.fixture(params=["row", "pipelined", "tma"])
 def force_tc(request):
-    """Every eligible stage on the tensor cores, in the row form (default) or the pipelined,
-    warp-specialised form (FMMFFT_TC_FORM=pipelined)."""
+    """Every eligible stage on the tensor cores, in the row form (default), the pipelined
+    warp-specialised form or the TMA-fed form (FMMFFT_TC_FORM=pipelined / tma)."""
     saved = {k: os.environ.get(k) for k in ("FMMFFT_TC_MIN_ROWS", "FMMFFT_TC_FORM", "FMMFFT_FUSE_S2M")}
     os.environ["FMMFFT_TC_MIN_ROWS"] = "1"
     os.environ["FMMFFT_TC_FORM"] = request.param
@@ -68,7 +68,7 @@ def test_tc_stagewise_vs_oracle(fm, force_tc, N, P, T, b):
     assert ol.rel_l2(y, o["y"]) < TOL
 
 
-@pytest.fixture(params=["row", "pipelined"])
+@pytest.fixture(params=["row", "pipelined", "tma"])
 def tc_form(request):
     """Default routing (stages of >= 8192 rows on the tensor cores) in either kernel form."""
     saved = os.environ.get("FMMFFT_TC_FORM")
