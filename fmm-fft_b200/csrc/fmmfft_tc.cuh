@@ -27,7 +27,6 @@
 namespace tc {
 
 constexpr int kRows = 128;         /* MMA M, rows per tile */
-constexpr long kWaitLimit = 1L << 26; /* try_wait polls before a wait is declared failed */
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -110,10 +109,18 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
+/* Waits for phase `parity` of `bar` for at most about 2 s (global timer). */
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
-  for (long i = 0; i < kWaitLimit; ++i)
+  unsigned long long t0 = 0;
+  for (unsigned it = 0;; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
-  return false;
+    if ((it & 1023) == 1023) {
+      unsigned long long now;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+      if (t0 == 0) t0 = now;
+      else if (now - t0 > 2000000000ull) return false;
+    }
+  }
 }
 
 __device__ __forceinline__ void fence_before_sync() {
@@ -367,6 +374,8 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
     }
     tile = ntile, slice = nslice;
   }
+  /* after an expired wait, give the MMAs in flight (bounded) time to finish before TMEM goes */
+  if (tid == 0 && abort_flag) mbar_wait_bounded(&mbar, phase ^ 1);
   fence_before_sync();
   __syncthreads();
   fence_after_sync();
