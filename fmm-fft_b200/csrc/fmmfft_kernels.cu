@@ -518,7 +518,7 @@ static void launch_rowgemm(const Prob &pb, long rows_per_batch, int N, int batch
   }
 }
 
-constexpr long kTcMinRows = 8192; /* default: below this a stage runs on the CUDA-core kernel */
+constexpr long kTcMinRows = 4096; /* default: below this a stage runs on the CUDA-core kernel */
 
 template <class Prob> static size_t tc_smem_bytes(const Prob &pb) {
   return tc::smem_bytes(pb.kpad, pb.npad);
@@ -1538,7 +1538,9 @@ template <typename R> static void coarse_setup(Dev<R> *d) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (sm <= (size_t)200 * 1024) {
-    cudaFuncSetAttribute(k_coarse<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    /* the attribute is the kernel's, not the plan's: always the full allowance, so that a plan
+     * with fewer terms made later does not shrink what an earlier plan's launch needs */
+    cudaFuncSetAttribute(k_coarse<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_coarse<R>, 256, sm);
   }
   d->coarse_grid = nsm * (nb < 2 ? nb : 2);
@@ -1862,9 +1864,15 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
                      d->sync, d->status};
     cudaMemsetAsync(d->sync, 0, sizeof(unsigned), st);
     void *args[] = {(void *)&ca};
-    const cudaError_t ce = cudaLaunchCooperativeKernel((const void *)k_coarse<R>,
-                                                       dim3((unsigned)d->coarse_grid), dim3(256), args,
-                                                       coarse_smem<R>(T), st);
+    /* one warp per row of the largest coarse level, 8 per block: small transforms take a few
+     * blocks and leave the rest of the GPU to concurrent work (batch branches, other streams) */
+    long maxrows = 2 * S1 * 4;
+    if (Lm >= 2 && 2 * S1 * (1L << Lm) > maxrows) maxrows = 2 * S1 * (1L << Lm);
+    if (Ll >= 3 && 2 * S1 * (1L << (Ll - 1)) > maxrows) maxrows = 2 * S1 * (1L << (Ll - 1));
+    long cgrid = (maxrows + 7) / 8;
+    if (cgrid > d->coarse_grid) cgrid = d->coarse_grid;
+    const cudaError_t ce = cudaLaunchCooperativeKernel((const void *)k_coarse<R>, dim3((unsigned)cgrid),
+                                                       dim3(256), args, coarse_smem<R>(T), st);
     if (ce != cudaSuccess) {
       snprintf(err, errlen, "coarse-tree launch: %s", cudaGetErrorString(ce));
       return 3;

@@ -2,7 +2,7 @@
 
 FMMFFT_TC_MIN_ROWS=1 (set before the plans are made) sends every eligible stage, however small,
 through the tensor-core kernel so that small cases cover it; the default threshold only routes
-stages with >= 8192 rows there.  Each test runs for the three kernel forms (FMMFFT_TC_FORM row,
+stages with >= 4096 rows there.  Each test runs for the three kernel forms (FMMFFT_TC_FORM row,
 pipelined and tma), with S2M as its own stage (FMMFFT_FUSE_S2M=0) so that it runs on the tensor cores.  Tolerance: rel-L2 <= 1e-6 against FP64, as for FP32 plans.
 """
 import os
@@ -70,7 +70,7 @@ def test_tc_stagewise_vs_oracle(fm, force_tc, N, P, T, b):
 
 @pytest.fixture(params=["row", "pipelined", "tma"])
 def tc_form(request):
-    """Default routing (stages of >= 8192 rows on the tensor cores) in either kernel form."""
+    """Default routing (stages of >= 4096 rows on the tensor cores) in either kernel form."""
     saved = os.environ.get("FMMFFT_TC_FORM")
     os.environ["FMMFFT_TC_FORM"] = request.param
     yield request.param
