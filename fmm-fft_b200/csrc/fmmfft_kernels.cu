@@ -1531,7 +1531,11 @@ constexpr long kCoarseRows = 4096; /* default: tree levels with fewer rows form 
 /* Coarse-tree settings of a plan: threshold (FMMFFT_COARSE_ROWS overrides, 0 turns the fused
  * kernel off) and the cooperative grid, at most two blocks per SM. */
 template <typename R> static void coarse_setup(Dev<R> *d) {
-  d->coarse_rows = kCoarseRows;
+  /* a cooperative launch does not overlap with other kernels, which costs more than it saves
+   * for the small transforms that batches and servers run side by side; it serves plans of
+   * N >= 2^23.  The choice depends on the plan only, so a transform gives the same bits alone,
+   * in a batch graph or in a server mix. */
+  d->coarse_rows = d->N >= (1L << 23) ? kCoarseRows : 0;
   if (const char *ev = getenv("FMMFFT_COARSE_ROWS")) d->coarse_rows = atol(ev);
   const size_t sm = coarse_smem<R>(d->T);
   int dev = 0, nsm = 0, nb = 0;

@@ -136,9 +136,9 @@ def test_repeat_runs_bitwise_deterministic(fm):
 
 def test_plan_made_before_a_smaller_one_still_runs(fm):
     """Kernel-wide launch limits set while making a plan must not depend on the plan made last:
-    a 24-term plan, then a 4-term plan, then the 24-term plan executes (the coarse-tree kernel's
-    shared memory grows with the terms)."""
-    N, P, b = 1 << 16, 16, 32
+    a 24-term plan, then a 4-term plan, then the 24-term plan executes (the coarse-tree kernel,
+    used from N = 2^23, takes shared memory that grows with the terms)."""
+    N, P, b = 1 << 23, 64, 32
     x = ol.seeded_input(N, 21)
     big = fm.Plan(N, P, 24, b, "f32")
     small = fm.Plan(N, P, 4, b, "f32")
