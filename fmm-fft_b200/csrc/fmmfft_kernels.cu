@@ -1334,57 +1334,69 @@ __device__ __forceinline__ bool grid_barrier(unsigned *sync, int *status) {
 }
 
 /* out[r][n] = sum_k A(r, k) Bs[k][n] for the rows of one level; B (K x N) is copied into the
- * shared array Bs first; arow(r, k) is the address of element k of row r's A. */
+ * shared array Bs, and each block stages 8 rows of A at a time into As (one row per warp), so a
+ * row costs one round of loads, issued together with the operator's; arow(r, k) is the address
+ * of element k of row r's A. */
 template <typename R, class Arow>
 __device__ __forceinline__ void coarse_rows(long rows, int K, int N, const R *__restrict__ B,
-                                            R *__restrict__ Bs, R *__restrict__ out, Arow arow) {
-  __syncthreads(); /* the previous level's reads of Bs are done */
+                                            R *__restrict__ Bs, R *__restrict__ As,
+                                            R *__restrict__ out, Arow arow) {
+  __syncthreads(); /* the previous level's reads of Bs and As are done */
   for (int e = threadIdx.x; e < K * N; e += blockDim.x) Bs[e] = B[e];
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const long w0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const long nw = ((long)gridDim.x * blockDim.x) >> 5;
-  for (long r = w0; r < rows; r += nw) {
-    R acc[4] = {0, 0, 0, 0};
-    for (int k0 = 0; k0 < K; k0 += 32) {
-      const R av = (k0 + lane < K) ? *arow(r, k0 + lane) : R(0);
-      R part[4] = {0, 0, 0, 0};
-      const int kn = K - k0 < 32 ? K - k0 : 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (long r0 = (long)blockIdx.x * 8; r0 < rows; r0 += (long)gridDim.x * 8) { /* block-uniform */
+    for (int e = threadIdx.x; e < 8 * K; e += blockDim.x) {
+      const int w = e / K, k = e - w * K;
+      const long r = r0 + w;
+      As[e] = r < rows ? *arow(r, k) : R(0);
+    }
+    __syncthreads();
+    const long r = r0 + warp;
+    if (r < rows) {
+      const R *ar = As + warp * K;
+      R acc[4] = {0, 0, 0, 0};
+      for (int k0 = 0; k0 < K; k0 += 32) {
+        R part[4] = {0, 0, 0, 0};
+        const int kn = K - k0 < 32 ? K - k0 : 32;
 #pragma unroll 8
-      for (int kk = 0; kk < kn; ++kk) {
-        const R a = __shfl_sync(0xffffffffu, av, kk);
-        const R *bk = Bs + (k0 + kk) * N;
+        for (int kk = 0; kk < kn; ++kk) {
+          const R a = ar[k0 + kk];
+          const R *bk = Bs + (k0 + kk) * N;
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-          if (lane + 32 * j < N) part[j] = fma(a, bk[lane + 32 * j], part[j]);
+          for (int j = 0; j < 4; ++j)
+            if (lane + 32 * j < N) part[j] = fma(a, bk[lane + 32 * j], part[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[j] += part[j];
       }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) acc[j] += part[j];
+      for (int j = 0; j < 4; ++j)
+        if (lane + 32 * j < N) out[r * N + lane + 32 * j] = acc[j];
     }
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-      if (lane + 32 * j < N) out[r * N + lane + 32 * j] = acc[j];
+    __syncthreads(); /* As is refilled next */
   }
 }
 
-/* Shared memory of the coarse kernel: the largest operator, the M2L one (5T x 2T). */
-template <typename R> static size_t coarse_smem(long T) { return sizeof(R) * 10 * (size_t)T * T; }
+/* Shared memory of the coarse kernel: the largest operator, the M2L one (5T x 2T), and 8 rows
+ * of the widest A (5T). */
+template <typename R> static size_t coarse_smem(long T) { return sizeof(R) * (10 * (size_t)T * T + 40 * (size_t)T); }
 
 template <typename R> __global__ void __launch_bounds__(256, 1) k_coarse(CoarseArgs<R> a) {
   extern __shared__ __align__(16) unsigned char coarse_raw[];
   R *Bs = reinterpret_cast<R *>(coarse_raw);
+  R *As = Bs + 10L * a.T * a.T;
   const long S1 = a.S1;
   const int T = a.T;
   for (int L = a.Lm; L >= 2; --L) { /* M2M: parent L from child pairs of L+1 */
     const R *child = a.phi + lvl_off(L + 1, S1, T);
-    coarse_rows<R>(2 * S1 * (1L << L), 2 * T, T, a.bm2m + (long)(L - 2) * 2 * T * T, Bs,
+    coarse_rows<R>(2 * S1 * (1L << L), 2 * T, T, a.bm2m + (long)(L - 2) * 2 * T * T, Bs, As,
                    a.phi + lvl_off(L, S1, T),
                    [=](long r, int k) { return child + r * 2 * T + k; });
     if (!grid_barrier(a.sync, a.status)) return;
   }
   { /* top flip: psi_2[c] = topflp . phi_2[(c + 2) mod 4] */
     const R *phi2 = a.phi + lvl_off(2, S1, T);
-    coarse_rows<R>(2 * S1 * 4, T, T, a.btop, Bs, a.psi + lvl_off(2, S1, T), [=](long r, int k) {
+    coarse_rows<R>(2 * S1 * 4, T, T, a.btop, Bs, As, a.psi + lvl_off(2, S1, T), [=](long r, int k) {
       const long pl = r >> 2, c = r & 3;
       return phi2 + (pl * 4 + ((c + 2) & 3)) * T + k;
     });
@@ -1393,7 +1405,7 @@ template <typename R> __global__ void __launch_bounds__(256, 1) k_coarse(CoarseA
     if (!grid_barrier(a.sync, a.status)) return;
     const R *psi_par = a.psi + lvl_off(l - 1, S1, T), *phi = a.phi + lvl_off(l, S1, T);
     const int lpar = l - 1;
-    coarse_rows<R>(2 * S1 * (1L << lpar), 5 * T, 2 * T, a.bm2l + (long)(l - 3) * 10 * T * T, Bs,
+    coarse_rows<R>(2 * S1 * (1L << lpar), 5 * T, 2 * T, a.bm2l + (long)(l - 3) * 10 * T * T, Bs, As,
                    a.psi + lvl_off(l, S1, T), [=](long r, int k) {
                      if (k < T) return psi_par + r * T + k;
                      const long pl = r >> lpar, Bx = r & ((1L << lpar) - 1), mask = (2L << lpar) - 1;
