@@ -3,10 +3,10 @@
  *
  * Every tree stage is D[r][0..N) = sum_k A(r, k) B[k][0..N) over many rows r (section, re/im
  * plane, box) with a small shared operator B (see fmmfft_kernels.cu).  This kernel runs that
- * contraction on the tensor cores in 3xTF32: each FP32 operand is split into a TF32 "hi" part
- * (round to nearest) and the TF32-rounded residual "lo", and D = A_hi B_hi + A_hi B_lo +
- * A_lo B_hi is accumulated in FP32 in tensor memory (TMEM).  The dropped A_lo B_lo term and the
- * rounding of the residuals leave about 2^-22 relative error per product.
+ * contraction on the tensor cores in 4xTF32: each FP32 operand is split into a TF32 "hi" part
+ * (round to nearest) and the TF32-rounded residual "lo", and the four products A_hi B_hi +
+ * A_hi B_lo + A_lo B_hi + A_lo B_lo are accumulated in FP32 in tensor memory (TMEM); the
+ * rounding of the residuals leaves about 2^-22 relative error per product.
  *
  * Per CTA (256 threads, two CTAs per SM, persistent over 128-row tiles), per K slice of up to
  * 64 columns:
@@ -194,7 +194,7 @@ __host__ __device__ constexpr size_t smem_bytes(int kpad, int npad) {
 /* Tensor-memory columns of one CTA: the accumulator (npad, rounded up to 32) plus A hi and A lo
  * of one K slice, as a power of two. */
 __host__ __device__ constexpr int tmem_cols(int kpad, int npad) {
-  int need = ((npad + 31) / 32) * 32 + 2 * (kpad < kSlice ? kpad : kSlice);
+  int need = ((2 * npad + 31) / 32) * 32 + 2 * (kpad < kSlice ? kpad : kSlice);
   return need <= 32 ? 32 : need <= 64 ? 64 : need <= 128 ? 128 : need <= 256 ? 256 : 512;
 }
 
@@ -245,9 +245,11 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
   __syncthreads();
   fence_after_sync();
   const uint32_t tmem = tmem_slot;
-  const uint32_t d_cols = (uint32_t)(((npad + 31) / 32) * 32);
+  /* accumulator columns [0, npad): A x B_hi, [npad, 2 npad): A x B_lo (B_lo follows B_hi in
+   * shared memory as the next row groups, so one descriptor of N = 2 npad covers both) */
+  const uint32_t d_cols = (uint32_t)(((2 * npad + 31) / 32) * 32);
   const uint32_t t_ahi = tmem + d_cols, t_alo = tmem + d_cols + (uint32_t)ks;
-  const uint32_t idesc = make_idesc_tf32(npad);
+  const uint32_t idesc = make_idesc_tf32(2 * npad);
   const uint32_t b_sbo = (uint32_t)kpad * 32, lbo = 128;
   const uint32_t bh = smem_addr(Bhi), bl = smem_addr(Blo);
   const int tiles_per_batch = (int)((pb.rows + kRows - 1) / kRows);
@@ -326,10 +328,10 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
         /* the last slice may extend past kpad: only its real K steps are issued */
         const int ksteps = ((k1 < kpad ? k1 : kpad) - k0) >> 3, kb = k0 >> 3;
 #pragma unroll 1
-        for (int s = 0; s < 3; ++s) {
-          uint32_t ta = (s == 2) ? t_alo : t_ahi;
+        for (int s = 0; s < 2; ++s) { /* A_hi x [B_hi; B_lo], A_lo x [B_hi; B_lo] */
+          uint32_t ta = (s == 1) ? t_alo : t_ahi;
           /* a K step of 8 TF32 is 256 bytes of B = 16 units of the descriptor's address */
-          uint64_t db = make_desc(((s == 1) ? bl : bh) + 256u * kb, lbo, b_sbo);
+          uint64_t db = make_desc(bh + 256u * kb, lbo, b_sbo);
 #pragma unroll 1
           for (int kk = 0; kk < ksteps; ++kk, ta += 8, db += 16)
             mma_tf32_ts(tmem, ta, db, idesc, (k0 | s | kk) != 0);
@@ -358,8 +360,11 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
       float *dst = (r < pb.rows) ? pb.dst(r, batch) : nullptr;
       const int cw = npad >> 1, cbeg = my_half * cw;
       for (int c0 = cbeg; c0 < cbeg + cw; c0 += 8) {
-        float t[8];
+        float t[8], tl[8];
         tmem_ld8(tmem + lane_addr + (uint32_t)c0, t);
+        tmem_ld8(tmem + lane_addr + (uint32_t)(npad + c0), tl);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) t[i] += tl[i];
         if (dst) {
           if (c0 + 8 <= pb.nout) {
             *reinterpret_cast<float4 *>(dst + c0) = make_float4(t[0], t[1], t[2], t[3]);
