@@ -196,10 +196,22 @@ __global__ void k_sections(const typename cplx<R>::T *__restrict__ x, R *__restr
   const int PP = P + 1, lp = __ffs(P) - 1, lt = __ffs(TMt) - 1;
   const long m0 = (long)blockIdx.x * TMt;
   const int E = TMt * P;
-  for (int e = threadIdx.x; e < E; e += blockDim.x) {
-    C v = x[m0 * P + e];
-    if (conj_in) v.y = -v.y;
-    tile[(e >> lp) * PP + (e & (P - 1))] = v;
+  /* loads issued 8 at a time before their stores, so their latencies overlap */
+  for (int e0 = threadIdx.x; e0 < E; e0 += 8 * blockDim.x) {
+    C v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = e0 + u * blockDim.x;
+      if (e < E) v[u] = x[m0 * P + e];
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = e0 + u * blockDim.x;
+      if (e < E) {
+        if (conj_in) v[u].y = -v[u].y;
+        tile[(e >> lp) * PP + (e & (P - 1))] = v[u];
+      }
+    }
   }
   if (phi_n != nullptr)
     for (int e = threadIdx.x; e < b * T; e += blockDim.x) ich[e] = initch[e];
@@ -663,7 +675,7 @@ __host__ __device__ __forceinline__ long skew_pitch(long n) {
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_leaf(const R *__restrict__ psi_n, const R *__restrict__ xt,
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 1) k_leaf(const R *__restrict__ psi_n, const R *__restrict__ xt,
                                               const R *__restrict__ evalmT, const R *__restrict__ evalmh,
                                               const R *__restrict__ cot, R *__restrict__ u, long M,
                                               long s, int T, int b, int P, int NB, int e_in_smem) {
@@ -687,18 +699,35 @@ __global__ void __launch_bounds__(256) k_leaf(const R *__restrict__ psi_n, const
   /* staging, 16 bytes per load where rows allow (b is a power of two >= 8) */
   {
     const int lv = __ffs(b / VW) - 1; /* vectors per x row = b / VW, a power of two */
-    for (int e = threadIdx.x; e < (NB + 3) * (b / VW); e += blockDim.x) {
-      const int row = e >> lv, c = e & ((b / VW) - 1);
-      *reinterpret_cast<V *>(xw + (long)row * xp + c * VW) =
-          *reinterpret_cast<const V *>(xs + ((B0 - 2 + row) & (s - 1)) * b + c * VW);
+    const int nx = (NB + 3) * (b / VW);
+    for (int e0 = threadIdx.x; e0 < nx; e0 += 4 * blockDim.x) { /* 4 loads in flight */
+      V v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * blockDim.x, row = e >> lv, c = e & ((b / VW) - 1);
+        if (e < nx) v[u] = *reinterpret_cast<const V *>(xs + ((B0 - 2 + row) & (s - 1)) * b + c * VW);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * blockDim.x, row = e >> lv, c = e & ((b / VW) - 1);
+        if (e < nx) *reinterpret_cast<V *>(xw + (long)row * xp + c * VW) = v[u];
+      }
     }
   }
   if (T % VW == 0) {
-    const int tv = T / VW;
-    for (int e = threadIdx.x; e < (NB + 1) * tv; e += blockDim.x) {
-      const int bx = e / tv, c = e - bx * tv;
-      *reinterpret_cast<V *>(ps + (long)bx * tp + c * VW) =
-          *reinterpret_cast<const V *>(pp + ((B0 - 1 + bx) & (s - 1)) * T + c * VW);
+    const int tv = T / VW, np_ = (NB + 1) * tv;
+    for (int e0 = threadIdx.x; e0 < np_; e0 += 4 * blockDim.x) { /* 4 loads in flight */
+      V v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * blockDim.x, bx = e / tv, c = e - bx * tv;
+        if (e < np_) v[u] = *reinterpret_cast<const V *>(pp + ((B0 - 1 + bx) & (s - 1)) * T + c * VW);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * blockDim.x, bx = e / tv, c = e - bx * tv;
+        if (e < np_) *reinterpret_cast<V *>(ps + (long)bx * tp + c * VW) = v[u];
+      }
     }
   } else {
     for (int e = threadIdx.x; e < (NB + 1) * T; e += blockDim.x) {
@@ -1342,13 +1371,28 @@ __device__ __forceinline__ void coarse_rows(long rows, int K, int N, const R *__
                                             R *__restrict__ Bs, R *__restrict__ As,
                                             R *__restrict__ out, Arow arow) {
   __syncthreads(); /* the previous level's reads of Bs and As are done */
-  for (int e = threadIdx.x; e < K * N; e += blockDim.x) Bs[e] = B[e];
+  for (int e0 = threadIdx.x; e0 < K * N; e0 += 8 * blockDim.x) { /* 8 loads in flight */
+    R v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (e0 + u * (int)blockDim.x < K * N) v[u] = B[e0 + u * blockDim.x];
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (e0 + u * (int)blockDim.x < K * N) Bs[e0 + u * blockDim.x] = v[u];
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (long r0 = (long)blockIdx.x * 8; r0 < rows; r0 += (long)gridDim.x * 8) { /* block-uniform */
-    for (int e = threadIdx.x; e < 8 * K; e += blockDim.x) {
-      const int w = e / K, k = e - w * K;
-      const long r = r0 + w;
-      As[e] = r < rows ? *arow(r, k) : R(0);
+    for (int e0 = threadIdx.x; e0 < 8 * K; e0 += 4 * blockDim.x) { /* 4 loads in flight */
+      R v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * blockDim.x, w = e / K, k = e - w * K;
+        const long r = r0 + w;
+        v[u] = (e < 8 * K && r < rows) ? *arow(r, k) : R(0);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (e0 + u * (int)blockDim.x < 8 * K) As[e0 + u * blockDim.x] = v[u];
     }
     __syncthreads();
     const long r = r0 + warp;
