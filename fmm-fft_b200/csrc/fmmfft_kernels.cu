@@ -279,7 +279,18 @@ __global__ void k_sum_sections(const typename cplx<R>::T *__restrict__ part, lon
   const int sc = blockIdx.x;
   C acc;
   acc.x = 0, acc.y = 0;
-  for (long t = threadIdx.x; t < ntile; t += blockDim.x) acc = cadd(acc, part[t * P + sc]);
+  /* loads 8 at a time, additions in the same fixed order */
+  for (long t0 = threadIdx.x; t0 < ntile; t0 += 8L * blockDim.x) {
+    C v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const long t = t0 + (long)u * blockDim.x;
+      if (t < ntile) v[u] = part[t * P + sc];
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (t0 + (long)u * blockDim.x < ntile) acc = cadd(acc, v[u]);
+  }
   red[threadIdx.x] = acc;
   __syncthreads();
   for (int w = blockDim.x / 2; w > 0; w >>= 1) {

@@ -290,11 +290,24 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
     const int k0 = slice * ks, k1 = k0 + ks;
     if (batch != cur_batch) { /* B of this batch; the previous step's MMAs have completed */
       const float *gbh = pb.bhi + (long)batch * pb.bstride, *gbl = pb.blo + (long)batch * pb.bstride;
-      for (int e = tid; e < npad * kpad; e += blockDim.x) {
-        int n = e / kpad, k = e - n * kpad;
-        uint32_t o = core_off(n, k, kpad) >> 2;
-        Bhi[o] = gbh[e];
-        Blo[o] = gbl[e];
+      const int nb = npad * kpad;
+      for (int e0 = tid; e0 < nb; e0 += 4 * (int)blockDim.x) { /* 8 loads in flight */
+        float vh[4], vl[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int e = e0 + u * blockDim.x;
+          if (e < nb) vh[u] = gbh[e], vl[u] = gbl[e];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int e = e0 + u * blockDim.x;
+          if (e < nb) {
+            const int n = e / kpad, k = e - n * kpad;
+            const uint32_t o = core_off(n, k, kpad) >> 2;
+            Bhi[o] = vh[u];
+            Blo[o] = vl[u];
+          }
+        }
       }
       fence_smem_to_async();
       cur_batch = batch;
