@@ -567,13 +567,25 @@ __global__ void __launch_bounds__(kTThreads, 1) k_tc_rowgemm_t(const __grid_cons
         if (k >= pb.coff[c] && k < pb.coff[c] + pb.clen[c]) e = c | ((k - pb.coff[c]) << 8);
     lmap[st][i] = e;
   }
-  /* operator: hi in rows 0..npad-1, lo in rows 64..64+npad-1, zero elsewhere */
-  for (int e = tid; e < 128 * kpad; e += blockDim.x) {
-    const int m = e / kpad, k = e - m * kpad;
-    float v = 0.f;
-    if (m < pb.npad) v = pb.bhi[(long)m * kpad + k];
-    else if (m >= 64 && m - 64 < pb.npad) v = pb.blo[(long)(m - 64) * kpad + k];
-    Op[core_off(m, k, kpad) >> 2] = v;
+  /* operator: hi in rows 0..npad-1, lo in rows 64..64+npad-1, zero elsewhere (loads issued
+   * 8 at a time before their stores) */
+  for (int e0 = tid; e0 < 128 * kpad; e0 += 8 * (int)blockDim.x) {
+    float v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = e0 + u * blockDim.x, m = e / kpad, k = e - m * kpad;
+      float x = 0.f;
+      if (e < 128 * kpad) {
+        if (m < pb.npad) x = pb.bhi[(long)m * kpad + k];
+        else if (m >= 64 && m - 64 < pb.npad) x = pb.blo[(long)(m - 64) * kpad + k];
+      }
+      v[u] = x;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = e0 + u * blockDim.x, m = e / kpad, k = e - m * kpad;
+      if (e < 128 * kpad) Op[core_off(m, k, kpad) >> 2] = v[u];
+    }
   }
   fence_smem_to_async();
   fence_before_sync();
@@ -845,16 +857,20 @@ __global__ void __launch_bounds__(kMThreads, 1)
   if (warp >= kMSplit && warp < kMSplit + 4) {
     const int q = warp & 3, m = q * 32 + lane;
     const uint32_t lane_addr = (uint32_t)(q * 32) << 16;
-    for (int k = 0; k < kpad; k += 8) {
-      float v[8];
+    for (int k0 = 0; k0 < kpad; k0 += 32) { /* 32 loads in flight, then four stores */
+      float v[32];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
+      for (int i = 0; i < 32; ++i) {
         float x = 0.f;
-        if (m < pb.npad) x = pb.bhi[(long)m * kpad + k + i];
-        else if (m >= 64 && m - 64 < pb.npad) x = pb.blo[(long)(m - 64) * kpad + k + i];
+        if (k0 + i < kpad) {
+          if (m < pb.npad) x = pb.bhi[(long)m * kpad + k0 + i];
+          else if (m >= 64 && m - 64 < pb.npad) x = pb.blo[(long)(m - 64) * kpad + k0 + i];
+        }
         v[i] = x;
       }
-      tmem_st8(tmem + lane_addr + 256u + (uint32_t)k, v);
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (k0 + 8 * q < kpad) tmem_st8(tmem + lane_addr + 256u + (uint32_t)(k0 + 8 * q), v + 8 * q);
     }
     tmem_st_wait();
   }
