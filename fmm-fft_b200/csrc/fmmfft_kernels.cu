@@ -226,8 +226,9 @@ __global__ void k_sections(const typename cplx<R>::T *__restrict__ x, R *__restr
    * whole boxes (b | TMt) and T % 4 == 0: phi_n[(2(sc-1) + ri) s + box][k] =
    * sum_j x_sc[box b + j] initch[j][k].  Work item: one section, 4 consecutive k, both planes;
    * the P tile sums are extra work items, so no thread waits for another. */
-  const int T4 = T >> 2, nbox = phi_n != nullptr ? TMt / b : 0;
-  const int nitems = nbox * (P - 1) * T4;
+  /* work item: sections sc, sc + 1 (sc odd; the last one alone when P - 1 is odd), 4 k */
+  const int T4 = T >> 2, nbox = phi_n != nullptr ? TMt / b : 0, npair = P / 2;
+  const int nitems = nbox * npair * T4;
   for (int o = threadIdx.x; o < nitems + P; o += blockDim.x) {
     if (o >= nitems) { /* tile sum of one section, fixed order */
       const int sc = o - nitems;
@@ -238,34 +239,53 @@ __global__ void k_sections(const typename cplx<R>::T *__restrict__ x, R *__restr
       continue;
     }
     const long s = M / b;
-    const int k0 = (o % T4) * 4, rest = o / T4, sc = rest % (P - 1) + 1, bx = rest / (P - 1);
-    R re[4] = {0, 0, 0, 0}, im[4] = {0, 0, 0, 0};
+    const int k0 = (o % T4) * 4, rest = o / T4, sc = 2 * (rest % npair) + 1, bx = rest / npair;
+    const bool two = sc + 1 <= P - 1;
+    R re[2][4] = {}, im[2][4] = {};
     if constexpr (sizeof(R) == 4) { /* (re, im) of one point in one f32x2 FMA per weight */
-      float2 acc[4];
+      float2 acc[2][4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) acc[q] = make_float2(0.f, 0.f);
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[h][q] = make_float2(0.f, 0.f);
       for (int j = 0; j < b; ++j) {
-        const C v = tile[(bx * b + j) * PP + sc];
+        const C *tr = tile + (bx * b + j) * PP + sc;
+        const C v0 = tr[0], v1 = two ? tr[1] : C{0.f, 0.f};
         const float4 w = *reinterpret_cast<const float4 *>(ich + j * T + k0);
-        acc[0] = ffma2(v, make_float2(w.x, w.x), acc[0]);
-        acc[1] = ffma2(v, make_float2(w.y, w.y), acc[1]);
-        acc[2] = ffma2(v, make_float2(w.z, w.z), acc[2]);
-        acc[3] = ffma2(v, make_float2(w.w, w.w), acc[3]);
+        const float wv[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          acc[0][q] = ffma2(v0, make_float2(wv[q], wv[q]), acc[0][q]);
+          acc[1][q] = ffma2(v1, make_float2(wv[q], wv[q]), acc[1][q]);
+        }
       }
 #pragma unroll
-      for (int q = 0; q < 4; ++q) re[q] = acc[q].x, im[q] = acc[q].y;
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) re[h][q] = acc[h][q].x, im[h][q] = acc[h][q].y;
     } else {
       for (int j = 0; j < b; ++j) {
-        const C v = tile[(bx * b + j) * PP + sc];
+        const C *tr = tile + (bx * b + j) * PP + sc;
+        const C v0 = tr[0];
+        C v1;
+        v1.x = 0, v1.y = 0;
+        if (two) v1 = tr[1];
         const R *w = ich + j * T + k0;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) re[q] = fma(v.x, w[q], re[q]), im[q] = fma(v.y, w[q], im[q]);
+        for (int q = 0; q < 4; ++q) {
+          re[0][q] = fma(v0.x, w[q], re[0][q]), im[0][q] = fma(v0.y, w[q], im[0][q]);
+          re[1][q] = fma(v1.x, w[q], re[1][q]), im[1][q] = fma(v1.y, w[q], im[1][q]);
+        }
       }
     }
     const long box = m0 / b + bx;
-    R *pr = phi_n + ((2L * (sc - 1)) * s + box) * T + k0, *pi = pr + s * T;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) pr[q] = re[q], pi[q] = im[q];
+    for (int h = 0; h < 2; ++h) {
+      if (h == 1 && !two) break;
+      R *pr = phi_n + ((2L * (sc + h - 1)) * s + box) * T + k0, *pi = pr + s * T;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) pr[q] = re[h][q], pi[q] = im[h][q];
+    }
   }
 }
 
@@ -852,8 +872,13 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 1) k_leaf(const R *_
       acc[0] = (2 * sc > P) ? v : R(0.5) * (acc[0] + v);
     }
     R *dst = u + (long)pl * M + (B0 + bi) * b + j0;
+    if constexpr (sizeof(R) == 4) { /* 32-byte aligned: b and j0 are multiples of 8 */
+      *reinterpret_cast<float4 *>(dst) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+      *reinterpret_cast<float4 *>(dst + 4) = make_float4(acc[4], acc[5], acc[6], acc[7]);
+    } else {
 #pragma unroll
-    for (int t = 0; t < 8; ++t) dst[t] = acc[t];
+      for (int t = 0; t < 8; ++t) dst[t] = acc[t];
+    }
   }
 }
 
