@@ -283,8 +283,13 @@ __global__ void k_sections(const typename cplx<R>::T *__restrict__ x, R *__restr
     for (int h = 0; h < 2; ++h) {
       if (h == 1 && !two) break;
       R *pr = phi_n + ((2L * (sc + h - 1)) * s + box) * T + k0, *pi = pr + s * T;
+      if constexpr (sizeof(R) == 4) { /* 16-byte aligned: T and k0 are multiples of 4 */
+        *reinterpret_cast<float4 *>(pr) = make_float4(re[h][0], re[h][1], re[h][2], re[h][3]);
+        *reinterpret_cast<float4 *>(pi) = make_float4(im[h][0], im[h][1], im[h][2], im[h][3]);
+      } else {
 #pragma unroll
-      for (int q = 0; q < 4; ++q) pr[q] = re[h][q], pi[q] = im[h][q];
+        for (int q = 0; q < 4; ++q) pr[q] = re[h][q], pi[q] = im[h][q];
+      }
     }
   }
 }
