@@ -2040,7 +2040,8 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
     }
     if (!done && b % 8 == 0) {
       /* direct form; it also evaluates the half-shifted first points */
-      int NB = (int)(256 / (b / 8));
+      /* boxes per block: two 8-target groups per thread for FP32, one for FP64 */
+      int NB = (int)((sizeof(R) == 4 ? 512 : 256) / (b / 8));
       if (NB < 1) NB = 1;
       if (NB > s) NB = (int)s;
       const int e_in_smem = (size_t)T * b * sizeof(R) <= 16384;
