@@ -290,7 +290,7 @@ def run_uneven_batch(a):
     line = {"metric": "Msamples/s, uneven batch of 512 transforms as one graph", "value": total / (ms / 1e3) / 1e6,
             "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": max(3, a.warmup), "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": {"f32": "fp32", "f32_tc": "fp32 (3xTF32 tcgen05)", "f64": "fp64"}[prec],
+            "dtype": {"f32": "fp32", "f32_tc": "fp32 (split-TF32 tcgen05)", "f64": "fp64"}[prec],
             "data": "synthetic", "impl": "ours",
             "config": {"workload": "uneven batch", "transforms": len(jobs), "N": "2^12..2^22 log-uniform",
                        "P": "{8,16,32,64}, M >= 256", "terms": 16, "b": 32, "graph_branches": 16,
@@ -409,7 +409,7 @@ def run_serving(a):
     line = {"metric": "Msamples/s and p99 latency, served vs plain FMM-FFT (Poisson arrivals)",
             "value": total / span_s / 1e6, "unit": UNIT, "n_gpus": 1, "steps": len(reqs),
             "warmup": 1, "ms_per_step": span_s * 1e3 / max(1, len(reqs)), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "fp32 / fp32 (3xTF32)",
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32 / fp32 (split-TF32)",
             "data": "synthetic", "impl": "ours",
             "config": {"workload": "serving", "rate_per_s": a.rate, "duration_s": a.duration,
                        "requests": len(reqs), "N": "2^10..2^24 log-uniform",
@@ -593,7 +593,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
             "warmup": max(3, a.warmup), "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": {"f32": "fp32", "f32_tc": "fp32 (3xTF32 tcgen05)", "f64": "fp64"}[prec],
+            "dtype": {"f32": "fp32", "f32_tc": "fp32 (split-TF32 tcgen05)", "f64": "fp64"}[prec],
             "data": "synthetic",
             "config": dict(cfg, precision=prec, l2="256 MB write before every timed step; "
                            "input 128 MiB > 126 MB L2", parallelism=f"replicas x{world}"),

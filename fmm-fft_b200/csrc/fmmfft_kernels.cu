@@ -1689,7 +1689,7 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   d->ok_m2m = fits(d->kp_m2m, d->np_m2m) && nlev > 0;
   d->ok_m2l = fits(d->kp_m2l, d->np_m2l) && nlev > 0;
   /* The leaf contraction multiplies inputs by near-singular cot weights (|w| ~ P/pi), and the
-   * 2^-22 split error of 3xTF32 there lifts the transform's rel-L2 from 2e-7 to 1.3e-6 at
+   * 2^-22 split error of split TF32 there lifts the transform's rel-L2 from 2e-7 to 1.3e-6 at
    * N = 2^24, P = 64, against 2e-7 when it runs in FP32; it stays on the CUDA cores unless
    * FMMFFT_TC_STAGES asks for it.  The tree stages on the tensor cores keep 2.4e-7. */
   d->ok_leaf = fits(d->kp_leaf, d->np_leaf) && getenv("FMMFFT_TC_STAGES") != NULL;

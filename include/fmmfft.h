@@ -50,7 +50,7 @@ typedef enum {
 typedef enum {
   FMMFFT_F64 = 0,     /* FP64 everywhere (the reference's precision) */
   FMMFFT_F32 = 1,     /* FP32 on CUDA cores: the plain GPU FMM-FFT */
-  FMMFFT_F32_TC = 2   /* operator contractions on tcgen05 tensor cores in 3xTF32, rest FP32 */
+  FMMFFT_F32_TC = 2   /* operator contractions on tcgen05 tensor cores in split TF32, rest FP32 */
 } fmmfft_precision;
 
 /* ------------------------------------------------------------------ reference-compatible */

@@ -1,4 +1,4 @@
-"""The 3xTF32 tcgen05 path (FMMFFT_F32_TC) against the FP64 oracle, stage by stage.
+"""The split-TF32 tcgen05 path (FMMFFT_F32_TC) against the FP64 oracle, stage by stage.
 
 FMMFFT_TC_MIN_ROWS=1 (set before the plans are made) sends every eligible stage, however small,
 through the tensor-core kernel so that small cases cover it; the default threshold only routes
@@ -15,7 +15,7 @@ from gpu_util import run_device
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-6          # the transform's output and z, against FP64
-TOL_STAGE = 1e-4    # intermediate expansions: 3xTF32 leaves ~2^-22 per product, and with few
+TOL_STAGE = 1e-4    # intermediate expansions: the TF32 split leaves ~2^-22 per product, and with few
                     # terms and wide boxes (S2M with K = b = 128) cancellation magnifies it
 
 CASES = [(4096, 4, 8, 16), (16384, 8, 12, 32), (65536, 16, 16, 32), (65536, 64, 24, 32),
