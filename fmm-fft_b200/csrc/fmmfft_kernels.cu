@@ -120,7 +120,7 @@ template <typename R> struct Dev {
   int ok_s2m, ok_m2m, ok_m2l, ok_leaf;
   long tc_min_rows; /* stages with fewer rows use the CUDA-core kernel */
   int fft_threads;  /* threads per block of the register FFT pass (power of two, <= 512) */
-  int tc_pipelined; /* tensor-core form of the tree stages: 0 row, 1 pipelined, 2 TMA-fed */
+  int tc_form; /* tensor-core form of the tree stages: 0 row, 1 pipelined, 2 TMA-fed */
   unsigned *sync;   /* grid barrier of the coarse-tree kernel: [0] arrivals, [32] generation */
   long coarse_rows; /* levels with fewer rows go to the coarse-tree kernel (0: none) */
   int coarse_grid;  /* its cooperative grid (blocks of 256) */
@@ -623,7 +623,7 @@ static bool tma_maps(TcLeaf &, tc::TmaMaps *) { return false; }
 
 /* The pipelined form (tc::k_tc_rowgemm_t) takes one operator of at most 64 outputs for all
  * rows and K <= 256 within 220 KB of shared memory; everything else runs the row form. */
-template <class Prob> static bool tc_pipelined_fits(const Prob &pb) {
+template <class Prob> static bool tc_form_fits(const Prob &pb) {
   return pb.batches == 1 && pb.npad <= 64 && pb.nout <= 64 && pb.kpad % 8 == 0 &&
          pb.kpad <= tc::kTKs * tc::kTMaxSteps && tc::t_smem_bytes(pb.kpad) <= (size_t)220 * 1024;
 }
@@ -645,7 +645,7 @@ static void launch_tc(const Prob &pb0, int num_sms, int *status, cudaStream_t st
     }
   }
   const int pipelined = form == 1;
-  if (pipelined && tc_pipelined_fits(pb)) {
+  if (pipelined && tc_form_fits(pb)) {
     const long tiles = (pb.rows + tc::kTRows - 1) / tc::kTRows;
     const int grid = (int)(tiles < num_sms ? tiles : num_sms); /* one CTA per SM: all of TMEM */
     tc::k_tc_rowgemm_t<Prob><<<grid, tc::kTThreads, tc::t_smem_bytes(pb.kpad), st>>>(pb, status);
@@ -1698,9 +1698,9 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   /* FMMFFT_TC_FORM=pipelined routes the tree stages that fit to the warp-specialised kernel
    * (4xTF32, rel-L2 2.4e-7 at N = 2^24, P = 64, 24 terms, against 2.7e-7); the row form stays
    * the default because it is faster there (M2L 0.47 ms against 0.58 ms on a B200) */
-  d->tc_pipelined = 0;
+  d->tc_form = 0;
   if (const char *ev = getenv("FMMFFT_TC_FORM"))
-    d->tc_pipelined = strcmp(ev, "pipelined") == 0 ? 1 : (strcmp(ev, "tma") == 0 ? 2 : 0);
+    d->tc_form = strcmp(ev, "pipelined") == 0 ? 1 : (strcmp(ev, "tma") == 0 ? 2 : 0);
   coarse_setup(d);
   /* FMMFFT_FUSE_S2M=0 keeps S2M a separate stage (on the tensor cores for FP32 TC plans) */
   d->fuse_s2m = 1;
@@ -1914,7 +1914,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.kpad = d->kp_s2m, q.npad = d->np_s2m, q.nout = (int)T;
         q.bhi = d->tc_s2m[0], q.blo = d->tc_s2m[1], q.bstride = 0;
         q.xt = d->xt, q.out = d->phi + lvl_off(n, S1, T), q.M = M, q.b = (int)b, q.T = (int)T;
-        launch_tc(q, d->num_sms, d->status, st, d->tc_pipelined);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form);
         done = true;
       }
     }
@@ -1947,7 +1947,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.bhi = d->tc_m2m[0] + (L - 2) * d->tc_m2m_stride, q.blo = d->tc_m2m[1] + (L - 2) * d->tc_m2m_stride;
         q.bstride = 0;
         q.child = d->phi + lvl_off(L + 1, S1, T), q.out = d->phi + lvl_off(L, S1, T), q.T = (int)T;
-        launch_tc(q, d->num_sms, d->status, st, d->tc_pipelined);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form);
         done = true;
       }
     }
@@ -2000,7 +2000,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.bstride = 0;
         q.psi_par = d->psi + lvl_off(l - 1, S1, T), q.phi = d->phi + lvl_off(l, S1, T);
         q.out = d->psi + lvl_off(l, S1, T), q.T = (int)T, q.lpar = (int)(l - 1);
-        launch_tc(q, d->num_sms, d->status, st, d->tc_pipelined);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form);
         done = true;
       }
     }
@@ -2034,7 +2034,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.bhi = d->tc_leaf[0], q.blo = d->tc_leaf[1], q.bstride = d->tc_leaf_stride;
         q.psi_n = pb.psi_n, q.xt = d->xt, q.u = d->u, q.M = M, q.s = s, q.T = (int)T, q.b = (int)b;
         q.log2s = (int)n;
-        launch_tc(q, d->num_sms, d->status, st, d->tc_pipelined);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form);
         done = true;
       }
     }

@@ -26,6 +26,12 @@
 
 namespace tc {
 
+/* Optional per-role cycle counters: empty unless a build defines them. */
+#ifndef TC_PHASE
+#define TC_CLOCK(tp)
+#define TC_PHASE(slot, tp)
+#endif
+
 constexpr int kRows = 128;         /* MMA M, rows per tile */
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
@@ -285,6 +291,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
   int tile = blockIdx.x, slice = 0;
   if (tile < ntiles) load_step(tile, 0);
   while (tile < ntiles) {
+    TC_CLOCK(tp);
     const int batch = tile / tiles_per_batch;
     const long r0 = (long)(tile - batch * tiles_per_batch) * kRows;
     const int k0 = slice * ks, k1 = k0 + ks;
@@ -312,6 +319,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
       fence_smem_to_async();
       cur_batch = batch;
     }
+    TC_PHASE(0, tp); /* operator staging */
     /* split into TF32 hi / lo and write both into this thread's TMEM lane */
     if (my_half * 32 < ks) {
       float h[32], l[32];
@@ -332,9 +340,12 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
         tmem_st8(t_alo + lane_addr + col + 8 * q, l + 8 * q);
       }
     }
+    TC_PHASE(1, tp); /* split + tcgen05.st issue */
     tmem_st_wait();
+    TC_PHASE(2, tp); /* wait::st */
     fence_before_sync();
     __syncthreads();
+    TC_PHASE(3, tp); /* barrier A */
     if (warp == 0) { /* lane 0 issues; the rest of warp 0 waits at __syncwarp */
       if (lane == 0) {
         fence_after_sync();
@@ -353,11 +364,13 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
       }
       __syncwarp();
     }
+    TC_PHASE(4, tp); /* MMA issue (warp 0) */
     /* next step: its loads go out while the MMAs (and at a tile's end the epilogue) run */
     const bool last_slice = slice == nslices - 1;
     const int ntile = last_slice ? tile + (int)gridDim.x : tile;
     const int nslice = last_slice ? 0 : slice + 1;
     if (ntile < ntiles) load_step(ntile, nslice);
+    TC_PHASE(5, tp); /* next loads issue */
     /* one thread polls the mbarrier; the other warps wait at the CTA barrier */
     if (tid == 0 && !mbar_wait_bounded(&mbar, phase)) {
       atomicExch(status, kErrWaitTimeout);
@@ -366,6 +379,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
     phase ^= 1;
     __syncthreads();
     fence_after_sync();
+    TC_PHASE(6, tp); /* MMA wait + barrier B */
     if (abort_flag) break;
     if (last_slice) {
       /* epilogue: this warp's TMEM lanes (= tile rows), columns of half (w / 4) of padded N */
@@ -389,6 +403,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
       }
       fence_before_sync();
       __syncthreads();
+      TC_PHASE(7, tp); /* epilogue */
     }
     tile = ntile, slice = nslice;
   }
@@ -532,11 +547,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-/* Optional per-role cycle counters: empty unless a build defines them. */
-#ifndef TC_PHASE
-#define TC_CLOCK(tp)
-#define TC_PHASE(slot, tp)
-#endif
 
 template <class Prob>
 __global__ void __launch_bounds__(kTThreads, 1) k_tc_rowgemm_t(const __grid_constant__ Prob pb, int *status) {
