@@ -115,6 +115,7 @@ template <typename R> struct Dev {
   float *tc_m2m[2];     /* per parent level L = 2..n-1, stride tc_m2m_stride */
   float *tc_m2l[2];     /* per child level l = 3..n, stride tc_m2l_stride */
   float *tc_leaf[2];    /* per section, stride tc_leaf_stride */
+  float *leaf_fix;      /* tensor-core leaf, section P/2: [2][s] first points from box-1 */
   long tc_m2m_stride, tc_m2l_stride, tc_leaf_stride;
   int kp_s2m, np_s2m, kp_m2m, np_m2m, kp_m2l, np_m2l, kp_leaf, np_leaf;
   int ok_s2m, ok_m2m, ok_m2l, ok_leaf;
@@ -427,6 +428,15 @@ struct TcBase {
   long bstride;
   int yoff[4]; /* TMA-fed form: row offset of chunk c's 2-D block (chunk c of row r = row r + yoff[c]) */
   __device__ bool wraps(int, long) const { return false; }
+  /* output columns c0..c0+7 of a row into dst (columns below nout; nout a multiple of 4) */
+  __device__ void put8(float *dst, long, int, int c0, const float *t) const {
+    if (c0 + 8 <= nout) {
+      *reinterpret_cast<float4 *>(dst + c0) = make_float4(t[0], t[1], t[2], t[3]);
+      *reinterpret_cast<float4 *>(dst + c0 + 4) = make_float4(t[4], t[5], t[6], t[7]);
+    } else if (c0 + 4 <= nout) {
+      *reinterpret_cast<float4 *>(dst + c0) = make_float4(t[0], t[1], t[2], t[3]);
+    }
+  }
 };
 
 struct TcS2M : TcBase {
@@ -466,11 +476,18 @@ struct TcM2L : TcBase {
   }
 };
 
+/* Leaf far field + near field of one section per batch (reference fmmfft.c:751-954).  The
+ * operator has b + 1 output columns: columns [0, b) are the box's targets; column b, for sections
+ * sc >= P/2, is the first target of the NEXT box shifted back into this one (weights evalmh and
+ * cot[0..3b), over exactly this row's A: the expansion of box B-1 and the window B-2..B), the
+ * reference's half-shifted first point (:771-803, :839-954).  For sc > P/2 that value replaces
+ * the next box's in-box first point, which is then not stored; for sc = P/2 it goes to fixbuf
+ * and k_leaf_mid averages the two. */
 struct TcLeaf : TcBase { /* batch z = section - 1; s is a power of two (log2s) */
   const float *psi_n, *xt;
-  float *u;
+  float *u, *fixbuf;
   long M, s;
-  int T, b, log2s;
+  int T, b, log2s, P;
   __device__ const float *src(int c, long r, int z) const {
     const long pl0 = 2L * z;
     if (c == 0) return psi_n + pl0 * s * T + r * T;
@@ -480,6 +497,26 @@ struct TcLeaf : TcBase { /* batch z = section - 1; s is a power of two (log2s) *
   __device__ float *dst(long r, int z) const {
     long ri = r >> log2s, bx = r & (s - 1);
     return u + (2L * z + ri) * M + bx * b;
+  }
+  __device__ void put8(float *dst, long r, int z, int c0, const float *t) const {
+    const int sc = z + 1;
+    const bool shifted = 2 * sc > P; /* the in-box first point is replaced */
+    if (c0 + 4 <= b) {
+      if (c0 == 0 && shifted) {
+        dst[1] = t[1], dst[2] = t[2], dst[3] = t[3];
+      } else {
+        *reinterpret_cast<float4 *>(dst + c0) = make_float4(t[0], t[1], t[2], t[3]);
+      }
+      if (c0 + 8 <= b) *reinterpret_cast<float4 *>(dst + c0 + 4) = make_float4(t[4], t[5], t[6], t[7]);
+    }
+    if (2 * sc >= P && c0 <= b && b < c0 + 8) { /* column b: b - c0 is 0 or 4 */
+      const float v = b == c0 ? t[0] : t[4];
+      const long ri = r >> log2s, nb = (r + 1) & (s - 1);
+      if (shifted)
+        u[(2L * z + ri) * M + nb * b] = v;
+      else
+        fixbuf[(ri << log2s) + nb] = v;
+    }
   }
 };
 
@@ -660,30 +697,54 @@ static void launch_tc(const Prob &pb0, int num_sms, int *status, cudaStream_t st
 /* First point of each leaf box for the sections whose shifted target leaves its box
  * (sc >= P/2): reference fmmfft.c:771-803 (far) and :839-954 (near).  For sc > P/2 the value
  * comes from box-1 (local expansion evalmh, window box-2..box with the cotsh offsets); for
- * sc = P/2 it is the mean of that and the in-box value the rowgemm stored. */
+ * sc = P/2 it is the mean of that and the in-box value the contraction stored.
+ * One warp per box: the lanes take the T far-field terms and the 3b window points (consecutive
+ * lanes on consecutive points, so every load is coalesced), then a warp sum.  Block: 8 warps,
+ * kFixBoxes boxes per warp, all of one section (grid y). */
+constexpr int kFixBoxes = 8;
 template <typename R>
-__global__ void k_leaf_fix(const R *__restrict__ psi_n, const R *__restrict__ xt,
-                           const R *__restrict__ evalmh, const R *__restrict__ cot,
-                           R *__restrict__ u, long M, long s, int T, int b, int P) {
+__global__ void __launch_bounds__(256) k_leaf_fix(const R *__restrict__ psi_n, const R *__restrict__ xt,
+                                                  const R *__restrict__ evalmh, const R *__restrict__ cot,
+                                                  R *__restrict__ u, long M, long s, int log2s, int T, int b,
+                                                  int P) {
   const int sc = P / 2 + blockIdx.y; /* sc in [P/2, P-1] */
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const R *eh = evalmh + (long)(sc - 1) * T;
+  const R *ct = cot + (long)(sc - 1) * 4 * b;
+  const long i0 = ((long)blockIdx.x * 8 + warp) * kFixBoxes;
+  for (int t = 0; t < kFixBoxes; ++t) {
+    const long idx = i0 + t;
+    if (idx >= 2 * s) break; /* warp-uniform */
+    const long ri = idx >> log2s, bx = idx & (s - 1);
+    const long pl = 2L * (sc - 1) + ri;
+    const R *pp = psi_n + (pl * s + ((bx - 1) & (s - 1))) * T;
+    const R *xs = xt + (pl + 2) * M;
+    R acc = 0;
+    for (int k = lane; k < T; k += 32) acc = fma(pp[k], eh[k], acc);
+    for (int q = lane; q < 3 * b; q += 32) acc = fma(xs[(bx * b - 2 * b + q) & (M - 1)], ct[q], acc);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) {
+      R *dst = u + pl * M + bx * b;
+      if (2 * sc > P)
+        *dst = acc;
+      else
+        *dst = R(0.5) * (*dst + acc);
+    }
+  }
+}
+
+/* Section sc = P/2 after the tensor-core leaf: the first point of each box is the mean of the
+ * in-box value and the value from box-1's expansion, which the contraction left in fixbuf
+ * ([2][s]; reference fmmfft.c:771-803, :839-954). */
+template <typename R>
+__global__ void k_leaf_mid(R *__restrict__ u, const float *__restrict__ fixbuf, long M, long s, int log2s, int b,
+                           int P) {
   const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= 2 * s) return;
-  const long ri = idx / s, bx = idx - ri * s;
-  const long pl = 2L * (sc - 1) + ri;
-  const R *pp = psi_n + (pl * s + ((bx - 1) & (s - 1))) * T;
-  const R *eh = evalmh + (long)(sc - 1) * T;
-  R far = 0;
-  for (int k = 0; k < T; ++k) far = fma(pp[k], eh[k], far);
-  const R *xs = xt + (pl + 2) * M;
-  const R *ct = cot + (long)(sc - 1) * 4 * b;
-  R near = 0;
-  for (int q = 0; q < 3 * b; ++q) near = fma(xs[(bx * b - 2 * b + q) & (M - 1)], ct[q], near);
-  R v = far + near;
-  R *dst = u + pl * M + bx * b;
-  if (2 * sc > P)
-    *dst = v;
-  else
-    *dst = R(0.5) * (*dst + v);
+  const long ri = idx >> log2s, bx = idx & (s - 1);
+  R *dst = u + (2L * (P / 2 - 1) + ri) * M + bx * b;
+  *dst = R(0.5) * (*dst + (R)fixbuf[idx]);
 }
 
 /* Leaf stage, direct form (b a multiple of 8): far field (L2T) plus near field of one re/im
@@ -1403,24 +1464,41 @@ __device__ __forceinline__ bool grid_barrier(unsigned *sync, int *status) {
   return gb_fail == 0;
 }
 
-/* out[r][n] = sum_k A(r, k) Bs[k][n] for the rows of one level; B (K x N) is copied into the
- * shared array Bs, and each block stages 8 rows of A at a time into As (one row per warp), so a
- * row costs one round of loads, issued together with the operator's; arow(r, k) is the address
- * of element k of row r's A. */
-template <typename R, class Arow>
-__device__ __forceinline__ void coarse_rows(long rows, int K, int N, const R *__restrict__ B,
-                                            R *__restrict__ Bs, R *__restrict__ As,
-                                            R *__restrict__ out, Arow arow) {
-  __syncthreads(); /* the previous level's reads of Bs and As are done */
-  for (int e0 = threadIdx.x; e0 < K * N; e0 += 8 * blockDim.x) { /* 8 loads in flight */
-    R v[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u)
-      if (e0 + u * (int)blockDim.x < K * N) v[u] = B[e0 + u * blockDim.x];
-#pragma unroll
-    for (int u = 0; u < 8; ++u)
-      if (e0 + u * (int)blockDim.x < K * N) Bs[e0 + u * blockDim.x] = v[u];
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+/* Issue the copy of a level's operator B (K x N, row-major) into the shared array Bs with
+ * cp.async, in 16-byte pieces where the size and address allow, else one element per copy.
+ * Nothing waits here: the level's operator does not depend on the previous level, so its copy
+ * is issued before the grid barrier and lands while the block waits there; coarse_rows waits
+ * for it.  The caller has finished reading Bs (coarse_rows ends on a block barrier). */
+template <typename R>
+__device__ __forceinline__ void coarse_stage_b(int K, int N, const R *__restrict__ B, R *__restrict__ Bs) {
+  const int n = K * N;
+  const uint32_t sb = (uint32_t)__cvta_generic_to_shared(Bs);
+  if (((size_t)n * sizeof(R)) % 16 == 0 && ((uintptr_t)B & 15) == 0) {
+    constexpr int per = 16 / sizeof(R);
+    for (int e = threadIdx.x * per; e < n; e += blockDim.x * per)
+      tc::cp_async16(sb + (uint32_t)(e * sizeof(R)), B + e);
+  } else {
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+      if constexpr (sizeof(R) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" : : "r"(sb + (uint32_t)(e * 8)), "l"(B + e) : "memory");
+      else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" : : "r"(sb + (uint32_t)(e * 4)), "l"(B + e) : "memory");
+    }
   }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+/* out[r][n] = sum_k A(r, k) Bs[k][n] for the rows of one level; B (K x N) is in flight into the
+ * shared array Bs (coarse_stage_b), and each block stages 8 rows of A at a time into As (one row
+ * per warp), so a row costs one round of loads; arow(r, k) is the address of element k of row
+ * r's A. */
+template <typename R, class Arow>
+__device__ __forceinline__ void coarse_rows(long rows, int K, int N, R *__restrict__ Bs, R *__restrict__ As,
+                                            R *__restrict__ out, Arow arow) {
+  cp_async_wait0(); /* this thread's copies of the operator */
+  __syncthreads();  /* everyone's copies; the previous level's reads of As are done */
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (long r0 = (long)blockIdx.x * 8; r0 < rows; r0 += (long)gridDim.x * 8) { /* block-uniform */
     for (int e0 = threadIdx.x; e0 < 8 * K; e0 += 4 * blockDim.x) { /* 4 loads in flight */
@@ -1472,32 +1550,48 @@ template <typename R> __global__ void __launch_bounds__(256, 1) k_coarse(CoarseA
   R *As = Bs + 10L * a.T * a.T;
   const long S1 = a.S1;
   const int T = a.T;
+  auto m2m_b = [&](int L) { return a.bm2m + (long)(L - 2) * 2 * T * T; };
+  auto m2l_b = [&](int l) { return a.bm2l + (long)(l - 3) * 10 * T * T; };
+  if (a.Lm >= 2)
+    coarse_stage_b<R>(2 * T, T, m2m_b(a.Lm), Bs);
+  else
+    coarse_stage_b<R>(T, T, a.btop, Bs);
   for (int L = a.Lm; L >= 2; --L) { /* M2M: parent L from child pairs of L+1 */
     const R *child = a.phi + lvl_off(L + 1, S1, T);
-    coarse_rows<R>(2 * S1 * (1L << L), 2 * T, T, a.bm2m + (long)(L - 2) * 2 * T * T, Bs, As,
-                   a.phi + lvl_off(L, S1, T),
+    coarse_rows<R>(2 * S1 * (1L << L), 2 * T, T, Bs, As, a.phi + lvl_off(L, S1, T),
                    [=](long r, int k) { return child + r * 2 * T + k; });
-    if (!grid_barrier(a.sync, a.status)) return;
+    if (L > 2)
+      coarse_stage_b<R>(2 * T, T, m2m_b(L - 1), Bs);
+    else
+      coarse_stage_b<R>(T, T, a.btop, Bs);
+    if (!grid_barrier(a.sync, a.status)) {
+      cp_async_wait0();
+      return;
+    }
   }
   { /* top flip: psi_2[c] = topflp . phi_2[(c + 2) mod 4] */
     const R *phi2 = a.phi + lvl_off(2, S1, T);
-    coarse_rows<R>(2 * S1 * 4, T, T, a.btop, Bs, As, a.psi + lvl_off(2, S1, T), [=](long r, int k) {
+    coarse_rows<R>(2 * S1 * 4, T, T, Bs, As, a.psi + lvl_off(2, S1, T), [=](long r, int k) {
       const long pl = r >> 2, c = r & 3;
       return phi2 + (pl * 4 + ((c + 2) & 3)) * T + k;
     });
   }
+  if (a.Ll >= 3) coarse_stage_b<R>(5 * T, 2 * T, m2l_b(3), Bs);
   for (int l = 3; l <= a.Ll; ++l) { /* M2L + L2L: child level l, one row per parent box */
-    if (!grid_barrier(a.sync, a.status)) return;
+    if (!grid_barrier(a.sync, a.status)) {
+      cp_async_wait0();
+      return;
+    }
     const R *psi_par = a.psi + lvl_off(l - 1, S1, T), *phi = a.phi + lvl_off(l, S1, T);
     const int lpar = l - 1;
-    coarse_rows<R>(2 * S1 * (1L << lpar), 5 * T, 2 * T, a.bm2l + (long)(l - 3) * 10 * T * T, Bs, As,
-                   a.psi + lvl_off(l, S1, T), [=](long r, int k) {
+    coarse_rows<R>(2 * S1 * (1L << lpar), 5 * T, 2 * T, Bs, As, a.psi + lvl_off(l, S1, T), [=](long r, int k) {
                      if (k < T) return psi_par + r * T + k;
                      const long pl = r >> lpar, Bx = r & ((1L << lpar) - 1), mask = (2L << lpar) - 1;
                      const long base = pl << (lpar + 1);
                      if (k < 3 * T) return phi + (base + ((2 * Bx - 2) & mask)) * T + (k - T);
                      return phi + (base + ((2 * Bx + 2) & mask)) * T + (k - 3 * T);
                    });
+    if (l < a.Ll) coarse_stage_b<R>(5 * T, 2 * T, m2l_b(l + 1), Bs);
   }
 }
 
@@ -1616,6 +1710,10 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
         for (long k = 0; k < T; ++k) v[j * kp + k] = o->evalm[(j * S1 + (sc - 1)) * T + k];
         for (long q = 0; q < 3 * b; ++q) v[j * kp + T + q] = ct[q + b - j];
       }
+      if (2 * sc >= P) { /* column b: the next box's half-shifted first point (TcLeaf) */
+        for (long k = 0; k < T; ++k) v[b * kp + k] = o->evalmh[(sc - P / 2) * T + k];
+        for (long q = 0; q < 3 * b; ++q) v[b * kp + T + q] = ct[q];
+      }
       rc |= tc_put(d->tc_leaf[0] + (sc - 1) * d->tc_leaf_stride, d->tc_leaf[1] + (sc - 1) * d->tc_leaf_stride,
                    v, (long)kp * np, err, errlen);
     }
@@ -1680,7 +1778,7 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   d->kp_s2m = up8(b), d->np_s2m = up16(T);
   d->kp_m2m = up8(2 * T), d->np_m2m = up16(T);
   d->kp_m2l = up8(5 * T), d->np_m2l = up16(2 * T);
-  d->kp_leaf = up8(T + 3 * b), d->np_leaf = up16(b);
+  d->kp_leaf = up8(T + 3 * b), d->np_leaf = up16(b + 1); /* + the half-shifted column */
   auto fits = [&](int kp, int np) {
     return tc && (T % 4 == 0) && (b % 4 == 0) && np <= 256 && kp <= 256 &&
            tc::smem_bytes(kp, np) <= (size_t)110 * 1024 && tc::tmem_cols(kp, np) <= 256;
@@ -1688,11 +1786,12 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   d->ok_s2m = fits(d->kp_s2m, d->np_s2m);
   d->ok_m2m = fits(d->kp_m2m, d->np_m2m) && nlev > 0;
   d->ok_m2l = fits(d->kp_m2l, d->np_m2l) && nlev > 0;
-  /* The leaf contraction multiplies inputs by near-singular cot weights (|w| ~ P/pi), and the
-   * 2^-22 split error of split TF32 there lifts the transform's rel-L2 from 2e-7 to 1.3e-6 at
-   * N = 2^24, P = 64, against 2e-7 when it runs in FP32; it stays on the CUDA cores unless
-   * FMMFFT_TC_STAGES asks for it.  The tree stages on the tensor cores keep 2.4e-7. */
-  d->ok_leaf = fits(d->kp_leaf, d->np_leaf) && getenv("FMMFFT_TC_STAGES") != NULL;
+  /* The leaf's near-field weights are near-singular (|w| ~ P/pi against O(1) sums), and the
+   * tensor core's FP32 accumulation over those cancelling sums lifts the transform's rel-L2 from
+   * 2.3e-7 (leaf on the CUDA cores) to 6.5e-7 at b = 32 (3.8e-7 at b = 8, 1.8e-7 at b = 16; the
+   * same with three TF32 parts per operand, so the split is not the cause), within the 1e-6 bar,
+   * for a 1.5x faster leaf.  FMMFFT_TC_STAGES without bit 8 keeps it on the CUDA cores. */
+  d->ok_leaf = fits(d->kp_leaf, d->np_leaf);
   d->tc_min_rows = kTcMinRows;
   if (const char *ev = getenv("FMMFFT_TC_MIN_ROWS")) d->tc_min_rows = atol(ev);
   /* FMMFFT_TC_FORM=pipelined routes the tree stages that fit to the warp-specialised kernel
@@ -1751,6 +1850,7 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   CARVE(tcm2m, 2 * sz_m2m, float)
   CARVE(tcm2l, 2 * sz_m2l, float)
   CARVE(tcleaf, 2 * sz_leaf, float)
+  CARVE(leaffix, d->ok_leaf ? 2 * s : 0, float)
 #undef CARVE
   void *pool = NULL;
   cudaError_t ce = cudaMalloc(&pool, off);
@@ -1786,6 +1886,7 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   d->tc_m2m[0] = (float *)(base + off_tcm2m), d->tc_m2m[1] = d->tc_m2m[0] + sz_m2m;
   d->tc_m2l[0] = (float *)(base + off_tcm2l), d->tc_m2l[1] = d->tc_m2l[0] + sz_m2l;
   d->tc_leaf[0] = (float *)(base + off_tcleaf), d->tc_leaf[1] = d->tc_leaf[0] + sz_leaf;
+  d->leaf_fix = (float *)(base + off_leaffix);
   cudaMemset(d->status, 0, sizeof(int));
   {
     int dev = 0;
@@ -2032,6 +2133,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.coff[0] = 0, q.coff[1] = (int)T, q.coff[2] = (int)(T + b), q.coff[3] = (int)(T + 2 * b);
         q.kpad = d->kp_leaf, q.npad = d->np_leaf, q.nout = (int)b;
         q.bhi = d->tc_leaf[0], q.blo = d->tc_leaf[1], q.bstride = d->tc_leaf_stride;
+        q.fixbuf = d->leaf_fix, q.P = (int)P;
         q.psi_n = pb.psi_n, q.xt = d->xt, q.u = d->u, q.M = M, q.s = s, q.T = (int)T, q.b = (int)b;
         q.log2s = (int)n;
         launch_tc(q, d->num_sms, d->status, st, d->tc_form);
@@ -2052,14 +2154,20 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
       k_leaf<R><<<g, 256, sm, st>>>(pb.psi_n, d->xt, d->evalmT, d->evalmh, d->cot, d->u, M, s,
                                     (int)T, (int)b, (int)P, NB, e_in_smem);
       pf.launches[ST_LEAF]++;
-    } else {
-      if (!done) launch_rowgemm<R>(pb, pb.rows, (int)b, (int)S1, st);
+    } else if (!done) {
+      launch_rowgemm<R>(pb, pb.rows, (int)b, (int)S1, st);
       pf.launches[ST_LEAF]++;
       stage(ST_LEAFFIX);
       pf.launches[ST_LEAFFIX]++;
-      dim3 g((unsigned)((2 * s + 127) / 128), (unsigned)(P - P / 2));
-      k_leaf_fix<R><<<g, 128, 0, st>>>(pb.psi_n, d->xt, d->evalmh, d->cot, d->u, M, s, (int)T,
+      dim3 g((unsigned)((2 * s + 8 * kFixBoxes - 1) / (8 * kFixBoxes)), (unsigned)(P - P / 2));
+      k_leaf_fix<R><<<g, 256, 0, st>>>(pb.psi_n, d->xt, d->evalmh, d->cot, d->u, M, s, (int)n, (int)T,
                                        (int)b, (int)P);
+    } else { /* tensor-core leaf: it stored the half-shifted points; section P/2 averages them */
+      pf.launches[ST_LEAF]++;
+      stage(ST_LEAFFIX);
+      pf.launches[ST_LEAFFIX]++;
+      k_leaf_mid<R><<<(unsigned)((2 * s + 255) / 256), 256, 0, st>>>(d->u, d->leaf_fix, M, s, (int)n, (int)b,
+                                                                      (int)P);
     }
   }
   /* 8: combine -> z[P][M] */

@@ -211,6 +211,8 @@ __host__ __device__ constexpr int tmem_cols(int kpad, int npad) {
  *   const float *bhi, *blo; long bstride;   pre-split B, [npad][kpad] per batch
  *   __device__ const float *src(int c, long r, int batch) const;
  *   __device__ float *dst(long r, int batch) const;
+ *   __device__ void put8(float *dst, long r, int batch, int c0, const float *t) const;
+ *                                     stores output columns c0..c0+7 of row r
  * A never touches shared memory: warp w, lane i owns tile row 32 (w % 4) + i (its TMEM lane)
  * and K columns [32 (w / 4), +32) of each 64-column slice; it loads them (8 float4, all issued
  * before use), splits them into TF32 hi/lo in registers and writes both into its TMEM lane with
@@ -288,9 +290,14 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
 
   int cur_batch = -1;
   uint32_t phase = 0;
-  int tile = blockIdx.x, slice = 0;
-  if (tile < ntiles) load_step(tile, 0);
-  while (tile < ntiles) {
+  /* one operator per batch: a CTA takes a contiguous run of tiles, so that it stages a new B
+   * once or twice rather than at almost every tile; one batch: tiles strided by the grid */
+  const bool runs = pb.batches > 1;
+  const int tile_end = runs ? (int)(((long)ntiles * (blockIdx.x + 1)) / gridDim.x) : ntiles;
+  const int tile_step = runs ? 1 : (int)gridDim.x;
+  int tile = runs ? (int)(((long)ntiles * blockIdx.x) / gridDim.x) : (int)blockIdx.x, slice = 0;
+  if (tile < tile_end) load_step(tile, 0);
+  while (tile < tile_end) {
     TC_CLOCK(tp);
     const int batch = tile / tiles_per_batch;
     const long r0 = (long)(tile - batch * tiles_per_batch) * kRows;
@@ -367,9 +374,9 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
     TC_PHASE(4, tp); /* MMA issue (warp 0) */
     /* next step: its loads go out while the MMAs (and at a tile's end the epilogue) run */
     const bool last_slice = slice == nslices - 1;
-    const int ntile = last_slice ? tile + (int)gridDim.x : tile;
+    const int ntile = last_slice ? tile + tile_step : tile;
     const int nslice = last_slice ? 0 : slice + 1;
-    if (ntile < ntiles) load_step(ntile, nslice);
+    if (ntile < tile_end) load_step(ntile, nslice);
     TC_PHASE(5, tp); /* next loads issue */
     /* one thread polls the mbarrier; the other warps wait at the CTA barrier */
     if (tid == 0 && !mbar_wait_bounded(&mbar, phase)) {
@@ -392,14 +399,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
         tmem_ld8(tmem + lane_addr + (uint32_t)(npad + c0), tl);
 #pragma unroll
         for (int i = 0; i < 8; ++i) t[i] += tl[i];
-        if (dst) {
-          if (c0 + 8 <= pb.nout) {
-            *reinterpret_cast<float4 *>(dst + c0) = make_float4(t[0], t[1], t[2], t[3]);
-            *reinterpret_cast<float4 *>(dst + c0 + 4) = make_float4(t[4], t[5], t[6], t[7]);
-          } else if (c0 + 4 <= pb.nout) {
-            *reinterpret_cast<float4 *>(dst + c0) = make_float4(t[0], t[1], t[2], t[3]);
-          }
-        }
+        if (dst) pb.put8(dst, r, batch, c0, t);
       }
       fence_before_sync();
       __syncthreads();

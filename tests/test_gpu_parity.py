@@ -146,3 +146,24 @@ def test_plan_made_before_a_smaller_one_still_runs(fm):
     assert ol.rel_l2(y, np.fft.fft(x)) < TOL_F32
     y2 = run_device(small, x)
     assert np.all(np.isfinite(y2))
+
+
+COARSE_CASES = [(4096, 16, 10, 16), (32768, 8, 7, 32), (65536, 32, 12, 16), (131072, 4, 9, 16)]
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("N,P,T,b", COARSE_CASES)
+def test_coarse_tree_kernel_forced(fm, monkeypatch, N, P, T, b, prec):
+    """Every tree level in the cooperative coarse-tree kernel (FMMFFT_COARSE_ROWS above every
+    level's row count; read when the plan is made).  The level operators are prefetched into
+    shared memory across the grid barriers: in 16-byte pieces for even T, one element per copy
+    for odd T.  Same tolerances as the plans' own paths."""
+    monkeypatch.setenv("FMMFFT_COARSE_ROWS", str(1 << 40))
+    x = ol.seeded_input(N, N + 3 * P)
+    o = ol.forward_ex(x, P, T, b)
+    plan = fm.Plan(N, P, T, b, prec)
+    plan.profile_start(1)
+    y = run_device(plan, x)
+    _, stages = plan.profile_stop()
+    assert stages["coarse_tree"][1] == 1, stages
+    assert ol.rel_l2(y, o["y"]) < (TOL_F64 if prec == "f64" else TOL_F32)

@@ -100,3 +100,46 @@ def test_tc_matches_plain_f32(fm):
     y2 = run_device(plan, x)
     plan.check()
     assert ol.rel_l2(y2, y1) < TOL
+
+
+LEAF_CASES = [(4096, 4, 8, 16), (16384, 8, 12, 32), (65536, 16, 16, 32), (65536, 64, 24, 32),
+              (1 << 18, 32, 24, 16), (1 << 18, 256, 12, 16), (1 << 20, 128, 24, 32), (1 << 20, 1024, 16, 8)]
+
+
+@pytest.mark.parametrize("N,P,T,b", LEAF_CASES)
+def test_tc_leaf_with_half_shift_column(fm, monkeypatch, N, P, T, b):
+    """The leaf contraction on the tensor cores at every size (FMMFFT_TC_MIN_ROWS=1, read when
+    the plan is made).  Its operator carries one extra output column, the next box's
+    half-shifted first point for sections sc >= P/2, which the epilogue stores in place of the
+    in-box value (sc > P/2) or leaves for the sc = P/2 mean; the half-shift stage is then that
+    mean alone.  The near-field weights grow like P/pi against O(1) sums, hence the large-P
+    cases.  u (the leaf output) and the transform against the FP64 oracle."""
+    monkeypatch.setenv("FMMFFT_TC_MIN_ROWS", "1")
+    x = ol.seeded_input(N, 29 + N % 89)
+    o = ol.forward_ex(x, P, T, b)
+    plan = fm.Plan(N, P, T, b, "f32_tc")
+    plan.profile_start(1)
+    y = run_device(plan, x)
+    _, stages = plan.profile_stop()
+    plan.check()
+    assert stages["leaf_halfshift"][1] == 1, stages
+    d = plan.debug_fetch()
+    assert ol.rel_l2(d["u"], o["u"]) < TOL_STAGE
+    assert ol.rel_l2(y, o["y"]) < TOL
+
+
+def test_tc_leaf_off_by_stage_mask(fm, monkeypatch):
+    """FMMFFT_TC_STAGES=7 (S2M, M2M, M2L; no leaf) keeps the leaf on the CUDA cores: the direct
+    leaf evaluates the half-shifted points itself, so no half-shift stage runs, and the result
+    is the FP32 leaf's."""
+    monkeypatch.setenv("FMMFFT_TC_STAGES", "7")
+    N, P, T, b = 1 << 18, 64, 24, 32  # 2s = 256 leaf rows: the tensor cores' by default
+    x = ol.seeded_input(N, 31)
+    o = ol.forward_ex(x, P, T, b)
+    plan = fm.Plan(N, P, T, b, "f32_tc")
+    plan.profile_start(1)
+    y = run_device(plan, x)
+    _, stages = plan.profile_stop()
+    plan.check()
+    assert stages["leaf_halfshift"][1] == 0, stages
+    assert ol.rel_l2(y, o["y"]) < TOL
