@@ -122,6 +122,7 @@ template <typename R> struct Dev {
   long tc_min_rows; /* stages with fewer rows use the CUDA-core kernel */
   int fft_threads;  /* threads per block of the register FFT pass (power of two, <= 512) */
   int tc_form; /* tensor-core form of the tree stages: 0 row, 1 pipelined, 2 TMA-fed */
+  int pdl;     /* row-form launches as programmatic dependent launches (FMMFFT_PDL=0: off) */
   unsigned *sync;   /* grid barrier of the coarse-tree kernel: [0] arrivals, [32] generation */
   long coarse_rows; /* levels with fewer rows go to the coarse-tree kernel (0: none) */
   int coarse_grid;  /* its cooperative grid (blocks of 256) */
@@ -666,7 +667,7 @@ template <class Prob> static bool tc_form_fits(const Prob &pb) {
 }
 
 template <class Prob>
-static void launch_tc(const Prob &pb0, int num_sms, int *status, cudaStream_t st, int form) {
+static void launch_tc(const Prob &pb0, int num_sms, int *status, cudaStream_t st, int form, int pdl) {
   Prob pb = pb0;
   if (form == 2 && pb.batches == 1 && pb.npad <= 64 && pb.nout <= 64 && pb.kpad % 8 == 0 &&
       pb.kpad <= 256) {
@@ -691,6 +692,24 @@ static void launch_tc(const Prob &pb0, int num_sms, int *status, cudaStream_t st
   long tiles = (pb.rows + tc::kRows - 1) / tc::kRows * pb.batches;
   long cap = 2L * num_sms; /* two CTAs per SM */
   int grid = (int)(tiles < cap ? tiles : cap);
+  if (pdl) {
+    /* programmatic dependent launch: the CTAs may start (and stage their operator) while the
+     * kernel before them finishes; the kernel waits for it before touching its data.  Only the
+     * row form is launched this way: two CTAs per SM by registers, so a waiting CTA never sits
+     * on tensor memory that a running one needs. */
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = tc_smem_bytes(pb);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, tc::k_tc_rowgemm<Prob>, pb, status);
+    return;
+  }
   tc::k_tc_rowgemm<Prob><<<grid, 256, tc_smem_bytes(pb), st>>>(pb, status);
 }
 
@@ -1800,6 +1819,8 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   d->tc_form = 0;
   if (const char *ev = getenv("FMMFFT_TC_FORM"))
     d->tc_form = strcmp(ev, "pipelined") == 0 ? 1 : (strcmp(ev, "tma") == 0 ? 2 : 0);
+  d->pdl = 1;
+  if (const char *ev = getenv("FMMFFT_PDL")) d->pdl = atoi(ev) != 0;
   coarse_setup(d);
   /* FMMFFT_FUSE_S2M=0 keeps S2M a separate stage (on the tensor cores for FP32 TC plans) */
   d->fuse_s2m = 1;
@@ -2015,7 +2036,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.kpad = d->kp_s2m, q.npad = d->np_s2m, q.nout = (int)T;
         q.bhi = d->tc_s2m[0], q.blo = d->tc_s2m[1], q.bstride = 0;
         q.xt = d->xt, q.out = d->phi + lvl_off(n, S1, T), q.M = M, q.b = (int)b, q.T = (int)T;
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form, d->pdl);
         done = true;
       }
     }
@@ -2048,7 +2069,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.bhi = d->tc_m2m[0] + (L - 2) * d->tc_m2m_stride, q.blo = d->tc_m2m[1] + (L - 2) * d->tc_m2m_stride;
         q.bstride = 0;
         q.child = d->phi + lvl_off(L + 1, S1, T), q.out = d->phi + lvl_off(L, S1, T), q.T = (int)T;
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form, d->pdl);
         done = true;
       }
     }
@@ -2101,7 +2122,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.bstride = 0;
         q.psi_par = d->psi + lvl_off(l - 1, S1, T), q.phi = d->phi + lvl_off(l, S1, T);
         q.out = d->psi + lvl_off(l, S1, T), q.T = (int)T, q.lpar = (int)(l - 1);
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form, d->pdl);
         done = true;
       }
     }
@@ -2136,7 +2157,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.fixbuf = d->leaf_fix, q.P = (int)P;
         q.psi_n = pb.psi_n, q.xt = d->xt, q.u = d->u, q.M = M, q.s = s, q.T = (int)T, q.b = (int)b;
         q.log2s = (int)n;
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form, d->pdl);
         done = true;
       }
     }

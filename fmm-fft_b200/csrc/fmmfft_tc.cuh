@@ -181,6 +181,14 @@ __device__ __forceinline__ uint32_t core_off(int m, int k, int kpad) {
   return (uint32_t)((m >> 3) * (kpad * 32) + (k >> 2) * 128 + (m & 7) * 16 + (k & 3) * 4);
 }
 
+/* Programmatic dependent launch: a kernel launched with programmatic stream serialisation may
+ * start while the kernel before it in the stream still runs; griddepcontrol.wait blocks until
+ * that kernel has completed and its memory is visible (without the attribute it returns at
+ * once), and launch_dependents lets the next such kernel start once every CTA of this one has
+ * issued it. */
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 /* Error codes a CTA records in the plan's device status word. */
 enum { kErrWaitTimeout = 1 };
 
@@ -295,37 +303,44 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
   const bool runs = pb.batches > 1;
   const int tile_end = runs ? (int)(((long)ntiles * (blockIdx.x + 1)) / gridDim.x) : ntiles;
   const int tile_step = runs ? 1 : (int)gridDim.x;
+  auto stage_b = [&](int batch) { /* B of this batch (pre-split), core-matrix layout */
+    const float *gbh = pb.bhi + (long)batch * pb.bstride, *gbl = pb.blo + (long)batch * pb.bstride;
+    const int nb = npad * kpad;
+    for (int e0 = tid; e0 < nb; e0 += 4 * (int)blockDim.x) { /* 8 loads in flight */
+      float vh[4], vl[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * blockDim.x;
+        if (e < nb) vh[u] = gbh[e], vl[u] = gbl[e];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * blockDim.x;
+        if (e < nb) {
+          const int n = e / kpad, k = e - n * kpad;
+          const uint32_t o = core_off(n, k, kpad) >> 2;
+          Bhi[o] = vh[u];
+          Blo[o] = vl[u];
+        }
+      }
+    }
+    fence_smem_to_async();
+    cur_batch = batch;
+  };
   int tile = runs ? (int)(((long)ntiles * blockIdx.x) / gridDim.x) : (int)blockIdx.x, slice = 0;
+  /* the operators are plan constants: the first one is staged before waiting for the kernel
+   * this one depends on (its rows are this kernel's A); nothing global is read or written
+   * before the wait */
+  pdl_trigger();
+  if (tile < tile_end) stage_b(tile / tiles_per_batch);
+  pdl_wait();
   if (tile < tile_end) load_step(tile, 0);
   while (tile < tile_end) {
     TC_CLOCK(tp);
     const int batch = tile / tiles_per_batch;
     const long r0 = (long)(tile - batch * tiles_per_batch) * kRows;
     const int k0 = slice * ks, k1 = k0 + ks;
-    if (batch != cur_batch) { /* B of this batch; the previous step's MMAs have completed */
-      const float *gbh = pb.bhi + (long)batch * pb.bstride, *gbl = pb.blo + (long)batch * pb.bstride;
-      const int nb = npad * kpad;
-      for (int e0 = tid; e0 < nb; e0 += 4 * (int)blockDim.x) { /* 8 loads in flight */
-        float vh[4], vl[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int e = e0 + u * blockDim.x;
-          if (e < nb) vh[u] = gbh[e], vl[u] = gbl[e];
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int e = e0 + u * blockDim.x;
-          if (e < nb) {
-            const int n = e / kpad, k = e - n * kpad;
-            const uint32_t o = core_off(n, k, kpad) >> 2;
-            Bhi[o] = vh[u];
-            Blo[o] = vl[u];
-          }
-        }
-      }
-      fence_smem_to_async();
-      cur_batch = batch;
-    }
+    if (batch != cur_batch) stage_b(batch); /* the previous step's MMAs have completed */
     TC_PHASE(0, tp); /* operator staging */
     /* split into TF32 hi / lo and write both into this thread's TMEM lane */
     if (my_half * 32 < ks) {
