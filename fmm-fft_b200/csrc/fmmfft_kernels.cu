@@ -121,7 +121,10 @@ template <typename R> struct Dev {
   int ok_s2m, ok_m2m, ok_m2l, ok_leaf;
   long tc_min_rows; /* stages with fewer rows use the CUDA-core kernel */
   int fft_threads;  /* threads per block of the register FFT pass (power of two, <= 512) */
-  int tc_form; /* tensor-core form of the tree stages: 0 row, 1 pipelined, 2 TMA-fed */
+  /* tensor-core form: 0 row (32 lanes), 1 pipelined, 2 TMA-fed, 3 row (16 lanes); -1 (default)
+   * per stage, as measured fastest: S2M and M2M the 16-lane row form, M2L and the leaf the
+   * 32-lane one (the same speed for M2L, faster and more accurate for the leaf) */
+  int tc_form;
   int pdl;     /* row-form launches as programmatic dependent launches (FMMFFT_PDL=0: off) */
   unsigned *sync;   /* grid barrier of the coarse-tree kernel: [0] arrivals, [32] generation */
   long coarse_rows; /* levels with fewer rows go to the coarse-tree kernel (0: none) */
@@ -438,6 +441,10 @@ struct TcBase {
       *reinterpret_cast<float4 *>(dst + c0) = make_float4(t[0], t[1], t[2], t[3]);
     }
   }
+  /* output columns c..c+3 of a row (16-lane row form; c a multiple of 4) */
+  __device__ void put4(float *dst, long, int, int c, float4 v) const {
+    if (c + 4 <= nout) *reinterpret_cast<float4 *>(dst + c) = v;
+  }
 };
 
 struct TcS2M : TcBase {
@@ -517,6 +524,21 @@ struct TcLeaf : TcBase { /* batch z = section - 1; s is a power of two (log2s) *
         u[(2L * z + ri) * M + nb * b] = v;
       else
         fixbuf[(ri << log2s) + nb] = v;
+    }
+  }
+  __device__ void put4(float *dst, long r, int z, int c, float4 v) const { /* c a multiple of 4 */
+    const int sc = z + 1;
+    if (c < b) {
+      if (c == 0 && 2 * sc > P) /* the in-box first point is replaced */
+        dst[1] = v.y, dst[2] = v.z, dst[3] = v.w;
+      else
+        *reinterpret_cast<float4 *>(dst + c) = v;
+    } else if (c == b && 2 * sc >= P) { /* column b */
+      const long ri = r >> log2s, nb = (r + 1) & (s - 1);
+      if (2 * sc > P)
+        u[(2L * z + ri) * M + nb * b] = v.x;
+      else
+        fixbuf[(ri << log2s) + nb] = v.x;
     }
   }
 };
@@ -692,6 +714,8 @@ static void launch_tc(const Prob &pb0, int num_sms, int *status, cudaStream_t st
   long tiles = (pb.rows + tc::kRows - 1) / tc::kRows * pb.batches;
   long cap = 2L * num_sms; /* two CTAs per SM */
   int grid = (int)(tiles < cap ? tiles : cap);
+  const bool r16 = form == 3; /* the 16-lane row form */
+  const size_t smem = r16 ? tc::smem16_bytes(pb.kpad, pb.npad) : tc_smem_bytes(pb);
   if (pdl) {
     /* programmatic dependent launch: the CTAs may start (and stage their operator) while the
      * kernel before them finishes; the kernel waits for it before touching its data.  Only the
@@ -700,17 +724,23 @@ static void launch_tc(const Prob &pb0, int num_sms, int *status, cudaStream_t st
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)grid);
     cfg.blockDim = dim3(256);
-    cfg.dynamicSmemBytes = tc_smem_bytes(pb);
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, tc::k_tc_rowgemm<Prob>, pb, status);
+    if (r16)
+      cudaLaunchKernelEx(&cfg, tc::k_tc_rowgemm16<Prob>, pb, status);
+    else
+      cudaLaunchKernelEx(&cfg, tc::k_tc_rowgemm<Prob>, pb, status);
     return;
   }
-  tc::k_tc_rowgemm<Prob><<<grid, 256, tc_smem_bytes(pb), st>>>(pb, status);
+  if (r16)
+    tc::k_tc_rowgemm16<Prob><<<grid, 256, smem, st>>>(pb, status);
+  else
+    tc::k_tc_rowgemm<Prob><<<grid, 256, smem, st>>>(pb, status);
 }
 
 /* First point of each leaf box for the sections whose shifted target leaves its box
@@ -1800,7 +1830,7 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   d->kp_leaf = up8(T + 3 * b), d->np_leaf = up16(b + 1); /* + the half-shifted column */
   auto fits = [&](int kp, int np) {
     return tc && (T % 4 == 0) && (b % 4 == 0) && np <= 256 && kp <= 256 &&
-           tc::smem_bytes(kp, np) <= (size_t)110 * 1024 && tc::tmem_cols(kp, np) <= 256;
+           tc::smem16_bytes(kp, np) <= (size_t)110 * 1024 && tc::tmem_cols(tc::round16(kp), np) <= 256;
   };
   d->ok_s2m = fits(d->kp_s2m, d->np_s2m);
   d->ok_m2m = fits(d->kp_m2m, d->np_m2m) && nlev > 0;
@@ -1816,9 +1846,9 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   /* FMMFFT_TC_FORM=pipelined routes the tree stages that fit to the warp-specialised kernel
    * (4xTF32, rel-L2 2.4e-7 at N = 2^24, P = 64, 24 terms, against 2.7e-7); the row form stays
    * the default because it is faster there (M2L 0.47 ms against 0.58 ms on a B200) */
-  d->tc_form = 0;
+  d->tc_form = -1;
   if (const char *ev = getenv("FMMFFT_TC_FORM"))
-    d->tc_form = strcmp(ev, "pipelined") == 0 ? 1 : (strcmp(ev, "tma") == 0 ? 2 : 0);
+    d->tc_form = strcmp(ev, "pipelined") == 0 ? 1 : strcmp(ev, "tma") == 0 ? 2 : strcmp(ev, "row") == 0 ? 0 : strcmp(ev, "row16") == 0 ? 3 : -1;
   d->pdl = 1;
   if (const char *ev = getenv("FMMFFT_PDL")) d->pdl = atoi(ev) != 0;
   coarse_setup(d);
@@ -2036,7 +2066,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.kpad = d->kp_s2m, q.npad = d->np_s2m, q.nout = (int)T;
         q.bhi = d->tc_s2m[0], q.blo = d->tc_s2m[1], q.bstride = 0;
         q.xt = d->xt, q.out = d->phi + lvl_off(n, S1, T), q.M = M, q.b = (int)b, q.T = (int)T;
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form, d->pdl);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 3 : d->tc_form, d->pdl);
         done = true;
       }
     }
@@ -2069,7 +2099,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.bhi = d->tc_m2m[0] + (L - 2) * d->tc_m2m_stride, q.blo = d->tc_m2m[1] + (L - 2) * d->tc_m2m_stride;
         q.bstride = 0;
         q.child = d->phi + lvl_off(L + 1, S1, T), q.out = d->phi + lvl_off(L, S1, T), q.T = (int)T;
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form, d->pdl);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 3 : d->tc_form, d->pdl);
         done = true;
       }
     }
@@ -2122,7 +2152,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.bstride = 0;
         q.psi_par = d->psi + lvl_off(l - 1, S1, T), q.phi = d->phi + lvl_off(l, S1, T);
         q.out = d->psi + lvl_off(l, S1, T), q.T = (int)T, q.lpar = (int)(l - 1);
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form, d->pdl);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 0 : d->tc_form, d->pdl);
         done = true;
       }
     }
@@ -2157,7 +2187,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.fixbuf = d->leaf_fix, q.P = (int)P;
         q.psi_n = pb.psi_n, q.xt = d->xt, q.u = d->u, q.M = M, q.s = s, q.T = (int)T, q.b = (int)b;
         q.log2s = (int)n;
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form, d->pdl);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 0 : d->tc_form, d->pdl);
         done = true;
       }
     }
@@ -2308,6 +2338,10 @@ static int set_smem_limits(void) {
   allow_dyn_smem(tc::k_tc_rowgemm<TcM2M>, lim);
   allow_dyn_smem(tc::k_tc_rowgemm<TcM2L>, lim);
   allow_dyn_smem(tc::k_tc_rowgemm<TcLeaf>, lim);
+  allow_dyn_smem(tc::k_tc_rowgemm16<TcS2M>, lim);
+  allow_dyn_smem(tc::k_tc_rowgemm16<TcM2M>, lim);
+  allow_dyn_smem(tc::k_tc_rowgemm16<TcM2L>, lim);
+  allow_dyn_smem(tc::k_tc_rowgemm16<TcLeaf>, lim);
   allow_dyn_smem(tc::k_tc_rowgemm_t<TcS2M>, lim);
   allow_dyn_smem(tc::k_tc_rowgemm_t<TcM2M>, lim);
   allow_dyn_smem(tc::k_tc_rowgemm_t<TcM2L>, lim);

@@ -92,6 +92,20 @@ __device__ __forceinline__ void tmem_st8(uint32_t taddr, const float *v) {
 }
 __device__ __forceinline__ void tmem_st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
+/* 16 TMEM lanes x 16 columns from registers (shape 16x256b, two 8-column chunks): thread t
+ * writes lanes t/4 and t/4 + 8 at columns 2 (t % 4) and 2 (t % 4) + 1 of each chunk, registers
+ * {lane t/4: chunk 0 two columns, lane t/4 + 8: chunk 0, lane t/4: chunk 1, lane t/4 + 8: chunk 1}.
+ * The lane field of taddr is the first of the 16 lanes (0 or 16 within the warp's quarter). */
+__device__ __forceinline__ void tmem_st16x2(uint32_t taddr, const float *v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.16x256b.x2.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};"
+      :
+      : "r"(taddr), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+        "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+        "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7]))
+      : "memory");
+}
+
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                :
@@ -159,6 +173,19 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v) {
   uint32_t r[8];
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+/* The same 16 lanes x 16 columns into registers (same register order as tmem_st16x2). */
+__device__ __forceinline__ void tmem_ld16x2(uint32_t taddr, float *v) {
+  uint32_t r[8];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.16x256b.x2.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
       : "r"(taddr)
       : "memory");
@@ -419,6 +446,241 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
       fence_before_sync();
       __syncthreads();
       TC_PHASE(7, tp); /* epilogue */
+    }
+    tile = ntile, slice = nslice;
+  }
+  /* after an expired wait, give the MMAs in flight (bounded) time to finish before TMEM goes */
+  if (tid == 0 && abort_flag) mbar_wait_bounded(&mbar, phase ^ 1);
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
+
+/* ===================================================================== 16-lane row form */
+
+/* Column permutation within each group of 16 (an involution-free bijection): TMEM / shared
+ * column 16g + 8h + 2j + e holds source column 16g + 4j + 2h + e (h, e in {0, 1}, j < 4). */
+__host__ __device__ __forceinline__ int perm16(int c) {
+  return (c & ~15) + 4 * ((c >> 1) & 3) + 2 * ((c >> 3) & 1) + (c & 1);
+}
+__host__ __device__ constexpr int round16(int v) { return (v + 15) & ~15; }
+
+/* Shared memory of the 16-lane row form: B hi and lo with K padded to 16. */
+__host__ __device__ constexpr size_t smem16_bytes(int kpad, int npad) {
+  return (size_t)(2 * npad * round16(kpad)) * sizeof(float);
+}
+
+/* The row contraction of k_tc_rowgemm (same TMEM budget, operator staging and MMAs, two CTAs
+ * per SM, persistent over tiles) with another path for A into TMEM and for D out of it.
+ * Warp w owns the 16 TMEM lanes (tile rows) 32 (w % 4) + 16 (w / 4) .. +15 across all K columns
+ * of a slice, through tcgen05.st / ld of shape 16x256b: thread t holds rows t/4 and t/4 + 8 and
+ * columns 2 (t % 4), 2 (t % 4) + 1 of each 8-column chunk.  K (A's columns and B's K columns) and
+ * N (B's rows, so D's columns) are permuted within each group of 16 by perm16, alike for A and
+ * B, which leaves the contraction unchanged up to the order of its sums; with it the column
+ * pairs a thread holds in two chunks are four consecutive source columns.  So a thread loads
+ * one float4 per row and 16-column group of A and stores one float4 per row and group of the
+ * output: 8 rows x 64 contiguous bytes per warp instruction, where one row per lane (the 32x32b
+ * shape) makes every instruction touch 32 rows x 16 bytes.  Prob supplies put4(dst, r, batch,
+ * c, v): output columns c..c+3 of row r. */
+template <class Prob>
+__global__ void __launch_bounds__(256, 2) k_tc_rowgemm16(const __grid_constant__ Prob pb, int *status) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+  /* load map: for slice s, 16-column group g and quad j (source columns 16g + 4j .. +3 of the
+   * slice), the A chunk (low byte, 0xFF = zero) and the float offset within that chunk's row */
+  __shared__ int lmap[4][4][4];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int kpad = pb.kpad, npad = pb.npad;
+  const int kp = round16(kpad);              /* K extent of staged B and of A in TMEM */
+  const int ks = kp < kSlice ? kp : kSlice;  /* a multiple of 16 */
+  const int nslices = (kp + ks - 1) / ks;    /* <= 4: kpad <= 256 */
+  const int ngroups = ks >> 4;
+  float *Bhi = reinterpret_cast<float *>(smem_raw);
+  float *Blo = Bhi + npad * kp;
+  const uint32_t ncols = (uint32_t)tmem_cols(kp, npad);
+  if (warp == 0) tmem_alloc(&tmem_slot, ncols);
+  if (tid == 0) {
+    mbar_init(&mbar, 1);
+    fence_mbar_init();
+    abort_flag = 0;
+  }
+  if (tid < 4 * 4 * 4) {
+    const int sl = tid >> 4, g = (tid >> 2) & 3, j = tid & 3;
+    const int k = sl * ks + 16 * g + 4 * j;
+    int e = 0xFF;
+    if (sl < nslices && 16 * g < ks && k < kpad)
+      for (int c = 0; c < pb.nchunks; ++c)
+        if (k >= pb.coff[c] && k < pb.coff[c] + pb.clen[c]) e = c | ((k - pb.coff[c]) << 8);
+    lmap[sl][g][j] = e;
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = tmem_slot;
+  /* accumulator columns [0, npad): A x B_hi, [npad, 2 npad): A x B_lo (B_lo follows B_hi in
+   * shared memory as the next row groups, so one descriptor of N = 2 npad covers both) */
+  const uint32_t d_cols = (uint32_t)(((2 * npad + 31) / 32) * 32);
+  const uint32_t t_ahi = tmem + d_cols, t_alo = tmem + d_cols + (uint32_t)ks;
+  const uint32_t idesc = make_idesc_tf32(2 * npad);
+  const uint32_t b_sbo = (uint32_t)kp * 32, lbo = 128;
+  const uint32_t bh = smem_addr(Bhi);
+  const int tiles_per_batch = (int)((pb.rows + kRows - 1) / kRows);
+  const int ntiles = tiles_per_batch * pb.batches;
+  const int quarter = warp & 3, half = warp >> 2, j4 = lane & 3;
+  const int row0 = quarter * 32 + half * 16 + (lane >> 2); /* tile rows row0 and row0 + 8 */
+  const uint32_t lane_addr = (uint32_t)(quarter * 32 + half * 16) << 16;
+
+  float4 v[2][4]; /* [row][16-column group] */
+  const float *rowp[2][4];
+  auto load_step = [&](int tile, int slice) {
+    if (slice == 0) {
+      const int batch = tile / tiles_per_batch;
+      const long rb = (long)(tile - batch * tiles_per_batch) * kRows + row0;
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const long r = rb + 8 * i;
+        const bool live = r < pb.rows;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) rowp[i][c] = (live && c < pb.nchunks) ? pb.src(c, r, batch) : nullptr;
+      }
+    }
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+      const int e = lmap[slice][g][j4];
+      const int c = e & 0xFF;
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        v[i][g] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (c != 0xFF) {
+          const float *rp = c == 0 ? rowp[i][0] : (c == 1 ? rowp[i][1] : (c == 2 ? rowp[i][2] : rowp[i][3]));
+          if (rp) v[i][g] = __ldg(reinterpret_cast<const float4 *>(rp + (e >> 8)));
+        }
+      }
+    }
+  };
+
+  int cur_batch = -1;
+  uint32_t phase = 0;
+  const bool runs = pb.batches > 1;
+  const int tile_end = runs ? (int)(((long)ntiles * (blockIdx.x + 1)) / gridDim.x) : ntiles;
+  const int tile_step = runs ? 1 : (int)gridDim.x;
+  /* B of a batch, pre-split, in the core-matrix layout with K extent kp; shared element
+   * (n, k) holds operator element (perm16(n), perm16(k)), zero for k >= kpad */
+  auto stage_b = [&](int batch) {
+    const float *gbh = pb.bhi + (long)batch * pb.bstride, *gbl = pb.blo + (long)batch * pb.bstride;
+    const int nb = npad * kp;
+    for (int e0 = tid; e0 < nb; e0 += 4 * (int)blockDim.x) { /* 8 loads in flight */
+      float vh[4], vl[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * blockDim.x;
+        vh[u] = 0.f, vl[u] = 0.f;
+        if (e < nb) {
+          const int n = e / kp, k = e - n * kp, ks_ = perm16(k);
+          if (ks_ < kpad) {
+            const long o = (long)perm16(n) * kpad + ks_;
+            vh[u] = gbh[o], vl[u] = gbl[o];
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * blockDim.x;
+        if (e < nb) {
+          const int n = e / kp, k = e - n * kp;
+          const uint32_t o = core_off(n, k, kp) >> 2;
+          Bhi[o] = vh[u];
+          Blo[o] = vl[u];
+        }
+      }
+    }
+    fence_smem_to_async();
+    cur_batch = batch;
+  };
+  int tile = runs ? (int)(((long)ntiles * blockIdx.x) / gridDim.x) : (int)blockIdx.x, slice = 0;
+  /* programmatic dependent launch: the first operator (a plan constant) is staged before the
+   * wait; nothing global is read or written before it */
+  pdl_trigger();
+  if (tile < tile_end) stage_b(tile / tiles_per_batch);
+  pdl_wait();
+  if (tile < tile_end) load_step(tile, 0);
+  while (tile < tile_end) {
+    const int batch = tile / tiles_per_batch;
+    const long r0 = (long)(tile - batch * tiles_per_batch) * kRows;
+    const int k0 = slice * ks, k1 = k0 + ks;
+    if (batch != cur_batch) stage_b(batch); /* the previous step's MMAs have completed */
+    /* split into TF32 hi / lo and write both into this warp's 16 TMEM lanes */
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+      if (g >= ngroups) break;
+      const float a[8] = {v[0][g].x, v[0][g].y, v[1][g].x, v[1][g].y, v[0][g].z, v[0][g].w, v[1][g].z, v[1][g].w};
+      float h[8], l[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        h[i] = tf32_rna(a[i]);
+        l[i] = tf32_rna(a[i] - h[i]);
+      }
+      tmem_st16x2(t_ahi + lane_addr + 16u * g, h);
+      tmem_st16x2(t_alo + lane_addr + 16u * g, l);
+    }
+    tmem_st_wait();
+    fence_before_sync();
+    __syncthreads();
+    if (warp == 0) { /* lane 0 issues; the rest of warp 0 waits at __syncwarp */
+      if (lane == 0) {
+        fence_after_sync();
+        const int ksteps = ((k1 < kp ? k1 : kp) - k0) >> 3, kb = k0 >> 3;
+#pragma unroll 1
+        for (int s = 0; s < 2; ++s) { /* A_hi x [B_hi; B_lo], A_lo x [B_hi; B_lo] */
+          uint32_t ta = (s == 1) ? t_alo : t_ahi;
+          uint64_t db = make_desc(bh + 256u * kb, lbo, b_sbo);
+#pragma unroll 1
+          for (int kk = 0; kk < ksteps; ++kk, ta += 8, db += 16)
+            mma_tf32_ts(tmem, ta, db, idesc, (k0 | s | kk) != 0);
+        }
+        mma_commit(&mbar);
+      }
+      __syncwarp();
+    }
+    /* next step: its loads go out while the MMAs (and at a tile's end the epilogue) run */
+    const bool last_slice = slice == nslices - 1;
+    const int ntile = last_slice ? tile + tile_step : tile;
+    const int nslice = last_slice ? 0 : slice + 1;
+    if (ntile < tile_end) load_step(ntile, nslice);
+    if (tid == 0 && !mbar_wait_bounded(&mbar, phase)) {
+      atomicExch(status, kErrWaitTimeout);
+      abort_flag = 1;
+    }
+    phase ^= 1;
+    __syncthreads();
+    fence_after_sync();
+    if (abort_flag) break;
+    if (last_slice) {
+      /* epilogue: D column 16g + 8h + 2j + e is output perm16(.) = 16g + 4j + 2h + e, so this
+       * thread's columns of a group are the four outputs 16g + 4j .. +3 of its two rows */
+      float *dst[2];
+      long rr[2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        rr[i] = r0 + row0 + 8 * i;
+        dst[i] = rr[i] < pb.rows ? pb.dst(rr[i], batch) : nullptr;
+      }
+      for (int g = 0; g < (npad >> 4); ++g) {
+        float t[8], tl[8];
+        tmem_ld16x2(tmem + lane_addr + 16u * g, t);
+        tmem_ld16x2(tmem + lane_addr + (uint32_t)npad + 16u * g, tl);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) t[i] += tl[i];
+        const int c = 16 * g + 4 * j4;
+        if (dst[0]) pb.put4(dst[0], rr[0], batch, c, make_float4(t[0], t[1], t[4], t[5]));
+        if (dst[1]) pb.put4(dst[1], rr[1], batch, c, make_float4(t[2], t[3], t[6], t[7]));
+      }
+      fence_before_sync();
+      __syncthreads();
     }
     tile = ntile, slice = nslice;
   }

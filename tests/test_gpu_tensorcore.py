@@ -2,8 +2,9 @@
 
 FMMFFT_TC_MIN_ROWS=1 (set before the plans are made) sends every eligible stage, however small,
 through the tensor-core kernel so that small cases cover it; the default threshold only routes
-stages with >= 4096 rows there.  Each test runs for the three kernel forms (FMMFFT_TC_FORM row,
-pipelined and tma), with S2M as its own stage (FMMFFT_FUSE_S2M=0) so that it runs on the tensor cores.  Tolerance: rel-L2 <= 1e-6 against FP64, as for FP32 plans.
+stages with >= 4096 rows there.  Each test runs for the default per-stage forms (16-lane row
+form for S2M and M2M, 32-lane row form for M2L and the leaf) and for each kernel form forced on
+every stage (FMMFFT_TC_FORM row, row16, pipelined and tma), with S2M as its own stage (FMMFFT_FUSE_S2M=0) so that it runs on the tensor cores.  Tolerance: rel-L2 <= 1e-6 against FP64, as for FP32 plans.
 """
 import os
 
@@ -29,13 +30,20 @@ def fm():
     return fmmfft
 
 
-@pytest.fixture(params=["row", "pipelined", "tma"])
+FORMS = ["default", "row", "row16", "pipelined", "tma"]
+
+
+@pytest.fixture(params=FORMS)
 def force_tc(request):
-    """Every eligible stage on the tensor cores, in the row form (default), the pipelined
-    warp-specialised form or the TMA-fed form (FMMFFT_TC_FORM=pipelined / tma)."""
+    """Every eligible stage on the tensor cores, in the default per-stage forms or in one form
+    forced on every stage: the 32-lane row form, the 16-lane row form, the pipelined
+    warp-specialised form or the TMA-fed form (FMMFFT_TC_FORM=row / row16 / pipelined / tma)."""
     saved = {k: os.environ.get(k) for k in ("FMMFFT_TC_MIN_ROWS", "FMMFFT_TC_FORM", "FMMFFT_FUSE_S2M")}
     os.environ["FMMFFT_TC_MIN_ROWS"] = "1"
-    os.environ["FMMFFT_TC_FORM"] = request.param
+    if request.param == "default":
+        os.environ.pop("FMMFFT_TC_FORM", None)
+    else:
+        os.environ["FMMFFT_TC_FORM"] = request.param
     os.environ["FMMFFT_FUSE_S2M"] = "0"  # S2M as its own tensor-core stage
     yield request.param
     for k, v in saved.items():
@@ -68,11 +76,14 @@ def test_tc_stagewise_vs_oracle(fm, force_tc, N, P, T, b):
     assert ol.rel_l2(y, o["y"]) < TOL
 
 
-@pytest.fixture(params=["row", "pipelined", "tma"])
+@pytest.fixture(params=FORMS)
 def tc_form(request):
-    """Default routing (stages of >= 4096 rows on the tensor cores) in either kernel form."""
+    """Default routing (stages of >= 4096 rows on the tensor cores) in each kernel form."""
     saved = os.environ.get("FMMFFT_TC_FORM")
-    os.environ["FMMFFT_TC_FORM"] = request.param
+    if request.param == "default":
+        os.environ.pop("FMMFFT_TC_FORM", None)
+    else:
+        os.environ["FMMFFT_TC_FORM"] = request.param
     yield request.param
     if saved is None:
         os.environ.pop("FMMFFT_TC_FORM", None)
