@@ -5,19 +5,28 @@
  * src/fmmfft.c mft -> mftint, :384-1081):
  *
  *   1  k_sections      x[M][P] -> xt[2P][M] planar sections + per-tile section sums
- *                      (deinterleave :419-439, section sums :441-457)
+ *                      (deinterleave :419-439, section sums :441-457); when a tile holds whole
+ *                      leaf boxes it also computes their S2M multipoles (:199-211, :465)
  *   2  k_sum_sections  tiles -> Sigma_m x_sc[m] (the MPI_Reduce/Bcast of :452-453)
- *   3  S2M             rowgemm: phi_n = xt . initch                      (:199-211, :465)
- *   4  M2M             rowgemm per level: phi_L = [phi_L+1 pair] . [S_L;S_R]  (:476-515)
- *   5  top flip        rowgemm: psi_2[c] = topflp . phi_2[c+2]          (:620-639)
- *   6  M2L + L2L       rowgemm per level over parent boxes, both children at once
- *                      (:643-749)
- *   7  leaf            rowgemm per section: u = [psi_n | x window] . [E_sc ; cot Toeplitz]
- *                      + k_leaf_fix for the half-shifted first point (:751-954)
- *   8  k_combine       pre-twiddle and length-P DFT over sections, transposed store
+ *   3  S2M             (when not fused into 1) row contraction: phi_n = xt . initch
+ *   4  M2M             row contraction per level: phi_L = [phi_L+1 pair] . [S_L;S_R]  (:476-515)
+ *   5  top flip        psi_2[c] = topflp . phi_2[c+2]                    (:620-639)
+ *   6  M2L + L2L       row contraction per level over parent boxes, both children at once
+ *                      (:643-749); the levels with few rows of 4-6 run in one cooperative
+ *                      launch, k_coarse
+ *   7  leaf            row contraction per section: u = [psi_n | x window] . [E_sc ; cot
+ *                      Toeplitz] with the half-shifted first point as one more operator column
+ *                      (tensor cores) + k_leaf_mid for section P/2; k_leaf (direct, CUDA cores)
+ *                      for FP32 / FP64 plans; rowgemm + k_leaf_fix when b % 8 != 0 (:751-954)
+ *   8  combine         pre-twiddle and length-P DFT over sections, transposed store, as a
+ *                      register Stockham pass (k_fft_reg with CombineLd; k_combine otherwise)
  *                      (:956-968 and the MPI_Alltoall of :970)
- *   9  k_fft_pass      size-M Stockham FFTs, one or two passes (FFTW at :1080)
+ *   9  size-M FFTs     register Stockham passes k_fft_reg (k_fft_pass for shapes they do not
+ *                      take) (FFTW at :1080)
+ *  10  k_block_dc      FP32 plans: the block-DC bins from the exact identity in FP64
  *
+ * Row contractions run on the tensor cores for split-TF32 plans (fmmfft_tc.cuh: k_tc_rowgemm,
+ * k_tc_rowgemm16) and as rowgemm on the CUDA cores otherwise.
  * All tree operators are shared by every section and box, so each tree stage is one dense
  * contraction over "rows" (section, re/im plane, box) with a small operator; rowgemm is the
  * CUDA-core form of that contraction.  Real type R = float (complex64 plans) or double
