@@ -12,8 +12,8 @@
  *   4  M2M             row contraction per level: phi_L = [phi_L+1 pair] . [S_L;S_R]  (:476-515)
  *   5  top flip        psi_2[c] = topflp . phi_2[c+2]                    (:620-639)
  *   6  M2L + L2L       row contraction per level over parent boxes, both children at once
- *                      (:643-749); the levels with few rows of 4-6 run in one cooperative
- *                      launch, k_coarse
+ *                      (:643-749); the tree levels of stages 4-6 with fewer than 4096 rows run
+ *                      in one cooperative launch, k_coarse (plans of N >= 2^23)
  *   7  leaf            row contraction per section: u = [psi_n | x window] . [E_sc ; cot
  *                      Toeplitz] with the half-shifted first point as one more operator column
  *                      (tensor cores) + k_leaf_mid for section P/2; k_leaf (direct, CUDA cores)
