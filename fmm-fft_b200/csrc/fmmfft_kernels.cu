@@ -2440,14 +2440,8 @@ extern "C" int fmmk_execute_host(fmmk_state *st, const void *h_in, void *h_out, 
     Dev<float> *d = (Dev<float> *)st->dev;
     N = d->N, esz = sizeof(float2), work = d->z;
   }
-  /* the input lands in z (dead until the combine), the output is produced in tmp's place by
-   * the FFT and copied back; z and tmp are both [P][M] complex */
-  void *outbuf = NULL;
-  if (st->precision == 0)
-    outbuf = ((Dev<double> *)st->dev)->tmp;
-  else
-    outbuf = ((Dev<float> *)st->dev)->tmp;
-  (void)outbuf;
+  /* the input is staged into the plan's z buffer ([P][M] complex, dead until the combine) and
+   * the transform runs in place on that copy; the result is copied back from it */
   FMM_CUDA_TRY(cudaMemcpyAsync(work, h_in, esz * (size_t)N, cudaMemcpyHostToDevice, s));
   /* in-place execute on the staged copy: stage 1 consumes z before z is rewritten */
   int rc = fmmk_execute(st, work, work, stream, 0, err, errlen);
