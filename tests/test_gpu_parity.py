@@ -1,6 +1,6 @@
 """GPU parity: the sm_100a FMM-FFT through the C-ABI against the oracle and the reference.
 
-Tolerances (stated per north star): FP64 plans agree with the reference's FP64 result to
+Tolerances: FP64 plans agree with the reference's FP64 result to
 rel-L2 <= 1e-12; FP32 plans (complex64) agree with the FP64 oracle / FP64 DFT to rel-L2 <= 1e-6.
 """
 import glob

@@ -1,4 +1,4 @@
-"""Graphs, batches and the request server (north-star batching and serving) on the GPU.
+"""Graphs, batches and the request server (batched and served transforms) on the GPU.
 
 Each transform is checked against the plain per-call execute of the same plan (bitwise: the
 graph replays the same kernels) and against an FP64 FFT (rel-L2 <= 1e-6 for FP32 plans)."""

@@ -1,4 +1,4 @@
-"""CPU tests of the oracle itself: it must agree with the reference before it can judge the GPU.
+"""CPU tests of the oracle itself: it must agree with the reference before it can check the GPU.
 
 Pins (reference = 97amarnathk/fmm-fft src/fmmfft.c):
   * golden vectors made by running the unmodified reference (tests/golden/make_golden.py);
