@@ -440,6 +440,7 @@ struct TcBase {
   const float *bhi, *blo;
   long bstride;
   int yoff[4]; /* TMA-fed form: row offset of chunk c's 2-D block (chunk c of row r = row r + yoff[c]) */
+  static constexpr bool kEpiAlternate = false; /* row-form epilogue: one half of N per warp */
   __device__ bool wraps(int, long) const { return false; }
   /* output columns c0..c0+7 of a row into dst (columns below nout; nout a multiple of 4) */
   __device__ void put8(float *dst, long, int, int c0, const float *t) const {
@@ -501,6 +502,9 @@ struct TcM2L : TcBase {
  * the next box's in-box first point, which is then not stored; for sc = P/2 it goes to fixbuf
  * and k_leaf_mid averages the two. */
 struct TcLeaf : TcBase { /* batch z = section - 1; s is a power of two (log2s) */
+  /* N = b + 1 padded to a multiple of 16: the upper half of N holds few stored columns, so the
+   * epilogue's 8-column chunks go alternately to the two halves of the warps */
+  static constexpr bool kEpiAlternate = true;
   const float *psi_n, *xt;
   float *u, *fixbuf;
   long M, s;

@@ -248,6 +248,7 @@ __host__ __device__ constexpr int tmem_cols(int kpad, int npad) {
  *   __device__ float *dst(long r, int batch) const;
  *   __device__ void put8(float *dst, long r, int batch, int c0, const float *t) const;
  *                                     stores output columns c0..c0+7 of row r
+ *   static constexpr bool kEpiAlternate;  epilogue chunks dealt alternately to the two halves
  * A never touches shared memory: warp w, lane i owns tile row 32 (w % 4) + i (its TMEM lane)
  * and K columns [32 (w / 4), +32) of each 64-column slice; it loads them (8 float4, all issued
  * before use), splits them into TF32 hi/lo in registers and writes both into its TMEM lane with
@@ -434,8 +435,12 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
       /* epilogue: this warp's TMEM lanes (= tile rows), columns of half (w / 4) of padded N */
       const long r = r0 + my_m;
       float *dst = (r < pb.rows) ? pb.dst(r, batch) : nullptr;
-      const int cw = npad >> 1, cbeg = my_half * cw;
-      for (int c0 = cbeg; c0 < cbeg + cw; c0 += 8) {
+      /* this warp's 8-column chunks of padded N: one half each, or dealt alternately to the two
+       * halves where the problem's stored columns are not split evenly by halves */
+      const int cstep = Prob::kEpiAlternate ? 16 : 8;
+      const int cbeg = Prob::kEpiAlternate ? 8 * my_half : my_half * (npad >> 1);
+      const int cend = Prob::kEpiAlternate ? npad : cbeg + (npad >> 1);
+      for (int c0 = cbeg; c0 < cend; c0 += cstep) {
         float t[8], tl[8];
         tmem_ld8(tmem + lane_addr + (uint32_t)c0, t);
         tmem_ld8(tmem + lane_addr + (uint32_t)(npad + c0), tl);
