@@ -47,6 +47,8 @@ def parse():
                          "of mixed N and P as one graph; serving: Poisson arrivals through the "
                          "request server")
     ap.add_argument("--rate", type=float, default=2000.0, help="serving: arrivals per second")
+    ap.add_argument("--requests", type=int, default=1200, help="serving: requests per rate")
+    ap.add_argument("--no-served", action="store_true", help="skip the served-vs-plain object")
     ap.add_argument("--duration", type=float, default=2.0, help="serving: seconds of arrivals")
     return ap.parse_args()
 
@@ -305,65 +307,62 @@ def run_uneven_batch(a):
 
 
 # ------------------------------------------------------------------------ serving
-def serving_requests(rate, duration, seed):
-    """Poisson arrivals; N log-uniform over powers of two 2^10..2^24; two accuracy classes
-    (rel-L2 1e-4 -> p = 8 on FP32 CUDA cores, 1e-6 -> p = 20 with the tensor-core tree)."""
+SERVE_CLASSES = {"1e-4": 8, "1e-6": 20}  # accuracy class -> Chebyshev terms
+
+
+def serving_requests(rate, count, seed):
+    """`count` Poisson arrivals at `rate` per second; N log-uniform over powers of two
+    2^10..2^24 (complex64, iid normal); two accuracy classes, rel-L2 1e-4 (p = 8) and 1e-6
+    (p = 20), equally likely; P = min(64, max(2, N / 512)), b = 32."""
     import numpy as np
     rng = np.random.Generator(np.random.PCG64(seed))
     t, reqs = 0.0, []
-    while True:
+    for _ in range(count):
         t += rng.exponential(1.0 / rate)
-        if t > duration:
-            break
         N = 1 << int(rng.integers(10, 25))
-        cls = int(rng.integers(0, 2))
+        terms = SERVE_CLASSES["1e-4" if int(rng.integers(0, 2)) == 0 else "1e-6"]
         P = max(2, min(64, N // 512))
-        terms, prec = (8, "f32") if cls == 0 else (20, "f32_tc")
-        reqs.append((t, N, P, terms, 32, prec))
+        reqs.append((t, N, P, terms, 32))
     return reqs
 
 
-def run_serving(a):
-    import numpy as np
+def serve_compare(rates, count=1200, seed=7, served_prec="f32_tc", plain_prec="f32"):
+    """Open-loop Poisson arrivals through the request server (continuous batching, mixed
+    precision on the tensor cores) against the plain per-request FMM-FFT (FP32 CUDA cores, one
+    request after another on one stream, no batching), at each rate.  Per rate: Msamples/s =
+    samples of all requests / (last completion - first arrival), and latency percentiles
+    (completion - arrival).  Inputs are device-resident (4 buffers per size)."""
     import torch
     import fmmfft
-    torch.cuda.set_device(0)
-    reqs = serving_requests(a.rate, a.duration, 7)
-    nbuf = 4
-    bufs = {}
-    for (_, N, P, T, b, prec) in reqs:
-        if N not in bufs:
-            bufs[N] = [(torch.randn(N, dtype=torch.complex64, device="cuda"),
-                        torch.empty(N, dtype=torch.complex64, device="cuda")) for _ in range(nbuf)]
-    total = sum(r[1] for r in reqs)
     budget = 120 << 30
-    srv = fmmfft.Server(budget, nstreams=8)
-    # warm: make every shape's plans and graphs resident (plan build is not a request cost)
-    seen = {}
-    for (_, N, P, T, b, prec) in reqs:
-        key = (N, P, T, b, prec)
-        if key in seen:
-            continue
-        seen[key] = 1
-        for k in range(nbuf):
-            x, y = bufs[N][k]
-            srv.wait(srv.submit(N, P, T, b, prec, x.data_ptr(), y.data_ptr()))
-    torch.cuda.synchronize()
+    nbuf = 4
+    out = {}
+    allreqs = {r: serving_requests(r, count, seed) for r in rates}
+    sizes = sorted({q[1] for reqs in allreqs.values() for q in reqs})
+    bufs = {N: [(torch.randn(N, dtype=torch.complex64, device="cuda"),
+                 torch.empty(N, dtype=torch.complex64, device="cuda")) for _ in range(nbuf)]
+            for N in sizes}
+    shapes = sorted({q[1:] for reqs in allreqs.values() for q in reqs})
 
-    def drive(submit, poll):
-        lat, pend, counter = [], [], {}
+    def pct(v, q):
+        v = sorted(v)
+        return v[min(len(v) - 1, int(q * len(v)))] * 1e3 if v else None
+
+    def drive(reqs, submit, poll):
+        lat, pend = [], []
+        counter = {}
         t0 = time.perf_counter()
         i = 0
         while i < len(reqs) or pend:
             now = time.perf_counter() - t0
             while i < len(reqs) and reqs[i][0] <= now:
-                arr, N, P, T, b, prec = reqs[i]
+                arr, N, P, T, b = reqs[i]
                 k = counter.get(N, 0)
-                counter[N] = k + 1
                 x, y = bufs[N][k % nbuf]
-                h = submit(N, P, T, b, prec, x, y)
-                if h is None:  # refused: retry on the next pass
+                h = submit(N, P, T, b, x, y)
+                if h is None:  # refused (admission): retried on the next pass
                     break
+                counter[N] = k + 1
                 pend.append((h, arr))
                 i += 1
             now = time.perf_counter() - t0
@@ -374,52 +373,85 @@ def run_serving(a):
                 else:
                     keep.append((h, arr))
             pend = keep
-        return time.perf_counter() - t0, lat
+        span = time.perf_counter() - t0 - reqs[0][0]
+        return span, lat
 
-    def srv_submit(N, P, T, b, prec, x, y):
+    # served: one server for all rates, warmed so that every lane's plans and graphs exist
+    srv = fmmfft.Server(budget, nstreams=3)
+
+    def srv_submit(N, P, T, b, x, y):
         try:
-            return srv.submit(N, P, T, b, prec, x.data_ptr(), y.data_ptr())
+            return srv.submit(N, P, T, b, served_prec, x.data_ptr(), y.data_ptr())
         except fmmfft.FmmFftError as e:
             if e.status == 7:
                 return None
             raise
 
-    span_s, lat_s = drive(srv_submit, srv.done)
+    for (N, P, T, b) in shapes:
+        nbmax = max(1, min(32, (1 << 21) // N))
+        for burst in (1, 2, 4, 8, 16, 32, 32, 32):
+            if burst > nbmax and burst != 1:
+                continue
+            hs = [srv_submit(N, P, T, b, *bufs[N][j % nbuf]) for j in range(burst)]
+            for h in hs:
+                srv.wait(h)
+    torch.cuda.synchronize()
+    served = {}
+    for r in rates:
+        reqs = allreqs[r]
+        total = sum(q[1] for q in reqs)
+        span, lat = drive(reqs, srv_submit, srv.done)
+        served[r] = (total / span / 1e6, pct(lat, 0.5), pct(lat, 0.99), len(reqs))
     st = srv.stats()
     srv.close()
 
-    # plain per-request comparator: resident plans, one request at a time, no graphs
-    plans = {}
+    # plain: resident FP32 plans, each request executed and synchronised before the next
+    plans = {sh: fmmfft.Plan(*sh, plain_prec) for sh in shapes}
     stream = torch.cuda.current_stream()
-    for (_, N, P, T, b, prec) in reqs:
-        if (N, P, T, b, prec) not in plans:
-            plans[(N, P, T, b, prec)] = fmmfft.Plan(N, P, T, b, prec)
+    for sh, pl in plans.items():
+        x, y = bufs[sh[0]][0]
+        pl.execute_ptr(x.data_ptr(), y.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
 
-    def plain_submit(N, P, T, b, prec, x, y):
-        plans[(N, P, T, b, prec)].execute_ptr(x.data_ptr(), y.data_ptr(), stream.cuda_stream)
+    def plain_submit(N, P, T, b, x, y):
+        plans[(N, P, T, b)].execute_ptr(x.data_ptr(), y.data_ptr(), stream.cuda_stream)
         torch.cuda.synchronize()
         return True
 
-    span_p, lat_p = drive(plain_submit, lambda h: True)
+    for r in rates:
+        reqs = allreqs[r]
+        total = sum(q[1] for q in reqs)
+        span, lat = drive(reqs, plain_submit, lambda h: True)
+        sv = served[r]
+        out[str(int(r))] = {
+            "requests": sv[3], "offered_msamples_s": total / reqs[-1][0] / 1e6,
+            "served": {"value": sv[0], "unit": UNIT, "p50_ms": sv[1], "p99_ms": sv[2]},
+            "plain": {"value": total / span / 1e6, "unit": UNIT, "p50_ms": pct(lat, 0.5),
+                      "p99_ms": pct(lat, 0.99)},
+            "ratio": sv[0] / (total / span / 1e6)}
+    for pl in plans.values():
+        pl.close()
+    return {"rates": out, "resident_plans": st["plans"], "resident_plan_bytes": st["hbm_used"],
+            "config": {"N": "2^10..2^24 log-uniform, complex64 iid normal", "P": "min(64, max(2, N/512))",
+                       "b": 32, "classes": {"1e-4": "p=8", "1e-6": "p=20"},
+                       "served": f"request server, continuous batching, {served_prec}",
+                       "plain": f"one request at a time, {plain_prec} plans on CUDA cores, no batching",
+                       "hbm_budget_bytes": budget, "requests_per_rate": count}}
 
-    def pct(v, q):
-        v = sorted(v)
-        return v[min(len(v) - 1, int(q * len(v)))] * 1e3 if v else None
 
+def run_serving(a):
+    import torch
+    torch.cuda.set_device(0)
+    res = serve_compare([a.rate], count=a.requests)
+    r = res["rates"][str(int(a.rate))]
     line = {"metric": "Msamples/s and p99 latency, served vs plain FMM-FFT (Poisson arrivals)",
-            "value": total / span_s / 1e6, "unit": UNIT, "n_gpus": 1, "steps": len(reqs),
-            "warmup": 1, "ms_per_step": span_s * 1e3 / max(1, len(reqs)), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "fp32 / fp32 (split-TF32)",
-            "data": "synthetic", "impl": "ours",
-            "config": {"workload": "serving", "rate_per_s": a.rate, "duration_s": a.duration,
-                       "requests": len(reqs), "N": "2^10..2^24 log-uniform",
-                       "classes": {"1e-4": "p=8 fp32", "1e-6": "p=20 tensor-core tree"},
-                       "hbm_budget_bytes": budget, "streams": 8, "resident_plans": st["plans"],
-                       "resident_plan_bytes": st["hbm_used"]},
-            "latency_ms": {"p50": pct(lat_s, 0.5), "p99": pct(lat_s, 0.99)},
-            "plain_per_request": {"value": total / span_p / 1e6, "unit": UNIT,
-                                  "latency_ms": {"p50": pct(lat_p, 0.5), "p99": pct(lat_p, 0.99)},
-                                  "how": "resident plans, fmmfft_execute + synchronise per request"}}
+            "value": r["served"]["value"], "unit": UNIT, "n_gpus": 1, "steps": r["requests"],
+            "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32 (split-TF32 tcgen05)", "data": "synthetic",
+            "impl": "ours", "config": dict(res["config"], workload="serving", rate_per_s=a.rate),
+            "latency_ms": {"p50": r["served"]["p50_ms"], "p99": r["served"]["p99_ms"]},
+            "plain_per_request": r["plain"], "served_over_plain": r["ratio"],
+            "resident_plans": res["resident_plans"]}
     print(json.dumps(line))
     return 0
 
@@ -616,6 +648,10 @@ def main():
             "gpu_launches": launches_per_exec * K,
             "clocks": clocks,
         }
+        if world == 1 and not a.no_served:
+            # the headline comparison: served (continuous batching, tensor cores) against the
+            # plain per-request FP32 FMM-FFT, Poisson arrivals at three rates
+            line["served_vs_plain"] = serve_compare([2000.0, 10000.0, 50000.0], count=a.requests)
         if world == 1 and not a.no_cpu_baseline:
             cpu = reference_cpu(N, P, T, b, 2, 0, budget_s=60.0)
             line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}

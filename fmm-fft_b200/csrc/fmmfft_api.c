@@ -14,6 +14,8 @@
 struct fmmfft_plan_s {
   long N, P, M, T, b;
   int precision;
+  int max_transforms; /* batch capacity: transforms one execute may carry */
+  size_t refine_bytes; /* FP64 companion plan + scratch of the residual pass, once enabled */
   size_t device_bytes;
   fmmk_state *dev;
 };
@@ -35,20 +37,42 @@ const char *fmmfft_last_error_string(void) { return t_msg; }
 
 /* ------------------------------------------------------------------ native API */
 int fmmfft_plan_create(fmmfft_plan *out, long N, long P, long terms, long b, int precision) {
-  if (!out) return set_err(FMMFFT_ERR_INVALID, "plan_create: NULL output pointer");
-  *out = NULL;
+  return fmmfft_plan_create_batched(out, N, P, terms, b, precision, 1);
+}
+
+static int check_shape(long N, long P, long terms, long b, int precision, int nb) {
   if (precision < FMMFFT_F64 || precision > FMMFFT_F32_TC)
     return set_err(FMMFFT_ERR_INVALID, "plan_create: unknown precision");
+  if (nb < 1 || nb > 64) return set_err(FMMFFT_ERR_INVALID, "plan_create: max_transforms outside 1..64");
   if (P < 2 || N <= 0 || N % P)
     return set_err(FMMFFT_ERR_INVALID, "plan_create: N must be a positive multiple of P >= 2");
-  long M = N / P;
-  if (!fmm_validate(M, P, terms, b)) {
+  if (!fmm_validate(N / P, P, terms, b)) {
     char m[200];
     snprintf(m, sizeof m,
              "plan_create: unsupported (N=%ld, P=%ld, terms=%ld, b=%ld): need powers of two, "
              "2<=P<=1024, b>=2, M/b>=4, 2<=terms<=64, M<=2^26", N, P, terms, b);
     return set_err(FMMFFT_ERR_INVALID, m);
   }
+  return FMMFFT_OK;
+}
+
+int fmmfft_plan_bytes(long N, long P, long terms, long b, int precision, int max_transforms,
+                      size_t *bytes) {
+  if (!bytes) return set_err(FMMFFT_ERR_INVALID, "plan_bytes: NULL output pointer");
+  int rc = check_shape(N, P, terms, b, precision, max_transforms);
+  if (rc) return rc;
+  char err[256] = {0};
+  rc = fmmk_plan_bytes(N / P, P, terms, b, precision, max_transforms, bytes, err, sizeof err);
+  return rc ? set_err(rc, err) : FMMFFT_OK;
+}
+
+int fmmfft_plan_create_batched(fmmfft_plan *out, long N, long P, long terms, long b, int precision,
+                               int max_transforms) {
+  if (!out) return set_err(FMMFFT_ERR_INVALID, "plan_create: NULL output pointer");
+  *out = NULL;
+  int rc0 = check_shape(N, P, terms, b, precision, max_transforms);
+  if (rc0) return rc0;
+  long M = N / P;
   fmm_ops64 ops;
   int rc = fmm_ops64_build(M, P, terms, b, &ops);
   if (rc) return set_err(FMMFFT_ERR_NOMEM, "plan_create: host allocation failed");
@@ -58,13 +82,14 @@ int fmmfft_plan_create(fmmfft_plan *out, long N, long P, long terms, long b, int
     return set_err(FMMFFT_ERR_NOMEM, "plan_create: host allocation failed");
   }
   char err[256] = {0};
-  rc = fmmk_create(&ops, precision, &pl->dev, &pl->device_bytes, err, sizeof err);
+  rc = fmmk_create_n(&ops, precision, max_transforms, &pl->dev, &pl->device_bytes, err, sizeof err);
   fmm_ops64_free(&ops);
   if (rc) {
     free(pl);
     return set_err(rc, err);
   }
   pl->N = N, pl->P = P, pl->M = M, pl->T = terms, pl->b = b, pl->precision = precision;
+  pl->max_transforms = max_transforms;
   *out = pl;
   return set_err(FMMFFT_OK, NULL);
 }
@@ -78,7 +103,7 @@ int fmmfft_plan_destroy(fmmfft_plan plan) {
 
 int fmmfft_plan_device_bytes(fmmfft_plan plan, size_t *bytes) {
   if (!plan || !bytes) return set_err(FMMFFT_ERR_INVALID, "plan_device_bytes: NULL argument");
-  *bytes = plan->device_bytes;
+  *bytes = plan->device_bytes + plan->refine_bytes;
   return FMMFFT_OK;
 }
 
@@ -95,6 +120,47 @@ int fmmfft_execute(fmmfft_plan plan, const void *d_in, void *d_out, void *stream
 
 int fmmfft_execute_inverse(fmmfft_plan plan, const void *d_in, void *d_out, void *stream) {
   return exec_common(plan, d_in, d_out, stream, 1);
+}
+
+int fmmfft_execute_many(fmmfft_plan plan, int count, const void *d_in, void *d_out, void *stream) {
+  if (!plan || !d_in || !d_out) return set_err(FMMFFT_ERR_INVALID, "execute_many: NULL argument");
+  if (count < 1 || count > plan->max_transforms)
+    return set_err(FMMFFT_ERR_INVALID, "execute_many: count outside 1..max_transforms of the plan");
+  char err[256] = {0};
+  int rc = fmmk_execute_n(plan->dev, d_in, d_out, stream, 0, count, err, sizeof err);
+  return rc ? set_err(rc, err) : FMMFFT_OK;
+}
+
+int fmmfft_execute_many_graph(fmmfft_plan plan, int count, const void *d_in, void *d_out, void *stream) {
+  if (!plan || !d_in || !d_out) return set_err(FMMFFT_ERR_INVALID, "execute_many_graph: NULL argument");
+  if (count < 1 || count > plan->max_transforms)
+    return set_err(FMMFFT_ERR_INVALID, "execute_many_graph: count outside 1..max_transforms of the plan");
+  char err[256] = {0};
+  int rc = fmmk_execute_graph_n(plan->dev, d_in, d_out, stream, 0, count, err, sizeof err);
+  return rc ? set_err(rc, err) : FMMFFT_OK;
+}
+
+int fmmfft_plan_enable_refinement(fmmfft_plan plan) {
+  if (!plan) return set_err(FMMFFT_ERR_INVALID, "enable_refinement: NULL plan");
+  if (plan->precision == FMMFFT_F64)
+    return set_err(FMMFFT_ERR_INVALID, "enable_refinement: the plan is FP64 already");
+  fmm_ops64 ops;
+  if (fmm_ops64_build(plan->M, plan->P, plan->T, plan->b, &ops))
+    return set_err(FMMFFT_ERR_NOMEM, "enable_refinement: host allocation failed");
+  char err[256] = {0};
+  size_t extra = 0;
+  int rc = fmmk_refine_enable(plan->dev, &ops, &extra, err, sizeof err);
+  fmm_ops64_free(&ops);
+  if (rc) return set_err(rc, err);
+  plan->refine_bytes = extra;
+  return FMMFFT_OK;
+}
+
+int fmmfft_execute_refined(fmmfft_plan plan, const void *d_in, void *d_out, void *stream) {
+  if (!plan || !d_in || !d_out) return set_err(FMMFFT_ERR_INVALID, "execute_refined: NULL argument");
+  char err[256] = {0};
+  int rc = fmmk_execute_refined(plan->dev, d_in, d_out, stream, err, sizeof err);
+  return rc ? set_err(rc, err) : FMMFFT_OK;
 }
 
 int fmmfft_execute_host(fmmfft_plan plan, const void *h_in, void *h_out, void *stream) {
@@ -135,6 +201,14 @@ int fmmfft_plan_check(fmmfft_plan plan) {
   if (rc == FMMFFT_ERR_TIMEOUT)
     return set_err(rc, "plan_check: a bounded wait in a tensor-core kernel gave up");
   return rc ? set_err(rc, "plan_check: CUDA error") : FMMFFT_OK;
+}
+
+int fmmfft_plan_selftest_wait(fmmfft_plan plan, int which, long limit_us) {
+  if (!plan || (which != 0 && which != 1) || limit_us < 1 || limit_us > 2000000)
+    return set_err(FMMFFT_ERR_INVALID, "plan_selftest_wait: which must be 0 or 1, limit 1..2e6 us");
+  char err[256] = {0};
+  int rc = fmmk_selftest_wait(plan->dev, which, limit_us, err, sizeof err);
+  return rc ? set_err(rc, err) : FMMFFT_OK;
 }
 
 int fmmfft_execute_graph(fmmfft_plan plan, const void *d_in, void *d_out, void *stream) {

@@ -46,6 +46,19 @@ int fmmk_create(const fmm_ops64 *ops, int precision, fmmk_state **out, size_t *d
 void fmmk_destroy(fmmk_state *st);
 int fmmk_execute(fmmk_state *st, const void *d_in, void *d_out, void *stream, int inverse,
                  char *err, size_t errlen);
+/* Batched forms: a plan made for up to nb transforms of its shape; an execute of nbt <= nb
+ * transforms whose inputs and outputs are N apart. */
+int fmmk_create_n(const fmm_ops64 *ops, int precision, int nb, fmmk_state **out, size_t *device_bytes,
+                  char *err, size_t errlen);
+int fmmk_execute_n(fmmk_state *st, const void *d_in, void *d_out, void *stream, int inverse, int nbt,
+                   char *err, size_t errlen);
+int fmmk_refine_enable(fmmk_state *st, const fmm_ops64 *ops, size_t *bytes, char *err, size_t errlen);
+int fmmk_execute_refined(fmmk_state *st, const void *d_in, void *d_out, void *stream, char *err,
+                         size_t errlen);
+int fmmk_plan_bytes(long M, long P, long T, long b, int precision, int nb, size_t *bytes, char *err,
+                    size_t errlen);
+int fmmk_execute_graph_n(fmmk_state *st, const void *d_in, void *d_out, void *stream, int inverse,
+                         int nbt, char *err, size_t errlen);
 int fmmk_execute_host(fmmk_state *st, const void *h_in, void *h_out, void *stream, char *err,
                       size_t errlen);
 int fmmk_debug_fetch(fmmk_state *st, double *u, double *z, double *phi, double *psi);
@@ -54,6 +67,7 @@ int fmmk_profile_start(fmmk_state *st, int cap);
 int fmmk_profile_stop(fmmk_state *st, double *stage_ms, int *stage_launches, int cap, int *nexec);
 const char *fmmk_stage_name(int i);
 int fmmk_check(fmmk_state *st);
+int fmmk_selftest_wait(fmmk_state *st, int which, long limit_us, char *err, size_t errlen);
 int fmmk_execute_graph(fmmk_state *st, const void *d_in, void *d_out, void *stream, int inverse,
                        char *err, size_t errlen);
 int fmmk_batch_capture(fmmk_state *const *sts, const void *const *ins, void *const *outs,

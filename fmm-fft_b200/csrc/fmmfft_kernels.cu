@@ -93,6 +93,8 @@ template <typename R> struct Dev {
   using C = typename cplx<R>::T;
   long M, P, T, b, s, n, N, S1;
   int precision;
+  int nbmax;    /* transforms one execute may carry (the workspace holds nbmax of each array) */
+  int last_nbt; /* transforms in the last execute (debug_fetch reads the first of them) */
   /* operators */
   R *initch;  /* [b][T] */
   R *btop;    /* [T][T]       btop[k][t] = topflp[t][k] */
@@ -108,10 +110,10 @@ template <typename R> struct Dev {
   R *xt;      /* [2P][M] */
   C *part;    /* [ntile][P] */
   C *ssum;    /* [P] */
-  R *phi, *psi;
-  R *u;       /* [2(P-1)][M] */
-  C *z;       /* [P][M] */
-  C *tmp;     /* [P][M] */
+  R *phi, *psi; /* per level l: [transform][2(P-1)][2^l][T], levels 2..n back to back */
+  R *u;       /* [transform][2(P-1)][M] */
+  C *z;       /* [transform][P][M] */
+  C *tmp;     /* [transform][P][M] */
   long ntile, tileM;
   long M1, M2; /* size-M FFT split (M2 = 1 when one pass) */
   size_t bytes;
@@ -126,6 +128,10 @@ template <typename R> struct Dev {
   float *tc_leaf[2];    /* per section, stride tc_leaf_stride */
   float *leaf_fix;      /* tensor-core leaf, section P/2: [2][s] first points from box-1 */
   long tc_m2m_stride, tc_m2l_stride, tc_leaf_stride;
+  /* the same operators for the warp-specialised kernel: hi rows then lo rows in the MMA's
+   * core-matrix layout (tc::ws_b_index), one block per level or section */
+  float *ws_s2m, *ws_m2m, *ws_m2l, *ws_leaf;
+  long ws_m2m_stride, ws_m2l_stride, ws_leaf_stride;
   int kp_s2m, np_s2m, kp_m2m, np_m2m, kp_m2l, np_m2l, kp_leaf, np_leaf;
   int ok_s2m, ok_m2m, ok_m2l, ok_leaf;
   long tc_min_rows; /* stages with fewer rows use the CUDA-core kernel */
@@ -143,18 +149,28 @@ template <typename R> struct Dev {
 
 /* Instantiated CUDA graphs of one plan's execute, keyed by (input, output, direction): the
  * ~35 kernel launches of a transform become one graph launch. */
-#define FMMK_GRAPHS 8
+#define FMMK_GRAPHS 24
+#define FMMK_MAX_BATCH 64 /* transforms one batched execute may carry */
 struct GraphSlot {
   const void *in;
   void *out;
-  int inverse;
+  int inverse, nbt;
   unsigned long long last_use;
   cudaGraphExec_t exec;
+};
+
+/* FP64 residual-correction companion of a complex64 plan (fmmk_refine_enable) */
+struct Refine {
+  fmmk_state *f64;  /* FP64 plan of the same (N, P, terms, b) */
+  float2 *a, *c;    /* [N] complex64 scratch */
+  double2 *bq;      /* [N] complex128 scratch */
+  size_t bytes;
 };
 
 struct fmmk_state {
   int precision;
   void *dev; /* Dev<float> or Dev<double> */
+  Refine *refine;
   GraphSlot graphs[FMMK_GRAPHS];
   unsigned long long graph_clock;
 };
@@ -205,6 +221,11 @@ __global__ void k_sections(const typename cplx<R>::T *__restrict__ x, R *__restr
                            int T) {
   using C = typename cplx<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  { /* transform blockIdx.y of a batch: inputs N apart, workspace arrays per transform */
+    const long tr = blockIdx.y;
+    x += tr * M * P, xt += tr * 2 * M * P, part += tr * (long)gridDim.x * P;
+    if (phi_n != nullptr) phi_n += tr * 2 * (long)(P - 1) * (M / b) * T;
+  }
   C *tile = reinterpret_cast<C *>(smem_raw); /* [TMt][P + 1]: the pad spreads a column over banks */
   R *ich = reinterpret_cast<R *>(tile + (long)TMt * (P + 1)); /* initch [b][T] when S2M is fused */
   const int PP = P + 1, lp = __ffs(P) - 1, lt = __ffs(TMt) - 1;
@@ -316,6 +337,7 @@ __global__ void k_sum_sections(const typename cplx<R>::T *__restrict__ part, lon
   using C = typename cplx<R>::T;
   __shared__ C red[256];
   const int sc = blockIdx.x;
+  part += (long)blockIdx.y * ntile * P, ssum += (long)blockIdx.y * P; /* transform of a batch */
   C acc;
   acc.x = 0, acc.y = 0;
   /* loads 8 at a time, additions in the same fixed order */
@@ -349,8 +371,9 @@ template <typename R> struct ProbS2M {
   R *out;
   long rows, M;
   int K, N;
+  long tr_rows; /* rows per transform: 2 (P - 1) s; transform tr's sections start 2 M (tr + 1) in */
   __device__ void begin(int) {}
-  __device__ R a(long r, int k) const { return xt[2 * M + r * K + k]; }
+  __device__ R a(long r, int k) const { return xt[2 * M * (r / tr_rows + 1) + r * K + k]; }
   __device__ R bv(int k, int n) const { return B[k * N + n]; }
   __device__ R *d(long r) const { return out + r * N; }
 };
@@ -439,6 +462,8 @@ struct TcBase {
   int batches, nchunks, clen[4], coff[4], kpad, npad, nout;
   const float *bhi, *blo;
   long bstride;
+  const float *wsb; /* warp-specialised form: operator of batch z at wsb + z * wsb_stride */
+  long wsb_stride;
   int yoff[4]; /* TMA-fed form: row offset of chunk c's 2-D block (chunk c of row r = row r + yoff[c]) */
   static constexpr bool kEpiAlternate = false; /* row-form epilogue: one half of N per warp */
   __device__ bool wraps(int, long) const { return false; }
@@ -460,9 +485,9 @@ struct TcBase {
 struct TcS2M : TcBase {
   const float *xt;
   float *out;
-  long M;
+  long M, tr_rows; /* rows per transform: 2 (P - 1) s */
   int b, T;
-  __device__ const float *src(int, long r, int) const { return xt + 2 * M + r * b; }
+  __device__ const float *src(int, long r, int) const { return xt + 2 * M * (r / tr_rows + 1) + r * b; }
   __device__ float *dst(long r, int) const { return out + r * T; }
 };
 
@@ -509,16 +534,17 @@ struct TcLeaf : TcBase { /* batch z = section - 1; s is a power of two (log2s) *
   float *u, *fixbuf;
   long M, s;
   int T, b, log2s, P;
+  /* row r = (transform tr, plane ri, box bx), r = (2 tr + ri) s + bx; plane pl of transform tr
+   * (pl = 2 z + ri) is expansion / field plane tr (2 (P - 1)) + pl and sample plane tr 2 P + pl + 2 */
+  __device__ long plane(long r, int z) const {
+    return (r >> (log2s + 1)) * 2 * (P - 1) + 2L * z + ((r >> log2s) & 1);
+  }
   __device__ const float *src(int c, long r, int z) const {
-    const long pl0 = 2L * z;
-    if (c == 0) return psi_n + pl0 * s * T + r * T;
-    long ri = r >> log2s, bx = r & (s - 1);
-    return xt + (pl0 + 2 + ri) * M + (((bx - 2 + c) * b) & (M - 1));
+    const long bx = r & (s - 1), pl = plane(r, z);
+    if (c == 0) return psi_n + (pl * s + bx) * T;
+    return xt + (pl + 2 * (r >> (log2s + 1)) + 2) * M + (((bx - 2 + c) * b) & (M - 1));
   }
-  __device__ float *dst(long r, int z) const {
-    long ri = r >> log2s, bx = r & (s - 1);
-    return u + (2L * z + ri) * M + bx * b;
-  }
+  __device__ float *dst(long r, int z) const { return u + plane(r, z) * M + (r & (s - 1)) * b; }
   __device__ void put8(float *dst, long r, int z, int c0, const float *t) const {
     const int sc = z + 1;
     const bool shifted = 2 * sc > P; /* the in-box first point is replaced */
@@ -532,11 +558,11 @@ struct TcLeaf : TcBase { /* batch z = section - 1; s is a power of two (log2s) *
     }
     if (2 * sc >= P && c0 <= b && b < c0 + 8) { /* column b: b - c0 is 0 or 4 */
       const float v = b == c0 ? t[0] : t[4];
-      const long ri = r >> log2s, nb = (r + 1) & (s - 1);
+      const long nb = (r + 1) & (s - 1);
       if (shifted)
-        u[(2L * z + ri) * M + nb * b] = v;
+        u[plane(r, z) * M + nb * b] = v;
       else
-        fixbuf[(ri << log2s) + nb] = v;
+        fixbuf[((r >> log2s) << log2s) + nb] = v; /* [transform][plane][box] */
     }
   }
   __device__ void put4(float *dst, long r, int z, int c, float4 v) const { /* c a multiple of 4 */
@@ -547,11 +573,11 @@ struct TcLeaf : TcBase { /* batch z = section - 1; s is a power of two (log2s) *
       else
         *reinterpret_cast<float4 *>(dst + c) = v;
     } else if (c == b && 2 * sc >= P) { /* column b */
-      const long ri = r >> log2s, nb = (r + 1) & (s - 1);
+      const long nb = (r + 1) & (s - 1);
       if (2 * sc > P)
-        u[(2L * z + ri) * M + nb * b] = v.x;
+        u[plane(r, z) * M + nb * b] = v.x;
       else
-        fixbuf[(ri << log2s) + nb] = v.x;
+        fixbuf[((r >> log2s) << log2s) + nb] = v.x;
     }
   }
 };
@@ -704,6 +730,23 @@ template <class Prob> static bool tc_form_fits(const Prob &pb) {
 template <class Prob>
 static void launch_tc(const Prob &pb0, int num_sms, int *status, cudaStream_t st, int form, int pdl) {
   Prob pb = pb0;
+  if (form == 4 && tc::ws_fits(pb.kpad, pb.npad)) {
+    const long tiles = (pb.rows + tc::kRows - 1) / tc::kRows * pb.batches;
+    const int grid = (int)(tiles < num_sms ? tiles : num_sms); /* one CTA per SM: all of TMEM */
+    const size_t smem = tc::ws_smem_bytes(pb.kpad, pb.npad);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(tc::kWThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, tc::k_tc_ws<Prob>, pb, status);
+    return;
+  }
   if (form == 2 && pb.batches == 1 && pb.npad <= 64 && pb.nout <= 64 && pb.kpad % 8 == 0 &&
       pb.kpad <= 256) {
     const int stages = tc::m_smem_bytes(pb.kpad, 4) <= (size_t)220 * 1024 ? 4 : 2;
@@ -771,6 +814,10 @@ __global__ void __launch_bounds__(256) k_leaf_fix(const R *__restrict__ psi_n, c
                                                   int P) {
   const int sc = P / 2 + blockIdx.y; /* sc in [P/2, P-1] */
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  { /* transform blockIdx.z of a batch */
+    const long tr = blockIdx.z;
+    psi_n += tr * 2 * (P - 1) * s * T, xt += tr * 2 * P * M, u += tr * 2 * (P - 1) * M;
+  }
   const R *eh = evalmh + (long)(sc - 1) * T;
   const R *ct = cot + (long)(sc - 1) * 4 * b;
   const long i0 = ((long)blockIdx.x * 8 + warp) * kFixBoxes;
@@ -804,9 +851,9 @@ __global__ void k_leaf_mid(R *__restrict__ u, const float *__restrict__ fixbuf, 
                            int P) {
   const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= 2 * s) return;
-  const long ri = idx >> log2s, bx = idx & (s - 1);
-  R *dst = u + (2L * (P / 2 - 1) + ri) * M + bx * b;
-  *dst = R(0.5) * (*dst + (R)fixbuf[idx]);
+  const long ri = idx >> log2s, bx = idx & (s - 1), tr = blockIdx.y;
+  R *dst = u + (tr * 2 * (P - 1) + 2L * (P / 2 - 1) + ri) * M + bx * b;
+  *dst = R(0.5) * (*dst + (R)fixbuf[tr * 2 * s + idx]);
 }
 
 /* Leaf stage, direct form (b a multiple of 8): far field (L2T) plus near field of one re/im
@@ -848,6 +895,10 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 1) k_leaf(const R *_
   R *cts = ct + 4 * b;                     /* 4b: cts[e] = ct[e + 1] (FP32 pairs of odd offset) */
   R *eh = cts + 4 * b;                     /* T (rounded up to 8) */
   R *Es = eh + ((T + 7) & ~7);             /* T b when e_in_smem */
+  { /* transform blockIdx.z of a batch */
+    const long tr = blockIdx.z;
+    psi_n += tr * 2 * (P - 1) * s * T, xt += tr * 2 * P * M, u += tr * 2 * (P - 1) * M;
+  }
   const int pl = blockIdx.y, sc = pl / 2 + 1;
   const long B0 = (long)blockIdx.x * NB;
   const R *xs = xt + (long)(pl + 2) * M;
@@ -1213,8 +1264,12 @@ template <typename R> struct CombineLd {
   const typename cplx<R>::T *__restrict__ ssum, *__restrict__ pretw;
   long M;
   R invM;
-  __device__ __forceinline__ void operator()(long, unsigned m, int t, int q,
+  int P;
+  /* row = transform of a batch: its sections, fields and section sums */
+  __device__ __forceinline__ void operator()(long row, unsigned m, int t, int q,
                                              typename cplx<R>::T (&v)[8]) const {
+    const R *xt = this->xt + row * 2 * P * M, *u = this->u + row * 2 * (P - 1) * M;
+    const typename cplx<R>::T *ssum = this->ssum + row * P;
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
       const int sc = t + r * q;
@@ -1411,6 +1466,10 @@ __global__ void k_combine(const R *__restrict__ xt, const R *__restrict__ u,
   C *alt = buf + (long)P * TMc;
   const long m0 = (long)blockIdx.x * TMc;
   const R invM = R(1) / R(M);
+  { /* transform blockIdx.y of a batch */
+    const long tr = blockIdx.y;
+    xt += tr * 2 * P * M, u += tr * 2 * (P - 1) * M, ssum += tr * P, z += tr * P * M;
+  }
   for (int e = threadIdx.x; e < P * TMc; e += blockDim.x) {
     int mm = e % TMc, sc = e / TMc;
     C w;
@@ -1447,6 +1506,7 @@ __global__ void k_block_dc(const typename cplx<R>::T *__restrict__ ssum,
   using C = typename cplx<R>::T;
   const int r = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (r >= P) return;
+  ssum += (long)blockIdx.y * P, y += (long)blockIdx.y * P * M; /* transform of a batch */
   double re = 0, im = 0;
   for (int sc = lane; sc < P; sc += 32) {
     double sn, cs;
@@ -1490,8 +1550,10 @@ template <typename R> struct CoarseArgs {
 
 constexpr unsigned long long kGridWaitNs = 1000000000ull; /* 1 s per barrier */
 
-/* Grid-wide barrier of a cooperative launch; false when a block waited 1 s (status set). */
-__device__ __forceinline__ bool grid_barrier(unsigned *sync, int *status) {
+/* Grid-wide barrier of a cooperative launch; false when a block waited limit_ns (1 s by
+ * default; status set). */
+__device__ __forceinline__ bool grid_barrier(unsigned *sync, int *status,
+                                             unsigned long long limit_ns = kGridWaitNs) {
   __shared__ int gb_fail;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -1512,7 +1574,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned *sync, int *status) {
           asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
           if (t0 == 0) {
             t0 = now;
-          } else if (now - t0 > kGridWaitNs) {
+          } else if (now - t0 > limit_ns) {
             atomicExch(status, 1);
             gb_fail = 1;
             break;
@@ -1657,6 +1719,38 @@ template <typename R> __global__ void __launch_bounds__(256, 1) k_coarse(CoarseA
   }
 }
 
+/* Self-test of the bounded device waits: the same wait routines as the tensor-core kernels
+ * (tc::t_wait on an mbarrier, with tensor memory held) and the coarse-tree kernel (grid_barrier),
+ * each made to wait for an event that never comes (an mbarrier nobody arrives on; a grid barrier
+ * whose arrival count starts past the grid size, so no block is ever the last), with a short
+ * limit.  The wait gives up, records the error in `status`, the tensor memory is freed and the
+ * kernel returns: the host then sees FMMFFT_ERR_TIMEOUT and the context stays usable.
+ * which = 0: mbarrier wait; 1: grid barrier (one block; sync[0] preset by the host). */
+__global__ void __launch_bounds__(64) k_selftest_wait(int which, unsigned long long limit_ns,
+                                                      unsigned *sync, int *status) {
+  __shared__ uint64_t bar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ volatile int abort_flag;
+  if (which == 0) {
+    if (threadIdx.x < 32) tc::tmem_alloc(&tmem_slot, 32);
+    if (threadIdx.x == 0) {
+      tc::mbar_init(&bar, 1);
+      tc::fence_mbar_init();
+      abort_flag = 0;
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (threadIdx.x == 0) tc::t_wait(&bar, 0, &abort_flag, status, limit_ns);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (threadIdx.x < 32) tc::tmem_dealloc(tmem_slot, 32);
+  } else {
+    grid_barrier(sync, status, limit_ns);
+  }
+}
+
 /* ======================================================================== host orchestration */
 
 template <typename R> static int upload(R **dst, const double *src, size_t n, char *err, size_t errlen) {
@@ -1692,18 +1786,28 @@ static float tf32_rna_host(float f) {
   return r;
 }
 
-/* Uploads one operator, given as FP64 [npad][kpad] K-major values, split into TF32 hi and lo. */
-static int tc_put(float *dhi, float *dlo, const double *v, long cnt, char *err, size_t errlen) {
-  float *h = (float *)malloc(sizeof(float) * 2 * (cnt ? cnt : 1));
+/* Uploads one operator, given as FP64 [npad][kpad] K-major values, split into TF32 hi and lo:
+ * as two [npad][kpad] arrays (dhi, dlo) and, when dws is given, as the warp-specialised
+ * kernel's block (hi rows 0..npad-1, lo rows npad..2 npad-1, core-matrix layout). */
+static int tc_put(float *dhi, float *dlo, float *dws, const double *v, int kpad, int npad, char *err,
+                  size_t errlen) {
+  const long cnt = (long)kpad * npad;
+  const size_t wsn = tc::ws_b_floats(kpad, npad);
+  float *h = (float *)calloc((size_t)2 * cnt + wsn + 1, sizeof(float));
   if (!h) return 2;
+  float *w = h + 2 * cnt;
   for (long i = 0; i < cnt; ++i) {
     float f = (float)v[i];
     float hi = tf32_rna_host(f);
     h[i] = hi;
     h[cnt + i] = tf32_rna_host(f - hi);
+    const int n = (int)(i / kpad), k = (int)(i % kpad);
+    w[tc::ws_b_index(n, k, kpad)] = h[i];
+    w[tc::ws_b_index(npad + n, k, kpad)] = h[cnt + i];
   }
   cudaError_t e = cudaMemcpy(dhi, h, sizeof(float) * cnt, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(dlo, h + cnt, sizeof(float) * cnt, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && dws) e = cudaMemcpy(dws, w, sizeof(float) * wsn, cudaMemcpyHostToDevice);
   free(h);
   if (e != cudaSuccess) {
     snprintf(err, errlen, "cudaMemcpy: %s", cudaGetErrorString(e));
@@ -1727,7 +1831,7 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
     for (long i = 0; i < (long)kp * np; ++i) v[i] = 0;
     for (long nn = 0; nn < T; ++nn)
       for (long k = 0; k < b; ++k) v[nn * kp + k] = o->initch[k * T + nn];
-    rc |= tc_put(d->tc_s2m[0], d->tc_s2m[1], v, (long)kp * np, err, errlen);
+    rc |= tc_put(d->tc_s2m[0], d->tc_s2m[1], d->ws_s2m, v, kp, np, err, errlen);
   }
   if (d->ok_m2m)
     for (long L = 2; L <= n - 1; ++L) {
@@ -1740,7 +1844,7 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
           v[t * kp + T + k] = ops[FMM_SHFTFP * T * T + t * T + k];
         }
       rc |= tc_put(d->tc_m2m[0] + (L - 2) * d->tc_m2m_stride, d->tc_m2m[1] + (L - 2) * d->tc_m2m_stride,
-                   v, (long)kp * np, err, errlen);
+                   d->ws_m2m + (L - 2) * d->ws_m2m_stride, v, kp, np, err, errlen);
     }
   if (d->ok_m2l)
     for (long l = 3; l <= n; ++l) {
@@ -1761,7 +1865,7 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
         }
 #undef OPT
       rc |= tc_put(d->tc_m2l[0] + (l - 3) * d->tc_m2l_stride, d->tc_m2l[1] + (l - 3) * d->tc_m2l_stride,
-                   v, (long)kp * np, err, errlen);
+                   d->ws_m2l + (l - 3) * d->ws_m2l_stride, v, kp, np, err, errlen);
     }
   if (d->ok_leaf)
     for (long sc = 1; sc < P; ++sc) {
@@ -1777,7 +1881,7 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
         for (long q = 0; q < 3 * b; ++q) v[b * kp + T + q] = ct[q];
       }
       rc |= tc_put(d->tc_leaf[0] + (sc - 1) * d->tc_leaf_stride, d->tc_leaf[1] + (sc - 1) * d->tc_leaf_stride,
-                   v, (long)kp * np, err, errlen);
+                   d->ws_leaf + (sc - 1) * d->ws_leaf_stride, v, kp, np, err, errlen);
     }
   free(v);
   return rc;
@@ -1808,8 +1912,12 @@ template <typename R> static void coarse_setup(Dev<R> *d) {
   if (d->coarse_grid < 1) d->coarse_rows = 0; /* operator too large for shared memory */
 }
 
+/* Builds the device plan: operators uploaded, workspace for nb transforms, one cudaMalloc.  With
+ * dry_bytes set it only computes the bytes that plan would hold (o needs its sizes only) and
+ * allocates nothing. */
 template <typename R>
-static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err, size_t errlen) {
+static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, char *err, size_t errlen,
+                      size_t *dry_bytes = nullptr) {
   using C = typename cplx<R>::T;
   Dev<R> *d = new (std::nothrow) Dev<R>();
   if (!d) return 2;
@@ -1817,6 +1925,7 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   const long M = o->M, P = o->P, T = o->T, b = o->b, s = o->s, n = o->n, S1 = P - 1;
   d->M = M, d->P = P, d->T = T, d->b = b, d->s = s, d->n = n, d->N = M * P, d->S1 = S1;
   d->precision = precision;
+  d->nbmax = nb, d->last_nbt = 1;
   d->tileM = P >= 2048 ? 1 : 2048 / P;
   if (d->tileM > M) d->tileM = M;
   d->ntile = M / d->tileM;
@@ -1843,7 +1952,8 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   d->kp_leaf = up8(T + 3 * b), d->np_leaf = up16(b + 1); /* + the half-shifted column */
   auto fits = [&](int kp, int np) {
     return tc && (T % 4 == 0) && (b % 4 == 0) && np <= 256 && kp <= 256 &&
-           tc::smem16_bytes(kp, np) <= (size_t)110 * 1024 && tc::tmem_cols(tc::round16(kp), np) <= 256;
+           tc::smem16_bytes(kp, np) <= (size_t)110 * 1024 && tc::tmem_cols(tc::round16(kp), np) <= 256 &&
+           tc::ws_fits(kp, np);
   };
   d->ok_s2m = fits(d->kp_s2m, d->np_s2m);
   d->ok_m2m = fits(d->kp_m2m, d->np_m2m) && nlev > 0;
@@ -1861,7 +1971,7 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
    * the default because it is faster there (M2L 0.47 ms against 0.58 ms on a B200) */
   d->tc_form = -1;
   if (const char *ev = getenv("FMMFFT_TC_FORM"))
-    d->tc_form = strcmp(ev, "pipelined") == 0 ? 1 : strcmp(ev, "tma") == 0 ? 2 : strcmp(ev, "row") == 0 ? 0 : strcmp(ev, "row16") == 0 ? 3 : -1;
+    d->tc_form = strcmp(ev, "pipelined") == 0 ? 1 : strcmp(ev, "tma") == 0 ? 2 : strcmp(ev, "row") == 0 ? 0 : strcmp(ev, "row16") == 0 ? 3 : strcmp(ev, "ws") == 0 ? 4 : -1;
   d->pdl = 1;
   if (const char *ev = getenv("FMMFFT_PDL")) d->pdl = atoi(ev) != 0;
   coarse_setup(d);
@@ -1886,6 +1996,13 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   const long sz_m2m = d->ok_m2m ? nlev * d->tc_m2m_stride : 0;
   const long sz_m2l = d->ok_m2l ? nlev * d->tc_m2l_stride : 0;
   const long sz_leaf = d->ok_leaf ? S1 * d->tc_leaf_stride : 0;
+  d->ws_m2m_stride = (long)tc::ws_b_floats(d->kp_m2m, d->np_m2m);
+  d->ws_m2l_stride = (long)tc::ws_b_floats(d->kp_m2l, d->np_m2l);
+  d->ws_leaf_stride = (long)tc::ws_b_floats(d->kp_leaf, d->np_leaf);
+  const long ws_s2m_n = d->ok_s2m ? (long)tc::ws_b_floats(d->kp_s2m, d->np_s2m) : 0;
+  const long ws_m2m_n = d->ok_m2m ? nlev * d->ws_m2m_stride : 0;
+  const long ws_m2l_n = d->ok_m2l ? nlev * d->ws_m2l_stride : 0;
+  const long ws_leaf_n = d->ok_leaf ? S1 * d->ws_leaf_stride : 0;
   size_t off = 0;
 #define CARVE(field, count, type)          \
   size_t off_##field = off;                \
@@ -1900,22 +2017,31 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   CARVE(pretw, P, C)
   CARVE(twP, P, C)
   CARVE(twM, M, C)
-  CARVE(xt, 2 * P * M, R)
-  CARVE(part, d->ntile * P, C)
-  CARVE(ssum, P, C)
-  CARVE(phi, lvtot, R)
-  CARVE(psi, lvtot, R)
-  CARVE(u, 2 * S1 * M, R)
-  CARVE(z, P * M, C)
-  CARVE(tmp, P * M, C)
+  CARVE(xt, nb * 2 * P * M, R)
+  CARVE(part, nb * d->ntile * P, C)
+  CARVE(ssum, nb * P, C)
+  CARVE(phi, nb * lvtot, R)
+  CARVE(psi, nb * lvtot, R)
+  CARVE(u, nb * 2 * S1 * M, R)
+  CARVE(z, nb * P * M, C)
+  CARVE(tmp, nb * P * M, C)
   CARVE(status, 1, int)
   CARVE(sync, 64, unsigned)
   CARVE(tcs2m, 2 * sz_s2m, float)
   CARVE(tcm2m, 2 * sz_m2m, float)
   CARVE(tcm2l, 2 * sz_m2l, float)
   CARVE(tcleaf, 2 * sz_leaf, float)
-  CARVE(leaffix, d->ok_leaf ? 2 * s : 0, float)
+  CARVE(leaffix, d->ok_leaf ? nb * 2 * s : 0, float)
+  CARVE(wss2m, ws_s2m_n, float)
+  CARVE(wsm2m, ws_m2m_n, float)
+  CARVE(wsm2l, ws_m2l_n, float)
+  CARVE(wsleaf, ws_leaf_n, float)
 #undef CARVE
+  if (dry_bytes) {
+    *dry_bytes = off;
+    delete d;
+    return 0;
+  }
   void *pool = NULL;
   cudaError_t ce = cudaMalloc(&pool, off);
   if (ce != cudaSuccess) {
@@ -1951,6 +2077,10 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
   d->tc_m2l[0] = (float *)(base + off_tcm2l), d->tc_m2l[1] = d->tc_m2l[0] + sz_m2l;
   d->tc_leaf[0] = (float *)(base + off_tcleaf), d->tc_leaf[1] = d->tc_leaf[0] + sz_leaf;
   d->leaf_fix = (float *)(base + off_leaffix);
+  d->ws_s2m = (float *)(base + off_wss2m);
+  d->ws_m2m = (float *)(base + off_wsm2m);
+  d->ws_m2l = (float *)(base + off_wsm2l);
+  d->ws_leaf = (float *)(base + off_wsleaf);
   cudaMemset(d->status, 0, sizeof(int));
   {
     int dev = 0;
@@ -2038,9 +2168,18 @@ static int dev_create(const fmm_ops64 *o, int precision, Dev<R> **out, char *err
 
 template <typename R>
 static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, int inverse,
-                       char *err, size_t errlen) {
+                       int nbt, char *err, size_t errlen) {
   using C = typename cplx<R>::T;
   const long M = d->M, P = d->P, T = d->T, b = d->b, s = d->s, n = d->n, S1 = d->S1;
+  /* nbt transforms of this shape, inputs and outputs N apart: every tree stage runs over the
+   * rows of all of them at once (the expansion planes of transform tr follow those of tr - 1
+   * within each level), the other stages take the transform as a grid dimension */
+  if (nbt < 1 || nbt > d->nbmax) {
+    snprintf(err, errlen, "execute of %d transforms on a plan that holds %d", nbt, d->nbmax);
+    return 1;
+  }
+  d->last_nbt = nbt;
+  const long S1e = (long)nbt * S1;
   const C *x = (const C *)vin;
   C *y = (C *)vout;
   Prof &pf = d->prof;
@@ -2059,13 +2198,12 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   {
     int TMt = (int)d->tileM;
     size_t sm = sizeof(C) * TMt * (P + 1) + (s2m_fused ? sizeof(R) * b * T : 0);
-    k_sections<R><<<(unsigned)d->ntile, 256, sm, st>>>(x, d->xt, d->part, M, (int)P, TMt, inverse,
-                                                        d->initch,
-                                                        s2m_fused ? d->phi + lvl_off(n, S1, T) : nullptr,
-                                                        (int)b, (int)T);
+    k_sections<R><<<dim3((unsigned)d->ntile, (unsigned)nbt), 256, sm, st>>>(
+        x, d->xt, d->part, M, (int)P, TMt, inverse, d->initch,
+        s2m_fused ? d->phi + lvl_off(n, S1e, T) : nullptr, (int)b, (int)T);
     pf.launches[ST_SECTIONS]++;
     stage(ST_SUMS);
-    k_sum_sections<R><<<(unsigned)P, 256, 0, st>>>(d->part, d->ntile, (int)P, d->ssum);
+    k_sum_sections<R><<<dim3((unsigned)P, (unsigned)nbt), 256, 0, st>>>(d->part, d->ntile, (int)P, d->ssum);
     pf.launches[ST_SUMS]++;
   }
   /* 3: S2M at level n (done in stage 1 when fused) */
@@ -2075,16 +2213,18 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
     if constexpr (sizeof(R) == 4) {
       if (d->tc && d->ok_s2m && 2 * S1 * s >= d->tc_min_rows) {
         TcS2M q{};
-        q.rows = 2 * S1 * s, q.batches = 1, q.nchunks = 1, q.clen[0] = (int)b, q.coff[0] = 0;
+        q.rows = 2 * S1e * s, q.batches = 1, q.nchunks = 1, q.clen[0] = (int)b, q.coff[0] = 0;
+        q.tr_rows = 2 * S1 * s;
         q.kpad = d->kp_s2m, q.npad = d->np_s2m, q.nout = (int)T;
-        q.bhi = d->tc_s2m[0], q.blo = d->tc_s2m[1], q.bstride = 0;
-        q.xt = d->xt, q.out = d->phi + lvl_off(n, S1, T), q.M = M, q.b = (int)b, q.T = (int)T;
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 3 : d->tc_form, d->pdl);
+        q.bhi = d->tc_s2m[0], q.blo = d->tc_s2m[1], q.bstride = 0, q.wsb = d->ws_s2m, q.wsb_stride = 0;
+        q.xt = d->xt, q.out = d->phi + lvl_off(n, S1e, T), q.M = M, q.b = (int)b, q.T = (int)T;
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 4 : d->tc_form, d->pdl);
         done = true;
       }
     }
     if (!done) {
-      ProbS2M<R> pb{d->xt, d->initch, d->phi + lvl_off(n, S1, T), 2 * S1 * s, M, (int)b, (int)T};
+      ProbS2M<R> pb{d->xt, d->initch, d->phi + lvl_off(n, S1e, T), 2 * S1e * s, M, (int)b, (int)T,
+                    2 * S1 * s};
       launch_rowgemm<R>(pb, pb.rows, (int)T, 1, st);
     }
     pf.launches[ST_S2M]++;
@@ -2092,6 +2232,8 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   /* coarse tree: levels below the row threshold run in one cooperative launch (stage 5) */
   long thr = d->coarse_rows;
   if (d->tc && d->tc_min_rows < thr) thr = d->tc_min_rows; /* never take a level off the TCs */
+  /* routing by the row counts of ONE transform, so that a transform takes the same kernels (and
+   * gives the same bits) alone and in a batch */
   const bool coarse = d->sync != nullptr && thr > 2 * S1 * 4;
   long Lm = 1, Ll = 2;
   if (coarse) {
@@ -2107,18 +2249,18 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
     if constexpr (sizeof(R) == 4) {
       if (d->tc && d->ok_m2m && 2 * S1 * (1L << L) >= d->tc_min_rows) {
         TcM2M q{};
-        q.rows = 2 * S1 * (1L << L), q.batches = 1, q.nchunks = 1, q.clen[0] = (int)(2 * T), q.coff[0] = 0;
+        q.rows = 2 * S1e * (1L << L), q.batches = 1, q.nchunks = 1, q.clen[0] = (int)(2 * T), q.coff[0] = 0;
         q.kpad = d->kp_m2m, q.npad = d->np_m2m, q.nout = (int)T;
         q.bhi = d->tc_m2m[0] + (L - 2) * d->tc_m2m_stride, q.blo = d->tc_m2m[1] + (L - 2) * d->tc_m2m_stride;
-        q.bstride = 0;
-        q.child = d->phi + lvl_off(L + 1, S1, T), q.out = d->phi + lvl_off(L, S1, T), q.T = (int)T;
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 3 : d->tc_form, d->pdl);
+        q.bstride = 0, q.wsb = d->ws_m2m + (L - 2) * d->ws_m2m_stride, q.wsb_stride = 0;
+        q.child = d->phi + lvl_off(L + 1, S1e, T), q.out = d->phi + lvl_off(L, S1e, T), q.T = (int)T;
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 4 : d->tc_form, d->pdl);
         done = true;
       }
     }
     if (!done) {
-      ProbM2M<R> pb{d->phi + lvl_off(L + 1, S1, T), d->bm2m + (L - 2) * 2 * T * T,
-                    d->phi + lvl_off(L, S1, T), 2 * S1 * (1L << L), (int)(2 * T), (int)T};
+      ProbM2M<R> pb{d->phi + lvl_off(L + 1, S1e, T), d->bm2m + (L - 2) * 2 * T * T,
+                    d->phi + lvl_off(L, S1e, T), 2 * S1e * (1L << L), (int)(2 * T), (int)T};
       launch_rowgemm<R>(pb, pb.rows, (int)T, 1, st);
     }
     pf.launches[ST_M2M]++;
@@ -2126,15 +2268,15 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   /* 5: top flip, or the whole coarse tree (M2M Lm..2, top flip, M2L 3..Ll) */
   stage(ST_TOP);
   if (coarse) {
-    CoarseArgs<R> ca{d->phi, d->psi, d->bm2m, d->btop, d->bm2l, S1, (int)T, (int)Lm, (int)Ll,
+    CoarseArgs<R> ca{d->phi, d->psi, d->bm2m, d->btop, d->bm2l, S1e, (int)T, (int)Lm, (int)Ll,
                      d->sync, d->status};
     cudaMemsetAsync(d->sync, 0, sizeof(unsigned), st);
     void *args[] = {(void *)&ca};
     /* one warp per row of the largest coarse level, 8 per block: small transforms take a few
      * blocks and leave the rest of the GPU to concurrent work (batch branches, other streams) */
-    long maxrows = 2 * S1 * 4;
-    if (Lm >= 2 && 2 * S1 * (1L << Lm) > maxrows) maxrows = 2 * S1 * (1L << Lm);
-    if (Ll >= 3 && 2 * S1 * (1L << (Ll - 1)) > maxrows) maxrows = 2 * S1 * (1L << (Ll - 1));
+    long maxrows = 2 * S1e * 4;
+    if (Lm >= 2 && 2 * S1e * (1L << Lm) > maxrows) maxrows = 2 * S1e * (1L << Lm);
+    if (Ll >= 3 && 2 * S1e * (1L << (Ll - 1)) > maxrows) maxrows = 2 * S1e * (1L << (Ll - 1));
     long cgrid = (maxrows + 7) / 8;
     if (cgrid > d->coarse_grid) cgrid = d->coarse_grid;
     const cudaError_t ce = cudaLaunchCooperativeKernel((const void *)k_coarse<R>, dim3((unsigned)cgrid),
@@ -2145,7 +2287,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
     }
     pf.launches[ST_TOP]++;
   } else {
-    ProbTop<R> pb{d->phi + lvl_off(2, S1, T), d->btop, d->psi + lvl_off(2, S1, T), 2 * S1 * 4,
+    ProbTop<R> pb{d->phi + lvl_off(2, S1e, T), d->btop, d->psi + lvl_off(2, S1e, T), 2 * S1e * 4,
                   (int)T, (int)T};
     launch_rowgemm<R>(pb, pb.rows, (int)T, 1, st);
     pf.launches[ST_TOP]++;
@@ -2157,22 +2299,22 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
     if constexpr (sizeof(R) == 4) {
       if (d->tc && d->ok_m2l && 2 * S1 * (1L << (l - 1)) >= d->tc_min_rows) {
         TcM2L q{};
-        q.rows = 2 * S1 * (1L << (l - 1)), q.batches = 1, q.nchunks = 3;
+        q.rows = 2 * S1e * (1L << (l - 1)), q.batches = 1, q.nchunks = 3;
         q.clen[0] = (int)T, q.clen[1] = (int)(2 * T), q.clen[2] = (int)(2 * T);
         q.coff[0] = 0, q.coff[1] = (int)T, q.coff[2] = (int)(3 * T);
         q.kpad = d->kp_m2l, q.npad = d->np_m2l, q.nout = (int)(2 * T);
         q.bhi = d->tc_m2l[0] + (l - 3) * d->tc_m2l_stride, q.blo = d->tc_m2l[1] + (l - 3) * d->tc_m2l_stride;
-        q.bstride = 0;
-        q.psi_par = d->psi + lvl_off(l - 1, S1, T), q.phi = d->phi + lvl_off(l, S1, T);
-        q.out = d->psi + lvl_off(l, S1, T), q.T = (int)T, q.lpar = (int)(l - 1);
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 0 : d->tc_form, d->pdl);
+        q.bstride = 0, q.wsb = d->ws_m2l + (l - 3) * d->ws_m2l_stride, q.wsb_stride = 0;
+        q.psi_par = d->psi + lvl_off(l - 1, S1e, T), q.phi = d->phi + lvl_off(l, S1e, T);
+        q.out = d->psi + lvl_off(l, S1e, T), q.T = (int)T, q.lpar = (int)(l - 1);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 4 : d->tc_form, d->pdl);
         done = true;
       }
     }
     if (!done) {
-      ProbM2L<R> pb{d->psi + lvl_off(l - 1, S1, T), d->phi + lvl_off(l, S1, T),
-                    d->bm2l + (l - 3) * 10 * T * T, d->psi + lvl_off(l, S1, T),
-                    2 * S1 * (1L << (l - 1)), (int)(5 * T), (int)(2 * T), (int)T, (int)(l - 1)};
+      ProbM2L<R> pb{d->psi + lvl_off(l - 1, S1e, T), d->phi + lvl_off(l, S1e, T),
+                    d->bm2l + (l - 3) * 10 * T * T, d->psi + lvl_off(l, S1e, T),
+                    2 * S1e * (1L << (l - 1)), (int)(5 * T), (int)(2 * T), (int)T, (int)(l - 1)};
       launch_rowgemm<R>(pb, pb.rows, (int)(2 * T), 1, st);
     }
     pf.launches[ST_M2L]++;
@@ -2181,7 +2323,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   stage(ST_LEAF);
   {
     ProbLeaf<R> pb{};
-    pb.psi_n = d->psi + lvl_off(n, S1, T);
+    pb.psi_n = d->psi + lvl_off(n, S1e, T);
     pb.xt = d->xt;
     pb.evalmT = d->evalmT;
     pb.cot = d->cot;
@@ -2192,15 +2334,16 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
     if constexpr (sizeof(R) == 4) {
       if (d->tc && d->ok_leaf && 2 * s >= (d->tc_min_rows < 256 ? d->tc_min_rows : 256)) {
         TcLeaf q{};
-        q.rows = 2 * s, q.batches = (int)S1, q.nchunks = 4;
+        q.rows = 2 * s * nbt, q.batches = (int)S1, q.nchunks = 4;
         q.clen[0] = (int)T, q.clen[1] = q.clen[2] = q.clen[3] = (int)b;
         q.coff[0] = 0, q.coff[1] = (int)T, q.coff[2] = (int)(T + b), q.coff[3] = (int)(T + 2 * b);
         q.kpad = d->kp_leaf, q.npad = d->np_leaf, q.nout = (int)b;
         q.bhi = d->tc_leaf[0], q.blo = d->tc_leaf[1], q.bstride = d->tc_leaf_stride;
+        q.wsb = d->ws_leaf, q.wsb_stride = d->ws_leaf_stride;
         q.fixbuf = d->leaf_fix, q.P = (int)P;
         q.psi_n = pb.psi_n, q.xt = d->xt, q.u = d->u, q.M = M, q.s = s, q.T = (int)T, q.b = (int)b;
         q.log2s = (int)n;
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 0 : d->tc_form, d->pdl);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 4 : d->tc_form, d->pdl);
         done = true;
       }
     }
@@ -2214,24 +2357,28 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
       size_t sm = sizeof(R) * ((size_t)(NB + 3) * skew_pitch(b) +
                                (((size_t)(NB + 1) * skew_pitch(T) + 7) & ~(size_t)7) + 8 * b +
                                ((T + 7) & ~7) + (e_in_smem ? (size_t)T * b : 0));
-      dim3 g((unsigned)(s / NB), (unsigned)(2 * S1));
+      dim3 g((unsigned)(s / NB), (unsigned)(2 * S1), (unsigned)nbt);
       k_leaf<R><<<g, 256, sm, st>>>(pb.psi_n, d->xt, d->evalmT, d->evalmh, d->cot, d->u, M, s,
                                     (int)T, (int)b, (int)P, NB, e_in_smem);
       pf.launches[ST_LEAF]++;
     } else if (!done) {
-      launch_rowgemm<R>(pb, pb.rows, (int)b, (int)S1, st);
-      pf.launches[ST_LEAF]++;
+      for (int tr = 0; tr < nbt; ++tr) { /* one launch per transform of the batch */
+        ProbLeaf<R> pt = pb;
+        pt.psi_n += (long)tr * 2 * S1 * s * T, pt.xt += (long)tr * 2 * P * M, pt.u += (long)tr * 2 * S1 * M;
+        launch_rowgemm<R>(pt, pt.rows, (int)b, (int)S1, st);
+        pf.launches[ST_LEAF]++;
+      }
       stage(ST_LEAFFIX);
       pf.launches[ST_LEAFFIX]++;
-      dim3 g((unsigned)((2 * s + 8 * kFixBoxes - 1) / (8 * kFixBoxes)), (unsigned)(P - P / 2));
+      dim3 g((unsigned)((2 * s + 8 * kFixBoxes - 1) / (8 * kFixBoxes)), (unsigned)(P - P / 2), (unsigned)nbt);
       k_leaf_fix<R><<<g, 256, 0, st>>>(pb.psi_n, d->xt, d->evalmh, d->cot, d->u, M, s, (int)n, (int)T,
                                        (int)b, (int)P);
     } else { /* tensor-core leaf: it stored the half-shifted points; section P/2 averages them */
       pf.launches[ST_LEAF]++;
       stage(ST_LEAFFIX);
       pf.launches[ST_LEAFFIX]++;
-      k_leaf_mid<R><<<(unsigned)((2 * s + 255) / 256), 256, 0, st>>>(d->u, d->leaf_fix, M, s, (int)n, (int)b,
-                                                                      (int)P);
+      k_leaf_mid<R><<<dim3((unsigned)((2 * s + 255) / 256), (unsigned)nbt), 256, 0, st>>>(
+          d->u, d->leaf_fix, M, s, (int)n, (int)b, (int)P);
     }
   }
   /* 8: combine -> z[P][M] */
@@ -2244,19 +2391,19 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
     if (Wc > M) Wc = (int)M;
     FftPass fp{};
     fp.L = (int)P, fp.W = Wc, fp.per = (int)(M < (1L << 30) ? M : (1L << 30)), fp.M = M;
-    fp.irow = 0, fp.orow = 0, fp.oseq = 1, fp.ostr = M, fp.tws = 1;
+    fp.irow = 0, fp.orow = P * M, fp.oseq = 1, fp.ostr = M, fp.tws = 1; /* row = transform */
     fp.twiddle_post = 0, fp.conj_out = 0, fp.twmul = 1, fp.twmask = 0, fp.twbits = 0;
-    const CombineLd<R> cl{d->xt, d->u, d->ssum, d->pretw, M, R(1) / R(M)};
+    const CombineLd<R> cl{d->xt, d->u, d->ssum, d->pretw, M, R(1) / R(M), (int)P};
     const int thr = Wc * (int)(P / 8);
     const size_t sm = sizeof(C) * ((size_t)Wc * fft_lp((int)P, Wc) + P + P / 16 + 1 + 8 * (size_t)Wc);
-    k_fft_reg<R, false, false, CombineLd<R>><<<(unsigned)(M / Wc), thr, sm, st>>>(cl, d->z, d->twP,
-                                                                                  d->twP, fp);
+    k_fft_reg<R, false, false, CombineLd<R>><<<dim3((unsigned)(M / Wc), (unsigned)nbt), thr, sm, st>>>(
+        cl, d->z, d->twP, d->twP, fp);
   } else {
     int TMc = (int)(P >= 1024 ? 1 : (1024 / P < 32 ? 1024 / P : 32));
     if (TMc > M) TMc = (int)M;
     size_t sm = 2 * sizeof(C) * (size_t)P * TMc;
-    k_combine<R><<<(unsigned)(M / TMc), 256, sm, st>>>(d->xt, d->u, d->ssum, d->pretw, d->twP,
-                                                        d->z, M, (int)P, TMc);
+    k_combine<R><<<dim3((unsigned)(M / TMc), (unsigned)nbt), 256, sm, st>>>(d->xt, d->u, d->ssum, d->pretw,
+                                                                             d->twP, d->z, M, (int)P, TMc);
   }
   /* 9: size-M FFTs, z -> y */
   stage(ST_FFT1);
@@ -2273,9 +2420,9 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         if (Wr > P) Wr = (int)P;
         if (Wr < 1) Wr = 1;
         fp.M = M * Wr;
-        launch_fft_pass<R>(d->z, y, d->twM, fp, Wr, P / Wr, W, d->fft_threads, st);
+        launch_fft_pass<R>(d->z, y, d->twM, fp, Wr, nbt * P / Wr, W, d->fft_threads, st);
       } else {
-        launch_fft_pass<R>(d->z, y, d->twM, fp, W, P / W, W, d->fft_threads, st);
+        launch_fft_pass<R>(d->z, y, d->twM, fp, W, nbt * P / W, W, d->fft_threads, st);
       }
       pf.launches[ST_FFT1]++;
     } else {
@@ -2285,7 +2432,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
       if (W1 > 16) W1 = 16;
       if (W1 > M1) W1 = (int)M1;
       FftPass f1{(int)M2, W1, (int)M1, M, 1, M1, 1, M1, 1, M / M2, 0};
-      launch_fft_pass<R>(d->z, d->tmp, d->twM, f1, M1, P, W1, d->fft_threads, st);
+      launch_fft_pass<R>(d->z, d->tmp, d->twM, f1, M1, nbt * P, W1, d->fft_threads, st);
       pf.launches[ST_FFT1]++;
       stage(ST_FFT2);
       /* pass 2: for each k2, DFT over m1 (contiguous), store y[k2 + M2*k1] */
@@ -2293,7 +2440,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
       if (W2 > 16) W2 = 16;
       if (W2 > M2) W2 = (int)M2;
       FftPass f2{(int)M1, W2, (int)M2, M, M1, 1, 1, M2, 0, M / M1, inverse};
-      launch_fft_pass<R>(d->tmp, y, d->twM, f2, M2, P, W2, d->fft_threads, st);
+      launch_fft_pass<R>(d->tmp, y, d->twM, f2, M2, nbt * P, W2, d->fft_threads, st);
       pf.launches[ST_FFT2]++;
     }
   }
@@ -2301,7 +2448,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   /* below 10 terms the FMM's own truncation at these bins exceeds FP32 resolution (3e-8 at
    * 10 terms, 5e-6 at 8), and the reference's value is the FMM one, so it is kept */
   if (sizeof(R) == 4 && T >= 10) {
-    k_block_dc<R><<<(unsigned)((P + 3) / 4), 128, 0, st>>>(d->ssum, y, M, (int)P, inverse);
+    k_block_dc<R><<<dim3((unsigned)((P + 3) / 4), (unsigned)nbt), 128, 0, st>>>(d->ssum, y, M, (int)P, inverse);
     pf.launches[ST_DC]++;
   }
   if (slot >= 0) cudaEventRecord(pf.ev[slot * (ST_COUNT + 1) + ST_COUNT], st);
@@ -2324,11 +2471,14 @@ template <typename K> static void allow_dyn_smem(K *kernel, int maxopt) {
                        maxopt - (int)a.sharedSizeBytes);
 }
 
+/* cudaFuncSetAttribute acts on the current device only, so the opt-in is made once per device
+ * (plans and allocation-free calls may run on several GPUs of one process). */
+#define FMMK_MAXDEV 64
 static int set_smem_limits(void) {
-  static int done = 0;
-  if (done) return 0;
+  static volatile int done[FMMK_MAXDEV];
   int maxopt = 0, dev = 0;
-  cudaGetDevice(&dev);
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return 3;
+  if (dev < FMMK_MAXDEV && done[dev]) return 0;
   cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   int lim = maxopt > 0 ? maxopt : 48 * 1024;
   cudaFuncSetAttribute(k_fft_pass<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
@@ -2361,7 +2511,11 @@ static int set_smem_limits(void) {
   allow_dyn_smem(tc::k_tc_tma<TcS2M>, lim);
   allow_dyn_smem(tc::k_tc_tma<TcM2M>, lim);
   allow_dyn_smem(tc::k_tc_tma<TcM2L>, lim);
-  done = 1;
+  allow_dyn_smem(tc::k_tc_ws<TcS2M>, lim);
+  allow_dyn_smem(tc::k_tc_ws<TcM2M>, lim);
+  allow_dyn_smem(tc::k_tc_ws<TcM2L>, lim);
+  allow_dyn_smem(tc::k_tc_ws<TcLeaf>, lim);
+  if (dev < FMMK_MAXDEV) done[dev] = 1;
   return 0;
 }
 
@@ -2385,6 +2539,15 @@ extern "C" int fmmk_device_ok(char *err, size_t errlen) {
 
 extern "C" int fmmk_create(const fmm_ops64 *ops, int precision, fmmk_state **out,
                            size_t *device_bytes, char *err, size_t errlen) {
+  return fmmk_create_n(ops, precision, 1, out, device_bytes, err, errlen);
+}
+
+extern "C" int fmmk_create_n(const fmm_ops64 *ops, int precision, int nb, fmmk_state **out,
+                             size_t *device_bytes, char *err, size_t errlen) {
+  if (nb < 1 || nb > FMMK_MAX_BATCH) {
+    snprintf(err, errlen, "batch capacity %d outside 1..%d", nb, FMMK_MAX_BATCH);
+    return 1;
+  }
   int rc = fmmk_device_ok(err, errlen);
   if (rc) return rc;
   set_smem_limits();
@@ -2393,12 +2556,12 @@ extern "C" int fmmk_create(const fmm_ops64 *ops, int precision, fmmk_state **out
   st->precision = precision;
   if (precision == 0) {
     Dev<double> *d = NULL;
-    rc = dev_create<double>(ops, precision, &d, err, errlen);
+    rc = dev_create<double>(ops, precision, nb, &d, err, errlen);
     st->dev = d;
     if (!rc && device_bytes) *device_bytes = d->bytes;
   } else {
     Dev<float> *d = NULL;
-    rc = dev_create<float>(ops, precision, &d, err, errlen);
+    rc = dev_create<float>(ops, precision, nb, &d, err, errlen);
     st->dev = d;
     if (!rc && device_bytes) *device_bytes = d->bytes;
   }
@@ -2410,8 +2573,29 @@ extern "C" int fmmk_create(const fmm_ops64 *ops, int precision, fmmk_state **out
   return 0;
 }
 
+/* Device bytes a plan of this shape, precision and batch capacity holds, without allocating. */
+extern "C" int fmmk_plan_bytes(long M, long P, long T, long b, int precision, int nb, size_t *bytes,
+                               char *err, size_t errlen) {
+  fmm_ops64 o;
+  memset(&o, 0, sizeof o);
+  o.M = M, o.P = P, o.T = T, o.b = b, o.s = M / b;
+  o.n = 0;
+  while ((1L << (o.n + 1)) <= o.s) ++o.n;
+  if (precision == 0) {
+    Dev<double> *d = NULL;
+    return dev_create<double>(&o, precision, nb, &d, err, errlen, bytes);
+  }
+  Dev<float> *d = NULL;
+  return dev_create<float>(&o, precision, nb, &d, err, errlen, bytes);
+}
+
 extern "C" void fmmk_destroy(fmmk_state *st) {
   if (!st) return;
+  if (st->refine) {
+    fmmk_destroy(st->refine->f64);
+    cudaFree(st->refine->a);
+    free(st->refine);
+  }
   for (int i = 0; i < FMMK_GRAPHS; ++i)
     if (st->graphs[i].exec) cudaGraphExecDestroy(st->graphs[i].exec);
   if (st->precision == 0) {
@@ -2424,11 +2608,17 @@ extern "C" void fmmk_destroy(fmmk_state *st) {
   free(st);
 }
 
+extern "C" int fmmk_execute_n(fmmk_state *st, const void *d_in, void *d_out, void *stream,
+                              int inverse, int nbt, char *err, size_t errlen) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (st->precision == 0)
+    return dev_execute<double>((Dev<double> *)st->dev, d_in, d_out, s, inverse, nbt, err, errlen);
+  return dev_execute<float>((Dev<float> *)st->dev, d_in, d_out, s, inverse, nbt, err, errlen);
+}
+
 extern "C" int fmmk_execute(fmmk_state *st, const void *d_in, void *d_out, void *stream,
                             int inverse, char *err, size_t errlen) {
-  cudaStream_t s = (cudaStream_t)stream;
-  if (st->precision == 0) return dev_execute<double>((Dev<double> *)st->dev, d_in, d_out, s, inverse, err, errlen);
-  return dev_execute<float>((Dev<float> *)st->dev, d_in, d_out, s, inverse, err, errlen);
+  return fmmk_execute_n(st, d_in, d_out, stream, inverse, 1, err, errlen);
 }
 
 extern "C" int fmmk_execute_host(fmmk_state *st, const void *h_in, void *h_out, void *stream,
@@ -2471,11 +2661,15 @@ static int fetch(Dev<R> *d, double *u, double *z, double *phi, double *psi) {
     return 0;
   };
   int rc = 0;
+  /* the first transform of the last execute: its planes lead each level's block */
   if (u) rc |= grab(d->u, (size_t)(2 * S1 * M), u);
   if (z) rc |= grab(d->z, (size_t)(2 * P * M), z);
-  size_t lv = (size_t)(2 * S1 * T * ((2L << n) - 4));
-  if (phi) rc |= grab(d->phi, lv, phi);
-  if (psi) rc |= grab(d->psi, lv, psi);
+  const long S1e = (long)d->last_nbt * S1;
+  for (long l = 2; l <= n; ++l) {
+    const size_t cnt = (size_t)(2 * S1 * T * (1L << l));
+    if (phi) rc |= grab(d->phi + lvl_off(l, S1e, T), cnt, phi + lvl_off(l, S1, T));
+    if (psi) rc |= grab(d->psi + lvl_off(l, S1e, T), cnt, psi + lvl_off(l, S1, T));
+  }
   return rc;
 }
 
@@ -2653,17 +2847,26 @@ extern "C" int fmmk_execute_noalloc(const fmm_ops64 *o, int reuse_ops, const voi
     return 1;
   }
   if (!g_noalloc_base[dev]) { /* set-up, once per device, with that device current */
+    int rc = fmmk_device_ok(err, errlen);
+    if (rc) return rc;
     void *p = NULL;
     FMM_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    g_noalloc_base[dev] = p;
     set_smem_limits();
+    g_noalloc_base[dev] = p;
   }
   Dev<float> d;
   memset((void *)&d, 0, sizeof(d));
   d.M = o->M, d.P = o->P, d.T = o->T, d.b = o->b, d.s = o->s, d.n = o->n;
   d.N = o->M * o->P, d.S1 = o->P - 1, d.precision = 1;
   d.fft_threads = 512;
-  coarse_setup(&d);
+  /* the same stage choices as an FMMFFT_F32 plan (dev_create), including its switches */
+  d.fuse_s2m = 1;
+  if (const char *ev = getenv("FMMFFT_FUSE_S2M")) d.fuse_s2m = atoi(ev) != 0;
+  d.pdl = 1;
+  if (const char *ev = getenv("FMMFFT_PDL")) d.pdl = atoi(ev) != 0;
+  /* no cooperative coarse-tree kernel here: a timeout of its grid barrier could not be
+   * reported by this entry point (sizes it serves never reach the coarse-tree threshold) */
+  d.coarse_rows = 0;
   d.tileM = d.P >= 2048 ? 1 : 2048 / d.P;
   if (d.tileM > d.M) d.tileM = d.M;
   d.ntile = d.M / d.tileM;
@@ -2716,7 +2919,31 @@ extern "C" int fmmk_execute_noalloc(const fmm_ops64 *o, int reuse_ops, const voi
   d.tmp = (float2 *)(base + L.tmp);
   d.sync = (unsigned *)(base + L.sync);
   d.status = (int *)(d.sync + 48); /* the coarse-tree barrier records a timeout here */
-  return dev_execute<float>(&d, d_in, d_out, st, 0, err, errlen);
+  d.nbmax = 1;
+  return dev_execute<float>(&d, d_in, d_out, st, 0, 1, err, errlen);
+}
+
+/* Runs k_selftest_wait against the plan's own status word (and, for the grid barrier, its
+ * barrier words) with a limit of limit_us microseconds, on the legacy stream, and waits for it.
+ * fmmk_check then reports the timeout. */
+extern "C" int fmmk_selftest_wait(fmmk_state *st, int which, long limit_us, char *err, size_t errlen) {
+  int *status;
+  unsigned *sync;
+  if (st->precision == 0) {
+    Dev<double> *d = (Dev<double> *)st->dev;
+    status = d->status, sync = d->sync;
+  } else {
+    Dev<float> *d = (Dev<float> *)st->dev;
+    status = d->status, sync = d->sync;
+  }
+  if (which == 1) { /* arrivals past the grid size: no block is ever the last to arrive */
+    const unsigned preset[64] = {7u};
+    FMM_CUDA_TRY(cudaMemcpy(sync, preset, sizeof preset, cudaMemcpyHostToDevice));
+  }
+  k_selftest_wait<<<1, 64>>>(which, (unsigned long long)limit_us * 1000ull, sync, status);
+  FMM_CUDA_TRY(cudaGetLastError());
+  FMM_CUDA_TRY(cudaDeviceSynchronize());
+  return 0;
 }
 
 /* Reads (and clears) the plan's device status word; synchronises the device. */
@@ -2729,6 +2956,99 @@ extern "C" int fmmk_check(fmmk_state *st) {
   return h ? 6 : 0;
 }
 
+/* ======================================================================== FP64 residual correction */
+/* One step of residual correction for complex64 plans (the forward transform F~ in FP32 or
+ * split TF32): with y1 = F~ x, the residual r = x - F64^-1 y1 / N is formed in FP64 through the
+ * FP64 plan of the same shape (the reference's arithmetic), and y = y1 + F~ r is accumulated in
+ * FP64 (complex128 output).  Since r is of the size of F~'s rounding error, F~ r adds only its
+ * relative error times that: the result moves from FP32-level agreement with the FP64 FMM
+ * output to the square of it, bounded below by the FMM's own truncation at this order. */
+
+__global__ void k_promote(const float2 *__restrict__ a, double2 *__restrict__ o, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    o[i] = make_double2((double)a[i].x, (double)a[i].y);
+}
+
+/* r = x - z / N in FP64, rounded once to complex64 */
+__global__ void k_residual(const float2 *__restrict__ x, const double2 *__restrict__ z, float2 *__restrict__ r,
+                           long n, double invN) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double2 v = z[i];
+    r[i] = make_float2((float)((double)x[i].x - v.x * invN), (float)((double)x[i].y - v.y * invN));
+  }
+}
+
+__global__ void k_accumulate(double2 *__restrict__ o, const float2 *__restrict__ c, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double2 v = o[i];
+    o[i] = make_double2(v.x + (double)c[i].x, v.y + (double)c[i].y);
+  }
+}
+
+/* Makes the FP64 companion plan and scratch of a complex64 plan (once). */
+extern "C" int fmmk_refine_enable(fmmk_state *st, const fmm_ops64 *ops, size_t *bytes, char *err, size_t errlen) {
+  if (st->precision == 0) {
+    snprintf(err, errlen, "residual correction applies to complex64 plans");
+    return 1;
+  }
+  if (st->refine) {
+    if (bytes) *bytes = st->refine->bytes;
+    return 0;
+  }
+  Refine *r = (Refine *)calloc(1, sizeof(Refine));
+  if (!r) return 2;
+  size_t b64 = 0;
+  int rc = fmmk_create(ops, 0, &r->f64, &b64, err, errlen);
+  if (rc) {
+    free(r);
+    return rc;
+  }
+  const long N = ((Dev<float> *)st->dev)->N;
+  char *base = NULL;
+  const size_t need = align_up(sizeof(float2) * N) * 2 + align_up(sizeof(double2) * N);
+  if (cudaMalloc((void **)&base, need) != cudaSuccess) {
+    fmmk_destroy(r->f64);
+    free(r);
+    snprintf(err, errlen, "cudaMalloc(%zu) for the residual pass failed", need);
+    return 2;
+  }
+  r->a = (float2 *)base;
+  r->c = (float2 *)(base + align_up(sizeof(float2) * N));
+  r->bq = (double2 *)(base + 2 * align_up(sizeof(float2) * N));
+  r->bytes = b64 + need;
+  st->refine = r;
+  if (bytes) *bytes = r->bytes;
+  return 0;
+}
+
+/* d_in: N complex64, d_out: N complex128 (not overlapping d_in). */
+extern "C" int fmmk_execute_refined(fmmk_state *st, const void *d_in, void *d_out, void *stream, char *err,
+                                    size_t errlen) {
+  Refine *r = st->refine;
+  if (!r) {
+    snprintf(err, errlen, "residual correction was not enabled on this plan");
+    return 1;
+  }
+  const long N = ((Dev<float> *)st->dev)->N;
+  cudaStream_t s = (cudaStream_t)stream;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const unsigned grid = (unsigned)(4 * nsm);
+  double2 *out = (double2 *)d_out;
+  int rc = fmmk_execute(st, d_in, r->a, stream, 0, err, errlen); /* y1 = F~ x */
+  if (rc) return rc;
+  k_promote<<<grid, 256, 0, s>>>(r->a, out, N);                     /* out = y1 */
+  rc = fmmk_execute(r->f64, out, r->bq, stream, 1, err, errlen);      /* bq = N F64^-1 y1 */
+  if (rc) return rc;
+  k_residual<<<grid, 256, 0, s>>>((const float2 *)d_in, r->bq, r->a, N, 1.0 / (double)N);
+  rc = fmmk_execute(st, r->a, r->c, stream, 0, err, errlen);          /* c = F~ r */
+  if (rc) return rc;
+  k_accumulate<<<grid, 256, 0, s>>>(out, r->c, N);                  /* out = y1 + F~ r */
+  FMM_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
 /* ======================================================================== CUDA graphs */
 
 /* Execute through a cached graph: the first call for a given (in, out, direction) captures the
@@ -2736,10 +3056,15 @@ extern "C" int fmmk_check(fmmk_state *st) {
  * on `stream`.  The least recently used of FMMK_GRAPHS graphs is replaced when full. */
 extern "C" int fmmk_execute_graph(fmmk_state *st, const void *d_in, void *d_out, void *stream,
                                   int inverse, char *err, size_t errlen) {
+  return fmmk_execute_graph_n(st, d_in, d_out, stream, inverse, 1, err, errlen);
+}
+
+extern "C" int fmmk_execute_graph_n(fmmk_state *st, const void *d_in, void *d_out, void *stream,
+                                    int inverse, int nbt, char *err, size_t errlen) {
   GraphSlot *hit = NULL, *victim = &st->graphs[0];
   for (int i = 0; i < FMMK_GRAPHS; ++i) {
     GraphSlot *g = &st->graphs[i];
-    if (g->exec && g->in == d_in && g->out == d_out && g->inverse == inverse) hit = g;
+    if (g->exec && g->in == d_in && g->out == d_out && g->inverse == inverse && g->nbt == nbt) hit = g;
     if (!g->exec || (victim->exec && g->last_use < victim->last_use)) victim = g;
   }
   if (!hit) {
@@ -2751,7 +3076,7 @@ extern "C" int fmmk_execute_graph(fmmk_state *st, const void *d_in, void *d_out,
       snprintf(err, errlen, "cudaStreamBeginCapture: %s", cudaGetErrorString(e));
       return 3;
     }
-    int rc = fmmk_execute(st, d_in, d_out, cap, inverse, err, errlen);
+    int rc = fmmk_execute_n(st, d_in, d_out, cap, inverse, nbt, err, errlen);
     cudaGraph_t graph = NULL;
     e = cudaStreamEndCapture(cap, &graph);
     cudaStreamDestroy(cap);
@@ -2771,7 +3096,7 @@ extern "C" int fmmk_execute_graph(fmmk_state *st, const void *d_in, void *d_out,
       return 3;
     }
     if (victim->exec) cudaGraphExecDestroy(victim->exec);
-    victim->in = d_in, victim->out = d_out, victim->inverse = inverse, victim->exec = exec;
+    victim->in = d_in, victim->out = d_out, victim->inverse = inverse, victim->nbt = nbt, victim->exec = exec;
     hit = victim;
   }
   hit->last_use = ++st->graph_clock;

@@ -747,7 +747,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 /* Waits for phase `parity` of `bar`; false when the CTA aborted or 2 s passed (then the abort
  * flag and the status word are set).  The clock is read only after 4096 unsuccessful polls. */
 __device__ __forceinline__ bool t_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag,
-                                       int *status) {
+                                       int *status, unsigned long long limit_ns = kWaitNs) {
   unsigned long long t0 = 0;
   for (unsigned it = 0;; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
@@ -756,7 +756,7 @@ __device__ __forceinline__ bool t_wait(uint64_t *bar, uint32_t parity, volatile 
       const unsigned long long now = global_ns();
       if (t0 == 0) {
         t0 = now;
-      } else if (now - t0 > kWaitNs) {
+      } else if (now - t0 > limit_ns) {
         atomicExch(status, kErrWaitTimeout);
         *abort_flag = 1;
         return false;
@@ -1337,6 +1337,313 @@ __global__ void __launch_bounds__(kMThreads, 1)
       const unsigned uses = tcount > (unsigned)b ? (tcount - 1 - b) / 2 + 1 : 0;
       if (uses) t_wait_time(&rawfull[b], (uses - 1) & 1);
     }
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  if (warp == mma_warp) tmem_dealloc(tmem, 512);
+}
+
+/* ======================================================================== warp-specialised form */
+
+/* The row contraction D[r][0..nout) = sum_k A(r, k) B[k][.] with every step of it overlapped:
+ * loads of A, its split into TF32 hi / lo, the MMAs and the epilogue run in separate warps that
+ * hand work to one another through mbarriers, so that no step waits for the one before it to
+ * finish on the same tile.  One CTA per SM (all of its tensor memory), persistent over 128-row
+ * tiles, K taken in slots of 32 columns:
+ *
+ *   warps 0-7   producers.  Global -> shared: the 128 x 32 floats of a slot are copied with
+ *               16-byte cp.async into a ring of kWStages shared-memory stages, consecutive threads
+ *               on consecutive 16 bytes of a row (coalesced), kWStages - 1 slots in flight.
+ *               Shared -> TMEM: warp w (lane quarter q = w % 4, column half h = w / 4) reads row
+ *               32 q + lane, columns 16 h .. 16 h + 15 of the slot, splits them into TF32 hi / lo
+ *               and writes both into one of kWSlots A slots in tensor memory (tcgen05.st), then
+ *               arrives on the slot's `full` barrier.  Row chunks are stored XOR-swizzled in
+ *               shared memory (16-byte unit j of row i at position j ^ (i & 7)), so both the
+ *               copies and the row reads take four wavefronts per warp instruction.
+ *   warp 16     one thread issues, per K step of 8, A_hi x [B_hi; B_lo] (N = 2 npad) and
+ *               A_lo x B_hi (N = npad) into one of two TMEM accumulators: split TF32 with three
+ *               products (the A_lo B_lo term, 2^-22 relative, is left out), FP32 accumulation;
+ *               it commits each slot to the slot's `empty` barrier and each tile to the
+ *               accumulator's `full` barrier.  It also stages B: the host lays each batch's
+ *               operator out in the MMA's K-major core-matrix layout (hi rows, then lo rows), so
+ *               one bulk copy brings it into shared memory.
+ *   warps 8-15  epilogue: warp (q, h) reads lane quarter q of the accumulator, adds its two
+ *               column halves and stores 8-column chunks 8 h, 8 h + 16, ... of each row through
+ *               Prob::put8, then frees the accumulator for the tile after next.
+ *
+ * Prob supplies rows, batches, nchunks / clen / coff (A chunks, multiples of 4 floats), kpad
+ * (multiple of 8), npad (multiple of 16, at most 64), nout, wsb (the B operator of batch z at
+ * wsb + z * wsb_stride floats, 2 npad rows x round32(kpad) columns in core-matrix layout),
+ * src(c, r, z) (16-byte-aligned row of chunk c), dst(r, z) and put8(dst, r, z, c0, t).
+ * Every wait is bounded (2 s); on expiry the CTA records kErrWaitTimeout, every role leaves its
+ * loop, copies in flight land and the MMAs in flight complete before TMEM is freed. */
+constexpr int kWKs = 32;       /* K columns per A slot */
+constexpr int kWSlots = 4;     /* A slots in tensor memory: hi + lo, 64 columns each */
+constexpr int kWStages = 6;    /* shared-memory ring of A: 128 rows x 32 floats per stage */
+constexpr int kWProd = 8;      /* producer warps */
+constexpr int kWEpi = 8;       /* epilogue warps */
+constexpr int kWThreads = (kWProd + kWEpi + 1) * 32;
+constexpr int kWMaxSlots = 8;  /* K <= 256 */
+constexpr int kWStageBytes = kRows * kWKs * 4;
+
+__host__ __device__ constexpr int round32(int v) { return (v + 31) & ~31; }
+/* accumulator columns of one tile: B_hi and B_lo products side by side */
+__host__ __device__ constexpr int ws_acc_cols(int npad) { return round32(2 * npad); }
+__host__ __device__ constexpr size_t ws_b_floats(int kpad, int npad) {
+  return (size_t)2 * npad * round32(kpad);
+}
+__host__ __device__ constexpr size_t ws_smem_bytes(int kpad, int npad) {
+  return ws_b_floats(kpad, npad) * 4 + (size_t)kWStages * kWStageBytes;
+}
+/* the operator fits: two accumulators and the A slots within 512 TMEM columns, K <= 256 */
+__host__ __device__ constexpr bool ws_fits(int kpad, int npad) {
+  return npad % 16 == 0 && npad <= 64 && kpad % 8 == 0 && kpad <= kWKs * kWMaxSlots &&
+         2 * ws_acc_cols(npad) + kWSlots * 2 * kWKs <= 512 && ws_smem_bytes(kpad, npad) <= 200 * 1024;
+}
+/* float index of operator element (n, k), n < 2 npad (hi rows, then lo rows), in the layout the
+ * kernel copies: 8-row groups of round32(kpad) / 4 core matrices of 8 rows x 4 floats */
+__host__ __device__ inline long ws_b_index(int n, int k, int kpad) {
+  return (long)(n >> 3) * (round32(kpad) * 8) + (k >> 2) * 32 + (n & 7) * 4 + (k & 3);
+}
+
+__device__ __forceinline__ void cp_async16_cg(uint32_t dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" : : "r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" : : "n"(N) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      :
+      : "r"(dst), "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+/* barrier `id` over `nthreads` threads that ORs a flag across them (the same answer for all) */
+__device__ __forceinline__ bool named_bar_or(int id, int nthreads, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(id), "r"(nthreads)
+      : "memory");
+  return r != 0;
+}
+
+template <class Prob>
+__global__ void __launch_bounds__(kWThreads, 1) k_tc_ws(const __grid_constant__ Prob pb, int *status) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ uint64_t tfull[kWSlots], tempty[kWSlots], afull[2], aempty[2], bbar, fin;
+  __shared__ uint32_t tmem_slot;
+  __shared__ volatile int abort_flag;
+  /* per slot j and 16-byte unit u of its 32 columns: A chunk (low byte, 0xFF = zero), float
+   * offset in that chunk's row (high bits) */
+  __shared__ int lmap[kWMaxSlots][8];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int kpad = pb.kpad, npad = pb.npad;
+  const int nsl = round32(kpad) / kWKs;
+  float *Bs = reinterpret_cast<float *>(smem_raw);
+  unsigned char *ring = smem_raw + ws_b_floats(kpad, npad) * 4;
+  const int mma_warp = kWProd + kWEpi;
+  if (warp == mma_warp) tmem_alloc(&tmem_slot, 512);
+  if (tid == 0) {
+    for (int i = 0; i < kWSlots; ++i) mbar_init(&tfull[i], kWProd), mbar_init(&tempty[i], 1);
+    for (int i = 0; i < 2; ++i) mbar_init(&afull[i], 1), mbar_init(&aempty[i], kWEpi);
+    mbar_init(&bbar, 1);
+    mbar_init(&fin, 1);
+    fence_mbar_init();
+    abort_flag = 0;
+  }
+  if (tid < kWMaxSlots * 8) {
+    const int j = tid >> 3, u = tid & 7, k = j * kWKs + 4 * u;
+    int e = 0xFF;
+    if (j < nsl && k < kpad)
+      for (int c = 0; c < pb.nchunks; ++c)
+        if (k >= pb.coff[c] && k < pb.coff[c] + pb.clen[c]) e = c | ((k - pb.coff[c]) << 8);
+    lmap[j][u] = e;
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = tmem_slot;
+  const int acc_cols = ws_acc_cols(npad);
+  const int tiles_per_batch = (int)((pb.rows + kRows - 1) / kRows);
+  const int ntiles = tiles_per_batch * pb.batches;
+  /* one operator per batch: a CTA takes a contiguous run of tiles (it restages B once or twice);
+   * one batch: tiles strided by the grid */
+  const bool runs = pb.batches > 1;
+  const int tile0 = runs ? (int)(((long)ntiles * blockIdx.x) / gridDim.x) : (int)blockIdx.x;
+  const int tile_end = runs ? (int)(((long)ntiles * (blockIdx.x + 1)) / gridDim.x) : ntiles;
+  const int tile_step = runs ? 1 : (int)gridDim.x;
+  const int my_tiles = tile0 < tile_end ? (tile_end - tile0 + tile_step - 1) / tile_step : 0;
+  const uint32_t b_bytes = (uint32_t)(ws_b_floats(kpad, npad) * 4);
+
+  /* the operators are plan constants: the first batch's is requested before waiting for the
+   * kernel this one depends on */
+  pdl_trigger();
+  if (warp == mma_warp && lane == 0 && my_tiles > 0) {
+    mbar_expect_tx(&bbar, b_bytes);
+    bulk_g2s(smem_addr(Bs), pb.wsb + (long)(tile0 / tiles_per_batch) * pb.wsb_stride, b_bytes, &bbar);
+  }
+  pdl_wait();
+
+  if (warp < kWProd) {
+    /* ------------------------------------------------------------ producers */
+    const int q = warp & 3, h = warp >> 2;
+    const int my_row = q * 32 + lane;                 /* TMEM lane = tile row this thread splits */
+    const uint32_t lane_addr = (uint32_t)(q * 32) << 16;
+    const int cu = tid & 7, crow = tid >> 3;          /* copy unit: 16 bytes cu of rows crow + 32 m */
+    const uint32_t ring0 = smem_addr(ring);
+    const long G = (long)my_tiles * nsl;
+    /* copies of global slot g (tile index g / nsl of this CTA, slot g % nsl) into its stage */
+    auto issue = [&](long g) {
+      if (g < G) {
+        const int t = tile0 + (int)(g / nsl) * tile_step, j = (int)(g % nsl);
+        const int batch = t / tiles_per_batch;
+        const long r0 = (long)(t - batch * tiles_per_batch) * kRows;
+        const int e = lmap[j][cu], c = e & 0xFF;
+        if (c != 0xFF) {
+          const uint32_t st = ring0 + (uint32_t)((g % kWStages) * kWStageBytes);
+#pragma unroll
+          for (int m = 0; m < 4; ++m) {
+            const int row = crow + 32 * m;
+            const long r = r0 + row;
+            if (r < pb.rows)
+              cp_async16_cg(st + (uint32_t)(row * 128 + ((cu ^ (row & 7)) << 4)), pb.src(c, r, batch) + (e >> 8));
+          }
+        }
+      }
+      cp_async_commit(); /* one group per slot, empty or not: wait_group counts stay exact */
+    };
+#pragma unroll 1
+    for (int g = 0; g < kWStages - 1; ++g) issue(g);
+    for (long g = 0; g < G; ++g) {
+      cp_async_wait<kWStages - 2>(); /* this thread's copies of slot g have landed */
+      /* every producer's copies of slot g have landed, and every producer has read slot g - 1,
+       * whose stage the next copies reuse; all leave together on an abort */
+      if (named_bar_or(1, kWProd * 32, abort_flag != 0)) break;
+      issue(g + kWStages - 1);
+      const int j = (int)(g % nsl);
+      const uint32_t st = ring0 + (uint32_t)((g % kWStages) * kWStageBytes) + (uint32_t)(my_row * 128);
+      float hv[16], lv[16];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int u = 4 * h + i;
+        float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+        if ((lmap[j][u] & 0xFF) != 0xFF)
+          asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                       : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w)
+                       : "r"(st + (uint32_t)((u ^ (my_row & 7)) << 4)));
+        const float av[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          hv[4 * i + k] = tf32_rna(av[k]);
+          lv[4 * i + k] = tf32_rna(av[k] - hv[4 * i + k]);
+        }
+      }
+      const int s = (int)(g % kWSlots);
+      bool ok = true;
+      if (lane == 0) ok = t_wait(&tempty[s], (uint32_t)(((g / kWSlots) & 1) ^ 1), &abort_flag, status);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) continue; /* the next barrier sees the abort */
+      fence_after_sync();
+      const uint32_t ahi = tmem + lane_addr + (uint32_t)(2 * acc_cols + s * 2 * kWKs + 16 * h);
+      tmem_st8(ahi, hv);
+      tmem_st8(ahi + 8, hv + 8);
+      tmem_st8(ahi + kWKs, lv);
+      tmem_st8(ahi + kWKs + 8, lv + 8);
+      tmem_st_wait();
+      fence_before_sync();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tfull[s]);
+    }
+    cp_async_wait<0>(); /* nothing may still write shared memory when the CTA ends */
+  } else if (warp < kWProd + kWEpi) {
+    /* ------------------------------------------------------------ epilogue */
+    const int q = warp & 3, h = (warp - kWProd) >> 2;
+    const uint32_t lane_addr = (uint32_t)(q * 32) << 16;
+    for (int lt = 0; lt < my_tiles; ++lt) {
+      const int t = tile0 + lt * tile_step, a = lt & 1;
+      bool ok = true;
+      if (lane == 0) ok = t_wait(&afull[a], (uint32_t)((lt >> 1) & 1), &abort_flag, status);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) break;
+      fence_after_sync();
+      const int batch = t / tiles_per_batch;
+      const long r = (long)(t - batch * tiles_per_batch) * kRows + q * 32 + lane;
+      float *dst = r < pb.rows ? pb.dst(r, batch) : nullptr;
+      const uint32_t acc = tmem + lane_addr + (uint32_t)(a * acc_cols);
+      for (int c0 = 8 * h; c0 < npad; c0 += 16) {
+        float v[8], w[8];
+        tmem_ld8(acc + (uint32_t)c0, v);
+        tmem_ld8(acc + (uint32_t)(npad + c0), w);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) v[i] += w[i];
+        if (dst) pb.put8(dst, r, batch, c0, v);
+      }
+      fence_before_sync();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&aempty[a]);
+    }
+  } else {
+   if (lane == 0) {
+    /* ---------------------------------------------------------- MMA issue, B staging */
+    const uint32_t idesc2 = make_idesc_tf32(2 * npad), idesc1 = make_idesc_tf32(npad);
+    const uint32_t bsm = smem_addr(Bs), b_sbo = (uint32_t)round32(kpad) * 32;
+    int cur_batch = my_tiles > 0 ? tile0 / tiles_per_batch : -1;
+    uint32_t bphase = 0;
+    bool ok = my_tiles == 0 || t_wait(&bbar, bphase, &abort_flag, status);
+    bphase ^= 1;
+    long g = 0;
+    for (int lt = 0; lt < my_tiles && ok; ++lt) {
+      const int t = tile0 + lt * tile_step, a = lt & 1;
+      const int batch = t / tiles_per_batch;
+      if (batch != cur_batch) { /* every MMA reading the old operator completes, then restage */
+        mma_commit(&bbar);
+        ok = t_wait(&bbar, bphase, &abort_flag, status);
+        bphase ^= 1;
+        if (!ok) break;
+        mbar_expect_tx(&bbar, b_bytes);
+        bulk_g2s(bsm, pb.wsb + (long)batch * pb.wsb_stride, b_bytes, &bbar);
+        ok = t_wait(&bbar, bphase, &abort_flag, status);
+        bphase ^= 1;
+        if (!ok) break;
+        cur_batch = batch;
+      }
+      ok = t_wait(&aempty[a], (uint32_t)(((lt >> 1) & 1) ^ 1), &abort_flag, status);
+      if (!ok) break;
+      fence_after_sync();
+      const uint32_t d = tmem + (uint32_t)(a * acc_cols);
+      for (int j = 0; j < nsl; ++j, ++g) {
+        const int s = (int)(g % kWSlots);
+        ok = t_wait(&tfull[s], (uint32_t)((g / kWSlots) & 1), &abort_flag, status);
+        if (!ok) break;
+        fence_after_sync();
+        const int k0 = j * kWKs;
+        const int ksteps = ((kpad - k0) < kWKs ? (kpad - k0) : kWKs) >> 3;
+        const uint32_t ahi = tmem + (uint32_t)(2 * acc_cols + s * 2 * kWKs);
+        for (int kk = 0; kk < ksteps; ++kk) {
+          /* K step of 8 TF32 = two core matrices along K = 256 bytes of each 8-row group */
+          const uint64_t db = make_desc(bsm + 256u * (uint32_t)((k0 >> 3) + kk), 128, b_sbo);
+          mma_tf32_ts(d, ahi + 8u * kk, db, idesc2, (j | kk) != 0);
+          mma_tf32_ts(d, ahi + kWKs + 8u * kk, db, idesc1, 1);
+        }
+        mma_commit(&tempty[s]);
+      }
+      if (!ok) break;
+      mma_commit(&afull[a]);
+    }
+    /* every MMA and copy issued has completed before shared and tensor memory go */
+    mma_commit(&fin);
+    if (!t_wait_time(&fin, 0)) atomicExch(status, kErrWaitTimeout);
+    if (!ok && my_tiles > 0) t_wait_time(&bbar, bphase ^ 1);
+   }
+    __syncwarp(); /* the MMA warp meets the CTA barrier converged */
   }
   fence_before_sync();
   __syncthreads();

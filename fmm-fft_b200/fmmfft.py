@@ -27,6 +27,9 @@ EXPORTS = ["getwlen2", "getvlen", "mfti", "mft", "fmmfft_last_error", "fmmfft_la
            "fmmfft_execute", "fmmfft_execute_inverse", "fmmfft_execute_host",
            "fmmfft_debug_fetch", "fmmfft_profile_start", "fmmfft_profile_stop",
            "fmmfft_stage_name", "fmmfft_execute_noalloc", "fmmfft_plan_check",
+           "fmmfft_plan_selftest_wait", "fmmfft_plan_create_batched", "fmmfft_execute_many",
+           "fmmfft_execute_many_graph", "fmmfft_plan_bytes", "fmmfft_server_counts",
+           "fmmfft_plan_enable_refinement", "fmmfft_execute_refined",
            "fmmfft_execute_graph", "fmmfft_batch_create", "fmmfft_batch_launch",
            "fmmfft_batch_destroy", "fmmfft_server_create", "fmmfft_server_destroy",
            "fmmfft_server_submit", "fmmfft_server_query", "fmmfft_server_wait",
@@ -76,6 +79,22 @@ def load(path=LIB_PATH):
     lib.fmmfft_execute_noalloc.restype = _I
     lib.fmmfft_plan_check.argtypes = [_VP]
     lib.fmmfft_plan_check.restype = _I
+    lib.fmmfft_plan_selftest_wait.argtypes = [_VP, _I, _L]
+    lib.fmmfft_plan_selftest_wait.restype = _I
+    lib.fmmfft_plan_create_batched.argtypes = [ctypes.POINTER(_VP), _L, _L, _L, _L, _I, _I]
+    lib.fmmfft_plan_create_batched.restype = _I
+    lib.fmmfft_execute_many.argtypes = [_VP, _I, _VP, _VP, _VP]
+    lib.fmmfft_execute_many.restype = _I
+    lib.fmmfft_execute_many_graph.argtypes = [_VP, _I, _VP, _VP, _VP]
+    lib.fmmfft_execute_many_graph.restype = _I
+    lib.fmmfft_plan_bytes.argtypes = [_L, _L, _L, _L, _I, _I, ctypes.POINTER(ctypes.c_size_t)]
+    lib.fmmfft_plan_bytes.restype = _I
+    lib.fmmfft_server_counts.argtypes = [_VP, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+    lib.fmmfft_server_counts.restype = _I
+    lib.fmmfft_plan_enable_refinement.argtypes = [_VP]
+    lib.fmmfft_plan_enable_refinement.restype = _I
+    lib.fmmfft_execute_refined.argtypes = [_VP, _VP, _VP, _VP]
+    lib.fmmfft_execute_refined.restype = _I
     lib.fmmfft_execute_graph.argtypes = [_VP, _VP, _VP, _VP]
     lib.fmmfft_execute_graph.restype = _I
     lib.fmmfft_batch_create.argtypes = [ctypes.POINTER(_VP), _VP, _VP, _VP, _I, _I]
@@ -149,6 +168,14 @@ def mft(lq, qr, dir, p, myid=0, terms=None, b=None, w=None, v=None, sz1=0, szwk=
         raise FmmFftError(st, msg)
 
 
+def plan_bytes(N, P, terms, b, precision="f32", max_transforms=1):
+    """Device bytes a plan would hold, computed without allocating."""
+    v = ctypes.c_size_t()
+    _check(load().fmmfft_plan_bytes(int(N), int(P), int(terms), int(b), PRECISIONS[precision],
+                                    int(max_transforms), ctypes.byref(v)))
+    return v.value
+
+
 def execute_noalloc(N, P, terms, b, d_in, d_out, stream=0):
     """complex64 forward transform between caller-owned device buffers (pointers) without any
     allocation: tables and workspace live in the library's static 32 MiB device array."""
@@ -161,15 +188,29 @@ class Plan:
     """One resident FMM-FFT plan: N points in P blocks, `terms` Chebyshev terms, b points per
     leaf box.  precision: 'f64' (complex128), 'f32' (complex64, CUDA cores) or 'f32_tc'."""
 
-    def __init__(self, N, P, terms, b, precision="f32"):
+    def __init__(self, N, P, terms, b, precision="f32", max_transforms=1):
         self.N, self.P, self.terms, self.b = int(N), int(P), int(terms), int(b)
         self.M = self.N // self.P
         self.precision = precision
+        self.max_transforms = int(max_transforms)
         self._p = PRECISIONS[precision]
         h = _VP()
-        _check(load().fmmfft_plan_create(ctypes.byref(h), self.N, self.P, self.terms, self.b,
-                                         self._p))
+        _check(load().fmmfft_plan_create_batched(ctypes.byref(h), self.N, self.P, self.terms,
+                                                 self.b, self._p, self.max_transforms))
         self._h = h
+
+    def enable_refinement(self):
+        """Build the FP64 companion plan of the residual-correction pass (once)."""
+        _check(load().fmmfft_plan_enable_refinement(self._h))
+
+    def execute_refined_ptr(self, d_in, d_out, stream=0):
+        """complex64 input -> complex128 output, one FP64 residual-correction step."""
+        _check(load().fmmfft_execute_refined(self._h, d_in, d_out, stream or None))
+
+    def execute_many_ptr(self, count, d_in, d_out, stream=0, graph=False):
+        """`count` transforms in one launch sequence; transform i at d_in / d_out + i N elements."""
+        f = load().fmmfft_execute_many_graph if graph else load().fmmfft_execute_many
+        _check(f(self._h, int(count), d_in, d_out, stream or None))
 
     @property
     def complex_dtype(self):
@@ -232,6 +273,11 @@ class Plan:
     def check(self):
         """Synchronise; raise FmmFftError(ERR_TIMEOUT) if a bounded device wait gave up."""
         _check(load().fmmfft_plan_check(self._h))
+
+    def selftest_wait(self, which, limit_us=2000):
+        """Run the bounded-wait self-test kernel (0: mbarrier wait holding tensor memory,
+        1: coarse-tree grid barrier) against this plan's status word."""
+        _check(load().fmmfft_plan_selftest_wait(self._h, int(which), int(limit_us)))
 
     def profile_start(self, max_executes):
         _check(load().fmmfft_profile_start(self._h, int(max_executes)))
@@ -307,6 +353,12 @@ class Server:
         if rc:
             raise FmmFftError(rc, "submit refused" if rc == 7 else "submit failed")
         return t.value
+
+    def counts(self):
+        """-> (requests dispatched, batched launch sequences)"""
+        r, l = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(load().fmmfft_server_counts(self._h, ctypes.byref(r), ctypes.byref(l)))
+        return r.value, l.value
 
     def done(self, ticket):
         rc = load().fmmfft_server_query(self._h, ticket)

@@ -93,6 +93,23 @@ int fmmfft_plan_destroy(fmmfft_plan plan);
 /* Device bytes the plan holds (operators + workspace). */
 int fmmfft_plan_device_bytes(fmmfft_plan plan, size_t *bytes);
 
+/* Batched plans: no counterpart in the reference, which transforms one vector per run.  A plan
+ * for up to max_transforms (1..64) transforms of one shape; fmmfft_execute_many runs `count` of
+ * them in one launch sequence: every tree stage is one contraction over the rows of all of them,
+ * the other stages carry the transform as a grid dimension.  Inputs and outputs are contiguous:
+ * transform i at d_in + i*N and d_out + i*N elements.  Each transform's result is bitwise the
+ * same as its own fmmfft_execute on a plan of capacity 1 (the arithmetic per row does not depend
+ * on the rows beside it).  Workspace is max_transforms times a single plan's. */
+int fmmfft_plan_create_batched(fmmfft_plan *out, long N, long P, long terms, long b, int precision,
+                               int max_transforms);
+int fmmfft_execute_many(fmmfft_plan plan, int count, const void *d_in, void *d_out, void *stream);
+/* The same through a CUDA graph cached per (d_in, d_out, count), as fmmfft_execute_graph. */
+int fmmfft_execute_many_graph(fmmfft_plan plan, int count, const void *d_in, void *d_out, void *stream);
+/* Device bytes a plan of this shape, precision and capacity would hold, computed without
+ * allocating anything (for admission under a memory budget). */
+int fmmfft_plan_bytes(long N, long P, long terms, long b, int precision, int max_transforms,
+                      size_t *bytes);
+
 /* Forward transform: d_in, d_out = N interleaved complex values in device memory (complex128
  * for FMMFFT_F64, complex64 otherwise), natural order; d_in is not modified; d_in == d_out is
  * allowed.  Enqueued on `stream` (a cudaStream_t, NULL = legacy default stream); returns once
@@ -102,6 +119,17 @@ int fmmfft_execute(fmmfft_plan plan, const void *d_in, void *d_out, void *stream
 /* Inverse transform (unnormalised: returns N * IDFT), computed as conj(F(conj(x))) with the
  * conjugations around the whole forward transform. */
 int fmmfft_execute_inverse(fmmfft_plan plan, const void *d_in, void *d_out, void *stream);
+
+/* Optional FP64 residual correction of complex64 plans (no counterpart in the reference, which
+ * computes in FP64 throughout).  fmmfft_plan_enable_refinement builds, once, an FP64 plan of the
+ * same (N, P, terms, b) and 32 N bytes of scratch beside the plan.  fmmfft_execute_refined then
+ * computes y1 = F x with the plan's own arithmetic, the residual r = x - F64^-1(y1) / N in FP64
+ * through the FP64 plan (an inverse FMM-FFT), and y = y1 + F r accumulated in FP64: d_in holds N
+ * complex64, d_out receives N complex128.  The result agrees with the FP64 FMM-FFT (the
+ * reference's arithmetic) to about the square of the plan's own relative error, and with the
+ * exact DFT to the FMM's truncation at this order. */
+int fmmfft_plan_enable_refinement(fmmfft_plan plan);
+int fmmfft_execute_refined(fmmfft_plan plan, const void *d_in, void *d_out, void *stream);
 
 /* Same transform from and to HOST memory: copies in, executes, copies out, synchronises. */
 int fmmfft_execute_host(fmmfft_plan plan, const void *h_in, void *h_out, void *stream);
@@ -118,6 +146,16 @@ int fmmfft_debug_fetch(fmmfft_plan plan, double *u, double *z, double *phi, doub
  * device-side wait (the tensor-core kernels' mbarrier waits) gave up instead of completing;
  * FMMFFT_OK otherwise.  Clears the recorded status. */
 int fmmfft_plan_check(fmmfft_plan plan);
+
+/* Self-test of the bounded device waits, for tests and health checks; no counterpart in the
+ * reference (which has no device code).  Runs one small kernel that waits, with the same wait
+ * routine as the plan's kernels, for an event that never comes -- which = 0: an mbarrier wait
+ * while holding tensor memory (the tensor-core kernels' wait); which = 1: the grid barrier of
+ * the cooperative coarse-tree kernel -- with a limit of limit_us microseconds (1 .. 2e6).  The
+ * wait gives up, records the timeout in the plan's status word, frees what it holds and
+ * returns; the call synchronises the device.  The next fmmfft_plan_check(plan) then returns
+ * FMMFFT_ERR_TIMEOUT, and the plan stays usable. */
+int fmmfft_plan_selftest_wait(fmmfft_plan plan, int which, long limit_us);
 
 /* Same transform as fmmfft_execute through a CUDA graph: the first call for a given
  * (d_in, d_out) captures the plan's launch sequence and instantiates it (make that call outside
@@ -156,6 +194,9 @@ int fmmfft_server_query(fmmfft_server server, fmmfft_ticket ticket);
 /* Waits up to timeout_ms; FMMFFT_OK or FMMFFT_ERR_TIMEOUT. */
 int fmmfft_server_wait(fmmfft_server server, fmmfft_ticket ticket, long timeout_ms);
 int fmmfft_server_stats(fmmfft_server server, size_t *hbm_used, int *plans, int *streams);
+/* Requests sent to the GPU so far and the batched launch sequences they went in (their ratio is
+ * the mean batch size). */
+int fmmfft_server_counts(fmmfft_server server, uint64_t *requests, uint64_t *launches);
 
 /* ------------------------------------------------------------------ stage timing */
 /* Records CUDA events around every stage of the next `max_executes` executes of this plan (on

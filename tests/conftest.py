@@ -26,3 +26,22 @@ def pytest_collection_modifyitems(config, items):
     for it in items:
         if "gpu" in it.keywords:
             it.add_marker(skip)
+
+
+# Accuracy figures that GPU tests record (rel-L2, max error per case), printed at the end of the
+# run so that they show under `pytest -q` too.
+_ACCURACY_LINES = []
+
+
+@pytest.fixture
+def accuracy_report():
+    def add(line):
+        _ACCURACY_LINES.append(str(line))
+    return add
+
+
+def pytest_terminal_summary(terminalreporter, exitstatus, config):
+    if _ACCURACY_LINES:
+        terminalreporter.write_sep("-", "accuracy per case")
+        for line in _ACCURACY_LINES:
+            terminalreporter.write_line(line)

@@ -2,8 +2,8 @@
 
 Run in the build container (it needs the reference sources, which are not shipped):
 
-    make -C oracle                      # builds oracle/_ref/libfmmfft_ref.so from src/fmmfft.c
-    python tests/golden/make_golden.py
+    make -C oracle REFERENCE=<reference checkout>   # builds oracle/_ref/libfmmfft_ref.so
+    FMMFFT_REFERENCE=<reference checkout> python tests/golden/make_golden.py
 
 Outputs
   ref_forward_<tag>.npz   seeded complex128 input (from its seed) -> output y of the UNMODIFIED
@@ -27,7 +27,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REFERENCE = os.environ.get("FMMFFT_REFERENCE", "/root/reference")
+REFERENCE = os.environ.get("FMMFFT_REFERENCE")  # the reference checkout: required
 
 # (N, P, terms, b): covers t = s/P = 1, 2 and > 2 (the reference's three near-field branches,
 # fmmfft.c:805-954), P = 2 (only the sc = P/2 averaging case), the sc > P/2 half-shift path,
@@ -56,6 +56,8 @@ def tag(N, P, T, b):
 
 
 def main():
+    if not REFERENCE:
+        sys.exit("set FMMFFT_REFERENCE to the reference checkout (its plotting/raw_data is read)")
     lib = ctypes.CDLL(os.path.join(REPO, "oracle", "_ref", "libfmmfft_ref.so"))
     L, VP = ctypes.c_long, ctypes.c_void_p
     lib.fmmref_forward.argtypes = [L, L, L, L, VP, VP, ctypes.c_int, VP]

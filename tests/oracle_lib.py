@@ -116,3 +116,36 @@ def rel_l2(a, ref):
     a = np.asarray(a)
     ref = np.asarray(ref)
     return float(np.linalg.norm((a - ref).ravel()) / np.linalg.norm(ref.ravel()))
+
+
+def tone_input(n, seed, ntones=32, noise=1e-3):
+    """Sum of `ntones` unit-modulus tones at real (off-bin) frequencies f_k ~ U[0, n) with random
+    phases, plus noise * (g_re + i g_im), g iid N(0, 1); numpy PCG64(seed).  Evaluated in FP64 in
+    blocks of 2^16 points: exp(2 pi i f (n0 + j) / n) = exp(2 pi i f n0 / n) exp(2 pi i f j / n)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    f = rng.uniform(0.0, float(n), ntones)
+    ph = rng.uniform(0.0, 2 * np.pi, ntones)
+    g = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    blk = min(n, 1 << 16)
+    j = np.arange(blk, dtype=np.float64)
+    base = np.exp(2j * np.pi * np.outer(f, j) / n)          # [ntones][blk]
+    x = np.empty(n, np.complex128)
+    for n0 in range(0, n, blk):
+        c = np.exp(1j * (ph + 2 * np.pi * f * (n0 / n)))       # [ntones]
+        x[n0:n0 + blk] = c @ base
+    x += noise * g
+    return x
+
+
+def reference_forward(x, P, terms, b):
+    """Output of the shim-built reference (oracle/_ref: src/fmmfft.c unmodified, P thread-ranks)
+    for input x, or None where it was not built."""
+    lib = load_reference()
+    if lib is None:
+        return None
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    y = np.zeros_like(x)
+    rc = lib.fmmref_forward(x.size, P, terms, b, x.ctypes.data, y.ctypes.data, 1, None)
+    if rc != 0:
+        raise RuntimeError(f"reference run failed rc={rc}")
+    return y

@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 import oracle_lib as ol
+from gpu_util import run_device
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-6
@@ -108,16 +109,18 @@ def test_server_mix_equals_alone(fm):
 
 
 def test_server_admission_by_budget(fm):
+    """Plans are admitted under the HBM budget: an idle plan is evicted to make room for a new
+    shape, and a request whose plan cannot fit even then is refused (FMMFFT_ERR_BUSY) before
+    anything is allocated: the device's free memory is the same before and after."""
     import torch
-    N, P, T, b = 1 << 20, 64, 16, 32
-    probe = fm.Plan(N, P, T, b, "f32")
-    one = probe.device_bytes
-    probe.close()
+    N, P, T, b = 1 << 21, 64, 16, 32  # 2^21 samples: a lane of one transform per launch
+    one = fm.plan_bytes(N, P, T, b, "f32")
     x = _dev(ol.seeded_input(N, 1), torch.complex64)
     y = torch.empty_like(x)
-    srv = fm.Server(int(one * 1.5), nstreams=2)  # room for one resident plan of this size
+    srv = fm.Server(int(one * 1.5), nstreams=1)  # room for one resident plan of this size
     t = srv.submit(N, P, T, b, "f32", x.data_ptr(), y.data_ptr())
     srv.wait(t)
+    assert srv.stats()["plans"] == 1
     # a different shape needs a new plan: the idle one is evicted to make room
     x2 = _dev(ol.seeded_input(N // 2, 2), torch.complex64)
     y2 = torch.empty_like(x2)
@@ -125,8 +128,79 @@ def test_server_admission_by_budget(fm):
     srv.wait(t2)
     assert srv.stats()["plans"] == 1
     assert ol.rel_l2(y2.cpu().numpy(), np.fft.fft(x2.cpu().numpy())) < TOL
-    # a plan larger than the whole budget is refused, not run
+    # a plan larger than the whole budget is refused, not built: nothing is allocated
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
     with pytest.raises(fm.FmmFftError) as ei:
         srv.submit(4 * N, P, T, b, "f32", x.data_ptr(), y.data_ptr())
     assert ei.value.status == 7
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert srv.stats()["plans"] == 1
     srv.close()
+
+
+def test_server_batches_concurrent_requests(fm):
+    """Continuous batching: 40 requests of one small shape submitted back to back leave in
+    batches (several transforms per launch sequence) and each result is bitwise the result of
+    the request run alone; requests of another shape interleaved with them are unaffected."""
+    import torch
+    N, P, T, b = 1 << 14, 16, 16, 32
+    xs = [ol.seeded_input(N, 300 + i) for i in range(40)]
+    din = [_dev(x, torch.complex64) for x in xs]
+    dout = [torch.empty_like(d) for d in din]
+    N2 = 1 << 16
+    x2 = [ol.seeded_input(N2, 500 + i) for i in range(6)]
+    d2 = [_dev(x, torch.complex64) for x in x2]
+    o2 = [torch.empty_like(d) for d in d2]
+    srv = fm.Server(4 << 30, nstreams=3)
+    tickets = []
+    for i in range(40):
+        tickets.append(srv.submit(N, P, T, b, "f32_tc", din[i].data_ptr(), dout[i].data_ptr()))
+        if i % 7 == 0:
+            j = i // 7
+            tickets.append(srv.submit(N2, 32, 20, 32, "f32_tc", d2[j].data_ptr(), o2[j].data_ptr()))
+    for t in tickets:
+        srv.wait(t)
+    nreq, nlaunch = srv.counts()
+    assert nreq == len(tickets) and nlaunch < nreq, (nreq, nlaunch)
+    srv.close()
+    plan = fm.Plan(N, P, T, b, "f32_tc")
+    s = torch.cuda.current_stream().cuda_stream
+    for i in range(40):
+        alone = torch.empty_like(din[i])
+        plan.execute_ptr(din[i].data_ptr(), alone.data_ptr(), s)
+        torch.cuda.synchronize()
+        assert torch.equal(alone, dout[i]), i
+    plan.close()
+    plan2 = fm.Plan(N2, 32, 20, 32, "f32_tc")
+    for j in range(6):
+        alone = torch.empty_like(d2[j])
+        plan2.execute_ptr(d2[j].data_ptr(), alone.data_ptr(), s)
+        torch.cuda.synchronize()
+        assert torch.equal(alone, o2[j]), j
+        assert ol.rel_l2(o2[j].cpu().numpy(), np.fft.fft(x2[j])) < TOL
+    plan2.close()
+
+
+@pytest.mark.parametrize("which", [0, 1], ids=["mbarrier_with_tmem", "grid_barrier"])
+def test_bounded_wait_gives_up_and_reports_timeout(fm, which):
+    """The device waits are bounded: a wait for an event that never comes (an mbarrier nobody
+    arrives on while the kernel holds tensor memory; a grid barrier that no block completes),
+    with a 2 ms limit, gives up, frees what it holds and returns.  The plan's check reports
+    FMMFFT_ERR_TIMEOUT once (the status is cleared by reading it), and the plan still computes
+    the right transform afterwards."""
+    N, P, T, b = 1 << 14, 16, 16, 32
+    plan = fm.Plan(N, P, T, b, "f32_tc")
+    x = ol.seeded_input(N, 3)
+    y0 = run_device(plan, x)
+    plan.check()
+    plan.selftest_wait(which, 2000)
+    with pytest.raises(fm.FmmFftError) as ei:
+        plan.check()
+    assert ei.value.status == 6  # FMMFFT_ERR_TIMEOUT
+    plan.check()  # cleared
+    y1 = run_device(plan, x)
+    plan.check()
+    assert np.array_equal(y0, y1)
+    plan.close()
