@@ -42,14 +42,15 @@ def parse():
     ap.add_argument("--precision", default=None, help="f32 | f32_tc | f64 (default: fastest)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
-    ap.add_argument("--workload", choices=["single", "uneven-batch", "serving"], default="single",
+    ap.add_argument("--workload", choices=["single", "uneven-batch", "serving", "precision-sweep"],
+                    default="single",
                     help="single: the headline transform (default); uneven-batch: 512 transforms "
                          "of mixed N and P as one graph; serving: Poisson arrivals through the "
-                         "request server")
+                         "request server; precision-sweep: N = 2^26, P = 256, tones + noise, every "
+                         "order and arithmetic, error against throughput")
     ap.add_argument("--rate", type=float, default=2000.0, help="serving: arrivals per second")
     ap.add_argument("--requests", type=int, default=1200, help="serving: requests per rate")
     ap.add_argument("--no-served", action="store_true", help="skip the served-vs-plain object")
-    ap.add_argument("--duration", type=float, default=2.0, help="serving: seconds of arrivals")
     return ap.parse_args()
 
 
@@ -456,8 +457,87 @@ def run_serving(a):
     return 0
 
 
+# ------------------------------------------------------------------------ precision sweep
+def run_precision_sweep(a):
+    """N = 2^26 complex64, 32 off-bin tones + 1e-3 noise (seeded), P = 256, b = 32, terms in
+    {8, 16, 24, 32}; per order and arithmetic (FP32 CUDA cores, split TF32 and BF16x3 with three
+    products on the tensor cores, each with and without the FP64 residual-correction pass): device-timed
+    Msamples/s, and rel-L2 / max error against the FP64 FFT (numpy) and against the FP64 FMM-FFT
+    of the same order (the reference's arithmetic).  One JSON line per point."""
+    import numpy as np
+    import torch
+    import fmmfft
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    import oracle_lib as ol
+    torch.cuda.set_device(0)
+    N, P, b = 1 << 26, 256, 32
+    x = ol.tone_input(N, 2026).astype(np.complex64)
+    ref = np.fft.fft(x.astype(np.complex128))
+    nref = np.linalg.norm(ref)
+    mref = np.max(np.abs(ref))
+    dx = torch.from_numpy(x).cuda()
+    dx64 = dx.to(torch.complex128)
+    y32 = torch.empty_like(dx)
+    y64 = torch.empty_like(dx64)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    K = max(3, a.steps // 2)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        evs = []
+        for i in range(K):
+            flush.fill_(float(i))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+        return sum(e0.elapsed_time(e1) for e0, e1 in evs) / K
+
+    def errs(y, fmm64):
+        y = y.astype(np.complex128)
+        return {"rel_l2_vs_fp64_fft": float(np.linalg.norm(y - ref) / nref),
+                "max_err_vs_fp64_fft": float(np.max(np.abs(y - ref)) / mref),
+                "rel_l2_vs_fp64_fmm": float(np.linalg.norm(y - fmm64) / np.linalg.norm(fmm64))}
+
+    for T in (8, 16, 24, 32):
+        p64 = fmmfft.Plan(N, P, T, b, "f64")
+        p64.execute_ptr(dx64.data_ptr(), y64.data_ptr(), stream.cuda_stream)
+        torch.cuda.synchronize()
+        fmm64 = y64.cpu().numpy()
+        ms64 = timed(lambda: p64.execute_ptr(dx64.data_ptr(), y64.data_ptr(), stream.cuda_stream))
+        p64.close()
+        pts = [("fp64", ms64, errs(fmm64, fmm64))]
+        for prec, name in (("f32", "fp32"), ("f32_tc", "tf32x3"), ("bf16x3", "bf16x3")):
+            plan = fmmfft.Plan(N, P, T, b, prec)
+            ms = timed(lambda: plan.execute_ptr(dx.data_ptr(), y32.data_ptr(), stream.cuda_stream))
+            plan.execute_ptr(dx.data_ptr(), y32.data_ptr(), stream.cuda_stream)
+            torch.cuda.synchronize()
+            pts.append((name, ms, errs(y32.cpu().numpy(), fmm64)))
+            plan.enable_refinement()
+            msr = timed(lambda: plan.execute_refined_ptr(dx.data_ptr(), y64.data_ptr(), stream.cuda_stream))
+            plan.execute_refined_ptr(dx.data_ptr(), y64.data_ptr(), stream.cuda_stream)
+            torch.cuda.synchronize()
+            pts.append((name + "+fp64_residual", msr, errs(y64.cpu().numpy(), fmm64)))
+            plan.check()
+            plan.close()
+        for name, ms, e in pts:
+            line = {"metric": "precision sweep: Msamples/s and error vs FP64", "workload": "precision-sweep",
+                    "N": N, "P": P, "terms": T, "b": b, "arithmetic": name,
+                    "value": N / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_transform": ms,
+                    "input": "32 off-bin unit tones + 1e-3 complex white noise, PCG64 seed 2026",
+                    "l2": "256 MB write before every timed step", **e}
+            print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = parse()
+    if a.workload == "precision-sweep":
+        return run_precision_sweep(a)
     if a.workload == "uneven-batch":
         return run_uneven_batch(a)
     if a.workload == "serving":

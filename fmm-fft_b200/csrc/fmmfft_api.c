@@ -7,6 +7,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #include "../../include/fmmfft.h"
 #include "fmmfft_internal.h"
@@ -41,7 +42,7 @@ int fmmfft_plan_create(fmmfft_plan *out, long N, long P, long terms, long b, int
 }
 
 static int check_shape(long N, long P, long terms, long b, int precision, int nb) {
-  if (precision < FMMFFT_F64 || precision > FMMFFT_F32_TC)
+  if (precision < FMMFFT_F64 || precision > FMMFFT_BF16X3)
     return set_err(FMMFFT_ERR_INVALID, "plan_create: unknown precision");
   if (nb < 1 || nb > 64) return set_err(FMMFFT_ERR_INVALID, "plan_create: max_transforms outside 1..64");
   if (P < 2 || N <= 0 || N % P)
@@ -383,9 +384,134 @@ void mfti(long lq, long p, long terms, long b, double *w, double *v, long szkeep
   if (st == FMMFFT_OK) set_err(FMMFFT_OK, NULL);
 }
 
+/* ------------------------------------------------------------------ block-distributed I/O */
+int fmmfft_execute_blocks(fmmfft_plan plan, const void *const *d_blocks_in, void *const *d_blocks_out,
+                          void *stream) {
+  if (!plan || !d_blocks_in || !d_blocks_out)
+    return set_err(FMMFFT_ERR_INVALID, "execute_blocks: NULL argument");
+  for (long r = 0; r < plan->P; ++r)
+    if (!d_blocks_in[r] || !d_blocks_out[r]) return set_err(FMMFFT_ERR_INVALID, "execute_blocks: NULL block");
+  char err[256] = {0};
+  int rc = fmmk_execute_blocks(plan->dev, d_blocks_in, d_blocks_out, 0, stream, err, sizeof err);
+  return rc ? set_err(rc, err) : FMMFFT_OK;
+}
+
+int fmmfft_execute_blocks_host(fmmfft_plan plan, const void *const *h_blocks_in, void *const *h_blocks_out,
+                               void *stream) {
+  if (!plan || !h_blocks_in || !h_blocks_out)
+    return set_err(FMMFFT_ERR_INVALID, "execute_blocks_host: NULL argument");
+  for (long r = 0; r < plan->P; ++r)
+    if (!h_blocks_in[r] || !h_blocks_out[r])
+      return set_err(FMMFFT_ERR_INVALID, "execute_blocks_host: NULL block");
+  char err[256] = {0};
+  int rc = fmmk_execute_blocks(plan->dev, h_blocks_in, h_blocks_out, 1, stream, err, sizeof err);
+  return rc ? set_err(rc, err) : FMMFFT_OK;
+}
+
+/* Rank mode of mft: the p calling threads (myid = 0 .. p-1) meet, as the reference's ranks do in
+ * their collectives; the last to arrive runs the transform over every rank's block and all
+ * return with their block transformed.  One collective at a time, like MPI_COMM_WORLD. */
+static int g_rank_mode = 0;
+static pthread_mutex_t g_meet_mu = PTHREAD_MUTEX_INITIALIZER;
+static pthread_cond_t g_meet_cv = PTHREAD_COND_INITIALIZER;
+static struct {
+  int active;
+  long lq, p, terms, b;
+  void **blocks;
+  long arrived;
+  unsigned long gen;
+  int status;
+  char msg[256];
+} g_meet;
+
+int fmmfft_mft_rank_mode(int on) {
+  pthread_mutex_lock(&g_meet_mu);
+  int busy = g_meet.active;
+  if (!busy) g_rank_mode = on != 0;
+  pthread_mutex_unlock(&g_meet_mu);
+  return busy ? set_err(FMMFFT_ERR_BUSY, "mft_rank_mode: a collective mft is in progress") : FMMFFT_OK;
+}
+
+static long rank_timeout_ms(void) {
+  const char *ev = getenv("FMMFFT_RANK_TIMEOUT_MS");
+  long v = ev ? atol(ev) : 0;
+  return v > 0 ? v : 120000;
+}
+
+static void mft_rank(long lq, void *qr, long p, long myid, long terms, long b) {
+  if (myid < 0 || myid >= p) {
+    set_err(FMMFFT_ERR_INVALID, "mft: myid outside 0..p-1");
+    return;
+  }
+  pthread_mutex_lock(&g_meet_mu);
+  if (!g_meet.active) {
+    g_meet.blocks = (void **)calloc((size_t)p, sizeof(void *));
+    if (!g_meet.blocks) {
+      pthread_mutex_unlock(&g_meet_mu);
+      set_err(FMMFFT_ERR_NOMEM, "mft: host allocation failed");
+      return;
+    }
+    g_meet.active = 1, g_meet.lq = lq, g_meet.p = p, g_meet.terms = terms, g_meet.b = b;
+    g_meet.arrived = 0;
+  } else if (g_meet.lq != lq || g_meet.p != p || g_meet.terms != terms || g_meet.b != b) {
+    pthread_mutex_unlock(&g_meet_mu);
+    set_err(FMMFFT_ERR_INVALID, "mft: ranks called with different (lq, p, terms, b)");
+    return;
+  }
+  if (g_meet.blocks[myid]) {
+    pthread_mutex_unlock(&g_meet_mu);
+    set_err(FMMFFT_ERR_INVALID, "mft: two calls with the same myid in one collective");
+    return;
+  }
+  g_meet.blocks[myid] = qr;
+  const unsigned long my_gen = g_meet.gen;
+  int status;
+  char msg[256];
+  if (++g_meet.arrived == p) {
+    void **blocks = g_meet.blocks;
+    pthread_mutex_unlock(&g_meet_mu);
+    int st;
+    fmmfft_plan pl = compat_plan(lq, p, terms, b, &st);
+    if (pl) st = fmmfft_execute_blocks_host(pl, (const void *const *)blocks, blocks, NULL);
+    pthread_mutex_lock(&g_meet_mu);
+    g_meet.status = st;
+    snprintf(g_meet.msg, sizeof g_meet.msg, "%s", st ? fmmfft_last_error_string() : "");
+    free(g_meet.blocks);
+    g_meet.blocks = NULL;
+    g_meet.active = 0;
+    g_meet.gen++;
+    pthread_cond_broadcast(&g_meet_cv);
+    status = st;
+    snprintf(msg, sizeof msg, "%s", g_meet.msg);
+  } else {
+    struct timespec dl;
+    clock_gettime(CLOCK_REALTIME, &dl);
+    const long ms = rank_timeout_ms();
+    dl.tv_sec += ms / 1000, dl.tv_nsec += (ms % 1000) * 1000000L;
+    if (dl.tv_nsec >= 1000000000L) dl.tv_sec++, dl.tv_nsec -= 1000000000L;
+    int w = 0;
+    while (g_meet.gen == my_gen && w == 0) w = pthread_cond_timedwait(&g_meet_cv, &g_meet_mu, &dl);
+    if (g_meet.gen == my_gen) { /* the other ranks never came: withdraw this rank's block */
+      g_meet.blocks[myid] = NULL;
+      if (--g_meet.arrived == 0) {
+        free(g_meet.blocks);
+        g_meet.blocks = NULL;
+        g_meet.active = 0;
+      }
+      status = FMMFFT_ERR_TIMEOUT;
+      snprintf(msg, sizeof msg, "mft: not every rank of the collective called within the time limit");
+    } else {
+      status = g_meet.status;
+      snprintf(msg, sizeof msg, "%s", g_meet.msg);
+    }
+  }
+  pthread_mutex_unlock(&g_meet_mu);
+  set_err(status, status ? msg : NULL);
+}
+
 void mft(long lq, void *qr, long dir, long p, long myid, long terms, long b, double *w, double *v,
          long sz1, long szwk, void *forward_plan) {
-  (void)myid, (void)w, (void)v, (void)sz1, (void)szwk, (void)forward_plan;
+  (void)w, (void)v, (void)sz1, (void)szwk, (void)forward_plan;
   if (!qr) {
     set_err(FMMFFT_ERR_INVALID, "mft: NULL qr");
     return;
@@ -400,6 +526,11 @@ void mft(long lq, void *qr, long dir, long p, long myid, long terms, long b, dou
     set_err(FMMFFT_ERR_INVALID, "mft: unsupported parameters");
     return;
   }
+  if (g_rank_mode) {
+    mft_rank(lq, qr, p, myid, terms, b);
+    return;
+  }
+  (void)myid;
   int st;
   fmmfft_plan pl = compat_plan(lq, p, terms, b, &st);
   if (!pl) return;
@@ -417,7 +548,7 @@ struct fmmfft_fft_s {
 int fmmfft_fft_create(fmmfft_fft *out, long N, int precision) {
   if (!out) return set_err(FMMFFT_ERR_INVALID, "fft_create: NULL output pointer");
   *out = NULL;
-  if (precision < FMMFFT_F64 || precision > FMMFFT_F32_TC)
+  if (precision < FMMFFT_F64 || precision > FMMFFT_BF16X3)
     return set_err(FMMFFT_ERR_INVALID, "fft_create: unknown precision");
   struct fmmfft_fft_s *f = (struct fmmfft_fft_s *)calloc(1, sizeof *f);
   if (!f) return set_err(FMMFFT_ERR_NOMEM, "fft_create: host allocation failed");

@@ -140,6 +140,7 @@ template <typename R> struct Dev {
    * per stage, as measured fastest: S2M and M2M the 16-lane row form, M2L and the leaf the
    * 32-lane one (the same speed for M2L, faster and more accurate for the leaf) */
   int tc_form;
+  int bf16;    /* FMMFFT_BF16X3: the tensor-core stages in BF16x3 instead of split TF32 */
   int pdl;     /* row-form launches as programmatic dependent launches (FMMFFT_PDL=0: off) */
   unsigned *sync;   /* grid barrier of the coarse-tree kernel: [0] arrivals, [32] generation */
   long coarse_rows; /* levels with fewer rows go to the coarse-tree kernel (0: none) */
@@ -728,12 +729,14 @@ template <class Prob> static bool tc_form_fits(const Prob &pb) {
 }
 
 template <class Prob>
-static void launch_tc(const Prob &pb0, int num_sms, int *status, cudaStream_t st, int form, int pdl) {
+static void launch_tc(const Prob &pb0, int num_sms, int *status, cudaStream_t st, int form, int pdl,
+                      int bf16 = 0) {
   Prob pb = pb0;
+  if (bf16) form = 4; /* BF16x3 exists in the warp-specialised form only */
   if (form == 4 && tc::ws_fits(pb.kpad, pb.npad)) {
     const long tiles = (pb.rows + tc::kRows - 1) / tc::kRows * pb.batches;
     const int grid = (int)(tiles < num_sms ? tiles : num_sms); /* one CTA per SM: all of TMEM */
-    const size_t smem = tc::ws_smem_bytes(pb.kpad, pb.npad);
+    const size_t smem = tc::ws_smem_bytes(pb.kpad, pb.npad, bf16 ? 2 : 4);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)grid);
     cfg.blockDim = dim3(tc::kWThreads);
@@ -744,7 +747,10 @@ static void launch_tc(const Prob &pb0, int num_sms, int *status, cudaStream_t st
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
     cfg.numAttrs = pdl ? 1 : 0;
-    cudaLaunchKernelEx(&cfg, tc::k_tc_ws<Prob>, pb, status);
+    if (bf16)
+      cudaLaunchKernelEx(&cfg, tc::k_tc_ws<Prob, true>, pb, status);
+    else
+      cudaLaunchKernelEx(&cfg, tc::k_tc_ws<Prob, false>, pb, status);
     return;
   }
   if (form == 2 && pb.batches == 1 && pb.npad <= 64 && pb.nout <= 64 && pb.kpad % 8 == 0 &&
@@ -1786,28 +1792,52 @@ static float tf32_rna_host(float f) {
   return r;
 }
 
+/* FP32 -> BF16 bits, round to nearest even (finite values): the upper 16 bits after adding half a
+ * BF16 unit minus one plus the lowest kept bit; and BF16 bits -> FP32. */
+static uint16_t bf16_rne_host(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  u += 0x7FFFu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+static float bf16_to_float_host(uint16_t b) {
+  const uint32_t u = (uint32_t)b << 16;
+  float f;
+  memcpy(&f, &u, 4);
+  return f;
+}
+
 /* Uploads one operator, given as FP64 [npad][kpad] K-major values, split into TF32 hi and lo:
  * as two [npad][kpad] arrays (dhi, dlo) and, when dws is given, as the warp-specialised
  * kernel's block (hi rows 0..npad-1, lo rows npad..2 npad-1, core-matrix layout). */
 static int tc_put(float *dhi, float *dlo, float *dws, const double *v, int kpad, int npad, char *err,
-                  size_t errlen) {
+                  size_t errlen, int bf16 = 0) {
   const long cnt = (long)kpad * npad;
   const size_t wsn = tc::ws_b_floats(kpad, npad);
   float *h = (float *)calloc((size_t)2 * cnt + wsn + 1, sizeof(float));
   if (!h) return 2;
   float *w = h + 2 * cnt;
+  uint16_t *wb = (uint16_t *)w; /* BF16 block: wsn 16-bit values */
   for (long i = 0; i < cnt; ++i) {
     float f = (float)v[i];
     float hi = tf32_rna_host(f);
     h[i] = hi;
     h[cnt + i] = tf32_rna_host(f - hi);
     const int n = (int)(i / kpad), k = (int)(i % kpad);
-    w[tc::ws_b_index(n, k, kpad)] = h[i];
-    w[tc::ws_b_index(npad + n, k, kpad)] = h[cnt + i];
+    if (bf16) {
+      const uint16_t bh = bf16_rne_host(f);
+      const float fh = bf16_to_float_host(bh);
+      wb[tc::ws_b_index_bf16(n, k, kpad)] = bh;
+      wb[tc::ws_b_index_bf16(npad + n, k, kpad)] = bf16_rne_host(f - fh);
+    } else {
+      w[tc::ws_b_index(n, k, kpad)] = h[i];
+      w[tc::ws_b_index(npad + n, k, kpad)] = h[cnt + i];
+    }
   }
   cudaError_t e = cudaMemcpy(dhi, h, sizeof(float) * cnt, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(dlo, h + cnt, sizeof(float) * cnt, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && dws) e = cudaMemcpy(dws, w, sizeof(float) * wsn, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && dws)
+    e = cudaMemcpy(dws, w, (bf16 ? 2 : 4) * wsn, cudaMemcpyHostToDevice);
   free(h);
   if (e != cudaSuccess) {
     snprintf(err, errlen, "cudaMemcpy: %s", cudaGetErrorString(e));
@@ -1831,7 +1861,7 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
     for (long i = 0; i < (long)kp * np; ++i) v[i] = 0;
     for (long nn = 0; nn < T; ++nn)
       for (long k = 0; k < b; ++k) v[nn * kp + k] = o->initch[k * T + nn];
-    rc |= tc_put(d->tc_s2m[0], d->tc_s2m[1], d->ws_s2m, v, kp, np, err, errlen);
+    rc |= tc_put(d->tc_s2m[0], d->tc_s2m[1], d->ws_s2m, v, kp, np, err, errlen, d->bf16);
   }
   if (d->ok_m2m)
     for (long L = 2; L <= n - 1; ++L) {
@@ -1844,7 +1874,7 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
           v[t * kp + T + k] = ops[FMM_SHFTFP * T * T + t * T + k];
         }
       rc |= tc_put(d->tc_m2m[0] + (L - 2) * d->tc_m2m_stride, d->tc_m2m[1] + (L - 2) * d->tc_m2m_stride,
-                   d->ws_m2m + (L - 2) * d->ws_m2m_stride, v, kp, np, err, errlen);
+                   d->ws_m2m + (L - 2) * d->ws_m2m_stride, v, kp, np, err, errlen, d->bf16);
     }
   if (d->ok_m2l)
     for (long l = 3; l <= n; ++l) {
@@ -1865,7 +1895,7 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
         }
 #undef OPT
       rc |= tc_put(d->tc_m2l[0] + (l - 3) * d->tc_m2l_stride, d->tc_m2l[1] + (l - 3) * d->tc_m2l_stride,
-                   d->ws_m2l + (l - 3) * d->ws_m2l_stride, v, kp, np, err, errlen);
+                   d->ws_m2l + (l - 3) * d->ws_m2l_stride, v, kp, np, err, errlen, d->bf16);
     }
   if (d->ok_leaf)
     for (long sc = 1; sc < P; ++sc) {
@@ -1881,7 +1911,7 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
         for (long q = 0; q < 3 * b; ++q) v[b * kp + T + q] = ct[q];
       }
       rc |= tc_put(d->tc_leaf[0] + (sc - 1) * d->tc_leaf_stride, d->tc_leaf[1] + (sc - 1) * d->tc_leaf_stride,
-                   d->ws_leaf + (sc - 1) * d->ws_leaf_stride, v, kp, np, err, errlen);
+                   d->ws_leaf + (sc - 1) * d->ws_leaf_stride, v, kp, np, err, errlen, d->bf16);
     }
   free(v);
   return rc;
@@ -1942,7 +1972,8 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
   const long nlev = n - 2 > 0 ? n - 2 : 0;
   const long lvtot = 2 * S1 * T * ((2L << n) - 4);
   /* tensor-core operator shapes (precision FMMFFT_F32_TC only) */
-  const int tc = (precision == 2 && sizeof(R) == 4);
+  const int tc = ((precision == 2 || precision == 3) && sizeof(R) == 4);
+  d->bf16 = precision == 3 && sizeof(R) == 4;
   auto up8 = [](long v) { return (int)((v + 7) / 8 * 8); };
   auto up16 = [](long v) { return (int)((v + 15) / 16 * 16); };
   d->tc = tc;
@@ -1996,10 +2027,12 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
   const long sz_m2m = d->ok_m2m ? nlev * d->tc_m2m_stride : 0;
   const long sz_m2l = d->ok_m2l ? nlev * d->tc_m2l_stride : 0;
   const long sz_leaf = d->ok_leaf ? S1 * d->tc_leaf_stride : 0;
-  d->ws_m2m_stride = (long)tc::ws_b_floats(d->kp_m2m, d->np_m2m);
-  d->ws_m2l_stride = (long)tc::ws_b_floats(d->kp_m2l, d->np_m2l);
-  d->ws_leaf_stride = (long)tc::ws_b_floats(d->kp_leaf, d->np_leaf);
-  const long ws_s2m_n = d->ok_s2m ? (long)tc::ws_b_floats(d->kp_s2m, d->np_s2m) : 0;
+  /* in floats; a BF16 block is half as many (its element count is even) */
+  const long wdiv = d->bf16 ? 2 : 1;
+  d->ws_m2m_stride = (long)tc::ws_b_floats(d->kp_m2m, d->np_m2m) / wdiv;
+  d->ws_m2l_stride = (long)tc::ws_b_floats(d->kp_m2l, d->np_m2l) / wdiv;
+  d->ws_leaf_stride = (long)tc::ws_b_floats(d->kp_leaf, d->np_leaf) / wdiv;
+  const long ws_s2m_n = d->ok_s2m ? (long)tc::ws_b_floats(d->kp_s2m, d->np_s2m) / wdiv : 0;
   const long ws_m2m_n = d->ok_m2m ? nlev * d->ws_m2m_stride : 0;
   const long ws_m2l_n = d->ok_m2l ? nlev * d->ws_m2l_stride : 0;
   const long ws_leaf_n = d->ok_leaf ? S1 * d->ws_leaf_stride : 0;
@@ -2218,7 +2251,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.kpad = d->kp_s2m, q.npad = d->np_s2m, q.nout = (int)T;
         q.bhi = d->tc_s2m[0], q.blo = d->tc_s2m[1], q.bstride = 0, q.wsb = d->ws_s2m, q.wsb_stride = 0;
         q.xt = d->xt, q.out = d->phi + lvl_off(n, S1e, T), q.M = M, q.b = (int)b, q.T = (int)T;
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 4 : d->tc_form, d->pdl);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 4 : d->tc_form, d->pdl, d->bf16);
         done = true;
       }
     }
@@ -2254,7 +2287,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.bhi = d->tc_m2m[0] + (L - 2) * d->tc_m2m_stride, q.blo = d->tc_m2m[1] + (L - 2) * d->tc_m2m_stride;
         q.bstride = 0, q.wsb = d->ws_m2m + (L - 2) * d->ws_m2m_stride, q.wsb_stride = 0;
         q.child = d->phi + lvl_off(L + 1, S1e, T), q.out = d->phi + lvl_off(L, S1e, T), q.T = (int)T;
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 4 : d->tc_form, d->pdl);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 4 : d->tc_form, d->pdl, d->bf16);
         done = true;
       }
     }
@@ -2307,7 +2340,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.bstride = 0, q.wsb = d->ws_m2l + (l - 3) * d->ws_m2l_stride, q.wsb_stride = 0;
         q.psi_par = d->psi + lvl_off(l - 1, S1e, T), q.phi = d->phi + lvl_off(l, S1e, T);
         q.out = d->psi + lvl_off(l, S1e, T), q.T = (int)T, q.lpar = (int)(l - 1);
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 4 : d->tc_form, d->pdl);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 4 : d->tc_form, d->pdl, d->bf16);
         done = true;
       }
     }
@@ -2343,7 +2376,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.fixbuf = d->leaf_fix, q.P = (int)P;
         q.psi_n = pb.psi_n, q.xt = d->xt, q.u = d->u, q.M = M, q.s = s, q.T = (int)T, q.b = (int)b;
         q.log2s = (int)n;
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 4 : d->tc_form, d->pdl);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 4 : d->tc_form, d->pdl, d->bf16);
         done = true;
       }
     }
@@ -2515,6 +2548,10 @@ static int set_smem_limits(void) {
   allow_dyn_smem(tc::k_tc_ws<TcM2M>, lim);
   allow_dyn_smem(tc::k_tc_ws<TcM2L>, lim);
   allow_dyn_smem(tc::k_tc_ws<TcLeaf>, lim);
+  allow_dyn_smem(tc::k_tc_ws<TcS2M, true>, lim);
+  allow_dyn_smem(tc::k_tc_ws<TcM2M, true>, lim);
+  allow_dyn_smem(tc::k_tc_ws<TcM2L, true>, lim);
+  allow_dyn_smem(tc::k_tc_ws<TcLeaf, true>, lim);
   if (dev < FMMK_MAXDEV) done[dev] = 1;
   return 0;
 }
@@ -2642,6 +2679,34 @@ extern "C" int fmmk_execute_host(fmmk_state *st, const void *h_in, void *h_out, 
   if (rc) return rc;
   FMM_CUDA_TRY(cudaMemcpyAsync(h_out, work, esz * (size_t)N, cudaMemcpyDeviceToHost, s));
   FMM_CUDA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
+/* Block-distributed input and output: block r (M complex values, rank r's lq-block `qr` in the
+ * reference) at in[r] / out[r], device or host memory.  The blocks are gathered into the plan's
+ * z buffer (dead until the combine), transformed in place there and scattered back; host
+ * blocks synchronise the stream at the end. */
+extern "C" int fmmk_execute_blocks(fmmk_state *st, const void *const *in, void *const *out, int host,
+                                   void *stream, char *err, size_t errlen) {
+  cudaStream_t s = (cudaStream_t)stream;
+  long M, P;
+  size_t esz;
+  char *work;
+  if (st->precision == 0) {
+    Dev<double> *d = (Dev<double> *)st->dev;
+    M = d->M, P = d->P, esz = sizeof(double2), work = (char *)d->z;
+  } else {
+    Dev<float> *d = (Dev<float> *)st->dev;
+    M = d->M, P = d->P, esz = sizeof(float2), work = (char *)d->z;
+  }
+  const size_t blk = esz * (size_t)M;
+  const cudaMemcpyKind kin = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  const cudaMemcpyKind kout = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  for (long r = 0; r < P; ++r) FMM_CUDA_TRY(cudaMemcpyAsync(work + r * blk, in[r], blk, kin, s));
+  int rc = fmmk_execute(st, work, work, stream, 0, err, errlen);
+  if (rc) return rc;
+  for (long r = 0; r < P; ++r) FMM_CUDA_TRY(cudaMemcpyAsync(out[r], work + r * blk, blk, kout, s));
+  if (host) FMM_CUDA_TRY(cudaStreamSynchronize(s));
   return 0;
 }
 

@@ -1393,18 +1393,46 @@ __host__ __device__ constexpr int ws_acc_cols(int npad) { return round32(2 * npa
 __host__ __device__ constexpr size_t ws_b_floats(int kpad, int npad) {
   return (size_t)2 * npad * round32(kpad);
 }
-__host__ __device__ constexpr size_t ws_smem_bytes(int kpad, int npad) {
-  return ws_b_floats(kpad, npad) * 4 + (size_t)kWStages * kWStageBytes;
+/* eb: bytes per operator element, 4 (TF32) or 2 (BF16) */
+__host__ __device__ constexpr size_t ws_smem_bytes(int kpad, int npad, int eb = 4) {
+  return ws_b_floats(kpad, npad) * eb + (size_t)kWStages * kWStageBytes;
 }
 /* the operator fits: two accumulators and the A slots within 512 TMEM columns, K <= 256 */
 __host__ __device__ constexpr bool ws_fits(int kpad, int npad) {
   return npad % 16 == 0 && npad <= 64 && kpad % 8 == 0 && kpad <= kWKs * kWMaxSlots &&
          2 * ws_acc_cols(npad) + kWSlots * 2 * kWKs <= 512 && ws_smem_bytes(kpad, npad) <= 200 * 1024;
 }
-/* float index of operator element (n, k), n < 2 npad (hi rows, then lo rows), in the layout the
- * kernel copies: 8-row groups of round32(kpad) / 4 core matrices of 8 rows x 4 floats */
+/* element index of operator element (n, k), n < 2 npad (hi rows, then lo rows), in the layout
+ * the kernel copies: 8-row groups of core matrices of 8 rows x 16 bytes along K (4 TF32 or 8
+ * BF16 values per row of a core matrix) */
 __host__ __device__ inline long ws_b_index(int n, int k, int kpad) {
   return (long)(n >> 3) * (round32(kpad) * 8) + (k >> 2) * 32 + (n & 7) * 4 + (k & 3);
+}
+__host__ __device__ inline long ws_b_index_bf16(int n, int k, int kpad) {
+  return (long)(n >> 3) * (round32(kpad) * 8) + (k >> 3) * 64 + (n & 7) * 8 + (k & 7);
+}
+
+/* Instruction descriptor, kind::f16 with BF16 A and B: D = F32, both K-major, M = 128. */
+__host__ __device__ constexpr uint32_t make_idesc_bf16(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+/* BF16 MMA, A from tensor memory (two values per 32-bit column, K = 16 per instruction). */
+__device__ __forceinline__ void mma_bf16_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc,
+                                            uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      :
+      : "r"(d_tmem), "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0),
+        "r"(0)
+      : "memory");
+}
+/* two floats to BF16 (round to nearest even), packed: `lo` in bits 0-15, `hi` in bits 16-31 */
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+  uint32_t d;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+  return d;
 }
 
 __device__ __forceinline__ void cp_async16_cg(uint32_t dst, const void *src) {
@@ -1435,8 +1463,12 @@ __device__ __forceinline__ bool named_bar_or(int id, int nthreads, bool v) {
   return r != 0;
 }
 
-template <class Prob>
+template <class Prob, bool kBF = false>
 __global__ void __launch_bounds__(kWThreads, 1) k_tc_ws(const __grid_constant__ Prob pb, int *status) {
+  /* kBF: BF16x3 instead of split TF32: A and B split into BF16 hi + lo (the lo part the BF16
+   * rounding of the residual), products A_hi B_hi + A_hi B_lo + A_lo B_hi, kind::f16 MMAs of
+   * K = 16; about 2^-17 relative per product, for orders whose truncation is far above that */
+  constexpr int kEB = kBF ? 2 : 4;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ uint64_t tfull[kWSlots], tempty[kWSlots], afull[2], aempty[2], bbar, fin;
   __shared__ uint32_t tmem_slot;
@@ -1448,7 +1480,7 @@ __global__ void __launch_bounds__(kWThreads, 1) k_tc_ws(const __grid_constant__ 
   const int kpad = pb.kpad, npad = pb.npad;
   const int nsl = round32(kpad) / kWKs;
   float *Bs = reinterpret_cast<float *>(smem_raw);
-  unsigned char *ring = smem_raw + ws_b_floats(kpad, npad) * 4;
+  unsigned char *ring = smem_raw + ws_b_floats(kpad, npad) * kEB;
   const int mma_warp = kWProd + kWEpi;
   if (warp == mma_warp) tmem_alloc(&tmem_slot, 512);
   if (tid == 0) {
@@ -1481,7 +1513,7 @@ __global__ void __launch_bounds__(kWThreads, 1) k_tc_ws(const __grid_constant__ 
   const int tile_end = runs ? (int)(((long)ntiles * (blockIdx.x + 1)) / gridDim.x) : ntiles;
   const int tile_step = runs ? 1 : (int)gridDim.x;
   const int my_tiles = tile0 < tile_end ? (tile_end - tile0 + tile_step - 1) / tile_step : 0;
-  const uint32_t b_bytes = (uint32_t)(ws_b_floats(kpad, npad) * 4);
+  const uint32_t b_bytes = (uint32_t)(ws_b_floats(kpad, npad) * kEB);
 
   /* the operators are plan constants: the first batch's is requested before waiting for the
    * kernel this one depends on */
@@ -1540,10 +1572,20 @@ __global__ void __launch_bounds__(kWThreads, 1) k_tc_ws(const __grid_constant__ 
                        : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w)
                        : "r"(st + (uint32_t)((u ^ (my_row & 7)) << 4)));
         const float av[4] = {a.x, a.y, a.z, a.w};
+        if constexpr (kBF) { /* packed BF16 pairs: hv / lv words 2i, 2i + 1 */
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          hv[4 * i + k] = tf32_rna(av[k]);
-          lv[4 * i + k] = tf32_rna(av[k] - hv[4 * i + k]);
+          for (int k = 0; k < 2; ++k) {
+            const uint32_t hw = pack_bf16x2(av[2 * k], av[2 * k + 1]);
+            const float h0 = __uint_as_float(hw << 16), h1 = __uint_as_float(hw & 0xFFFF0000u);
+            hv[2 * i + k] = __uint_as_float(hw);
+            lv[2 * i + k] = __uint_as_float(pack_bf16x2(av[2 * k] - h0, av[2 * k + 1] - h1));
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            hv[4 * i + k] = tf32_rna(av[k]);
+            lv[4 * i + k] = tf32_rna(av[k] - hv[4 * i + k]);
+          }
         }
       }
       const int s = (int)(g % kWSlots);
@@ -1552,11 +1594,17 @@ __global__ void __launch_bounds__(kWThreads, 1) k_tc_ws(const __grid_constant__ 
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (!ok) continue; /* the next barrier sees the abort */
       fence_after_sync();
-      const uint32_t ahi = tmem + lane_addr + (uint32_t)(2 * acc_cols + s * 2 * kWKs + 16 * h);
-      tmem_st8(ahi, hv);
-      tmem_st8(ahi + 8, hv + 8);
-      tmem_st8(ahi + kWKs, lv);
-      tmem_st8(ahi + kWKs + 8, lv + 8);
+      if constexpr (kBF) { /* 16 values = 8 columns per half; lo 16 columns after hi */
+        const uint32_t ahi = tmem + lane_addr + (uint32_t)(2 * acc_cols + s * 2 * kWKs + 8 * h);
+        tmem_st8(ahi, hv);
+        tmem_st8(ahi + kWKs / 2, lv);
+      } else {
+        const uint32_t ahi = tmem + lane_addr + (uint32_t)(2 * acc_cols + s * 2 * kWKs + 16 * h);
+        tmem_st8(ahi, hv);
+        tmem_st8(ahi + 8, hv + 8);
+        tmem_st8(ahi + kWKs, lv);
+        tmem_st8(ahi + kWKs + 8, lv + 8);
+      }
       tmem_st_wait();
       fence_before_sync();
       __syncwarp();
@@ -1593,8 +1641,9 @@ __global__ void __launch_bounds__(kWThreads, 1) k_tc_ws(const __grid_constant__ 
   } else {
    if (lane == 0) {
     /* ---------------------------------------------------------- MMA issue, B staging */
-    const uint32_t idesc2 = make_idesc_tf32(2 * npad), idesc1 = make_idesc_tf32(npad);
-    const uint32_t bsm = smem_addr(Bs), b_sbo = (uint32_t)round32(kpad) * 32;
+    const uint32_t idesc2 = kBF ? make_idesc_bf16(2 * npad) : make_idesc_tf32(2 * npad);
+    const uint32_t idesc1 = kBF ? make_idesc_bf16(npad) : make_idesc_tf32(npad);
+    const uint32_t bsm = smem_addr(Bs), b_sbo = (uint32_t)round32(kpad) * 8 * kEB;
     int cur_batch = my_tiles > 0 ? tile0 / tiles_per_batch : -1;
     uint32_t bphase = 0;
     bool ok = my_tiles == 0 || t_wait(&bbar, bphase, &abort_flag, status);
@@ -1625,13 +1674,23 @@ __global__ void __launch_bounds__(kWThreads, 1) k_tc_ws(const __grid_constant__ 
         if (!ok) break;
         fence_after_sync();
         const int k0 = j * kWKs;
-        const int ksteps = ((kpad - k0) < kWKs ? (kpad - k0) : kWKs) >> 3;
         const uint32_t ahi = tmem + (uint32_t)(2 * acc_cols + s * 2 * kWKs);
-        for (int kk = 0; kk < ksteps; ++kk) {
-          /* K step of 8 TF32 = two core matrices along K = 256 bytes of each 8-row group */
-          const uint64_t db = make_desc(bsm + 256u * (uint32_t)((k0 >> 3) + kk), 128, b_sbo);
-          mma_tf32_ts(d, ahi + 8u * kk, db, idesc2, (j | kk) != 0);
-          mma_tf32_ts(d, ahi + kWKs + 8u * kk, db, idesc1, 1);
+        if constexpr (kBF) {
+          /* K step of 16 BF16 = two core matrices along K = 256 bytes; 8 TMEM columns of A */
+          const int ksteps = (((kpad - k0) < kWKs ? (kpad - k0) : kWKs) + 15) >> 4;
+          for (int kk = 0; kk < ksteps; ++kk) {
+            const uint64_t db = make_desc(bsm + 256u * (uint32_t)((k0 >> 4) + kk), 128, b_sbo);
+            mma_bf16_ts(d, ahi + 8u * kk, db, idesc2, (j | kk) != 0);
+            mma_bf16_ts(d, ahi + kWKs / 2 + 8u * kk, db, idesc1, 1);
+          }
+        } else {
+          const int ksteps = ((kpad - k0) < kWKs ? (kpad - k0) : kWKs) >> 3;
+          for (int kk = 0; kk < ksteps; ++kk) {
+            /* K step of 8 TF32 = two core matrices along K = 256 bytes of each 8-row group */
+            const uint64_t db = make_desc(bsm + 256u * (uint32_t)((k0 >> 3) + kk), 128, b_sbo);
+            mma_tf32_ts(d, ahi + 8u * kk, db, idesc2, (j | kk) != 0);
+            mma_tf32_ts(d, ahi + kWKs + 8u * kk, db, idesc1, 1);
+          }
         }
         mma_commit(&tempty[s]);
       }

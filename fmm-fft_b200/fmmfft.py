@@ -16,8 +16,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libfmmfft_b200.so")
 
-F64, F32, F32_TC = 0, 1, 2
-PRECISIONS = {"f64": F64, "f32": F32, "f32_tc": F32_TC}
+F64, F32, F32_TC, BF16X3 = 0, 1, 2, 3
+PRECISIONS = {"f64": F64, "f32": F32, "f32_tc": F32_TC, "bf16x3": BF16X3}
 STATUS = {0: "OK", 1: "ERR_INVALID", 2: "ERR_NOMEM", 3: "ERR_CUDA", 4: "ERR_NO_DEVICE",
           5: "ERR_UNSUPPORTED", 6: "ERR_TIMEOUT", 7: "ERR_BUSY"}
 
@@ -29,7 +29,8 @@ EXPORTS = ["getwlen2", "getvlen", "mfti", "mft", "fmmfft_last_error", "fmmfft_la
            "fmmfft_stage_name", "fmmfft_execute_noalloc", "fmmfft_plan_check",
            "fmmfft_plan_selftest_wait", "fmmfft_plan_create_batched", "fmmfft_execute_many",
            "fmmfft_execute_many_graph", "fmmfft_plan_bytes", "fmmfft_server_counts",
-           "fmmfft_plan_enable_refinement", "fmmfft_execute_refined",
+           "fmmfft_plan_enable_refinement", "fmmfft_execute_refined", "fmmfft_mft_rank_mode",
+           "fmmfft_execute_blocks", "fmmfft_execute_blocks_host",
            "fmmfft_execute_graph", "fmmfft_batch_create", "fmmfft_batch_launch",
            "fmmfft_batch_destroy", "fmmfft_server_create", "fmmfft_server_destroy",
            "fmmfft_server_submit", "fmmfft_server_query", "fmmfft_server_wait",
@@ -95,6 +96,11 @@ def load(path=LIB_PATH):
     lib.fmmfft_plan_enable_refinement.restype = _I
     lib.fmmfft_execute_refined.argtypes = [_VP, _VP, _VP, _VP]
     lib.fmmfft_execute_refined.restype = _I
+    lib.fmmfft_mft_rank_mode.argtypes = [_I]
+    lib.fmmfft_mft_rank_mode.restype = _I
+    for f in ("fmmfft_execute_blocks", "fmmfft_execute_blocks_host"):
+        getattr(lib, f).argtypes = [_VP, _VP, _VP, _VP]
+        getattr(lib, f).restype = _I
     lib.fmmfft_execute_graph.argtypes = [_VP, _VP, _VP, _VP]
     lib.fmmfft_execute_graph.restype = _I
     lib.fmmfft_batch_create.argtypes = [ctypes.POINTER(_VP), _VP, _VP, _VP, _I, _I]
@@ -157,9 +163,14 @@ def mfti(lq, p, terms, b, w, v=None, szkeep=0, sztemp=0):
         raise FmmFftError(st, msg)
 
 
+_rank_mode = False
+
+
 def mft(lq, qr, dir, p, myid=0, terms=None, b=None, w=None, v=None, sz1=0, szwk=0, plan=None):
-    """In-place forward FMM-FFT of the full vector qr (complex128, p*lq values, host)."""
-    assert qr.dtype == np.complex128 and qr.flags.c_contiguous and qr.size == p * lq
+    """In-place forward FMM-FFT of the full vector qr (complex128, p*lq values, host); in rank
+    mode, rank myid's block of lq values, collectively with the other p - 1 ranks' calls."""
+    assert qr.dtype == np.complex128 and qr.flags.c_contiguous
+    assert qr.size == (lq if _rank_mode else p * lq)
     load().mft(lq, qr.ctypes.data, dir, p, myid, terms, b,
                None if w is None else w.ctypes.data, None if v is None else v.ctypes.data,
                sz1, szwk, plan)
@@ -174,6 +185,13 @@ def plan_bytes(N, P, terms, b, precision="f32", max_transforms=1):
     _check(load().fmmfft_plan_bytes(int(N), int(P), int(terms), int(b), PRECISIONS[precision],
                                     int(max_transforms), ctypes.byref(v)))
     return v.value
+
+
+def mft_rank_mode(on):
+    """Switch mft between full-vector calls and collective per-rank calls (see fmmfft.h)."""
+    global _rank_mode
+    _check(load().fmmfft_mft_rank_mode(1 if on else 0))
+    _rank_mode = bool(on)
 
 
 def execute_noalloc(N, P, terms, b, d_in, d_out, stream=0):
@@ -198,6 +216,15 @@ class Plan:
         _check(load().fmmfft_plan_create_batched(ctypes.byref(h), self.N, self.P, self.terms,
                                                  self.b, self._p, self.max_transforms))
         self._h = h
+
+    def execute_blocks_ptr(self, ins, outs, stream=0, host=False):
+        """Block-distributed transform: P input / output block pointers (M values each)."""
+        n = self.P
+        assert len(ins) == n and len(outs) == n
+        a = (_VP * n)(*ins)
+        o = (_VP * n)(*outs)
+        f = load().fmmfft_execute_blocks_host if host else load().fmmfft_execute_blocks
+        _check(f(self._h, a, o, stream or None))
 
     def enable_refinement(self):
         """Build the FP64 companion plan of the residual-correction pass (once)."""

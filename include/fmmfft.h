@@ -50,7 +50,11 @@ typedef enum {
 typedef enum {
   FMMFFT_F64 = 0,     /* FP64 everywhere (the reference's precision) */
   FMMFFT_F32 = 1,     /* FP32 on CUDA cores: the plain GPU FMM-FFT */
-  FMMFFT_F32_TC = 2   /* operator contractions on tcgen05 tensor cores in split TF32, rest FP32 */
+  FMMFFT_F32_TC = 2,  /* operator contractions on tcgen05 tensor cores in split TF32 (operands
+                         split into TF32 hi + lo, three products, FP32 accumulation), rest FP32 */
+  FMMFFT_BF16X3 = 3   /* the same contractions in BF16x3 (BF16 hi + lo, three products, FP32
+                         accumulation, ~2^-17 per product): for orders whose truncation error is
+                         well above 1e-5 (the 1e-4 accuracy class); rest FP32 */
 } fmmfft_precision;
 
 /* ------------------------------------------------------------------ reference-compatible */
@@ -75,6 +79,20 @@ void mfti(long lq, long p, long terms, long b, double *w, double *v, long szkeep
  * forward_plan are accepted for signature compatibility and not used (w may be NULL). */
 void mft(long lq, void *qr, long dir, long p, long myid, long terms, long b, double *w, double *v,
          long sz1, long szwk, void *forward_plan);
+
+/* Rank mode of mft for SPMD callers whose ranks are threads of one process (the reference's
+ * ranks are MPI processes, src/fmmfft.c:980): after fmmfft_mft_rank_mode(1), mft(lq, qr, dir,
+ * p, myid, ...) is collective over p calls from p threads with myid = 0 .. p-1, each passing
+ * ONLY its own block qr of lq complex128 values (rank myid's block, the reference's per-rank
+ * buffer); the last caller to arrive runs the transform of the whole vector on the GPU, and
+ * every call returns with its block holding its lq outputs, as the reference's mft does.  A
+ * call whose partners do not all arrive within FMMFFT_RANK_TIMEOUT_MS (120 s by default) returns
+ * with FMMFFT_ERR_TIMEOUT and its block untouched.  Calls with mismatched (lq, p, terms, b) or
+ * a repeated myid are refused.  fmmfft_mft_rank_mode(0) restores full-vector calls; switching
+ * is refused with FMMFFT_ERR_BUSY while a collective is in progress.  MPI callers whose ranks
+ * are processes gather the blocks to one rank and call fmmfft_execute_blocks_host there
+ * (INTEGRATION.md shows the binding). */
+int fmmfft_mft_rank_mode(int on);
 
 /* Status of the calling thread's last compatibility call (FMMFFT_OK after success). */
 int fmmfft_last_error(void);
@@ -133,6 +151,16 @@ int fmmfft_execute_refined(fmmfft_plan plan, const void *d_in, void *d_out, void
 
 /* Same transform from and to HOST memory: copies in, executes, copies out, synchronises. */
 int fmmfft_execute_host(fmmfft_plan plan, const void *h_in, void *h_out, void *stream);
+
+/* Block-distributed transform: P input blocks of M = N/P complex values each (block r = rank
+ * r's lq-block qr of the reference's SPMD layout, i.e. elements r*M .. r*M+M-1 of the vector)
+ * and P output blocks (block r receives outputs r*M .. r*M+M-1, rank r's result in the
+ * reference).  _blocks: device pointers, enqueued on `stream`; _blocks_host: host pointers,
+ * synchronises.  Input and output blocks may be the same buffers. */
+int fmmfft_execute_blocks(fmmfft_plan plan, const void *const *d_blocks_in, void *const *d_blocks_out,
+                          void *stream);
+int fmmfft_execute_blocks_host(fmmfft_plan plan, const void *const *h_blocks_in, void *const *h_blocks_out,
+                               void *stream);
 
 /* Stage-level access for parity tests: copies the plan's intermediate arrays after the last
  * execute into host memory as float64 (NULL to skip):

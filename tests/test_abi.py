@@ -113,3 +113,43 @@ def test_mft_rejects_inverse_direction(fm):
     with pytest.raises(fm.FmmFftError) as ei:
         fm.mft(256, qr, -1, 4, 0, 8, 8)
     assert ei.value.status == 5
+
+
+def _rank_call(fm, results, key, *args):
+    try:
+        fm.mft(*args)
+        results[key] = 0
+    except fm.FmmFftError as e:
+        results[key] = e.status
+
+
+def test_rank_mode_collective_refuses_mismatch_and_times_out(fm, monkeypatch):
+    """Rank mode of mft (no GPU reached): a call whose (lq, p, terms, b) differ from the
+    collective in progress, or that repeats a myid, is refused at once; a rank whose partners
+    never come returns FMMFFT_ERR_TIMEOUT with its block untouched; the mode cannot be switched
+    while a collective is open."""
+    import threading
+    monkeypatch.setenv("FMMFFT_RANK_TIMEOUT_MS", "1500")
+    fm.mft_rank_mode(True)
+    try:
+        lq, p, T, b = 256, 4, 8, 8
+        blk = np.arange(lq, dtype=np.complex128)
+        keep = blk.copy()
+        res = {}
+        t0 = threading.Thread(target=_rank_call, args=(fm, res, "r0", lq, blk, 1, p, 0, T, b))
+        t0.start()
+        import time
+        time.sleep(0.2)
+        with pytest.raises(fm.FmmFftError) as ei:
+            fm.mft_rank_mode(False)
+        assert ei.value.status == 7
+        other = np.zeros(2 * lq, dtype=np.complex128)
+        _rank_call(fm, res, "mismatch", 2 * lq, other, 1, p, 1, T, b)
+        dup = np.zeros(lq, dtype=np.complex128)
+        _rank_call(fm, res, "dup", lq, dup, 1, p, 0, T, b)
+        t0.join()
+        assert res["mismatch"] == 1 and res["dup"] == 1, res
+        assert res["r0"] == 6, res
+        assert np.array_equal(blk, keep)
+    finally:
+        fm.mft_rank_mode(False)

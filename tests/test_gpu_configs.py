@@ -116,3 +116,32 @@ def test_single_large_transform_vs_reference_output(fm, accuracy_report):
         accuracy_report(f"N=2^24 P=64 T=24 b=32 normal: {prec} vs reference output rel-L2 {e:.3e} "
                         f"max {max_err(y, yr):.3e}")
         assert e < TOL, (prec, e)
+
+
+BF16_CASES = [(65536, 16, 8, 32), (1 << 18, 64, 8, 32), (1 << 18, 256, 12, 16), (1 << 16, 8, 16, 64)]
+
+
+@pytest.mark.parametrize("N,P,T,b", BF16_CASES)
+def test_bf16x3_tensor_core_stages(fm, monkeypatch, accuracy_report, N, P, T, b):
+    """BF16x3 (BF16 hi + lo operands, three products, FP32 accumulation) on every tensor-core
+    stage, for the 1e-4 accuracy class: stage outputs and the transform against the FP64 oracle
+    of the same order, rel-L2 <= 1e-4."""
+    monkeypatch.setenv("FMMFFT_TC_MIN_ROWS", "1")
+    monkeypatch.setenv("FMMFFT_FUSE_S2M", "0")
+    x = ol.seeded_input(N, 91 + N % 41)
+    o = ol.forward_ex(x, P, T, b)
+    plan = fm.Plan(N, P, T, b, "bf16x3")
+    y = run_device(plan, x)
+    plan.check()
+    d = plan.debug_fetch()
+    M = N // P
+    n = (M // b).bit_length() - 1
+    for lev in range(2, n + 1):
+        gs = fm.level_planar(d["psi"], P, T, n, lev)
+        gs = (gs[:, 0] + 1j * gs[:, 1]).transpose(1, 0, 2)
+        assert ol.rel_l2(gs, o["psi"][ol.level_slice(lev)]) < 1e-3, ("psi", lev)
+    eu = ol.rel_l2(d["u"], o["u"])
+    e = ol.rel_l2(y, o["y"])
+    accuracy_report(f"N={N} P={P} T={T} b={b} bf16x3 every stage on the tensor cores: u rel-L2 {eu:.3e}, "
+                    f"y vs oracle rel-L2 {e:.3e} max {max_err(y, o['y']):.3e}")
+    assert e < 1e-4

@@ -167,3 +167,59 @@ def test_coarse_tree_kernel_forced(fm, monkeypatch, N, P, T, b, prec):
     _, stages = plan.profile_stop()
     assert stages["coarse_tree"][1] == 1, stages
     assert ol.rel_l2(y, o["y"]) < (TOL_F64 if prec == "f64" else TOL_F32)
+
+
+@pytest.mark.parametrize("lq,p,T,b", [(4096, 4, 12, 32), (16384, 16, 16, 32), (2048, 8, 10, 16)])
+def test_mft_rank_mode_per_rank_blocks(fm, lq, p, T, b):
+    """The reference's SPMD calling pattern: p threads call mft, each with ONLY its own block
+    (rank myid's lq values); every block comes back holding that rank's outputs, equal to the
+    full-vector call's and to the reference's golden outputs where the shape has one."""
+    import threading
+    N = lq * p
+    x = ol.seeded_input(N, 5 + p)
+    full = x.copy()
+    fm.mft(lq, full, 1, p, 0, T, b)
+    blocks = [x[r * lq:(r + 1) * lq].copy() for r in range(p)]
+    res = {}
+
+    def rank(r):
+        try:
+            fm.mft(lq, blocks[r], 1, p, r, T, b)
+            res[r] = 0
+        except fm.FmmFftError as e:
+            res[r] = e.status
+
+    fm.mft_rank_mode(True)
+    try:
+        th = [threading.Thread(target=rank, args=(r,)) for r in range(p)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+    finally:
+        fm.mft_rank_mode(False)
+    assert all(v == 0 for v in res.values()) and len(res) == p, res
+    got = np.concatenate(blocks)
+    assert np.array_equal(got, full)
+    assert ol.rel_l2(got, ol.forward(x, p, T, b)) < TOL_F64
+
+
+def test_execute_blocks_device_and_host(fm):
+    """Block-distributed I/O: P separate device blocks (and P host blocks) in, P blocks out,
+    bitwise the result of the contiguous execute."""
+    import torch
+    N, P, T, b = 1 << 16, 16, 16, 32
+    x = ol.seeded_input(N, 41)
+    plan = fm.Plan(N, P, T, b, "f32_tc")
+    y = run_device(plan, x)
+    M = N // P
+    xs = [torch.from_numpy(x[r * M:(r + 1) * M]).to(torch.complex64).cuda() for r in range(P)]
+    ys = [torch.empty_like(t) for t in xs]
+    plan.execute_blocks_ptr([t.data_ptr() for t in xs], [t.data_ptr() for t in ys])
+    torch.cuda.synchronize()
+    got = np.concatenate([t.cpu().numpy() for t in ys]).astype(np.complex128)
+    assert np.array_equal(got, y)
+    hx = [np.ascontiguousarray(x[r * M:(r + 1) * M].astype(np.complex64)) for r in range(P)]
+    plan.execute_blocks_ptr([a.ctypes.data for a in hx], [a.ctypes.data for a in hx], host=True)
+    assert np.array_equal(np.concatenate(hx).astype(np.complex128), y)
+    plan.close()
