@@ -141,6 +141,12 @@ int fmmfft_execute_many_graph(fmmfft_plan plan, int count, const void *d_in, voi
   return rc ? set_err(rc, err) : FMMFFT_OK;
 }
 
+int fmmfft_plan_describe(fmmfft_plan plan, char *buf, size_t len) {
+  if (!plan || !buf || len == 0) return set_err(FMMFFT_ERR_INVALID, "plan_describe: NULL argument");
+  fmmk_describe(plan->dev, buf, len);
+  return FMMFFT_OK;
+}
+
 int fmmfft_plan_enable_refinement(fmmfft_plan plan) {
   if (!plan) return set_err(FMMFFT_ERR_INVALID, "enable_refinement: NULL plan");
   if (plan->precision == FMMFFT_F64)

@@ -54,6 +54,7 @@ int fmmk_execute_n(fmmk_state *st, const void *d_in, void *d_out, void *stream, 
                    char *err, size_t errlen);
 int fmmk_execute_blocks(fmmk_state *st, const void *const *in, void *const *out, int host, void *stream,
                         char *err, size_t errlen);
+int fmmk_describe(fmmk_state *st, char *buf, size_t len);
 int fmmk_refine_enable(fmmk_state *st, const fmm_ops64 *ops, size_t *bytes, char *err, size_t errlen);
 int fmmk_execute_refined(fmmk_state *st, const void *d_in, void *d_out, void *stream, char *err,
                          size_t errlen);

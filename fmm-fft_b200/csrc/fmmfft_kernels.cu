@@ -39,6 +39,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <mutex>
 #include <new>
 
 #include "fmmfft_internal.h"
@@ -146,7 +147,10 @@ template <typename R> struct Dev {
   long coarse_rows; /* levels with fewer rows go to the coarse-tree kernel (0: none) */
   int coarse_grid;  /* its cooperative grid (blocks of 256) */
   int fuse_s2m;     /* S2M inside the sections pass where tiles hold whole boxes */
+  unsigned env_set; /* knobs an environment switch fixed (the autotuner leaves them): bits below */
+  int tuned;        /* the knobs come from the autotuner */
 };
+enum { KNOB_FFT = 1, KNOB_COARSE = 2, KNOB_TCMIN = 4, KNOB_FUSE = 8 };
 
 /* Instantiated CUDA graphs of one plan's execute, keyed by (input, output, direction): the
  * ~35 kernel launches of a transform become one graph launch. */
@@ -1927,7 +1931,7 @@ template <typename R> static void coarse_setup(Dev<R> *d) {
    * N >= 2^23.  The choice depends on the plan only, so a transform gives the same bits alone,
    * in a batch graph or in a server mix. */
   d->coarse_rows = d->N >= (1L << 23) ? kCoarseRows : 0;
-  if (const char *ev = getenv("FMMFFT_COARSE_ROWS")) d->coarse_rows = atol(ev);
+  if (const char *ev = getenv("FMMFFT_COARSE_ROWS")) d->coarse_rows = atol(ev), d->env_set |= KNOB_COARSE;
   const size_t sm = coarse_smem<R>(d->T);
   int dev = 0, nsm = 0, nb = 0;
   cudaGetDevice(&dev);
@@ -1996,7 +2000,7 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
    * for a 1.5x faster leaf.  FMMFFT_TC_STAGES without bit 8 keeps it on the CUDA cores. */
   d->ok_leaf = fits(d->kp_leaf, d->np_leaf);
   d->tc_min_rows = kTcMinRows;
-  if (const char *ev = getenv("FMMFFT_TC_MIN_ROWS")) d->tc_min_rows = atol(ev);
+  if (const char *ev = getenv("FMMFFT_TC_MIN_ROWS")) d->tc_min_rows = atol(ev), d->env_set |= KNOB_TCMIN;
   /* FMMFFT_TC_FORM=pipelined routes the tree stages that fit to the warp-specialised kernel
    * (4xTF32, rel-L2 2.4e-7 at N = 2^24, P = 64, 24 terms, against 2.7e-7); the row form stays
    * the default because it is faster there (M2L 0.47 ms against 0.58 ms on a B200) */
@@ -2008,11 +2012,11 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
   coarse_setup(d);
   /* FMMFFT_FUSE_S2M=0 keeps S2M a separate stage (on the tensor cores for FP32 TC plans) */
   d->fuse_s2m = 1;
-  if (const char *ev = getenv("FMMFFT_FUSE_S2M")) d->fuse_s2m = atoi(ev) != 0;
+  if (const char *ev = getenv("FMMFFT_FUSE_S2M")) d->fuse_s2m = atoi(ev) != 0, d->env_set |= KNOB_FUSE;
   d->fft_threads = 512;
   if (const char *ev = getenv("FMMFFT_FFT_THREADS")) {
     const int v = atoi(ev);
-    if (v >= 32 && v <= 512 && (v & (v - 1)) == 0) d->fft_threads = v;
+    if (v >= 32 && v <= 512 && (v & (v - 1)) == 0) d->fft_threads = v, d->env_set |= KNOB_FFT;
   }
   /* FMMFFT_TC_STAGES: bit mask of the stages routed to the tensor cores (1 S2M, 2 M2M, 4 M2L,
    * 8 leaf); default all */
@@ -2493,6 +2497,110 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   return 0;
 }
 
+/* ======================================================================== autotuner */
+/* The plan's stage choices that do not change what is computed, only which kernels compute it
+ * and how: FFT block size, coarse-tree threshold (the one-launch coarse levels), the row count
+ * from which tree stages run on the tensor cores, and S2M fused into the sections pass.  On the
+ * first plan of each (N, P, terms, b, precision, capacity) in a process the autotuner times the
+ * candidates (coordinate descent: each knob over its values with the others at their best so
+ * far; each candidate the fastest of 5 executes after 2 warm-ups, in place on the plan's own
+ * workspace) and caches the winner; every later plan of that key takes the cached choice, so
+ * transforms of one shape give the same bits alone, in a batch or in a server mix.  Knobs an
+ * environment switch fixed are not tuned.  FP64 plans keep the defaults. */
+struct TuneKey {
+  long N, P, T, b;
+  int prec, nb;
+};
+struct TuneVal {
+  int fft_threads, fuse_s2m;
+  long coarse_rows, tc_min_rows;
+};
+static std::mutex g_tune_mu;
+static TuneKey g_tune_key[256];
+static TuneVal g_tune_val[256];
+static int g_ntune;
+
+template <typename R> static void tune_apply(Dev<R> *d, const TuneVal &v) {
+  if (!(d->env_set & KNOB_FFT)) d->fft_threads = v.fft_threads;
+  if (!(d->env_set & KNOB_FUSE)) d->fuse_s2m = v.fuse_s2m;
+  if (!(d->env_set & KNOB_COARSE)) d->coarse_rows = v.coarse_rows;
+  if (!(d->env_set & KNOB_TCMIN)) d->tc_min_rows = v.tc_min_rows;
+  d->tuned = 1;
+}
+
+template <typename R>
+static int dev_autotune(Dev<R> *d, char *err, size_t errlen) {
+  using C = typename cplx<R>::T;
+  const TuneKey key{d->N, d->P, d->T, d->b, d->precision, d->nbmax};
+  {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    for (int i = 0; i < g_ntune; ++i)
+      if (!memcmp(&g_tune_key[i], &key, sizeof key)) {
+        tune_apply(d, g_tune_val[i]);
+        return 0;
+      }
+  }
+  cudaStream_t st;
+  FMM_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0), cudaEventCreate(&e1);
+  const int nbt = d->nbmax;
+  FMM_CUDA_TRY(cudaMemsetAsync(d->z, 0, sizeof(C) * (size_t)d->N * nbt, st));
+  int rc = 0;
+  auto measure = [&]() -> float {
+    float best = 1e30f;
+    for (int it = 0; it < 7 && !rc; ++it) {
+      cudaEventRecord(e0, st);
+      rc = dev_execute(d, d->z, d->z, st, 0, nbt, err, errlen);
+      cudaEventRecord(e1, st);
+      cudaEventSynchronize(e1);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (it >= 2 && ms < best) best = ms;
+    }
+    return best;
+  };
+  TuneVal cur{d->fft_threads, d->fuse_s2m, d->coarse_rows, d->tc_min_rows};
+  float best = measure();
+  auto knob = [&](unsigned bit, auto set, const long *vals, int nv) {
+    if (d->env_set & bit) return;
+    TuneVal keep = cur;
+    for (int i = 0; i < nv && !rc; ++i) {
+      TuneVal c = cur;
+      set(c, vals[i]);
+      if (!memcmp(&c, &cur, sizeof c)) continue;
+      tune_apply(d, c);
+      const float t = measure();
+      if (t < best * 0.98f) best = t, keep = c; /* a 2% margin: noise does not flip the choice */
+    }
+    cur = keep;
+    tune_apply(d, cur);
+  };
+  if (d->tc) {
+    const long v[] = {1024, 4096, 16384};
+    knob(KNOB_TCMIN, [](TuneVal &c, long x) { c.tc_min_rows = x; }, v, 3);
+  }
+  if (d->N >= (1L << 23) && d->coarse_grid >= 1) { /* cooperative launches serve large plans only */
+    const long v[] = {0, 2048, 4096, 8192};
+    knob(KNOB_COARSE, [](TuneVal &c, long x) { c.coarse_rows = x; }, v, 4);
+  }
+  if (d->tileM % d->b == 0 && d->T % 4 == 0) {
+    const long v[] = {0, 1};
+    knob(KNOB_FUSE, [](TuneVal &c, long x) { c.fuse_s2m = (int)x; }, v, 2);
+  }
+  {
+    const long v[] = {256, 512};
+    knob(KNOB_FFT, [](TuneVal &c, long x) { c.fft_threads = (int)x; }, v, 2);
+  }
+  cudaEventDestroy(e0), cudaEventDestroy(e1);
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  if (g_ntune < 256) g_tune_key[g_ntune] = key, g_tune_val[g_ntune] = cur, ++g_ntune;
+  return 0;
+}
+
 /* ======================================================================== C interface */
 
 /* Opt a kernel in to the largest dynamic shared memory the device allows next to its static
@@ -2601,6 +2709,11 @@ extern "C" int fmmk_create_n(const fmm_ops64 *ops, int precision, int nb, fmmk_s
     rc = dev_create<float>(ops, precision, nb, &d, err, errlen);
     st->dev = d;
     if (!rc && device_bytes) *device_bytes = d->bytes;
+    const char *ev = getenv("FMMFFT_AUTOTUNE");
+    if (!rc && !(ev && atoi(ev) == 0)) {
+      rc = dev_autotune<float>(d, err, errlen);
+      if (rc) cudaFree(d->pool), delete d;
+    }
   }
   if (rc) {
     free(st);
@@ -3008,6 +3121,21 @@ extern "C" int fmmk_selftest_wait(fmmk_state *st, int which, long limit_us, char
   k_selftest_wait<<<1, 64>>>(which, (unsigned long long)limit_us * 1000ull, sync, status);
   FMM_CUDA_TRY(cudaGetLastError());
   FMM_CUDA_TRY(cudaDeviceSynchronize());
+  return 0;
+}
+
+/* The plan's stage choices as text (for benchmark records). */
+extern "C" int fmmk_describe(fmmk_state *st, char *buf, size_t len) {
+  if (st->precision == 0) {
+    Dev<double> *d = (Dev<double> *)st->dev;
+    snprintf(buf, len, "fft_threads=%d coarse_rows=%ld fuse_s2m=%d tuned=0", d->fft_threads, d->coarse_rows,
+             d->fuse_s2m);
+  } else {
+    Dev<float> *d = (Dev<float> *)st->dev;
+    snprintf(buf, len, "fft_threads=%d coarse_rows=%ld tc_min_rows=%ld fuse_s2m=%d tensor_cores=%s tuned=%d",
+             d->fft_threads, d->coarse_rows, d->tc_min_rows, d->fuse_s2m,
+             d->tc ? (d->bf16 ? "bf16x3" : "tf32x3") : "none", d->tuned);
+  }
   return 0;
 }
 

@@ -30,7 +30,7 @@ EXPORTS = ["getwlen2", "getvlen", "mfti", "mft", "fmmfft_last_error", "fmmfft_la
            "fmmfft_plan_selftest_wait", "fmmfft_plan_create_batched", "fmmfft_execute_many",
            "fmmfft_execute_many_graph", "fmmfft_plan_bytes", "fmmfft_server_counts",
            "fmmfft_plan_enable_refinement", "fmmfft_execute_refined", "fmmfft_mft_rank_mode",
-           "fmmfft_execute_blocks", "fmmfft_execute_blocks_host",
+           "fmmfft_execute_blocks", "fmmfft_execute_blocks_host", "fmmfft_plan_describe",
            "fmmfft_execute_graph", "fmmfft_batch_create", "fmmfft_batch_launch",
            "fmmfft_batch_destroy", "fmmfft_server_create", "fmmfft_server_destroy",
            "fmmfft_server_submit", "fmmfft_server_query", "fmmfft_server_wait",
@@ -96,6 +96,8 @@ def load(path=LIB_PATH):
     lib.fmmfft_plan_enable_refinement.restype = _I
     lib.fmmfft_execute_refined.argtypes = [_VP, _VP, _VP, _VP]
     lib.fmmfft_execute_refined.restype = _I
+    lib.fmmfft_plan_describe.argtypes = [_VP, ctypes.c_char_p, ctypes.c_size_t]
+    lib.fmmfft_plan_describe.restype = _I
     lib.fmmfft_mft_rank_mode.argtypes = [_I]
     lib.fmmfft_mft_rank_mode.restype = _I
     for f in ("fmmfft_execute_blocks", "fmmfft_execute_blocks_host"):
@@ -216,6 +218,12 @@ class Plan:
         _check(load().fmmfft_plan_create_batched(ctypes.byref(h), self.N, self.P, self.terms,
                                                  self.b, self._p, self.max_transforms))
         self._h = h
+
+    def describe(self):
+        """The plan's stage choices (autotuned or default) as text."""
+        buf = ctypes.create_string_buffer(256)
+        _check(load().fmmfft_plan_describe(self._h, buf, 256))
+        return buf.value.decode()
 
     def execute_blocks_ptr(self, ins, outs, stream=0, host=False):
         """Block-distributed transform: P input / output block pointers (M values each)."""
