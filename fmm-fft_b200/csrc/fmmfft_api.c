@@ -233,8 +233,17 @@ struct fmmfft_batch_s {
 
 int fmmfft_batch_create(fmmfft_batch *out, const fmmfft_plan *plans, const void *const *d_in,
                         void *const *d_out, int n, int nbranch) {
+  return fmmfft_batch_create_many(out, plans, NULL, d_in, d_out, n, nbranch);
+}
+
+int fmmfft_batch_create_many(fmmfft_batch *out, const fmmfft_plan *plans, const int *counts,
+                             const void *const *d_in, void *const *d_out, int n, int nbranch) {
   if (!out || !plans || !d_in || !d_out || n < 1 || nbranch < 1 || nbranch > 64)
     return set_err(FMMFFT_ERR_INVALID, "batch_create: bad arguments");
+  if (counts)
+    for (int i = 0; i < n; ++i)
+      if (!plans[i] || counts[i] < 1 || counts[i] > plans[i]->max_transforms)
+        return set_err(FMMFFT_ERR_INVALID, "batch_create: count outside 1..max_transforms of its plan");
   *out = NULL;
   fmmk_state **sts = (fmmk_state **)calloc((size_t)n, sizeof(fmmk_state *));
   int *branch = (int *)calloc((size_t)n, sizeof(int));
@@ -261,10 +270,10 @@ int fmmfft_batch_create(fmmfft_batch *out, const fmmfft_plan *plans, const void 
         if (load[k] < load[br]) br = k;
     }
     branch[i] = br;
-    load[br] += (double)plans[i]->N;
+    load[br] += (double)plans[i]->N * (counts ? counts[i] : 1);
   }
   char err[256] = {0};
-  int rc = fmmk_batch_capture(sts, d_in, d_out, NULL, branch, n, nbranch, &b->exec, err, sizeof err);
+  int rc = fmmk_batch_capture(sts, d_in, d_out, NULL, counts, branch, n, nbranch, &b->exec, err, sizeof err);
   free(sts), free(branch), free(load);
   if (rc) {
     free(b);

@@ -74,8 +74,8 @@ int fmmk_selftest_wait(fmmk_state *st, int which, long limit_us, char *err, size
 int fmmk_execute_graph(fmmk_state *st, const void *d_in, void *d_out, void *stream, int inverse,
                        char *err, size_t errlen);
 int fmmk_batch_capture(fmmk_state *const *sts, const void *const *ins, void *const *outs,
-                       const int *inverse, const int *branch, int n, int nbranch, void **exec_out,
-                       char *err, size_t errlen);
+                       const int *inverse, const int *counts, const int *branch, int n, int nbranch,
+                       void **exec_out, char *err, size_t errlen);
 int fmmk_batch_launch(void *exec, void *stream);
 void fmmk_batch_free(void *exec);
 int fmmk_execute_noalloc(const fmm_ops64 *ops, int reuse_ops, const void *d_in, void *d_out,

@@ -3299,13 +3299,14 @@ extern "C" int fmmk_execute_graph_n(fmmk_state *st, const void *d_in, void *d_ou
 
 /* ======================================================================== batches */
 
-/* Captures n transforms into one graph: a fork from the capturing stream into nbranch
- * streams, transform i enqueued on branch[i] (all transforms of one plan must share a branch:
+/* Captures n executes into one graph (execute i carries counts[i] transforms of its plan, 1 when
+ * counts is NULL): a fork from the capturing stream into nbranch streams, execute i enqueued on
+ * branch[i] (all transforms of one plan must share a branch:
  * they share its workspace), and a join.  One cudaGraphLaunch then runs the whole batch, the
  * branches overlapping on the device. */
 extern "C" int fmmk_batch_capture(fmmk_state *const *sts, const void *const *ins, void *const *outs,
-                                  const int *inverse, const int *branch, int n, int nbranch,
-                                  void **exec_out, char *err, size_t errlen) {
+                                  const int *inverse, const int *counts, const int *branch, int n,
+                                  int nbranch, void **exec_out, char *err, size_t errlen) {
   cudaStream_t root;
   FMM_CUDA_TRY(cudaStreamCreateWithFlags(&root, cudaStreamNonBlocking));
   cudaStream_t *br = (cudaStream_t *)calloc((size_t)nbranch, sizeof(cudaStream_t));
@@ -3322,7 +3323,8 @@ extern "C" int fmmk_batch_capture(fmmk_state *const *sts, const void *const *ins
     cudaEventRecord(ev[nbranch], root);
     for (int b = 0; b < nbranch; ++b) cudaStreamWaitEvent(br[b], ev[nbranch], 0);
     for (int i = 0; i < n && !rc; ++i)
-      rc = fmmk_execute(sts[i], ins[i], outs[i], br[branch[i]], inverse ? inverse[i] : 0, err, errlen);
+      rc = fmmk_execute_n(sts[i], ins[i], outs[i], br[branch[i]], inverse ? inverse[i] : 0,
+                          counts ? counts[i] : 1, err, errlen);
     for (int b = 0; b < nbranch; ++b) {
       cudaEventRecord(ev[b], br[b]);
       cudaStreamWaitEvent(root, ev[b], 0);

@@ -31,6 +31,7 @@ EXPORTS = ["getwlen2", "getvlen", "mfti", "mft", "fmmfft_last_error", "fmmfft_la
            "fmmfft_execute_many_graph", "fmmfft_plan_bytes", "fmmfft_server_counts",
            "fmmfft_plan_enable_refinement", "fmmfft_execute_refined", "fmmfft_mft_rank_mode",
            "fmmfft_execute_blocks", "fmmfft_execute_blocks_host", "fmmfft_plan_describe",
+           "fmmfft_batch_create_many",
            "fmmfft_execute_graph", "fmmfft_batch_create", "fmmfft_batch_launch",
            "fmmfft_batch_destroy", "fmmfft_server_create", "fmmfft_server_destroy",
            "fmmfft_server_submit", "fmmfft_server_query", "fmmfft_server_wait",
@@ -96,6 +97,8 @@ def load(path=LIB_PATH):
     lib.fmmfft_plan_enable_refinement.restype = _I
     lib.fmmfft_execute_refined.argtypes = [_VP, _VP, _VP, _VP]
     lib.fmmfft_execute_refined.restype = _I
+    lib.fmmfft_batch_create_many.argtypes = [ctypes.POINTER(_VP), _VP, _VP, _VP, _VP, _I, _I]
+    lib.fmmfft_batch_create_many.restype = _I
     lib.fmmfft_plan_describe.argtypes = [_VP, ctypes.c_char_p, ctypes.c_size_t]
     lib.fmmfft_plan_describe.restype = _I
     lib.fmmfft_mft_rank_mode.argtypes = [_I]
@@ -346,14 +349,18 @@ class Batch:
     """Transforms plans[i]: d_in[i] -> d_out[i] (device pointers) as one CUDA graph with
     `nbranch` parallel branches; launch() runs them all."""
 
-    def __init__(self, plans, d_in, d_out, nbranch=8):
+    def __init__(self, plans, d_in, d_out, nbranch=8, counts=None):
         n = len(plans)
         self._plans = list(plans)  # keep the plans alive
         ph = (_VP * n)(*[p._h for p in plans])
         ins = (_VP * n)(*d_in)
         outs = (_VP * n)(*d_out)
         h = _VP()
-        _check(load().fmmfft_batch_create(ctypes.byref(h), ph, ins, outs, n, int(nbranch)))
+        if counts is None:
+            _check(load().fmmfft_batch_create(ctypes.byref(h), ph, ins, outs, n, int(nbranch)))
+        else:  # entry i: counts[i] transforms of batched plan i, contiguous
+            cs = (_I * n)(*[int(c) for c in counts])
+            _check(load().fmmfft_batch_create_many(ctypes.byref(h), ph, cs, ins, outs, n, int(nbranch)))
         self._h = h
 
     def launch(self, stream=0):

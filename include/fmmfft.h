@@ -207,6 +207,11 @@ int fmmfft_execute_graph(fmmfft_plan plan, const void *d_in, void *d_out, void *
 typedef struct fmmfft_batch_s *fmmfft_batch;
 int fmmfft_batch_create(fmmfft_batch *out, const fmmfft_plan *plans, const void *const *d_in,
                         void *const *d_out, int n, int nbranch);
+/* The same with batched plans: entry i runs counts[i] transforms of plans[i] (contiguous, N
+ * apart, from d_in[i] to d_out[i]) in one launch sequence; counts[i] <= the plan's capacity.  An
+ * uneven batch grouped by shape is then one graph of one launch sequence per shape. */
+int fmmfft_batch_create_many(fmmfft_batch *out, const fmmfft_plan *plans, const int *counts,
+                             const void *const *d_in, void *const *d_out, int n, int nbranch);
 int fmmfft_batch_launch(fmmfft_batch batch, void *stream);
 int fmmfft_batch_destroy(fmmfft_batch batch);
 

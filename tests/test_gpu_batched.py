@@ -89,3 +89,44 @@ def test_plan_bytes_matches_plan(fm):
         plan = fm.Plan(*args[:5], max_transforms=args[5])
         assert plan.device_bytes == est, args
         plan.close()
+
+
+def test_uneven_batch_grouped_by_shape_one_graph(fm):
+    """Transforms of uneven sizes grouped by shape: one batched launch sequence per shape, all
+    groups as branches of one graph (fmmfft_batch_create_many); every transform bitwise equal to
+    its own execute, and within 1e-6 of the FP64 FFT."""
+    import torch
+    rng = np.random.Generator(np.random.PCG64(12))
+    jobs = []
+    while len(jobs) < 30:
+        N = 1 << int(rng.integers(12, 18))
+        P = int(rng.choice([8, 16, 32, 64]))
+        if N // P >= 256:
+            jobs.append((N, P, 16, 32))
+    groups = {}
+    for i, j in enumerate(jobs):
+        groups.setdefault(j, []).append(i)
+    shapes = sorted(groups)
+    xs = {i: ol.seeded_input(j[0], 700 + i) for i, j in enumerate(jobs)}
+    plans = [fm.Plan(*sh, "f32_tc", max_transforms=len(groups[sh])) for sh in shapes]
+    xin = [torch.from_numpy(np.concatenate([xs[i] for i in groups[sh]])).to(torch.complex64).cuda()
+           for sh in shapes]
+    yout = [torch.empty_like(x) for x in xin]
+    batch = fm.Batch(plans, [x.data_ptr() for x in xin], [y.data_ptr() for y in yout], nbranch=5,
+                     counts=[len(groups[sh]) for sh in shapes])
+    batch.launch(torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    s = torch.cuda.current_stream().cuda_stream
+    for gi, sh in enumerate(shapes):
+        alone_plan = fm.Plan(*sh, "f32_tc")
+        N = sh[0]
+        for j, i in enumerate(groups[sh]):
+            d = xin[gi][j * N:(j + 1) * N]
+            alone = torch.empty_like(d)
+            alone_plan.execute_ptr(d.data_ptr(), alone.data_ptr(), s)
+            torch.cuda.synchronize()
+            got = yout[gi][j * N:(j + 1) * N]
+            assert torch.equal(alone, got), (sh, j)
+            assert ol.rel_l2(got.cpu().numpy(), np.fft.fft(xs[i])) < 1e-6
+        alone_plan.close()
+    batch.close()
