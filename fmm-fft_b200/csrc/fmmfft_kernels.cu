@@ -65,6 +65,18 @@ template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
   r.y = a.x * b.y + a.y * b.x;
   return r;
 }
+/* a * (h + l) for a twiddle carried as an FP32 pair (h its rounding, l the rounding of the
+ * remainder): the small product a l first, then a h added through fused multiply-adds, so the
+ * twiddle enters with about 2^-48 relative error instead of its 2^-24 rounding ("compensated"
+ * twiddles; the arithmetic's own roundings remain). */
+__device__ __forceinline__ float2 cmul_comp(float2 a, float2 h, float2 l) {
+  const float tx = a.x * l.x - a.y * l.y, ty = a.x * l.y + a.y * l.x;
+  return make_float2(fmaf(a.x, h.x, fmaf(-a.y, h.y, tx)), fmaf(a.x, h.y, fmaf(a.y, h.x, ty)));
+}
+__device__ __forceinline__ double2 cmul_comp(double2 a, double2 h, double2 l) { /* same, in FP64 */
+  const double tx = a.x * l.x - a.y * l.y, ty = a.x * l.y + a.y * l.x;
+  return make_double2(fma(a.x, h.x, fma(-a.y, h.y, tx)), fma(a.x, h.y, fma(a.y, h.x, ty)));
+}
 template <typename C> __device__ __forceinline__ C cadd(C a, C b) {
   a.x += b.x, a.y += b.y;
   return a;
@@ -107,6 +119,9 @@ template <typename R> struct Dev {
   C *pretw;   /* [P]  c_sc = -exp(-i pi sc/P) sin(pi sc/P) */
   C *twP;     /* [P]  exp(-2 pi i k / P) */
   C *twM;     /* [M]  exp(-2 pi i k / M) */
+  /* compensated twiddles (FP32 plans with comp_tw): the FP32 rounding of each entry's remainder */
+  C *pretw_lo, *twP_lo, *twM_lo;
+  int comp_tw;
   /* workspace */
   R *xt;      /* [2P][M] */
   C *part;    /* [ntile][P] */
@@ -1275,6 +1290,7 @@ template <typename R> struct CombineLd {
   long M;
   R invM;
   int P;
+  const typename cplx<R>::T *__restrict__ pretw_lo; /* compensated pre-twiddle (FP32), or null */
   /* row = transform of a batch: its sections, fields and section sums */
   __device__ __forceinline__ void operator()(long row, unsigned m, int t, int q,
                                              typename cplx<R>::T (&v)[8]) const {
@@ -1290,17 +1306,29 @@ template <typename R> struct CombineLd {
         typename cplx<R>::T a;
         a.x = u[(2L * (sc - 1)) * M + m] + S.y * invM;
         a.y = u[(2L * (sc - 1) + 1) * M + m] - S.x * invM;
+        if constexpr (sizeof(R) == 4) {
+          if (pretw_lo) {
+            v[r] = cmul_comp(a, pretw[sc], pretw_lo[sc]);
+            continue;
+          }
+        }
         v[r] = cmul(pretw[sc], a);
       }
     }
   }
 };
 
-template <typename R, bool TIN, bool TOUT, class Ld = StridedLd<R>>
+/* COMP (FP32): compensated twiddles.  twD_lo / twP_lo hold the FP32 rounding of each table
+ * entry's remainder; the stage twiddles are applied with cmul_comp from a second shared table,
+ * and the 4-step post-twiddle of output i of sequence g is read directly as twP[(g i) mod T]
+ * (hi and lo; single-level tables, twbits = 0) instead of as a product of two rounded factors.
+ * Shared memory: L + L/16 + 1 more elements. */
+template <typename R, bool TIN, bool TOUT, class Ld = StridedLd<R>, bool COMP = false>
 __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
     k_fft_reg(const Ld ld, typename cplx<R>::T *__restrict__ out,
               const typename cplx<R>::T *__restrict__ twD, const typename cplx<R>::T *__restrict__ twP,
-              FftPass fp) {
+              FftPass fp, const typename cplx<R>::T *__restrict__ twD_lo = nullptr,
+              const typename cplx<R>::T *__restrict__ twP_lo = nullptr) {
   using C = typename cplx<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int L = fp.L, W = fp.W, q = L >> 3;
@@ -1309,6 +1337,7 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
   C *buf = reinterpret_cast<C *>(smem_raw);
   C *twl = buf + W * LP;    /* exp(-2 pi i m / L) at m + m/16 */
   C *twq = twl + L + L / 16 + 1; /* 4-step twiddle steps exp(-2 pi i g q r / M), [w][r] */
+  C *twl_lo = twq + 8 * W;       /* COMP: the remainders of twl */
   const int tid = threadIdx.x;
   const unsigned g0 = blockIdx.x * (unsigned)W;
   /* post-twiddle exp(-2 pi i e / T) for e = g * i */
@@ -1319,9 +1348,20 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
     return cmul(twP[lo + 1 + (e >> fp.twbits)], twP[e & lo]);
   };
   for (int m = tid; m < L; m += blockDim.x) twl[m + (m >> 4)] = twD[(long)m * fp.tws];
-  if (fp.twiddle_post)
+  if constexpr (COMP)
+    for (int m = tid; m < L; m += blockDim.x) twl_lo[m + (m >> 4)] = twD_lo[(long)m * fp.tws];
+  if (fp.twiddle_post && !COMP)
     for (int m = tid; m < 8 * W; m += blockDim.x)
       twq[m] = post((g0 + (m >> 3)) * (unsigned)q * (unsigned)(m & 7));
+  /* COMP: x times exp(-2 pi i e / T), e = g i twmul mod T, from the hi / lo tables */
+  auto post_comp = [&](C x, unsigned gi) -> C {
+    if constexpr (COMP) {
+      const unsigned e = (gi * fp.twmul) & fp.twmask;
+      return cmul_comp(x, twP[e], twP_lo[e]);
+    } else {
+      return x;
+    }
+  };
   int t, w;
   if (TIN) t = tid & (q - 1), w = tid >> lq;
   else w = tid & (W - 1), t = tid >> lW;
@@ -1371,7 +1411,10 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
 #pragma unroll
     for (int r = 1; r < 8; ++r) {
       const int m = r * ts;
-      v[r] = cmul(v[r], twl[m + (m >> 4)]);
+      if constexpr (COMP)
+        v[r] = cmul_comp(v[r], twl[m + (m >> 4)], twl_lo[m + (m >> 4)]);
+      else
+        v[r] = cmul(v[r], twl[m + (m >> 4)]);
     }
     dft8(v);
     if (lNs + 3 == lg) break; /* v[r] = output t + r q */
@@ -1390,11 +1433,16 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
     C *op = dp + g * fp.oseq + t * ostr;
     const unsigned qs = (unsigned)q * ostr;
     C a;
-    if (fp.twiddle_post) a = post(g * (unsigned)t);
+    if (fp.twiddle_post && !COMP) a = post(g * (unsigned)t);
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
       C x = v[r];
-      if (fp.twiddle_post) x = cmul(x, cmul(a, twq[w * 8 + r]));
+      if (fp.twiddle_post) {
+        if constexpr (COMP)
+          x = post_comp(x, g * (unsigned)(t + r * q));
+        else
+          x = cmul(x, cmul(a, twq[w * 8 + r]));
+      }
       if (fp.conj_out) x.y = -x.y;
       op[r * qs] = x;
     }
@@ -1414,12 +1462,17 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
     C *op = dp + g * fp.oseq + t2 * ostr;
     const unsigned qs = (unsigned)q * ostr;
     C a;
-    if (fp.twiddle_post) a = post(g * (unsigned)t2);
+    if (fp.twiddle_post && !COMP) a = post(g * (unsigned)t2);
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
       const int i = t2 + r * q;
       C x = b2[i + (i >> 3)];
-      if (fp.twiddle_post) x = cmul(x, cmul(a, twq[w2 * 8 + r]));
+      if (fp.twiddle_post) {
+        if constexpr (COMP)
+          x = post_comp(x, g * (unsigned)i);
+        else
+          x = cmul(x, cmul(a, twq[w2 * 8 + r]));
+      }
       if (fp.conj_out) x.y = -x.y;
       op[r * qs] = x;
     }
@@ -1431,7 +1484,8 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
 template <typename R>
 static void launch_fft_pass(const typename cplx<R>::T *in, typename cplx<R>::T *out,
                             const typename cplx<R>::T *twM, FftPass fp, long per, long rows,
-                            int W_old, int reg_threads, cudaStream_t st) {
+                            int W_old, int reg_threads, cudaStream_t st,
+                            const typename cplx<R>::T *twM_lo = nullptr) {
   using C = typename cplx<R>::T;
   const int L = fp.L;
   const bool tin = fp.istr == 1, tout = fp.ostr == 1;
@@ -1446,6 +1500,21 @@ static void launch_fft_pass(const typename cplx<R>::T *in, typename cplx<R>::T *
       const int thr = W * (L / 8);
       const size_t sm = sizeof(C) * ((size_t)W * fft_lp(L, W) + L + L / 16 + 1 + 8 * W);
       dim3 g((unsigned)(per / W), (unsigned)rows);
+      if constexpr (sizeof(R) == 4) {
+        if (twM_lo) { /* compensated twiddles */
+          const size_t smc = sm + sizeof(C) * (size_t)(L + L / 16 + 1);
+          if (tin && tout)
+            k_fft_reg<R, true, true, StridedLd<R>, true><<<g, thr, smc, st>>>(sld, out, twM, twM, fmm_pass(fp),
+                                                                              twM_lo, twM_lo);
+          else if (tin)
+            k_fft_reg<R, true, false, StridedLd<R>, true><<<g, thr, smc, st>>>(sld, out, twM, twM, fmm_pass(fp),
+                                                                               twM_lo, twM_lo);
+          else
+            k_fft_reg<R, false, false, StridedLd<R>, true><<<g, thr, smc, st>>>(sld, out, twM, twM, fmm_pass(fp),
+                                                                                twM_lo, twM_lo);
+          return;
+        }
+      }
       if (tin && tout)
         k_fft_reg<R, true, true><<<g, thr, sm, st>>>(sld, out, twM, twM, fmm_pass(fp));
       else if (tin)
@@ -1777,6 +1846,20 @@ template <typename R> static int upload(R **dst, const double *src, size_t n, ch
 }
 
 static inline size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
+
+/* The FP32 remainders of FP64 values, v - (float)v rounded to FP32, into dst (device). */
+template <typename P_> static int upload_lo(P_ *dst, const double *src, size_t n, char *err, size_t errlen) {
+  float *h = (float *)malloc(sizeof(float) * (n ? n : 1));
+  if (!h) return 2;
+  for (size_t i = 0; i < n; ++i) h[i] = (float)(src[i] - (double)(float)src[i]);
+  cudaError_t e = cudaMemcpy(dst, h, sizeof(float) * n, cudaMemcpyHostToDevice);
+  free(h);
+  if (e != cudaSuccess) {
+    snprintf(err, errlen, "cudaMemcpy: %s", cudaGetErrorString(e));
+    return 3;
+  }
+  return 0;
+}
 static inline long pow2_floor(long v) {
   long p = 1;
   while (p * 2 <= v) p *= 2;
@@ -2013,6 +2096,10 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
   /* FMMFFT_FUSE_S2M=0 keeps S2M a separate stage (on the tensor cores for FP32 TC plans) */
   d->fuse_s2m = 1;
   if (const char *ev = getenv("FMMFFT_FUSE_S2M")) d->fuse_s2m = atoi(ev) != 0, d->env_set |= KNOB_FUSE;
+  /* compensated twiddles in the FP32 FFT passes of the mixed-precision plans (tensor-core stages);
+   * the plain FP32 plan keeps single FP32 twiddles.  FMMFFT_COMP_TWIDDLES=0/1 overrides. */
+  d->comp_tw = sizeof(R) == 4 && tc;
+  if (const char *ev = getenv("FMMFFT_COMP_TWIDDLES")) d->comp_tw = sizeof(R) == 4 && atoi(ev) != 0;
   d->fft_threads = 512;
   if (const char *ev = getenv("FMMFFT_FFT_THREADS")) {
     const int v = atoi(ev);
@@ -2054,6 +2141,9 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
   CARVE(pretw, P, C)
   CARVE(twP, P, C)
   CARVE(twM, M, C)
+  CARVE(pretwlo, d->comp_tw ? P : 0, C)
+  CARVE(twPlo, d->comp_tw ? P : 0, C)
+  CARVE(twMlo, d->comp_tw ? M : 0, C)
   CARVE(xt, nb * 2 * P * M, R)
   CARVE(part, nb * d->ntile * P, C)
   CARVE(ssum, nb * P, C)
@@ -2099,6 +2189,9 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
   d->pretw = (C *)(base + off_pretw);
   d->twP = (C *)(base + off_twP);
   d->twM = (C *)(base + off_twM);
+  d->pretw_lo = (C *)(base + off_pretwlo);
+  d->twP_lo = (C *)(base + off_twPlo);
+  d->twM_lo = (C *)(base + off_twMlo);
   d->xt = (R *)(base + off_xt);
   d->part = (C *)(base + off_part);
   d->ssum = (C *)(base + off_ssum);
@@ -2182,8 +2275,10 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
     h[2 * sc + 1] = sin(PI * sc / P) * sin(PI * sc / P);
   }
   rc |= upload<R>((R **)&d->pretw, h, 2 * P, err, errlen);
+  if (d->comp_tw) rc |= upload_lo(d->pretw_lo, h, 2 * P, err, errlen);
   for (long k = 0; k < P; ++k) h[2 * k] = cos(2 * PI * k / P), h[2 * k + 1] = -sin(2 * PI * k / P);
   rc |= upload<R>((R **)&d->twP, h, 2 * P, err, errlen);
+  if (d->comp_tw) rc |= upload_lo(d->twP_lo, h, 2 * P, err, errlen);
   free(h);
   double *hm = (double *)malloc(sizeof(double) * 2 * (size_t)M);
   if (!hm) return 2;
@@ -2192,6 +2287,7 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
     hm[2 * k] = cos(a), hm[2 * k + 1] = -sin(a);
   }
   rc |= upload<R>((R **)&d->twM, hm, 2 * M, err, errlen);
+  if (d->comp_tw) rc |= upload_lo(d->twM_lo, hm, 2 * M, err, errlen);
   free(hm);
   if (tc && !rc) rc = tc_upload_ops(d, o, err, errlen);
   if (rc) {
@@ -2430,11 +2526,17 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
     fp.L = (int)P, fp.W = Wc, fp.per = (int)(M < (1L << 30) ? M : (1L << 30)), fp.M = M;
     fp.irow = 0, fp.orow = P * M, fp.oseq = 1, fp.ostr = M, fp.tws = 1; /* row = transform */
     fp.twiddle_post = 0, fp.conj_out = 0, fp.twmul = 1, fp.twmask = 0, fp.twbits = 0;
-    const CombineLd<R> cl{d->xt, d->u, d->ssum, d->pretw, M, R(1) / R(M), (int)P};
+    const CombineLd<R> cl{d->xt, d->u, d->ssum, d->pretw, M, R(1) / R(M), (int)P,
+                          d->comp_tw ? d->pretw_lo : nullptr};
     const int thr = Wc * (int)(P / 8);
     const size_t sm = sizeof(C) * ((size_t)Wc * fft_lp((int)P, Wc) + P + P / 16 + 1 + 8 * (size_t)Wc);
-    k_fft_reg<R, false, false, CombineLd<R>><<<dim3((unsigned)(M / Wc), (unsigned)nbt), thr, sm, st>>>(
-        cl, d->z, d->twP, d->twP, fp);
+    if (d->comp_tw && sizeof(R) == 4)
+      k_fft_reg<R, false, false, CombineLd<R>, true>
+          <<<dim3((unsigned)(M / Wc), (unsigned)nbt), thr, sm + sizeof(C) * (size_t)(P + P / 16 + 1), st>>>(
+              cl, d->z, d->twP, d->twP, fp, d->twP_lo, d->twP_lo);
+    else
+      k_fft_reg<R, false, false, CombineLd<R>><<<dim3((unsigned)(M / Wc), (unsigned)nbt), thr, sm, st>>>(
+          cl, d->z, d->twP, d->twP, fp);
   } else {
     int TMc = (int)(P >= 1024 ? 1 : (1024 / P < 32 ? 1024 / P : 32));
     if (TMc > M) TMc = (int)M;
@@ -2457,9 +2559,11 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         if (Wr > P) Wr = (int)P;
         if (Wr < 1) Wr = 1;
         fp.M = M * Wr;
-        launch_fft_pass<R>(d->z, y, d->twM, fp, Wr, nbt * P / Wr, W, d->fft_threads, st);
+        launch_fft_pass<R>(d->z, y, d->twM, fp, Wr, nbt * P / Wr, W, d->fft_threads, st,
+                           d->comp_tw ? d->twM_lo : nullptr);
       } else {
-        launch_fft_pass<R>(d->z, y, d->twM, fp, W, nbt * P / W, W, d->fft_threads, st);
+        launch_fft_pass<R>(d->z, y, d->twM, fp, W, nbt * P / W, W, d->fft_threads, st,
+                           d->comp_tw ? d->twM_lo : nullptr);
       }
       pf.launches[ST_FFT1]++;
     } else {
@@ -2469,7 +2573,8 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
       if (W1 > 16) W1 = 16;
       if (W1 > M1) W1 = (int)M1;
       FftPass f1{(int)M2, W1, (int)M1, M, 1, M1, 1, M1, 1, M / M2, 0};
-      launch_fft_pass<R>(d->z, d->tmp, d->twM, f1, M1, nbt * P, W1, d->fft_threads, st);
+      launch_fft_pass<R>(d->z, d->tmp, d->twM, f1, M1, nbt * P, W1, d->fft_threads, st,
+                         d->comp_tw ? d->twM_lo : nullptr);
       pf.launches[ST_FFT1]++;
       stage(ST_FFT2);
       /* pass 2: for each k2, DFT over m1 (contiguous), store y[k2 + M2*k1] */
@@ -2477,7 +2582,8 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
       if (W2 > 16) W2 = 16;
       if (W2 > M2) W2 = (int)M2;
       FftPass f2{(int)M1, W2, (int)M2, M, M1, 1, 1, M2, 0, M / M1, inverse};
-      launch_fft_pass<R>(d->tmp, y, d->twM, f2, M2, nbt * P, W2, d->fft_threads, st);
+      launch_fft_pass<R>(d->tmp, y, d->twM, f2, M2, nbt * P, W2, d->fft_threads, st,
+                         d->comp_tw ? d->twM_lo : nullptr);
       pf.launches[ST_FFT2]++;
     }
   }
@@ -2628,6 +2734,10 @@ static int set_smem_limits(void) {
   cudaFuncSetAttribute(k_fft_reg<float, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_fft_reg<float, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_fft_reg<float, false, false, CombineLd<float>>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<float, false, false, CombineLd<float>, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<float, true, true, StridedLd<float>, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<float, true, false, StridedLd<float>, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<float, false, false, StridedLd<float>, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_fft_reg<double, false, false, CombineLd<double>>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_fft_reg<double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_fft_reg<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);

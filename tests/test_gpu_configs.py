@@ -145,3 +145,23 @@ def test_bf16x3_tensor_core_stages(fm, monkeypatch, accuracy_report, N, P, T, b)
     accuracy_report(f"N={N} P={P} T={T} b={b} bf16x3 every stage on the tensor cores: u rel-L2 {eu:.3e}, "
                     f"y vs oracle rel-L2 {e:.3e} max {max_err(y, o['y']):.3e}")
     assert e < 1e-4
+
+
+@pytest.mark.parametrize("N,P,T,b", [(1 << 20, 64, 24, 32), (1 << 22, 16, 20, 32), (1 << 18, 256, 16, 16)])
+def test_compensated_twiddles(fm, monkeypatch, accuracy_report, N, P, T, b):
+    """The FP32 FFT passes (the combine's length-P DFT and the size-M FFTs) with twiddles carried
+    as FP32 hi + lo pairs (the tensor-core plans' default) against single FP32 twiddles: both
+    within 1e-6 of the FP64 FFT; the errors of both are reported."""
+    x = ol.seeded_input(N, 19 + N % 13)
+    ref = np.fft.fft(x.astype(np.complex64).astype(np.complex128))
+    errs = {}
+    for comp in ("1", "0"):
+        monkeypatch.setenv("FMMFFT_COMP_TWIDDLES", comp)
+        plan = fm.Plan(N, P, T, b, "f32_tc")
+        y = run_device(plan, x)
+        plan.check()
+        plan.close()
+        errs[comp] = (ol.rel_l2(y, ref), max_err(y, ref))
+    accuracy_report(f"N={N} P={P} T={T} b={b} f32_tc: compensated twiddles rel-L2 {errs['1'][0]:.3e} "
+                    f"max {errs['1'][1]:.3e}; single FP32 twiddles rel-L2 {errs['0'][0]:.3e} max {errs['0'][1]:.3e}")
+    assert errs["1"][0] < TOL and errs["0"][0] < TOL
