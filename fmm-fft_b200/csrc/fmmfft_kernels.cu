@@ -2096,9 +2096,11 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
   /* FMMFFT_FUSE_S2M=0 keeps S2M a separate stage (on the tensor cores for FP32 TC plans) */
   d->fuse_s2m = 1;
   if (const char *ev = getenv("FMMFFT_FUSE_S2M")) d->fuse_s2m = atoi(ev) != 0, d->env_set |= KNOB_FUSE;
-  /* compensated twiddles in the FP32 FFT passes of the mixed-precision plans (tensor-core stages);
-   * the plain FP32 plan keeps single FP32 twiddles.  FMMFFT_COMP_TWIDDLES=0/1 overrides. */
-  d->comp_tw = sizeof(R) == 4 && tc;
+  /* compensated twiddles in the FP32 FFT passes: off by default.  Measured on a B200 (N = 2^20
+   * .. 2^22, split-TF32 plans): rel-L2 5.2e-7 against 5.6e-7, for FFT pass 1 taking 0.19 ms
+   * instead of 0.09 ms at N = 2^24 (the post-twiddle is then gathered per element).
+   * FMMFFT_COMP_TWIDDLES=1 turns them on. */
+  d->comp_tw = 0;
   if (const char *ev = getenv("FMMFFT_COMP_TWIDDLES")) d->comp_tw = sizeof(R) == 4 && atoi(ev) != 0;
   d->fft_threads = 512;
   if (const char *ev = getenv("FMMFFT_FFT_THREADS")) {
@@ -2607,15 +2609,16 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
 /* The plan's stage choices that do not change what is computed, only which kernels compute it
  * and how: FFT block size, coarse-tree threshold (the one-launch coarse levels), the row count
  * from which tree stages run on the tensor cores, and S2M fused into the sections pass.  On the
- * first plan of each (N, P, terms, b, precision, capacity) in a process the autotuner times the
- * candidates (coordinate descent: each knob over its values with the others at their best so
- * far; each candidate the fastest of 5 executes after 2 warm-ups, in place on the plan's own
- * workspace) and caches the winner; every later plan of that key takes the cached choice, so
+ * first plan of each (N, P, terms, b, precision) in a process the autotuner times the
+ * candidates on one transform (coordinate descent: each knob over its values with the others at
+ * their best so far; each candidate the fastest of 5 executes after 2 warm-ups, in place on the
+ * plan's own workspace) and caches the winner; every later plan of that key, batched or not,
+ * takes the cached choice, so
  * transforms of one shape give the same bits alone, in a batch or in a server mix.  Knobs an
  * environment switch fixed are not tuned.  FP64 plans keep the defaults. */
-struct TuneKey {
+struct TuneKey { /* the capacity is not part of it: a batch must take its transforms' choice */
   long N, P, T, b;
-  int prec, nb;
+  int prec;
 };
 struct TuneVal {
   int fft_threads, fuse_s2m;
@@ -2637,7 +2640,9 @@ template <typename R> static void tune_apply(Dev<R> *d, const TuneVal &v) {
 template <typename R>
 static int dev_autotune(Dev<R> *d, char *err, size_t errlen) {
   using C = typename cplx<R>::T;
-  const TuneKey key{d->N, d->P, d->T, d->b, d->precision, d->nbmax};
+  TuneKey key;
+  memset(&key, 0, sizeof key);
+  key.N = d->N, key.P = d->P, key.T = d->T, key.b = d->b, key.prec = d->precision;
   {
     std::lock_guard<std::mutex> g(g_tune_mu);
     for (int i = 0; i < g_ntune; ++i)
@@ -2650,7 +2655,7 @@ static int dev_autotune(Dev<R> *d, char *err, size_t errlen) {
   FMM_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0), cudaEventCreate(&e1);
-  const int nbt = d->nbmax;
+  const int nbt = 1; /* one transform: the choice is per transform, whatever the capacity */
   FMM_CUDA_TRY(cudaMemsetAsync(d->z, 0, sizeof(C) * (size_t)d->N * nbt, st));
   int rc = 0;
   auto measure = [&]() -> float {

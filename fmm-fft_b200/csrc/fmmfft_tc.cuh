@@ -1352,15 +1352,16 @@ __global__ void __launch_bounds__(kMThreads, 1)
  * finish on the same tile.  One CTA per SM (all of its tensor memory), persistent over 128-row
  * tiles, K taken in slots of 32 columns:
  *
- *   warps 0-7   producers.  Global -> shared: the 128 x 32 floats of a slot are copied with
- *               16-byte cp.async into a ring of kWStages shared-memory stages, consecutive threads
- *               on consecutive 16 bytes of a row (coalesced), kWStages - 1 slots in flight.
- *               Shared -> TMEM: warp w (lane quarter q = w % 4, column half h = w / 4) reads row
- *               32 q + lane, columns 16 h .. 16 h + 15 of the slot, splits them into TF32 hi / lo
- *               and writes both into one of kWSlots A slots in tensor memory (tcgen05.st), then
- *               arrives on the slot's `full` barrier.  Row chunks are stored XOR-swizzled in
- *               shared memory (16-byte unit j of row i at position j ^ (i & 7)), so both the
- *               copies and the row reads take four wavefronts per warp instruction.
+ *   warps 0-7   producers, each on its own: warp w (lane quarter q = w % 4, column half
+ *               h = w / 4) owns rows 32 q .. 32 q + 31 and columns 16 h .. 16 h + 15 of every
+ *               slot.  Global -> shared: it copies that block with 16-byte cp.async (8 rows x 64
+ *               bytes per instruction) into a ring of kWStages shared-memory stages, kWStages - 1
+ *               slots in flight.  Shared -> TMEM: lane i reads its row 32 q + i, splits it into
+ *               hi / lo and writes both into one of kWSlots A slots in tensor memory
+ *               (tcgen05.st), then the warp arrives on the slot's `full` barrier.  A warp reads
+ *               only what it copied, so warps wait for nothing but their own copies.  Units are
+ *               stored XOR-swizzled in shared memory (16-byte unit j of row i at position
+ *               j ^ (i & 7)): copies and row reads take four wavefronts per warp instruction.
  *   warp 16     one thread issues, per K step of 8, A_hi x [B_hi; B_lo] (N = 2 npad) and
  *               A_lo x B_hi (N = npad) into one of two TMEM accumulators: split TF32 with three
  *               products (the A_lo B_lo term, 2^-22 relative, is left out), FP32 accumulation;
@@ -1529,7 +1530,10 @@ __global__ void __launch_bounds__(kWThreads, 1) k_tc_ws(const __grid_constant__ 
     const int q = warp & 3, h = warp >> 2;
     const int my_row = q * 32 + lane;                 /* TMEM lane = tile row this thread splits */
     const uint32_t lane_addr = (uint32_t)(q * 32) << 16;
-    const int cu = tid & 7, crow = tid >> 3;          /* copy unit: 16 bytes cu of rows crow + 32 m */
+    /* this warp copies exactly what it splits: its 32 rows, 16-byte units 4 h .. 4 h + 3 of each;
+     * lane: unit 4 h + lane % 4 of rows 32 q + 8 m + lane / 4 (8 rows x 64 bytes per copy
+     * instruction), so a warp needs no other warp's copies and no CTA-wide barrier */
+    const int cu = 4 * h + (lane & 3), crow = q * 32 + (lane >> 2);
     const uint32_t ring0 = smem_addr(ring);
     const long G = (long)my_tiles * nsl;
     /* copies of global slot g (tile index g / nsl of this CTA, slot g % nsl) into its stage */
@@ -1543,7 +1547,7 @@ __global__ void __launch_bounds__(kWThreads, 1) k_tc_ws(const __grid_constant__ 
           const uint32_t st = ring0 + (uint32_t)((g % kWStages) * kWStageBytes);
 #pragma unroll
           for (int m = 0; m < 4; ++m) {
-            const int row = crow + 32 * m;
+            const int row = crow + 8 * m;
             const long r = r0 + row;
             if (r < pb.rows)
               cp_async16_cg(st + (uint32_t)(row * 128 + ((cu ^ (row & 7)) << 4)), pb.src(c, r, batch) + (e >> 8));
@@ -1556,9 +1560,10 @@ __global__ void __launch_bounds__(kWThreads, 1) k_tc_ws(const __grid_constant__ 
     for (int g = 0; g < kWStages - 1; ++g) issue(g);
     for (long g = 0; g < G; ++g) {
       cp_async_wait<kWStages - 2>(); /* this thread's copies of slot g have landed */
-      /* every producer's copies of slot g have landed, and every producer has read slot g - 1,
-       * whose stage the next copies reuse; all leave together on an abort */
-      if (named_bar_or(1, kWProd * 32, abort_flag != 0)) break;
+      /* the warp's copies of slot g have landed and its lanes have read slot g - 1, whose stage
+       * the next copies reuse; the warp leaves as one on an abort */
+      __syncwarp();
+      if (__any_sync(0xffffffffu, abort_flag != 0)) break;
       issue(g + kWStages - 1);
       const int j = (int)(g % nsl);
       const uint32_t st = ring0 + (uint32_t)((g % kWStages) * kWStageBytes) + (uint32_t)(my_row * 128);
@@ -1592,7 +1597,7 @@ __global__ void __launch_bounds__(kWThreads, 1) k_tc_ws(const __grid_constant__ 
       bool ok = true;
       if (lane == 0) ok = t_wait(&tempty[s], (uint32_t)(((g / kWSlots) & 1) ^ 1), &abort_flag, status);
       ok = __shfl_sync(0xffffffffu, ok, 0);
-      if (!ok) continue; /* the next barrier sees the abort */
+      if (!ok) continue; /* the next iteration sees the abort */
       fence_after_sync();
       if constexpr (kBF) { /* 16 values = 8 columns per half; lo 16 columns after hi */
         const uint32_t ahi = tmem + lane_addr + (uint32_t)(2 * acc_cols + s * 2 * kWKs + 8 * h);

@@ -108,8 +108,8 @@ typedef struct fmmfft_plan_s *fmmfft_plan;
  * plan-owned. */
 int fmmfft_plan_create(fmmfft_plan *out, long N, long P, long terms, long b, int precision);
 int fmmfft_plan_destroy(fmmfft_plan plan);
-/* complex64 plans are autotuned when the first plan of their (N, P, terms, b, precision,
- * capacity) is made in a process: FFT block size, coarse-tree threshold, tensor-core row
+/* complex64 plans are autotuned when the first plan of their (N, P, terms, b, precision) is
+ * made in a process: FFT block size, coarse-tree threshold, tensor-core row
  * threshold and the fused S2M are timed and the fastest kept; later plans of that key take the
  * same choice (so they compute the same bits).  FMMFFT_AUTOTUNE=0 keeps the defaults; a knob
  * set by its environment switch is not tuned.  fmmfft_plan_describe writes the plan's choices
