@@ -211,8 +211,8 @@ int fmmfft_plan_check(fmmfft_plan plan) {
 }
 
 int fmmfft_plan_selftest_wait(fmmfft_plan plan, int which, long limit_us) {
-  if (!plan || (which != 0 && which != 1) || limit_us < 1 || limit_us > 2000000)
-    return set_err(FMMFFT_ERR_INVALID, "plan_selftest_wait: which must be 0 or 1, limit 1..2e6 us");
+  if (!plan || which != 0 || limit_us < 1 || limit_us > 2000000)
+    return set_err(FMMFFT_ERR_INVALID, "plan_selftest_wait: which must be 0, limit 1..2e6 us");
   char err[256] = {0};
   int rc = fmmk_selftest_wait(plan->dev, which, limit_us, err, sizeof err);
   return rc ? set_err(rc, err) : FMMFFT_OK;

@@ -12,8 +12,8 @@
  *   4  M2M             row contraction per level: phi_L = [phi_L+1 pair] . [S_L;S_R]  (:476-515)
  *   5  top flip        psi_2[c] = topflp . phi_2[c+2]                    (:620-639)
  *   6  M2L + L2L       row contraction per level over parent boxes, both children at once
- *                      (:643-749); the tree levels of stages 4-6 with fewer than 4096 rows run
- *                      in one cooperative launch, k_coarse (plans of N >= 2^23)
+ *                      (:643-749); the tree levels of stages 4-6 with fewer than 4096 rows (at
+ *                      most 64 boxes per plane) run in one launch, k_coarse, a block per plane
  *   7  leaf            row contraction per section: u = [psi_n | x window] . [E_sc ; cot
  *                      Toeplitz] with the half-shifted first point as one more operator column
  *                      (tensor cores) + k_leaf_mid for section P/2; k_leaf (direct, CUDA cores)
@@ -160,7 +160,7 @@ template <typename R> struct Dev {
   int pdl;     /* row-form launches as programmatic dependent launches (FMMFFT_PDL=0: off) */
   unsigned *sync;   /* grid barrier of the coarse-tree kernel: [0] arrivals, [32] generation */
   long coarse_rows; /* levels with fewer rows go to the coarse-tree kernel (0: none) */
-  int coarse_grid;  /* its cooperative grid (blocks of 256) */
+  int coarse_grid;  /* blocks of the coarse-tree kernel an SM holds (0: its operators do not fit) */
   int fuse_s2m;     /* S2M inside the sections pass where tiles hold whole boxes */
   unsigned env_set; /* knobs an environment switch fixed (the autotuner leaves them): bits below */
   int tuned;        /* the knobs come from the autotuner */
@@ -1609,63 +1609,25 @@ __global__ void k_block_dc(const typename cplx<R>::T *__restrict__ ssum,
 
 /* ======================================================================== coarse tree */
 
-/* The coarse levels of the tree (few boxes: every level whose row count is below a threshold)
- * in one cooperative launch instead of one launch per level: the upward M2M for parent levels
- * Lm .. 2, the top flip, and the downward M2L + L2L for child levels 3 .. Ll, with a grid-wide
- * barrier between levels.  Same operators, layouts and outputs (every level's phi / psi) as the
- * per-level launches (reference fmmfft.c:476-515 upward, :620-749 top and downward).  Each
- * level's operator is first staged in shared memory by the whole block; then one warp per
+/* The coarse levels of the tree (few boxes: every level whose row count per transform is below
+ * a threshold, at most 64 boxes per plane) in one launch instead of one launch per level: the
+ * upward M2M for parent levels Lm .. 2, the top flip, and the downward M2L + L2L for child levels
+ * 3 .. Ll.  Every expansion plane (section, re/im, transform) is independent of the others at
+ * every level (its neighbours wrap within the plane), so one block takes one plane through all
+ * of these levels, with block barriers between levels and no grid-wide synchronisation.  Same
+ * operators, layouts and outputs (every level's phi / psi) as the per-level launches (reference
+ * fmmfft.c:476-515 upward, :620-749 top and downward).  Each level's operator is staged in shared
+ * memory by the whole block (its copy issued while the level before it runs); then one warp per
  * output row, lane = output column (N / 32 columns per lane), the row's A values broadcast from
  * the lanes that loaded them; the K sum accumulates per 32-column block, then into the total
  * (two-level FP32 accumulation, as in the row kernels). */
 template <typename R> struct CoarseArgs {
   R *phi, *psi;
   const R *bm2m, *btop, *bm2l;
-  long S1;
+  long S1; /* planes / 2, all transforms of the execute */
   int T, Lm, Ll; /* coarse M2M parent levels Lm..2 (none when Lm < 2); M2L child levels 3..Ll */
-  unsigned *sync; /* [0] arrivals, [32] generation: separate 128-byte lines; [0] zeroed first */
-  int *status;
 };
-
-constexpr unsigned long long kGridWaitNs = 1000000000ull; /* 1 s per barrier */
-
-/* Grid-wide barrier of a cooperative launch; false when a block waited limit_ns (1 s by
- * default; status set). */
-__device__ __forceinline__ bool grid_barrier(unsigned *sync, int *status,
-                                             unsigned long long limit_ns = kGridWaitNs) {
-  __shared__ int gb_fail;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    gb_fail = 0;
-    volatile unsigned *gen = sync + 32;
-    const unsigned g = *gen;
-    __threadfence();
-    if (atomicAdd(sync, 1u) == gridDim.x - 1) {
-      atomicExch(sync, 0u);
-      __threadfence();
-      atomicAdd(sync + 32, 1u);
-    } else {
-      unsigned long long t0 = 0;
-      for (unsigned it = 0; *gen == g; ++it) {
-        __nanosleep(32);
-        if ((it & 255) == 255) {
-          unsigned long long now;
-          asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
-          if (t0 == 0) {
-            t0 = now;
-          } else if (now - t0 > limit_ns) {
-            atomicExch(status, 1);
-            gb_fail = 1;
-            break;
-          }
-        }
-      }
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return gb_fail == 0;
-}
+constexpr int kCoarseMaxLevel = 6; /* coarse M2M parents hold at most 2^6 boxes per plane */
 
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
@@ -1693,17 +1655,18 @@ __device__ __forceinline__ void coarse_stage_b(int K, int N, const R *__restrict
   asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
-/* out[r][n] = sum_k A(r, k) Bs[k][n] for the rows of one level; B (K x N) is in flight into the
- * shared array Bs (coarse_stage_b), and each block stages 8 rows of A at a time into As (one row
- * per warp), so a row costs one round of loads; arow(r, k) is the address of element k of row
- * r's A. */
+/* out[r][n] = sum_k A(r, k) Bs[k][n] for the rows of one level of one plane, all by this block;
+ * B (K x N) is in flight into the shared array Bs (coarse_stage_b), and the block stages 8 rows
+ * of A at a time into As (one row per warp), so a row costs one round of loads; arow(r, k) is
+ * the address of element k of row r's A.  Ends on a block barrier after the last stores, so the
+ * next level reads this one's output. */
 template <typename R, class Arow>
 __device__ __forceinline__ void coarse_rows(long rows, int K, int N, R *__restrict__ Bs, R *__restrict__ As,
                                             R *__restrict__ out, Arow arow) {
   cp_async_wait0(); /* this thread's copies of the operator */
   __syncthreads();  /* everyone's copies; the previous level's reads of As are done */
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (long r0 = (long)blockIdx.x * 8; r0 < rows; r0 += (long)gridDim.x * 8) { /* block-uniform */
+  for (long r0 = 0; r0 < rows; r0 += 8) { /* block-uniform */
     for (int e0 = threadIdx.x; e0 < 8 * K; e0 += 4 * blockDim.x) { /* 4 loads in flight */
       R v[4];
 #pragma unroll
@@ -1747,12 +1710,14 @@ __device__ __forceinline__ void coarse_rows(long rows, int K, int N, R *__restri
  * of the widest A (5T). */
 template <typename R> static size_t coarse_smem(long T) { return sizeof(R) * (10 * (size_t)T * T + 40 * (size_t)T); }
 
-template <typename R> __global__ void __launch_bounds__(256, 1) k_coarse(CoarseArgs<R> a) {
+template <typename R> __global__ void __launch_bounds__(256) k_coarse(CoarseArgs<R> a) {
   extern __shared__ __align__(16) unsigned char coarse_raw[];
   R *Bs = reinterpret_cast<R *>(coarse_raw);
   R *As = Bs + 10L * a.T * a.T;
-  const long S1 = a.S1;
+  const long S1 = a.S1, pl = blockIdx.x;
   const int T = a.T;
+  /* level l of this block's plane: 2^l boxes of T values */
+  auto lv = [&](R *base, int l) { return base + lvl_off(l, S1, T) + pl * (1L << l) * T; };
   auto m2m_b = [&](int L) { return a.bm2m + (long)(L - 2) * 2 * T * T; };
   auto m2l_b = [&](int l) { return a.bm2l + (long)(l - 3) * 10 * T * T; };
   if (a.Lm >= 2)
@@ -1760,57 +1725,41 @@ template <typename R> __global__ void __launch_bounds__(256, 1) k_coarse(CoarseA
   else
     coarse_stage_b<R>(T, T, a.btop, Bs);
   for (int L = a.Lm; L >= 2; --L) { /* M2M: parent L from child pairs of L+1 */
-    const R *child = a.phi + lvl_off(L + 1, S1, T);
-    coarse_rows<R>(2 * S1 * (1L << L), 2 * T, T, Bs, As, a.phi + lvl_off(L, S1, T),
-                   [=](long r, int k) { return child + r * 2 * T + k; });
+    const R *child = lv(a.phi, L + 1);
+    coarse_rows<R>(1L << L, 2 * T, T, Bs, As, lv(a.phi, L), [=](long r, int k) { return child + r * 2 * T + k; });
     if (L > 2)
       coarse_stage_b<R>(2 * T, T, m2m_b(L - 1), Bs);
     else
       coarse_stage_b<R>(T, T, a.btop, Bs);
-    if (!grid_barrier(a.sync, a.status)) {
-      cp_async_wait0();
-      return;
-    }
   }
   { /* top flip: psi_2[c] = topflp . phi_2[(c + 2) mod 4] */
-    const R *phi2 = a.phi + lvl_off(2, S1, T);
-    coarse_rows<R>(2 * S1 * 4, T, T, Bs, As, a.psi + lvl_off(2, S1, T), [=](long r, int k) {
-      const long pl = r >> 2, c = r & 3;
-      return phi2 + (pl * 4 + ((c + 2) & 3)) * T + k;
-    });
+    const R *phi2 = lv(a.phi, 2);
+    coarse_rows<R>(4, T, T, Bs, As, lv(a.psi, 2), [=](long r, int k) { return phi2 + ((r + 2) & 3) * T + k; });
   }
   if (a.Ll >= 3) coarse_stage_b<R>(5 * T, 2 * T, m2l_b(3), Bs);
   for (int l = 3; l <= a.Ll; ++l) { /* M2L + L2L: child level l, one row per parent box */
-    if (!grid_barrier(a.sync, a.status)) {
-      cp_async_wait0();
-      return;
-    }
-    const R *psi_par = a.psi + lvl_off(l - 1, S1, T), *phi = a.phi + lvl_off(l, S1, T);
-    const int lpar = l - 1;
-    coarse_rows<R>(2 * S1 * (1L << lpar), 5 * T, 2 * T, Bs, As, a.psi + lvl_off(l, S1, T), [=](long r, int k) {
-                     if (k < T) return psi_par + r * T + k;
-                     const long pl = r >> lpar, Bx = r & ((1L << lpar) - 1), mask = (2L << lpar) - 1;
-                     const long base = pl << (lpar + 1);
-                     if (k < 3 * T) return phi + (base + ((2 * Bx - 2) & mask)) * T + (k - T);
-                     return phi + (base + ((2 * Bx + 2) & mask)) * T + (k - 3 * T);
-                   });
+    const R *psi_par = lv(a.psi, l - 1), *phi = lv(a.phi, l);
+    const long mask = (1L << l) - 1;
+    coarse_rows<R>(1L << (l - 1), 5 * T, 2 * T, Bs, As, lv(a.psi, l), [=](long r, int k) {
+      if (k < T) return psi_par + r * T + k;
+      if (k < 3 * T) return phi + ((2 * r - 2) & mask) * T + (k - T);
+      return phi + ((2 * r + 2) & mask) * T + (k - 3 * T);
+    });
     if (l < a.Ll) coarse_stage_b<R>(5 * T, 2 * T, m2l_b(l + 1), Bs);
   }
+  cp_async_wait0();
 }
 
-/* Self-test of the bounded device waits: the same wait routines as the tensor-core kernels
- * (tc::t_wait on an mbarrier, with tensor memory held) and the coarse-tree kernel (grid_barrier),
- * each made to wait for an event that never comes (an mbarrier nobody arrives on; a grid barrier
- * whose arrival count starts past the grid size, so no block is ever the last), with a short
- * limit.  The wait gives up, records the error in `status`, the tensor memory is freed and the
- * kernel returns: the host then sees FMMFFT_ERR_TIMEOUT and the context stays usable.
- * which = 0: mbarrier wait; 1: grid barrier (one block; sync[0] preset by the host). */
-__global__ void __launch_bounds__(64) k_selftest_wait(int which, unsigned long long limit_ns,
-                                                      unsigned *sync, int *status) {
+/* Self-test of the bounded device waits: the same wait routine as the tensor-core kernels
+ * (tc::t_wait on an mbarrier, with tensor memory held), made to wait for an event that never
+ * comes (an mbarrier nobody arrives on) with a short limit.  The wait gives up, records the error
+ * in `status`, the tensor memory is freed and the kernel returns: the host then sees
+ * FMMFFT_ERR_TIMEOUT and the context stays usable. */
+__global__ void __launch_bounds__(64) k_selftest_wait(unsigned long long limit_ns, int *status) {
   __shared__ uint64_t bar;
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int abort_flag;
-  if (which == 0) {
+  {
     if (threadIdx.x < 32) tc::tmem_alloc(&tmem_slot, 32);
     if (threadIdx.x == 0) {
       tc::mbar_init(&bar, 1);
@@ -1825,8 +1774,6 @@ __global__ void __launch_bounds__(64) k_selftest_wait(int which, unsigned long l
     __syncthreads();
     tc::fence_after_sync();
     if (threadIdx.x < 32) tc::tmem_dealloc(tmem_slot, 32);
-  } else {
-    grid_barrier(sync, status, limit_ns);
   }
 }
 
@@ -2006,32 +1953,24 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
 
 constexpr long kCoarseRows = 4096; /* default: tree levels with fewer rows form the coarse tree */
 
-/* Coarse-tree settings of a plan: threshold (FMMFFT_COARSE_ROWS overrides, 0 turns the fused
- * kernel off) and the cooperative grid, at most two blocks per SM. */
+/* Coarse-tree settings of a plan: threshold (FMMFFT_COARSE_ROWS overrides, 0 turns the
+ * one-launch coarse tree off) and whether the kernel's shared memory fits.  The choice depends on
+ * the plan only, so a transform gives the same bits alone, in a batch or in a server mix. */
 template <typename R> static void coarse_setup(Dev<R> *d) {
-  /* a cooperative launch does not overlap with other kernels, which costs more than it saves
-   * for the small transforms that batches and servers run side by side; it serves plans of
-   * N >= 2^23.  The choice depends on the plan only, so a transform gives the same bits alone,
-   * in a batch graph or in a server mix. */
-  d->coarse_rows = d->N >= (1L << 23) ? kCoarseRows : 0;
+  d->coarse_rows = kCoarseRows;
   if (const char *ev = getenv("FMMFFT_COARSE_ROWS")) d->coarse_rows = atol(ev), d->env_set |= KNOB_COARSE;
   const size_t sm = coarse_smem<R>(d->T);
-  int dev = 0, nsm = 0, nb = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  int nb = 0;
   if (sm <= (size_t)200 * 1024) {
     /* the attribute is the kernel's, not the plan's: always the full allowance, so that a plan
      * with fewer terms made later does not shrink what an earlier plan's launch needs */
     cudaFuncSetAttribute(k_coarse<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_coarse<R>, 256, sm);
   }
-  d->coarse_grid = nsm * (nb < 2 ? nb : 2);
+  d->coarse_grid = nb;
   if (d->coarse_grid < 1) d->coarse_rows = 0; /* operator too large for shared memory */
 }
 
-/* Builds the device plan: operators uploaded, workspace for nb transforms, one cudaMalloc.  With
- * dry_bytes set it only computes the bytes that plan would hold (o needs its sizes only) and
- * allocates nothing. */
 template <typename R>
 static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, char *err, size_t errlen,
                       size_t *dry_bytes = nullptr) {
@@ -2369,12 +2308,12 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   if (d->tc && d->tc_min_rows < thr) thr = d->tc_min_rows; /* never take a level off the TCs */
   /* routing by the row counts of ONE transform, so that a transform takes the same kernels (and
    * gives the same bits) alone and in a batch */
-  const bool coarse = d->sync != nullptr && thr > 2 * S1 * 4;
+  const bool coarse = d->coarse_grid >= 1 && thr > 2 * S1 * 4;
   long Lm = 1, Ll = 2;
-  if (coarse) {
-    for (long L = 2; L <= n - 1; ++L)
+  if (coarse) { /* and at most 2^kCoarseMaxLevel boxes per plane (one block runs a plane) */
+    for (long L = 2; L <= n - 1 && L <= kCoarseMaxLevel; ++L)
       if (2 * S1 * (1L << L) < thr) Lm = L;
-    for (long l = 3; l <= n; ++l)
+    for (long l = 3; l <= n && l - 1 <= kCoarseMaxLevel; ++l)
       if (2 * S1 * (1L << (l - 1)) < thr) Ll = l;
   }
   /* 4: M2M, parent level L = n-1 .. 2 (.. Lm+1 with the coarse tree) */
@@ -2403,23 +2342,9 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   /* 5: top flip, or the whole coarse tree (M2M Lm..2, top flip, M2L 3..Ll) */
   stage(ST_TOP);
   if (coarse) {
-    CoarseArgs<R> ca{d->phi, d->psi, d->bm2m, d->btop, d->bm2l, S1e, (int)T, (int)Lm, (int)Ll,
-                     d->sync, d->status};
-    cudaMemsetAsync(d->sync, 0, sizeof(unsigned), st);
-    void *args[] = {(void *)&ca};
-    /* one warp per row of the largest coarse level, 8 per block: small transforms take a few
-     * blocks and leave the rest of the GPU to concurrent work (batch branches, other streams) */
-    long maxrows = 2 * S1e * 4;
-    if (Lm >= 2 && 2 * S1e * (1L << Lm) > maxrows) maxrows = 2 * S1e * (1L << Lm);
-    if (Ll >= 3 && 2 * S1e * (1L << (Ll - 1)) > maxrows) maxrows = 2 * S1e * (1L << (Ll - 1));
-    long cgrid = (maxrows + 7) / 8;
-    if (cgrid > d->coarse_grid) cgrid = d->coarse_grid;
-    const cudaError_t ce = cudaLaunchCooperativeKernel((const void *)k_coarse<R>, dim3((unsigned)cgrid),
-                                                       dim3(256), args, coarse_smem<R>(T), st);
-    if (ce != cudaSuccess) {
-      snprintf(err, errlen, "coarse-tree launch: %s", cudaGetErrorString(ce));
-      return 3;
-    }
+    CoarseArgs<R> ca{d->phi, d->psi, d->bm2m, d->btop, d->bm2l, S1e, (int)T, (int)Lm, (int)Ll};
+    /* one block per expansion plane of every transform of the execute */
+    k_coarse<R><<<(unsigned)(2 * S1e), 256, coarse_smem<R>(T), st>>>(ca);
     pf.launches[ST_TOP]++;
   } else {
     ProbTop<R> pb{d->phi + lvl_off(2, S1e, T), d->btop, d->psi + lvl_off(2, S1e, T), 2 * S1e * 4,
@@ -2691,7 +2616,7 @@ static int dev_autotune(Dev<R> *d, char *err, size_t errlen) {
     const long v[] = {1024, 4096, 16384};
     knob(KNOB_TCMIN, [](TuneVal &c, long x) { c.tc_min_rows = x; }, v, 3);
   }
-  if (d->N >= (1L << 23) && d->coarse_grid >= 1) { /* cooperative launches serve large plans only */
+  if (d->coarse_grid >= 1) {
     const long v[] = {0, 2048, 4096, 8192};
     knob(KNOB_COARSE, [](TuneVal &c, long x) { c.coarse_rows = x; }, v, 4);
   }
@@ -3216,24 +3141,12 @@ extern "C" int fmmk_execute_noalloc(const fmm_ops64 *o, int reuse_ops, const voi
   return dev_execute<float>(&d, d_in, d_out, st, 0, 1, err, errlen);
 }
 
-/* Runs k_selftest_wait against the plan's own status word (and, for the grid barrier, its
- * barrier words) with a limit of limit_us microseconds, on the legacy stream, and waits for it.
- * fmmk_check then reports the timeout. */
+/* Runs k_selftest_wait against the plan's own status word with a limit of limit_us
+ * microseconds, on the legacy stream, and waits for it.  fmmk_check then reports the timeout. */
 extern "C" int fmmk_selftest_wait(fmmk_state *st, int which, long limit_us, char *err, size_t errlen) {
-  int *status;
-  unsigned *sync;
-  if (st->precision == 0) {
-    Dev<double> *d = (Dev<double> *)st->dev;
-    status = d->status, sync = d->sync;
-  } else {
-    Dev<float> *d = (Dev<float> *)st->dev;
-    status = d->status, sync = d->sync;
-  }
-  if (which == 1) { /* arrivals past the grid size: no block is ever the last to arrive */
-    const unsigned preset[64] = {7u};
-    FMM_CUDA_TRY(cudaMemcpy(sync, preset, sizeof preset, cudaMemcpyHostToDevice));
-  }
-  k_selftest_wait<<<1, 64>>>(which, (unsigned long long)limit_us * 1000ull, sync, status);
+  (void)which;
+  int *status = st->precision == 0 ? ((Dev<double> *)st->dev)->status : ((Dev<float> *)st->dev)->status;
+  k_selftest_wait<<<1, 64>>>((unsigned long long)limit_us * 1000ull, status);
   FMM_CUDA_TRY(cudaGetLastError());
   FMM_CUDA_TRY(cudaDeviceSynchronize());
   return 0;

@@ -313,8 +313,8 @@ class Plan:
         _check(load().fmmfft_plan_check(self._h))
 
     def selftest_wait(self, which, limit_us=2000):
-        """Run the bounded-wait self-test kernel (0: mbarrier wait holding tensor memory,
-        1: coarse-tree grid barrier) against this plan's status word."""
+        """Run the bounded-wait self-test kernel (0: an mbarrier wait holding tensor memory)
+        against this plan's status word."""
         _check(load().fmmfft_plan_selftest_wait(self._h, int(which), int(limit_us)))
 
     def profile_start(self, max_executes):

@@ -184,12 +184,11 @@ int fmmfft_plan_check(fmmfft_plan plan);
 
 /* Self-test of the bounded device waits, for tests and health checks; no counterpart in the
  * reference (which has no device code).  Runs one small kernel that waits, with the same wait
- * routine as the plan's kernels, for an event that never comes -- which = 0: an mbarrier wait
- * while holding tensor memory (the tensor-core kernels' wait); which = 1: the grid barrier of
- * the cooperative coarse-tree kernel -- with a limit of limit_us microseconds (1 .. 2e6).  The
- * wait gives up, records the timeout in the plan's status word, frees what it holds and
- * returns; the call synchronises the device.  The next fmmfft_plan_check(plan) then returns
- * FMMFFT_ERR_TIMEOUT, and the plan stays usable. */
+ * routine as the tensor-core kernels, on an mbarrier nobody arrives on while it holds tensor
+ * memory (which must be 0), with a limit of limit_us microseconds (1 .. 2e6).  The wait gives up,
+ * records the timeout in the plan's status word, frees the tensor memory and returns; the call
+ * synchronises the device.  The next fmmfft_plan_check(plan) then returns FMMFFT_ERR_TIMEOUT,
+ * and the plan stays usable. */
 int fmmfft_plan_selftest_wait(fmmfft_plan plan, int which, long limit_us);
 
 /* Same transform as fmmfft_execute through a CUDA graph: the first call for a given

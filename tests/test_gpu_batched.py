@@ -73,7 +73,7 @@ def test_batch_equals_alone_bitwise(fm, N, P, T, b, prec, nbt):
 
 
 def test_batch_with_coarse_tree_and_tc_everywhere(fm, monkeypatch):
-    """The cooperative coarse-tree kernel (forced below 4096 rows) and every stage on the tensor
+    """The coarse-tree kernel (forced below 4096 rows) and every stage on the tensor
     cores, with S2M as its own stage, in a batch of 5."""
     monkeypatch.setenv("FMMFFT_COARSE_ROWS", "4096")
     monkeypatch.setenv("FMMFFT_TC_MIN_ROWS", "1")

@@ -136,8 +136,8 @@ def test_repeat_runs_bitwise_deterministic(fm):
 
 def test_plan_made_before_a_smaller_one_still_runs(fm):
     """Kernel-wide launch limits set while making a plan must not depend on the plan made last:
-    a 24-term plan, then a 4-term plan, then the 24-term plan executes (the coarse-tree kernel,
-    used from N = 2^23, takes shared memory that grows with the terms)."""
+    a 24-term plan, then a 4-term plan, then the 24-term plan executes (the coarse-tree kernel
+    takes shared memory that grows with the terms)."""
     N, P, b = 1 << 23, 64, 32
     x = ol.seeded_input(N, 21)
     big = fm.Plan(N, P, 24, b, "f32")
@@ -154,10 +154,11 @@ COARSE_CASES = [(4096, 16, 10, 16), (32768, 8, 7, 32), (65536, 32, 12, 16), (131
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 @pytest.mark.parametrize("N,P,T,b", COARSE_CASES)
 def test_coarse_tree_kernel_forced(fm, monkeypatch, N, P, T, b, prec):
-    """Every tree level in the cooperative coarse-tree kernel (FMMFFT_COARSE_ROWS above every
-    level's row count; read when the plan is made).  The level operators are prefetched into
-    shared memory across the grid barriers: in 16-byte pieces for even T, one element per copy
-    for odd T.  Same tolerances as the plans' own paths."""
+    """Every tree level the coarse-tree kernel takes (FMMFFT_COARSE_ROWS above every level's row
+    count, read when the plan is made: levels up to 64 boxes per plane, one block per plane)
+    there.  The level operators are prefetched into shared memory while the level before runs:
+    in 16-byte pieces for even T, one element per copy for odd T.  Same tolerances as the
+    plans' own paths."""
     monkeypatch.setenv("FMMFFT_COARSE_ROWS", str(1 << 40))
     x = ol.seeded_input(N, N + 3 * P)
     o = ol.forward_ex(x, P, T, b)
