@@ -1379,14 +1379,16 @@ __global__ void __launch_bounds__(kMThreads, 1)
  * src(c, r, z) (16-byte-aligned row of chunk c), dst(r, z) and put8(dst, r, z, c0, t).
  * Every wait is bounded (2 s); on expiry the CTA records kErrWaitTimeout, every role leaves its
  * loop, copies in flight land and the MMAs in flight complete before TMEM is freed. */
-constexpr int kWKs = 32;       /* K columns per A slot */
-constexpr int kWSlots = 4;     /* A slots in tensor memory: hi + lo, 64 columns each */
-constexpr int kWStages = 6;    /* shared-memory ring of A: 128 rows x 32 floats per stage */
+constexpr int kWKs = 64;       /* K columns per A slot */
+constexpr int kWSlots = 2;     /* A slots in tensor memory: hi + lo, 128 columns each */
+constexpr int kWStages = 4;    /* shared-memory ring of A: 128 rows x 64 floats (32 KB) per stage */
 constexpr int kWProd = 8;      /* producer warps */
 constexpr int kWEpi = 8;       /* epilogue warps */
 constexpr int kWThreads = (kWProd + kWEpi + 1) * 32;
-constexpr int kWMaxSlots = 8;  /* K <= 256 */
-constexpr int kWStageBytes = kRows * kWKs * 4;
+constexpr int kWMaxSlots = 4;  /* K <= 256 */
+constexpr int kWUnits = kWKs / 4;       /* 16-byte units per row of a slot */
+constexpr int kWRowBytes = kWKs * 4;    /* a slot row in the ring */
+constexpr int kWStageBytes = kRows * kWRowBytes;
 
 __host__ __device__ constexpr int round32(int v) { return (v + 31) & ~31; }
 /* accumulator columns of one tile: B_hi and B_lo products side by side */
@@ -1401,7 +1403,7 @@ __host__ __device__ constexpr size_t ws_smem_bytes(int kpad, int npad, int eb = 
 /* the operator fits: two accumulators and the A slots within 512 TMEM columns, K <= 256 */
 __host__ __device__ constexpr bool ws_fits(int kpad, int npad) {
   return npad % 16 == 0 && npad <= 64 && kpad % 8 == 0 && kpad <= kWKs * kWMaxSlots &&
-         2 * ws_acc_cols(npad) + kWSlots * 2 * kWKs <= 512 && ws_smem_bytes(kpad, npad) <= 200 * 1024;
+         2 * ws_acc_cols(npad) + kWSlots * 2 * kWKs <= 512 && ws_smem_bytes(kpad, npad) <= 220 * 1024;
 }
 /* element index of operator element (n, k), n < 2 npad (hi rows, then lo rows), in the layout
  * the kernel copies: 8-row groups of core matrices of 8 rows x 16 bytes along K (4 TF32 or 8
@@ -1465,7 +1467,7 @@ __device__ __forceinline__ bool named_bar_or(int id, int nthreads, bool v) {
 }
 
 template <class Prob, bool kBF = false>
-__global__ void __launch_bounds__(kWThreads, 1) k_tc_ws(const __grid_constant__ Prob pb, int *status) {
+__global__ void __maxnreg__(120) k_tc_ws(const __grid_constant__ Prob pb, int *status) {
   /* kBF: BF16x3 instead of split TF32: A and B split into BF16 hi + lo (the lo part the BF16
    * rounding of the residual), products A_hi B_hi + A_hi B_lo + A_lo B_hi, kind::f16 MMAs of
    * K = 16; about 2^-17 relative per product, for orders whose truncation is far above that */
@@ -1476,10 +1478,10 @@ __global__ void __launch_bounds__(kWThreads, 1) k_tc_ws(const __grid_constant__ 
   __shared__ volatile int abort_flag;
   /* per slot j and 16-byte unit u of its 32 columns: A chunk (low byte, 0xFF = zero), float
    * offset in that chunk's row (high bits) */
-  __shared__ int lmap[kWMaxSlots][8];
+  __shared__ int lmap[kWMaxSlots][kWUnits];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int kpad = pb.kpad, npad = pb.npad;
-  const int nsl = round32(kpad) / kWKs;
+  const int nsl = (kpad + kWKs - 1) / kWKs;
   float *Bs = reinterpret_cast<float *>(smem_raw);
   unsigned char *ring = smem_raw + ws_b_floats(kpad, npad) * kEB;
   const int mma_warp = kWProd + kWEpi;
@@ -1492,8 +1494,8 @@ __global__ void __launch_bounds__(kWThreads, 1) k_tc_ws(const __grid_constant__ 
     fence_mbar_init();
     abort_flag = 0;
   }
-  if (tid < kWMaxSlots * 8) {
-    const int j = tid >> 3, u = tid & 7, k = j * kWKs + 4 * u;
+  if (tid < kWMaxSlots * kWUnits) {
+    const int j = tid / kWUnits, u = tid % kWUnits, k = j * kWKs + 4 * u;
     int e = 0xFF;
     if (j < nsl && k < kpad)
       for (int c = 0; c < pb.nchunks; ++c)
@@ -1530,10 +1532,10 @@ __global__ void __launch_bounds__(kWThreads, 1) k_tc_ws(const __grid_constant__ 
     const int q = warp & 3, h = warp >> 2;
     const int my_row = q * 32 + lane;                 /* TMEM lane = tile row this thread splits */
     const uint32_t lane_addr = (uint32_t)(q * 32) << 16;
-    /* this warp copies exactly what it splits: its 32 rows, 16-byte units 4 h .. 4 h + 3 of each;
-     * lane: unit 4 h + lane % 4 of rows 32 q + 8 m + lane / 4 (8 rows x 64 bytes per copy
-     * instruction), so a warp needs no other warp's copies and no CTA-wide barrier */
-    const int cu = 4 * h + (lane & 3), crow = q * 32 + (lane >> 2);
+    /* this warp copies exactly what it splits: its 32 rows, 16-byte units 8 h .. 8 h + 7 of each
+     * (32 columns); lane: unit 8 h + lane % 8 of rows 32 q + 4 m + lane / 8, so each copy
+     * instruction moves 4 rows x 128 contiguous bytes, and a warp waits for no other warp */
+    const int cu = 8 * h + (lane & 7), crow = q * 32 + (lane >> 3);
     const uint32_t ring0 = smem_addr(ring);
     const long G = (long)my_tiles * nsl;
     /* copies of global slot g (tile index g / nsl of this CTA, slot g % nsl) into its stage */
@@ -1546,38 +1548,42 @@ __global__ void __launch_bounds__(kWThreads, 1) k_tc_ws(const __grid_constant__ 
         if (c != 0xFF) {
           const uint32_t st = ring0 + (uint32_t)((g % kWStages) * kWStageBytes);
 #pragma unroll
-          for (int m = 0; m < 4; ++m) {
-            const int row = crow + 8 * m;
+          for (int m = 0; m < 8; ++m) {
+            const int row = crow + 4 * m;
             const long r = r0 + row;
             if (r < pb.rows)
-              cp_async16_cg(st + (uint32_t)(row * 128 + ((cu ^ (row & 7)) << 4)), pb.src(c, r, batch) + (e >> 8));
+              cp_async16_cg(st + (uint32_t)(row * kWRowBytes + ((cu ^ (row & 7)) << 4)),
+                            pb.src(c, r, batch) + (e >> 8));
           }
         }
       }
       cp_async_commit(); /* one group per slot, empty or not: wait_group counts stay exact */
     };
-#pragma unroll 1
-    for (int g = 0; g < kWStages - 1; ++g) issue(g);
-    for (long g = 0; g < G; ++g) {
+    /* this lane's row of slot g from the ring (after its copies have landed) */
+    float4 a[8];
+    auto fetch = [&](long g) {
       cp_async_wait<kWStages - 2>(); /* this thread's copies of slot g have landed */
-      /* the warp's copies of slot g have landed and its lanes have read slot g - 1, whose stage
-       * the next copies reuse; the warp leaves as one on an abort */
-      __syncwarp();
-      if (__any_sync(0xffffffffu, abort_flag != 0)) break;
+      __syncwarp(); /* ... and the warp's; its lanes have read slot g - 1, whose stage is refilled */
       issue(g + kWStages - 1);
       const int j = (int)(g % nsl);
-      const uint32_t st = ring0 + (uint32_t)((g % kWStages) * kWStageBytes) + (uint32_t)(my_row * 128);
-      float hv[16], lv[16];
+      const uint32_t st = ring0 + (uint32_t)((g % kWStages) * kWStageBytes) + (uint32_t)(my_row * kWRowBytes);
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int u = 4 * h + i;
-        float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int i = 0; i < 8; ++i) {
+        const int u = 8 * h + i;
+        a[i] = make_float4(0.f, 0.f, 0.f, 0.f);
         if ((lmap[j][u] & 0xFF) != 0xFF)
           asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
-                       : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w)
+                       : "=f"(a[i].x), "=f"(a[i].y), "=f"(a[i].z), "=f"(a[i].w)
                        : "r"(st + (uint32_t)((u ^ (my_row & 7)) << 4)));
-        const float av[4] = {a.x, a.y, a.z, a.w};
-        if constexpr (kBF) { /* packed BF16 pairs: hv / lv words 2i, 2i + 1 */
+      }
+    };
+    /* split into hi / lo: 32 TF32 pairs, or 16 packed BF16 pairs of words */
+    float hv[32], lv[32];
+    auto split = [&]() {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const float av[4] = {a[i].x, a[i].y, a[i].z, a[i].w};
+        if constexpr (kBF) {
 #pragma unroll
           for (int k = 0; k < 2; ++k) {
             const uint32_t hw = pack_bf16x2(av[2 * k], av[2 * k + 1]);
@@ -1593,27 +1599,43 @@ __global__ void __launch_bounds__(kWThreads, 1) k_tc_ws(const __grid_constant__ 
           }
         }
       }
+    };
+#pragma unroll 1
+    for (int g = 0; g < kWStages - 1; ++g) issue(g);
+    if (G > 0) {
+      fetch(0);
+      split();
+    }
+    /* per slot: wait for its TMEM slot, store hi / lo, then (while the stores complete) fetch the
+     * next slot's row, then wait for the stores, signal, and split the next slot */
+    for (long g = 0; g < G; ++g) {
       const int s = (int)(g % kWSlots);
       bool ok = true;
       if (lane == 0) ok = t_wait(&tempty[s], (uint32_t)(((g / kWSlots) & 1) ^ 1), &abort_flag, status);
       ok = __shfl_sync(0xffffffffu, ok, 0);
-      if (!ok) continue; /* the next iteration sees the abort */
+      if (!ok) break;
       fence_after_sync();
-      if constexpr (kBF) { /* 16 values = 8 columns per half; lo 16 columns after hi */
-        const uint32_t ahi = tmem + lane_addr + (uint32_t)(2 * acc_cols + s * 2 * kWKs + 8 * h);
-        tmem_st8(ahi, hv);
-        tmem_st8(ahi + kWKs / 2, lv);
+      const uint32_t base = tmem + lane_addr + (uint32_t)(2 * acc_cols + s * 2 * kWKs);
+      if constexpr (kBF) { /* 32 values = 16 columns per half; lo 32 columns after hi */
+        tmem_st8(base + 16 * h, hv);
+        tmem_st8(base + 16 * h + 8, hv + 8);
+        tmem_st8(base + kWKs / 2 + 16 * h, lv);
+        tmem_st8(base + kWKs / 2 + 16 * h + 8, lv + 8);
       } else {
-        const uint32_t ahi = tmem + lane_addr + (uint32_t)(2 * acc_cols + s * 2 * kWKs + 16 * h);
-        tmem_st8(ahi, hv);
-        tmem_st8(ahi + 8, hv + 8);
-        tmem_st8(ahi + kWKs, lv);
-        tmem_st8(ahi + kWKs + 8, lv + 8);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          tmem_st8(base + 32 * h + 8 * i, hv + 8 * i);
+          tmem_st8(base + kWKs + 32 * h + 8 * i, lv + 8 * i);
+        }
       }
+      const bool more = g + 1 < G && !__any_sync(0xffffffffu, abort_flag != 0);
+      if (more) fetch(g + 1);
       tmem_st_wait();
       fence_before_sync();
       __syncwarp();
       if (lane == 0) mbar_arrive(&tfull[s]);
+      if (!more) break;
+      split();
     }
     cp_async_wait<0>(); /* nothing may still write shared memory when the CTA ends */
   } else if (warp < kWProd + kWEpi) {
@@ -1681,7 +1703,8 @@ __global__ void __launch_bounds__(kWThreads, 1) k_tc_ws(const __grid_constant__ 
         const int k0 = j * kWKs;
         const uint32_t ahi = tmem + (uint32_t)(2 * acc_cols + s * 2 * kWKs);
         if constexpr (kBF) {
-          /* K step of 16 BF16 = two core matrices along K = 256 bytes; 8 TMEM columns of A */
+          /* K step of 16 BF16 = two core matrices along K = 256 bytes; 8 TMEM columns of A (lo
+           * 32 columns after hi) */
           const int ksteps = (((kpad - k0) < kWKs ? (kpad - k0) : kWKs) + 15) >> 4;
           for (int kk = 0; kk < ksteps; ++kk) {
             const uint64_t db = make_desc(bsm + 256u * (uint32_t)((k0 >> 4) + kk), 128, b_sbo);
