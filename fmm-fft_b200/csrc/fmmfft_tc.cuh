@@ -1362,16 +1362,16 @@ __global__ void __launch_bounds__(kMThreads, 1)
  *               only what it copied, so warps wait for nothing but their own copies.  Units are
  *               stored XOR-swizzled in shared memory (16-byte unit j of row i at position
  *               j ^ (i & 7)): copies and row reads take four wavefronts per warp instruction.
- *   warp 16     one thread issues, per K step of 8, A_hi x [B_hi; B_lo] (N = 2 npad) and
+ *   warp 12     one thread issues, per K step of 8, A_hi x [B_hi; B_lo] (N = 2 npad) and
  *               A_lo x B_hi (N = npad) into one of two TMEM accumulators: split TF32 with three
  *               products (the A_lo B_lo term, 2^-22 relative, is left out), FP32 accumulation;
  *               it commits each slot to the slot's `empty` barrier and each tile to the
  *               accumulator's `full` barrier.  It also stages B: the host lays each batch's
  *               operator out in the MMA's K-major core-matrix layout (hi rows, then lo rows), so
  *               one bulk copy brings it into shared memory.
- *   warps 8-15  epilogue: warp (q, h) reads lane quarter q of the accumulator, adds its two
- *               column halves and stores 8-column chunks 8 h, 8 h + 16, ... of each row through
- *               Prob::put8, then frees the accumulator for the tile after next.
+ *   warps 8-11  epilogue: warp 8 + q reads lane quarter q of the accumulator, adds its two
+ *               column halves and stores each row's 8-column chunks through Prob::put8, then
+ *               frees the accumulator for the tile after next.
  *
  * Prob supplies rows, batches, nchunks / clen / coff (A chunks, multiples of 4 floats), kpad
  * (multiple of 8), npad (multiple of 16, at most 64), nout, wsb (the B operator of batch z at
@@ -1383,7 +1383,7 @@ constexpr int kWKs = 64;       /* K columns per A slot */
 constexpr int kWSlots = 2;     /* A slots in tensor memory: hi + lo, 128 columns each */
 constexpr int kWStages = 4;    /* shared-memory ring of A: 128 rows x 64 floats (32 KB) per stage */
 constexpr int kWProd = 8;      /* producer warps */
-constexpr int kWEpi = 8;       /* epilogue warps */
+constexpr int kWEpi = 4;       /* epilogue warps: one per TMEM lane quarter */
 constexpr int kWThreads = (kWProd + kWEpi + 1) * 32;
 constexpr int kWMaxSlots = 4;  /* K <= 256 */
 constexpr int kWUnits = kWKs / 4;       /* 16-byte units per row of a slot */
@@ -1467,7 +1467,8 @@ __device__ __forceinline__ bool named_bar_or(int id, int nthreads, bool v) {
 }
 
 template <class Prob, bool kBF = false>
-__global__ void __maxnreg__(120) k_tc_ws(const __grid_constant__ Prob pb, int *status) {
+/* 13 warps: at most 4 on an SM sub-partition, so up to 128 registers a thread */
+__global__ void __maxnreg__(128) k_tc_ws(const __grid_constant__ Prob pb, int *status) {
   /* kBF: BF16x3 instead of split TF32: A and B split into BF16 hi + lo (the lo part the BF16
    * rounding of the residual), products A_hi B_hi + A_hi B_lo + A_lo B_hi, kind::f16 MMAs of
    * K = 16; about 2^-17 relative per product, for orders whose truncation is far above that */
@@ -1640,7 +1641,7 @@ __global__ void __maxnreg__(120) k_tc_ws(const __grid_constant__ Prob pb, int *s
     cp_async_wait<0>(); /* nothing may still write shared memory when the CTA ends */
   } else if (warp < kWProd + kWEpi) {
     /* ------------------------------------------------------------ epilogue */
-    const int q = warp & 3, h = (warp - kWProd) >> 2;
+    const int q = warp & 3, eh = (warp - kWProd) >> 2, estep = 8 * (kWEpi / 4);
     const uint32_t lane_addr = (uint32_t)(q * 32) << 16;
     for (int lt = 0; lt < my_tiles; ++lt) {
       const int t = tile0 + lt * tile_step, a = lt & 1;
@@ -1653,7 +1654,7 @@ __global__ void __maxnreg__(120) k_tc_ws(const __grid_constant__ Prob pb, int *s
       const long r = (long)(t - batch * tiles_per_batch) * kRows + q * 32 + lane;
       float *dst = r < pb.rows ? pb.dst(r, batch) : nullptr;
       const uint32_t acc = tmem + lane_addr + (uint32_t)(a * acc_cols);
-      for (int c0 = 8 * h; c0 < npad; c0 += 16) {
+      for (int c0 = 8 * eh; c0 < npad; c0 += estep) {
         float v[8], w[8];
         tmem_ld8(acc + (uint32_t)c0, v);
         tmem_ld8(acc + (uint32_t)(npad + c0), w);
