@@ -1628,6 +1628,7 @@ template <typename R> struct CoarseArgs {
   int T, Lm, Ll; /* coarse M2M parent levels Lm..2 (none when Lm < 2); M2L child levels 3..Ll */
 };
 constexpr int kCoarseMaxLevel = 6; /* coarse M2M parents hold at most 2^6 boxes per plane */
+constexpr int kCoarseWarps = 32;   /* a block: one warp per row, a coarse level's rows in one pass */
 
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
@@ -1656,8 +1657,9 @@ __device__ __forceinline__ void coarse_stage_b(int K, int N, const R *__restrict
 }
 
 /* out[r][n] = sum_k A(r, k) Bs[k][n] for the rows of one level of one plane, all by this block;
- * B (K x N) is in flight into the shared array Bs (coarse_stage_b), and the block stages 8 rows
- * of A at a time into As (one row per warp), so a row costs one round of loads; arow(r, k) is
+ * B (K x N) is in flight into the shared array Bs (coarse_stage_b), and the block stages
+ * kCoarseWarps rows of A at a time into As (one row per warp), so a row costs one round of
+ * loads (a coarse level's rows are one round); arow(r, k) is
  * the address of element k of row r's A.  Ends on a block barrier after the last stores, so the
  * next level reads this one's output. */
 template <typename R, class Arow>
@@ -1666,18 +1668,19 @@ __device__ __forceinline__ void coarse_rows(long rows, int K, int N, R *__restri
   cp_async_wait0(); /* this thread's copies of the operator */
   __syncthreads();  /* everyone's copies; the previous level's reads of As are done */
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (long r0 = 0; r0 < rows; r0 += 8) { /* block-uniform */
-    for (int e0 = threadIdx.x; e0 < 8 * K; e0 += 4 * blockDim.x) { /* 4 loads in flight */
+  const int W = kCoarseWarps;
+  for (long r0 = 0; r0 < rows; r0 += W) { /* block-uniform */
+    for (int e0 = threadIdx.x; e0 < W * K; e0 += 4 * blockDim.x) { /* 4 loads in flight */
       R v[4];
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         const int e = e0 + u * blockDim.x, w = e / K, k = e - w * K;
         const long r = r0 + w;
-        v[u] = (e < 8 * K && r < rows) ? *arow(r, k) : R(0);
+        v[u] = (e < W * K && r < rows) ? *arow(r, k) : R(0);
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u)
-        if (e0 + u * (int)blockDim.x < 8 * K) As[e0 + u * blockDim.x] = v[u];
+        if (e0 + u * (int)blockDim.x < W * K) As[e0 + u * blockDim.x] = v[u];
     }
     __syncthreads();
     const long r = r0 + warp;
@@ -1708,9 +1711,11 @@ __device__ __forceinline__ void coarse_rows(long rows, int K, int N, R *__restri
 
 /* Shared memory of the coarse kernel: the largest operator, the M2L one (5T x 2T), and 8 rows
  * of the widest A (5T). */
-template <typename R> static size_t coarse_smem(long T) { return sizeof(R) * (10 * (size_t)T * T + 40 * (size_t)T); }
+template <typename R> static size_t coarse_smem(long T) {
+  return sizeof(R) * (10 * (size_t)T * T + 5 * kCoarseWarps * (size_t)T);
+}
 
-template <typename R> __global__ void __launch_bounds__(256) k_coarse(CoarseArgs<R> a) {
+template <typename R> __global__ void __launch_bounds__(32 * kCoarseWarps) k_coarse(CoarseArgs<R> a) {
   extern __shared__ __align__(16) unsigned char coarse_raw[];
   R *Bs = reinterpret_cast<R *>(coarse_raw);
   R *As = Bs + 10L * a.T * a.T;
@@ -1965,7 +1970,7 @@ template <typename R> static void coarse_setup(Dev<R> *d) {
     /* the attribute is the kernel's, not the plan's: always the full allowance, so that a plan
      * with fewer terms made later does not shrink what an earlier plan's launch needs */
     cudaFuncSetAttribute(k_coarse<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_coarse<R>, 256, sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_coarse<R>, 32 * kCoarseWarps, sm);
   }
   d->coarse_grid = nb;
   if (d->coarse_grid < 1) d->coarse_rows = 0; /* operator too large for shared memory */
@@ -2344,7 +2349,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   if (coarse) {
     CoarseArgs<R> ca{d->phi, d->psi, d->bm2m, d->btop, d->bm2l, S1e, (int)T, (int)Lm, (int)Ll};
     /* one block per expansion plane of every transform of the execute */
-    k_coarse<R><<<(unsigned)(2 * S1e), 256, coarse_smem<R>(T), st>>>(ca);
+    k_coarse<R><<<(unsigned)(2 * S1e), 32 * kCoarseWarps, coarse_smem<R>(T), st>>>(ca);
     pf.launches[ST_TOP]++;
   } else {
     ProbTop<R> pb{d->phi + lvl_off(2, S1e, T), d->btop, d->psi + lvl_off(2, S1e, T), 2 * S1e * 4,
