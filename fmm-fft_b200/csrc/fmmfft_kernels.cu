@@ -386,16 +386,17 @@ __global__ void k_sum_sections(const typename cplx<R>::T *__restrict__ part, lon
  * stage's arrays by the problem object; B is a dense operator in global memory or generated
  * (leaf).  Tile BM x BN x BK; each thread owns a TM x TN block of outputs. */
 
-template <typename R> struct ProbS2M {
+template <typename R> struct ProbS2M { /* batch z = transform: its sections 1..P-1, planar */
   const R *xt, *B;
   R *out;
-  long rows, M;
-  int K, N;
-  long tr_rows; /* rows per transform: 2 (P - 1) s; transform tr's sections start 2 M (tr + 1) in */
-  __device__ void begin(int) {}
-  __device__ R a(long r, int k) const { return xt[2 * M * (r / tr_rows + 1) + r * K + k]; }
+  long rows, M; /* rows per transform: 2 (P - 1) s */
+  int K, N, P;
+  const R *xs;
+  R *os;
+  __device__ void begin(int z) { xs = xt + (2L * P * z + 2) * M, os = out + (long)z * rows * N; }
+  __device__ R a(long r, int k) const { return xs[r * K + k]; }
   __device__ R bv(int k, int n) const { return B[k * N + n]; }
-  __device__ R *d(long r) const { return out + r * N; }
+  __device__ R *d(long r) const { return os + r * N; }
 };
 
 template <typename R> struct ProbM2M { /* parent level L: A row = children pair of level L+1 */
@@ -502,13 +503,13 @@ struct TcBase {
   }
 };
 
-struct TcS2M : TcBase {
+struct TcS2M : TcBase { /* batch z = transform (one operator for all: wsb_stride 0) */
   const float *xt;
   float *out;
-  long M, tr_rows; /* rows per transform: 2 (P - 1) s */
-  int b, T;
-  __device__ const float *src(int, long r, int) const { return xt + 2 * M * (r / tr_rows + 1) + r * b; }
-  __device__ float *dst(long r, int) const { return out + r * T; }
+  long M;
+  int b, T, P;
+  __device__ const float *src(int, long r, int z) const { return xt + (2L * P * z + 2) * M + r * b; }
+  __device__ float *dst(long r, int z) const { return out + ((long)z * rows + r) * T; }
 };
 
 struct TcM2M : TcBase {
@@ -2292,8 +2293,8 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
     if constexpr (sizeof(R) == 4) {
       if (d->tc && d->ok_s2m && 2 * S1 * s >= d->tc_min_rows) {
         TcS2M q{};
-        q.rows = 2 * S1e * s, q.batches = 1, q.nchunks = 1, q.clen[0] = (int)b, q.coff[0] = 0;
-        q.tr_rows = 2 * S1 * s;
+        q.rows = 2 * S1 * s, q.batches = nbt, q.nchunks = 1, q.clen[0] = (int)b, q.coff[0] = 0;
+        q.P = (int)P;
         q.kpad = d->kp_s2m, q.npad = d->np_s2m, q.nout = (int)T;
         q.bhi = d->tc_s2m[0], q.blo = d->tc_s2m[1], q.bstride = 0, q.wsb = d->ws_s2m, q.wsb_stride = 0;
         q.xt = d->xt, q.out = d->phi + lvl_off(n, S1e, T), q.M = M, q.b = (int)b, q.T = (int)T;
@@ -2302,9 +2303,8 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
       }
     }
     if (!done) {
-      ProbS2M<R> pb{d->xt, d->initch, d->phi + lvl_off(n, S1e, T), 2 * S1e * s, M, (int)b, (int)T,
-                    2 * S1 * s};
-      launch_rowgemm<R>(pb, pb.rows, (int)T, 1, st);
+      ProbS2M<R> pb{d->xt, d->initch, d->phi + lvl_off(n, S1e, T), 2 * S1 * s, M, (int)b, (int)T, (int)P};
+      launch_rowgemm<R>(pb, pb.rows, (int)T, nbt, st);
     }
     pf.launches[ST_S2M]++;
   }

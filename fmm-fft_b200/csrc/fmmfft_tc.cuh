@@ -1538,45 +1538,56 @@ __global__ void __maxnreg__(128) k_tc_ws(const __grid_constant__ Prob pb, int *s
      * instruction moves 4 rows x 128 contiguous bytes, and a warp waits for no other warp */
     const int cu = 8 * h + (lane & 7), crow = q * 32 + (lane >> 3);
     const uint32_t ring0 = smem_addr(ring);
-    const long G = (long)my_tiles * nsl;
-    /* copies of global slot g (tile index g / nsl of this CTA, slot g % nsl) into its stage */
-    auto issue = [&](long g) {
-      if (g < G) {
-        const int t = tile0 + (int)(g / nsl) * tile_step, j = (int)(g % nsl);
-        const int batch = t / tiles_per_batch;
-        const long r0 = (long)(t - batch * tiles_per_batch) * kRows;
-        const int e = lmap[j][cu], c = e & 0xFF;
+    const int G = my_tiles * nsl;
+    /* copy cursor: the next slot whose copies are issued, kept incrementally (no divisions by
+     * runtime values per slot: those run on the conversion pipe) */
+    int c_g = 0, c_j = 0, c_t = tile0, c_batch = 0;
+    long c_r0 = 0;
+    auto c_tile = [&]() {
+      c_batch = c_t / tiles_per_batch;
+      c_r0 = (long)(c_t - c_batch * tiles_per_batch) * kRows;
+    };
+    if (G > 0) c_tile();
+    auto issue = [&]() {
+      if (c_g < G) {
+        const int e = lmap[c_j][cu], c = e & 0xFF;
         if (c != 0xFF) {
-          const uint32_t st = ring0 + (uint32_t)((g % kWStages) * kWStageBytes);
+          const uint32_t st = ring0 + (uint32_t)((c_g & (kWStages - 1)) * kWStageBytes);
 #pragma unroll
           for (int m = 0; m < 8; ++m) {
             const int row = crow + 4 * m;
-            const long r = r0 + row;
+            const long r = c_r0 + row;
             if (r < pb.rows)
               cp_async16_cg(st + (uint32_t)(row * kWRowBytes + ((cu ^ (row & 7)) << 4)),
-                            pb.src(c, r, batch) + (e >> 8));
+                            pb.src(c, r, c_batch) + (e >> 8));
           }
+        }
+        ++c_g;
+        if (++c_j == nsl) {
+          c_j = 0, c_t += tile_step;
+          if (c_g < G) c_tile();
         }
       }
       cp_async_commit(); /* one group per slot, empty or not: wait_group counts stay exact */
     };
-    /* this lane's row of slot g from the ring (after its copies have landed) */
+    /* this lane's row of slot g (slot f_j of its tile) from the ring, after its copies landed */
     float4 a[8];
-    auto fetch = [&](long g) {
+    int f_j = 0;
+    auto fetch = [&](int g) {
       cp_async_wait<kWStages - 2>(); /* this thread's copies of slot g have landed */
       __syncwarp(); /* ... and the warp's; its lanes have read slot g - 1, whose stage is refilled */
-      issue(g + kWStages - 1);
-      const int j = (int)(g % nsl);
-      const uint32_t st = ring0 + (uint32_t)((g % kWStages) * kWStageBytes) + (uint32_t)(my_row * kWRowBytes);
+      issue();      /* slot g + kWStages - 1 */
+      const uint32_t st = ring0 + (uint32_t)((g & (kWStages - 1)) * kWStageBytes) + (uint32_t)(my_row * kWRowBytes);
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
         const int u = 8 * h + i;
         a[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if ((lmap[j][u] & 0xFF) != 0xFF)
+        if ((lmap[f_j][u] & 0xFF) != 0xFF)
           asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
                        : "=f"(a[i].x), "=f"(a[i].y), "=f"(a[i].z), "=f"(a[i].w)
                        : "r"(st + (uint32_t)((u ^ (my_row & 7)) << 4)));
       }
+      if (++f_j == nsl) f_j = 0;
     };
     /* split into hi / lo: 32 TF32 pairs, or 16 packed BF16 pairs of words */
     float hv[32], lv[32];
@@ -1602,17 +1613,18 @@ __global__ void __maxnreg__(128) k_tc_ws(const __grid_constant__ Prob pb, int *s
       }
     };
 #pragma unroll 1
-    for (int g = 0; g < kWStages - 1; ++g) issue(g);
+    for (int g = 0; g < kWStages - 1; ++g) issue();
     if (G > 0) {
       fetch(0);
       split();
     }
     /* per slot: wait for its TMEM slot, store hi / lo, then (while the stores complete) fetch the
      * next slot's row, then wait for the stores, signal, and split the next slot */
-    for (long g = 0; g < G; ++g) {
-      const int s = (int)(g % kWSlots);
+    static_assert(kWSlots == 2 && (kWStages & (kWStages - 1)) == 0, "slot and stage indices are masks");
+    for (int g = 0; g < G; ++g) {
+      const int s = g & 1;
       bool ok = true;
-      if (lane == 0) ok = t_wait(&tempty[s], (uint32_t)(((g / kWSlots) & 1) ^ 1), &abort_flag, status);
+      if (lane == 0) ok = t_wait(&tempty[s], (uint32_t)(((g >> 1) & 1) ^ 1), &abort_flag, status);
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (!ok) break;
       fence_after_sync();
@@ -1676,11 +1688,12 @@ __global__ void __maxnreg__(128) k_tc_ws(const __grid_constant__ Prob pb, int *s
     uint32_t bphase = 0;
     bool ok = my_tiles == 0 || t_wait(&bbar, bphase, &abort_flag, status);
     bphase ^= 1;
-    long g = 0;
+    int g = 0;
     for (int lt = 0; lt < my_tiles && ok; ++lt) {
       const int t = tile0 + lt * tile_step, a = lt & 1;
       const int batch = t / tiles_per_batch;
-      if (batch != cur_batch) { /* every MMA reading the old operator completes, then restage */
+      if (batch != cur_batch && pb.wsb_stride != 0) { /* the MMAs reading the old operator
+                                                        * complete, then the new one is staged */
         mma_commit(&bbar);
         ok = t_wait(&bbar, bphase, &abort_flag, status);
         bphase ^= 1;
@@ -1697,8 +1710,8 @@ __global__ void __maxnreg__(128) k_tc_ws(const __grid_constant__ Prob pb, int *s
       fence_after_sync();
       const uint32_t d = tmem + (uint32_t)(a * acc_cols);
       for (int j = 0; j < nsl; ++j, ++g) {
-        const int s = (int)(g % kWSlots);
-        ok = t_wait(&tfull[s], (uint32_t)((g / kWSlots) & 1), &abort_flag, status);
+        const int s = g & 1;
+        ok = t_wait(&tfull[s], (uint32_t)((g >> 1) & 1), &abort_flag, status);
         if (!ok) break;
         fence_after_sync();
         const int k0 = j * kWKs;
