@@ -485,6 +485,7 @@ struct TcBase {
   long bstride;
   const float *wsb; /* warp-specialised form: operator of batch z at wsb + z * wsb_stride */
   long wsb_stride;
+  int nap; /* ns an epilogue warp sleeps between failed polls (producers nap / 4, MMA nap / 8) */
   int yoff[4]; /* TMA-fed form: row offset of chunk c's 2-D block (chunk c of row r = row r + yoff[c]) */
   static constexpr bool kEpiAlternate = false; /* row-form epilogue: one half of N per warp */
   __device__ bool wraps(int, long) const { return false; }
@@ -748,10 +749,21 @@ template <class Prob> static bool tc_form_fits(const Prob &pb) {
          pb.kpad <= tc::kTKs * tc::kTMaxSteps && tc::t_smem_bytes(pb.kpad) <= (size_t)220 * 1024;
 }
 
+static int ws_nap_ns() {
+  static int v = -1;
+  if (v < 0) {
+    const char *ev = getenv("FMMFFT_WS_NAP");
+    v = ev ? atoi(ev) : 256;
+    if (v < 0 || v > 100000) v = 256;
+  }
+  return v;
+}
+
 template <class Prob>
 static void launch_tc(const Prob &pb0, int num_sms, int *status, cudaStream_t st, int form, int pdl,
                       int bf16 = 0) {
   Prob pb = pb0;
+  pb.nap = ws_nap_ns();
   if (bf16) form = 4; /* BF16x3 exists in the warp-specialised form only */
   if (form == 4 && tc::ws_fits(pb.kpad, pb.npad)) {
     const long tiles = (pb.rows + tc::kRows - 1) / tc::kRows * pb.batches;

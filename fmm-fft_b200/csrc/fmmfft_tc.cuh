@@ -765,6 +765,31 @@ __device__ __forceinline__ bool t_wait(uint64_t *bar, uint32_t parity, volatile 
   }
 }
 
+/* t_wait that sleeps nap_ns between polls once the first few have failed, so that a warp
+ * waiting for long (an epilogue warp for its next tile) leaves its sub-partition's issue slots to
+ * the warps that have work; nap_ns = 0 polls without sleeping. */
+__device__ __forceinline__ bool t_wait_nap(uint64_t *bar, uint32_t parity, volatile int *abort_flag,
+                                           int *status, unsigned nap_ns) {
+  if (nap_ns == 0) return t_wait(bar, parity, abort_flag, status);
+  unsigned long long t0 = 0;
+  for (unsigned it = 0;; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (it < 4) continue;
+    __nanosleep(nap_ns);
+    if ((it & 15) == 15 && *abort_flag) return false;
+    if ((it & 63) == 63) {
+      const unsigned long long now = global_ns();
+      if (t0 == 0) {
+        t0 = now;
+      } else if (now - t0 > kWaitNs) {
+        atomicExch(status, kErrWaitTimeout);
+        *abort_flag = 1;
+        return false;
+      }
+    }
+  }
+}
+
 /* Waits for phase `parity` of `bar` for at most about 2 s, whatever the abort flag says. */
 __device__ __forceinline__ bool t_wait_time(uint64_t *bar, uint32_t parity) {
   unsigned long long t0 = 0;
@@ -1624,7 +1649,7 @@ __global__ void __maxnreg__(128) k_tc_ws(const __grid_constant__ Prob pb, int *s
     for (int g = 0; g < G; ++g) {
       const int s = g & 1;
       bool ok = true;
-      if (lane == 0) ok = t_wait(&tempty[s], (uint32_t)(((g >> 1) & 1) ^ 1), &abort_flag, status);
+      if (lane == 0) ok = t_wait_nap(&tempty[s], (uint32_t)(((g >> 1) & 1) ^ 1), &abort_flag, status, pb.nap / 4);
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (!ok) break;
       fence_after_sync();
@@ -1658,7 +1683,7 @@ __global__ void __maxnreg__(128) k_tc_ws(const __grid_constant__ Prob pb, int *s
     for (int lt = 0; lt < my_tiles; ++lt) {
       const int t = tile0 + lt * tile_step, a = lt & 1;
       bool ok = true;
-      if (lane == 0) ok = t_wait(&afull[a], (uint32_t)((lt >> 1) & 1), &abort_flag, status);
+      if (lane == 0) ok = t_wait_nap(&afull[a], (uint32_t)((lt >> 1) & 1), &abort_flag, status, pb.nap);
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (!ok) break;
       fence_after_sync();
@@ -1705,13 +1730,13 @@ __global__ void __maxnreg__(128) k_tc_ws(const __grid_constant__ Prob pb, int *s
         if (!ok) break;
         cur_batch = batch;
       }
-      ok = t_wait(&aempty[a], (uint32_t)(((lt >> 1) & 1) ^ 1), &abort_flag, status);
+      ok = t_wait_nap(&aempty[a], (uint32_t)(((lt >> 1) & 1) ^ 1), &abort_flag, status, pb.nap / 8);
       if (!ok) break;
       fence_after_sync();
       const uint32_t d = tmem + (uint32_t)(a * acc_cols);
       for (int j = 0; j < nsl; ++j, ++g) {
         const int s = g & 1;
-        ok = t_wait(&tfull[s], (uint32_t)((g >> 1) & 1), &abort_flag, status);
+        ok = t_wait_nap(&tfull[s], (uint32_t)((g >> 1) & 1), &abort_flag, status, pb.nap / 8);
         if (!ok) break;
         fence_after_sync();
         const int k0 = j * kWKs;
