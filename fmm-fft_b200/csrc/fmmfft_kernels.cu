@@ -43,7 +43,6 @@
 #include <new>
 
 #include "fmmfft_internal.h"
-#include <cudaTypedefs.h>
 #include "fmmfft_tc.cuh"
 
 #define FMM_CUDA_TRY(call)                                                              \
@@ -152,9 +151,9 @@ template <typename R> struct Dev {
   int ok_s2m, ok_m2m, ok_m2l, ok_leaf;
   long tc_min_rows; /* stages with fewer rows use the CUDA-core kernel */
   int fft_threads;  /* threads per block of the register FFT pass (power of two, <= 512) */
-  /* tensor-core form: 0 row (32 lanes), 1 pipelined, 2 TMA-fed, 3 row (16 lanes); -1 (default)
-   * per stage, as measured fastest: S2M and M2M the 16-lane row form, M2L and the leaf the
-   * 32-lane one (the same speed for M2L, faster and more accurate for the leaf) */
+  /* tensor-core kernel: 0 row form (32 lanes), 3 row form (16 lanes), 4 warp-specialised; -1
+   * per stage: S2M and M2M the 16-lane row form, M2L and the leaf the 32-lane one.  The autotuner
+   * chooses among -1, 3 and 4; BF16x3 plans always use 4 (the only BF16x3 kernel). */
   int tc_form;
   int bf16;    /* FMMFFT_BF16X3: the tensor-core stages in BF16x3 instead of split TF32 */
   int pdl;     /* row-form launches as programmatic dependent launches (FMMFFT_PDL=0: off) */
@@ -165,7 +164,7 @@ template <typename R> struct Dev {
   unsigned env_set; /* knobs an environment switch fixed (the autotuner leaves them): bits below */
   int tuned;        /* the knobs come from the autotuner */
 };
-enum { KNOB_FFT = 1, KNOB_COARSE = 2, KNOB_TCMIN = 4, KNOB_FUSE = 8 };
+enum { KNOB_FFT = 1, KNOB_COARSE = 2, KNOB_TCMIN = 4, KNOB_FUSE = 8, KNOB_FORM = 16 };
 
 /* Instantiated CUDA graphs of one plan's execute, keyed by (input, output, direction): the
  * ~35 kernel launches of a transform become one graph launch. */
@@ -486,9 +485,7 @@ struct TcBase {
   const float *wsb; /* warp-specialised form: operator of batch z at wsb + z * wsb_stride */
   long wsb_stride;
   int nap; /* ns an epilogue warp sleeps between failed polls (producers nap / 4, MMA nap / 8) */
-  int yoff[4]; /* TMA-fed form: row offset of chunk c's 2-D block (chunk c of row r = row r + yoff[c]) */
   static constexpr bool kEpiAlternate = false; /* row-form epilogue: one half of N per warp */
-  __device__ bool wraps(int, long) const { return false; }
   /* output columns c0..c0+7 of a row into dst (columns below nout; nout a multiple of 4) */
   __device__ void put8(float *dst, long, int, int c0, const float *t) const {
     if (c0 + 8 <= nout) {
@@ -533,12 +530,6 @@ struct TcM2L : TcBase {
     return phi + (base + box) * T;
   }
   __device__ float *dst(long r, int) const { return out + r * 2 * T; }
-  /* chunks 1 and 2 (the neighbour pairs) wrap around within a section at its first / last
-   * parent; the TMA's 2-D block has the neighbouring section's pair there */
-  __device__ bool wraps(int c, long r) const {
-    const long Bx = r & ((1L << lpar) - 1);
-    return (c == 1 && Bx == 0) || (c == 2 && Bx == (1L << lpar) - 1);
-  }
 };
 
 /* Leaf far field + near field of one section per batch (reference fmmfft.c:751-954).  The
@@ -693,62 +684,6 @@ template <class Prob> static size_t tc_smem_bytes(const Prob &pb) {
   return tc::smem_bytes(pb.kpad, pb.npad);
 }
 
-/* cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link). */
-static PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static int tried = 0;
-  if (!tried) {
-    tried = 1;
-    void *p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-  }
-  return fn;
-}
-
-/* 2-D FP32 tensor map: `rows` rows of `width` floats, `pitch` floats apart, read as boxes of
- * the full width x tc::kMRows rows (no swizzle; rows outside the tensor read as zero). */
-static bool tma_map(CUtensorMap *m, const float *base, int width, long rows, long pitch) {
-  PFN_cuTensorMapEncodeTiled_v12000 enc = tma_encoder();
-  if (!enc || width > 256 || (width * 4) % 16 != 0 || (pitch * 4) % 16 != 0 ||
-      ((uintptr_t)base & 15) != 0)
-    return false;
-  cuuint64_t dims[2] = {(cuuint64_t)width, (cuuint64_t)rows};
-  cuuint64_t strides[1] = {(cuuint64_t)pitch * 4};
-  cuuint32_t box[2] = {(cuuint32_t)width, (cuuint32_t)tc::kMRows};
-  cuuint32_t es[2] = {1, 1};
-  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)base, dims, strides, box, es,
-             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
-
-/* Tensor maps of each problem's A chunks (and their row offsets), for the TMA-fed form. */
-static bool tma_maps(TcS2M &q, tc::TmaMaps *m) {
-  q.yoff[0] = 0;
-  return tma_map(&m->m[0], q.xt + 2 * q.M, q.b, q.rows, q.b);
-}
-static bool tma_maps(TcM2M &q, tc::TmaMaps *m) {
-  q.yoff[0] = 0;
-  return tma_map(&m->m[0], q.child, 2 * q.T, q.rows, 2 * q.T);
-}
-static bool tma_maps(TcM2L &q, tc::TmaMaps *m) {
-  /* chunk 0: the parent's local expansion; chunks 1, 2: pairs of child boxes (2B-2, 2B-1) and
-   * (2B+2, 2B+3) = pair rows r - 1 and r + 1 of the child level read as pairs */
-  q.yoff[0] = 0, q.yoff[1] = -1, q.yoff[2] = 1;
-  return tma_map(&m->m[0], q.psi_par, q.T, q.rows, q.T) &&
-         tma_map(&m->m[1], q.phi, 2 * q.T, q.rows, 2 * q.T) && tma_map(&m->m[2], q.phi, 2 * q.T, q.rows, 2 * q.T);
-}
-static bool tma_maps(TcLeaf &, tc::TmaMaps *) { return false; }
-
-/* The pipelined form (tc::k_tc_rowgemm_t) takes one operator of at most 64 outputs for all
- * rows and K <= 256 within 220 KB of shared memory; everything else runs the row form. */
-template <class Prob> static bool tc_form_fits(const Prob &pb) {
-  return pb.batches == 1 && pb.npad <= 64 && pb.nout <= 64 && pb.kpad % 8 == 0 &&
-         pb.kpad <= tc::kTKs * tc::kTMaxSteps && tc::t_smem_bytes(pb.kpad) <= (size_t)220 * 1024;
-}
-
 static int ws_nap_ns() {
   static int v = -1;
   if (v < 0) {
@@ -765,6 +700,7 @@ static void launch_tc(const Prob &pb0, int num_sms, int *status, cudaStream_t st
   Prob pb = pb0;
   pb.nap = ws_nap_ns();
   if (bf16) form = 4; /* BF16x3 exists in the warp-specialised form only */
+  if (!tc::ws_fits(pb.kpad, pb.npad)) form = form == 4 ? 0 : form;
   if (form == 4 && tc::ws_fits(pb.kpad, pb.npad)) {
     const long tiles = (pb.rows + tc::kRows - 1) / tc::kRows * pb.batches;
     const int grid = (int)(tiles < num_sms ? tiles : num_sms); /* one CTA per SM: all of TMEM */
@@ -783,26 +719,6 @@ static void launch_tc(const Prob &pb0, int num_sms, int *status, cudaStream_t st
       cudaLaunchKernelEx(&cfg, tc::k_tc_ws<Prob, true>, pb, status);
     else
       cudaLaunchKernelEx(&cfg, tc::k_tc_ws<Prob, false>, pb, status);
-    return;
-  }
-  if (form == 2 && pb.batches == 1 && pb.npad <= 64 && pb.nout <= 64 && pb.kpad % 8 == 0 &&
-      pb.kpad <= 256) {
-    const int stages = tc::m_smem_bytes(pb.kpad, 4) <= (size_t)220 * 1024 ? 4 : 2;
-    tc::TmaMaps maps;
-    memset((void *)&maps, 0, sizeof maps);
-    if (tc::m_smem_bytes(pb.kpad, stages) <= (size_t)220 * 1024 && tma_maps(pb, &maps)) {
-      const long tiles = (pb.rows + tc::kMRows - 1) / tc::kMRows;
-      const int grid = (int)(tiles < num_sms ? tiles : num_sms); /* one CTA per SM: all of TMEM */
-      tc::k_tc_tma<Prob><<<grid, tc::kMThreads, tc::m_smem_bytes(pb.kpad, stages), st>>>(pb, maps, stages,
-                                                                                       status);
-      return;
-    }
-  }
-  const int pipelined = form == 1;
-  if (pipelined && tc_form_fits(pb)) {
-    const long tiles = (pb.rows + tc::kTRows - 1) / tc::kTRows;
-    const int grid = (int)(tiles < num_sms ? tiles : num_sms); /* one CTA per SM: all of TMEM */
-    tc::k_tc_rowgemm_t<Prob><<<grid, tc::kTThreads, tc::t_smem_bytes(pb.kpad), st>>>(pb, status);
     return;
   }
   long tiles = (pb.rows + tc::kRows - 1) / tc::kRows * pb.batches;
@@ -2046,7 +1962,8 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
    * the default because it is faster there (M2L 0.47 ms against 0.58 ms on a B200) */
   d->tc_form = -1;
   if (const char *ev = getenv("FMMFFT_TC_FORM"))
-    d->tc_form = strcmp(ev, "pipelined") == 0 ? 1 : strcmp(ev, "tma") == 0 ? 2 : strcmp(ev, "row") == 0 ? 0 : strcmp(ev, "row16") == 0 ? 3 : strcmp(ev, "ws") == 0 ? 4 : -1;
+    d->tc_form = strcmp(ev, "row") == 0 ? 0 : strcmp(ev, "row16") == 0 ? 3 : strcmp(ev, "ws") == 0 ? 4 : -1,
+    d->env_set |= KNOB_FORM;
   d->pdl = 1;
   if (const char *ev = getenv("FMMFFT_PDL")) d->pdl = atoi(ev) != 0;
   coarse_setup(d);
@@ -2310,7 +2227,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.kpad = d->kp_s2m, q.npad = d->np_s2m, q.nout = (int)T;
         q.bhi = d->tc_s2m[0], q.blo = d->tc_s2m[1], q.bstride = 0, q.wsb = d->ws_s2m, q.wsb_stride = 0;
         q.xt = d->xt, q.out = d->phi + lvl_off(n, S1e, T), q.M = M, q.b = (int)b, q.T = (int)T;
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 4 : d->tc_form, d->pdl, d->bf16);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 3 : d->tc_form, d->pdl, d->bf16);
         done = true;
       }
     }
@@ -2345,7 +2262,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.bhi = d->tc_m2m[0] + (L - 2) * d->tc_m2m_stride, q.blo = d->tc_m2m[1] + (L - 2) * d->tc_m2m_stride;
         q.bstride = 0, q.wsb = d->ws_m2m + (L - 2) * d->ws_m2m_stride, q.wsb_stride = 0;
         q.child = d->phi + lvl_off(L + 1, S1e, T), q.out = d->phi + lvl_off(L, S1e, T), q.T = (int)T;
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 4 : d->tc_form, d->pdl, d->bf16);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 3 : d->tc_form, d->pdl, d->bf16);
         done = true;
       }
     }
@@ -2384,7 +2301,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.bstride = 0, q.wsb = d->ws_m2l + (l - 3) * d->ws_m2l_stride, q.wsb_stride = 0;
         q.psi_par = d->psi + lvl_off(l - 1, S1e, T), q.phi = d->phi + lvl_off(l, S1e, T);
         q.out = d->psi + lvl_off(l, S1e, T), q.T = (int)T, q.lpar = (int)(l - 1);
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 4 : d->tc_form, d->pdl, d->bf16);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 0 : d->tc_form, d->pdl, d->bf16);
         done = true;
       }
     }
@@ -2420,7 +2337,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.fixbuf = d->leaf_fix, q.P = (int)P;
         q.psi_n = pb.psi_n, q.xt = d->xt, q.u = d->u, q.M = M, q.s = s, q.T = (int)T, q.b = (int)b;
         q.log2s = (int)n;
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 4 : d->tc_form, d->pdl, d->bf16);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 0 : d->tc_form, d->pdl, d->bf16);
         done = true;
       }
     }
@@ -2565,6 +2482,7 @@ struct TuneKey { /* the capacity is not part of it: a batch must take its transf
 struct TuneVal {
   int fft_threads, fuse_s2m;
   long coarse_rows, tc_min_rows;
+  int tc_form;
 };
 static std::mutex g_tune_mu;
 static TuneKey g_tune_key[256];
@@ -2576,6 +2494,7 @@ template <typename R> static void tune_apply(Dev<R> *d, const TuneVal &v) {
   if (!(d->env_set & KNOB_FUSE)) d->fuse_s2m = v.fuse_s2m;
   if (!(d->env_set & KNOB_COARSE)) d->coarse_rows = v.coarse_rows;
   if (!(d->env_set & KNOB_TCMIN)) d->tc_min_rows = v.tc_min_rows;
+  if (!(d->env_set & KNOB_FORM)) d->tc_form = v.tc_form;
   d->tuned = 1;
 }
 
@@ -2613,7 +2532,10 @@ static int dev_autotune(Dev<R> *d, char *err, size_t errlen) {
     }
     return best;
   };
-  TuneVal cur{d->fft_threads, d->fuse_s2m, d->coarse_rows, d->tc_min_rows};
+  TuneVal cur;
+  memset(&cur, 0, sizeof cur);
+  cur.fft_threads = d->fft_threads, cur.fuse_s2m = d->fuse_s2m, cur.coarse_rows = d->coarse_rows;
+  cur.tc_min_rows = d->tc_min_rows, cur.tc_form = d->tc_form;
   float best = measure();
   auto knob = [&](unsigned bit, auto set, const long *vals, int nv) {
     if (d->env_set & bit) return;
@@ -2629,12 +2551,16 @@ static int dev_autotune(Dev<R> *d, char *err, size_t errlen) {
     cur = keep;
     tune_apply(d, cur);
   };
+  if (d->tc && !d->bf16) { /* tensor-core kernel: per-stage row forms, 16-lane everywhere, warp-specialised */
+    const long v[] = {-1, 3, 4};
+    knob(KNOB_FORM, [](TuneVal &c, long x) { c.tc_form = (int)x; }, v, 3);
+  }
   if (d->tc) {
     const long v[] = {1024, 4096, 16384};
     knob(KNOB_TCMIN, [](TuneVal &c, long x) { c.tc_min_rows = x; }, v, 3);
   }
   if (d->coarse_grid >= 1) {
-    const long v[] = {0, 2048, 4096, 8192};
+    const long v[] = {0, 2048, 4096, 8192, 16384};
     knob(KNOB_COARSE, [](TuneVal &c, long x) { c.coarse_rows = x; }, v, 4);
   }
   if (d->tileM % d->b == 0 && d->T % 4 == 0) {
@@ -2703,12 +2629,6 @@ static int set_smem_limits(void) {
   allow_dyn_smem(tc::k_tc_rowgemm16<TcM2M>, lim);
   allow_dyn_smem(tc::k_tc_rowgemm16<TcM2L>, lim);
   allow_dyn_smem(tc::k_tc_rowgemm16<TcLeaf>, lim);
-  allow_dyn_smem(tc::k_tc_rowgemm_t<TcS2M>, lim);
-  allow_dyn_smem(tc::k_tc_rowgemm_t<TcM2M>, lim);
-  allow_dyn_smem(tc::k_tc_rowgemm_t<TcM2L>, lim);
-  allow_dyn_smem(tc::k_tc_tma<TcS2M>, lim);
-  allow_dyn_smem(tc::k_tc_tma<TcM2M>, lim);
-  allow_dyn_smem(tc::k_tc_tma<TcM2L>, lim);
   allow_dyn_smem(tc::k_tc_ws<TcS2M>, lim);
   allow_dyn_smem(tc::k_tc_ws<TcM2M>, lim);
   allow_dyn_smem(tc::k_tc_ws<TcM2L>, lim);

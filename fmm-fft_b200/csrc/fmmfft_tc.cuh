@@ -1,36 +1,29 @@
 /*
- * tcgen05 (5th-generation tensor core) form of the FMM tree contractions, sm_100a.
+ * tcgen05 (5th-generation tensor core) kernels of the FMM tree and leaf contractions, sm_100a.
  *
  * Every tree stage is D[r][0..N) = sum_k A(r, k) B[k][0..N) over many rows r (section, re/im
- * plane, box) with a small shared operator B (see fmmfft_kernels.cu).  This kernel runs that
- * contraction on the tensor cores in 4xTF32: each FP32 operand is split into a TF32 "hi" part
- * (round to nearest) and the TF32-rounded residual "lo", and the four products A_hi B_hi +
- * A_hi B_lo + A_lo B_hi + A_lo B_lo are accumulated in FP32 in tensor memory (TMEM); the
- * rounding of the residuals leaves about 2^-22 relative error per product.
+ * plane, box) with a small shared operator B (see fmmfft_kernels.cu).  The kernels run that
+ * contraction on the tensor cores with each FP32 operand split into a hi part and the rounding of
+ * the remainder lo, products accumulated in FP32 in tensor memory (TMEM):
  *
- * Per CTA (256 threads, two CTAs per SM, persistent over 128-row tiles), per K slice of up to
- * 64 columns:
- *   1. every thread loads its part of one tile row from HBM into registers, splits it into TF32
- *      hi and lo, and writes both into the row's TMEM lane (tcgen05.st);
- *   2. one thread issues 3 * slice/8 tcgen05.mma (M = 128, N = Npad, K = 8; A from TMEM, B from
- *      shared memory in the canonical K-major no-swizzle layout) into one TMEM accumulator and
- *      commits them to an mbarrier;
- * then every warp reads its 32 TMEM lanes (= its 32 rows) with tcgen05.ld and stores them.
- * B (hi/lo, pre-split on the host) is staged once per CTA, or once per section for the leaf.
- * Waits on the mbarrier are bounded; on expiry the CTA records an error code and leaves.
+ *   k_tc_rowgemm    row form: A loaded by every thread into registers, split into TF32 hi / lo,
+ *                   written into the row's TMEM lane (tcgen05.st); one thread issues the MMAs
+ *                   (A from TMEM, B from shared memory), four products (4xTF32); two CTAs per
+ *                   SM, persistent over 128-row tiles, 64-column K steps;
+ *   k_tc_rowgemm16  the same with the 16x256b TMEM shape (K and N permuted within 16-column
+ *                   groups, so a thread moves four consecutive columns with one float4);
+ *   k_tc_ws         warp-specialised: producer warps copy A through a shared-memory ring into
+ *                   TMEM slots, one thread issues the MMAs (three products), epilogue warps drain
+ *                   two accumulators; split TF32 or BF16x3 (the only kernel for BF16x3).
+ *
+ * The autotuner picks among them per plan shape.  Every mbarrier wait is bounded; on expiry the
+ * CTA records an error code, stops and frees its tensor memory.
  */
 #pragma once
-#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 namespace tc {
-
-/* Optional per-role cycle counters: empty unless a build defines them. */
-#ifndef TC_PHASE
-#define TC_CLOCK(tp)
-#define TC_PHASE(slot, tp)
-#endif
 
 constexpr int kRows = 128;         /* MMA M, rows per tile */
 
@@ -364,12 +357,10 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
   pdl_wait();
   if (tile < tile_end) load_step(tile, 0);
   while (tile < tile_end) {
-    TC_CLOCK(tp);
     const int batch = tile / tiles_per_batch;
     const long r0 = (long)(tile - batch * tiles_per_batch) * kRows;
     const int k0 = slice * ks, k1 = k0 + ks;
     if (batch != cur_batch) stage_b(batch); /* the previous step's MMAs have completed */
-    TC_PHASE(0, tp); /* operator staging */
     /* split into TF32 hi / lo and write both into this thread's TMEM lane */
     if (my_half * 32 < ks) {
       float h[32], l[32];
@@ -390,12 +381,9 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
         tmem_st8(t_alo + lane_addr + col + 8 * q, l + 8 * q);
       }
     }
-    TC_PHASE(1, tp); /* split + tcgen05.st issue */
     tmem_st_wait();
-    TC_PHASE(2, tp); /* wait::st */
     fence_before_sync();
     __syncthreads();
-    TC_PHASE(3, tp); /* barrier A */
     if (warp == 0) { /* lane 0 issues; the rest of warp 0 waits at __syncwarp */
       if (lane == 0) {
         fence_after_sync();
@@ -414,13 +402,11 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
       }
       __syncwarp();
     }
-    TC_PHASE(4, tp); /* MMA issue (warp 0) */
     /* next step: its loads go out while the MMAs (and at a tile's end the epilogue) run */
     const bool last_slice = slice == nslices - 1;
     const int ntile = last_slice ? tile + tile_step : tile;
     const int nslice = last_slice ? 0 : slice + 1;
     if (ntile < tile_end) load_step(ntile, nslice);
-    TC_PHASE(5, tp); /* next loads issue */
     /* one thread polls the mbarrier; the other warps wait at the CTA barrier */
     if (tid == 0 && !mbar_wait_bounded(&mbar, phase)) {
       atomicExch(status, kErrWaitTimeout);
@@ -429,7 +415,6 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
     phase ^= 1;
     __syncthreads();
     fence_after_sync();
-    TC_PHASE(6, tp); /* MMA wait + barrier B */
     if (abort_flag) break;
     if (last_slice) {
       /* epilogue: this warp's TMEM lanes (= tile rows), columns of half (w / 4) of padded N */
@@ -450,7 +435,6 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
       }
       fence_before_sync();
       __syncthreads();
-      TC_PHASE(7, tp); /* epilogue */
     }
     tile = ntile, slice = nslice;
   }
@@ -698,41 +682,8 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm16(const __grid_constant__
 }
 
 
-/* ======================================================================== pipelined form */
-
-/* The same contraction with the roles of the operands exchanged, for operators of at most 64
- * outputs shared by all rows (one batch): the tensor core computes D = Op X^T with
- *   Op (MMA M = 128): rows 0..63 the operator's TF32 hi part, rows 64..127 its lo part;
- *   X  (MMA N = 256): 256 data rows of the tile, as TF32 hi or lo (two MMAs per K step);
- * so that D[n][c] + D[64 + n][c] = sum over the four hi/lo products of output n of data row c
- * (the lo*lo product too: 4xTF32).  Each MMA is M = 128, N = 256, K = 8, five times the work of
- * the row form's M = 128, N = 48 instruction.  One CTA per SM, warp-specialised:
- *   warps 0-7  producers: thread p loads data row p of the tile from HBM (16 K columns per
- *              stage, four stages of loads in flight), splits it into TF32 hi / lo and writes
- *              both into a shared-memory stage in the K-major no-swizzle layout; kTStages
- *              stages in a ring (mbarriers full / empty);
- *   warps 8-15 epilogue: two per TMEM lane quarter q = warp & 3; per 32 rows the hi quarters
- *              0-1 and the lo quarters 2-3 write their columns into two staging blocks in
- *              shared memory, which all eight warps add and store with float4 (Prob::dst(r)
- *              must be dst(0) + r * nout: rows stored back to back, as every tree stage
- *              stores them);
- *   warp 16    one thread issues the MMAs into one of two TMEM accumulators of 256 columns
- *              (mbarriers dfull / dempty), so the epilogue of a tile overlaps the next tile.
- * Every wait is bounded by the global timer; on expiry the CTA records kErrWaitTimeout, every
- * role leaves its loop, the MMA thread waits (bounded) for its MMAs in flight, and TMEM is
- * freed. */
-constexpr int kTRows = 256;     /* data rows per tile: MMA N */
-constexpr int kTKs = 16;        /* K columns per stage */
-constexpr int kTStages = 4;     /* shared-memory stages in the ring */
-constexpr int kTProd = 8;       /* producer warps: one thread per data row */
-constexpr int kTEpi = 8;        /* epilogue warps: two per TMEM lane quarter */
-constexpr int kTThreads = (kTProd + kTEpi + 1) * 32;
-constexpr int kTMaxSteps = 16;  /* K <= 256 */
 constexpr unsigned long long kWaitNs = 2000000000ull; /* 2 s per wait */
 
-__host__ __device__ constexpr size_t t_smem_bytes(int kpad) {
-  return (size_t)128 * kpad * 4 + (size_t)kTStages * 2 * kTRows * kTKs * 4 + (size_t)2 * 32 * 64 * 4;
-}
 
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
@@ -803,321 +754,6 @@ __device__ __forceinline__ bool t_wait_time(uint64_t *bar, uint32_t parity) {
   }
 }
 
-__device__ __forceinline__ void named_bar(int id, int nthreads) {
-  asm volatile("bar.sync %0, %1;" : : "r"(id), "r"(nthreads) : "memory");
-}
-
-/* Barrier `id` over `nthreads` threads that also ANDs a flag across them: every participant
- * gets the same answer, so they all take the same branch afterwards. */
-__device__ __forceinline__ bool named_bar_and(int id, int nthreads, bool v) {
-  uint32_t r;
-  asm volatile(
-      "{\n\t.reg .pred p, q;\n\t"
-      "setp.ne.u32 p, %1, 0;\n\t"
-      "bar.red.and.pred q, %2, %3, p;\n\t"
-      "selp.u32 %0, 1, 0, q;\n\t}\n"
-      : "=r"(r)
-      : "r"((uint32_t)v), "r"(id), "r"(nthreads)
-      : "memory");
-  return r != 0;
-}
-
-/* 16 consecutive TMEM columns of this thread's lane (two x8 loads, one wait). */
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
-  uint32_t r[16];
-#pragma unroll
-  for (int q = 0; q < 2; ++q)
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-        : "=r"(r[8 * q]), "=r"(r[8 * q + 1]), "=r"(r[8 * q + 2]), "=r"(r[8 * q + 3]),
-          "=r"(r[8 * q + 4]), "=r"(r[8 * q + 5]), "=r"(r[8 * q + 6]), "=r"(r[8 * q + 7])
-        : "r"(taddr + 8 * q)
-        : "memory");
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-/* 32 consecutive TMEM columns of this thread's lane (four x8 loads, one wait). */
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
-  uint32_t r[32];
-#pragma unroll
-  for (int q = 0; q < 4; ++q)
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-        : "=r"(r[8 * q]), "=r"(r[8 * q + 1]), "=r"(r[8 * q + 2]), "=r"(r[8 * q + 3]),
-          "=r"(r[8 * q + 4]), "=r"(r[8 * q + 5]), "=r"(r[8 * q + 6]), "=r"(r[8 * q + 7])
-        : "r"(taddr + 8 * q)
-        : "memory");
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-
-template <class Prob>
-__global__ void __launch_bounds__(kTThreads, 1) k_tc_rowgemm_t(const __grid_constant__ Prob pb, int *status) {
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
-  __shared__ uint64_t full[kTStages], empty[kTStages], dfull[2], dempty[2], fin;
-  __shared__ uint32_t tmem_slot;
-  __shared__ volatile int abort_flag;
-  __shared__ int lmap[kTMaxSteps][4]; /* per step and float4: chunk (low byte, 0xFF none), offset */
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int kpad = pb.kpad, nsteps = (kpad + kTKs - 1) / kTKs;
-  float *Op = reinterpret_cast<float *>(smem_raw);
-  float *Xs = Op + 128 * kpad;                    /* stage s: hi, then lo */
-  float *xch = Xs + kTStages * 2 * kTRows * kTKs; /* epilogue staging: hi, lo [32 rows][nout] */
-  const int mma_warp = kTProd + kTEpi;
-  if (warp == mma_warp) tmem_alloc(&tmem_slot, 512);
-  if (tid == 0) {
-    for (int i = 0; i < kTStages; ++i) mbar_init(&full[i], kTProd), mbar_init(&empty[i], 1);
-    for (int i = 0; i < 2; ++i) mbar_init(&dfull[i], 1), mbar_init(&dempty[i], kTEpi);
-    mbar_init(&fin, 1);
-    fence_mbar_init();
-    abort_flag = 0;
-  }
-  if (tid < kTMaxSteps * 4) {
-    const int st = tid >> 2, i = tid & 3, k = st * kTKs + 4 * i;
-    int e = 0xFF;
-    if (k < kpad)
-      for (int c = 0; c < pb.nchunks; ++c)
-        if (k >= pb.coff[c] && k < pb.coff[c] + pb.clen[c]) e = c | ((k - pb.coff[c]) << 8);
-    lmap[st][i] = e;
-  }
-  /* operator: hi in rows 0..npad-1, lo in rows 64..64+npad-1, zero elsewhere (loads issued
-   * 8 at a time before their stores) */
-  for (int e0 = tid; e0 < 128 * kpad; e0 += 8 * (int)blockDim.x) {
-    float v[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int e = e0 + u * blockDim.x, m = e / kpad, k = e - m * kpad;
-      float x = 0.f;
-      if (e < 128 * kpad) {
-        if (m < pb.npad) x = pb.bhi[(long)m * kpad + k];
-        else if (m >= 64 && m - 64 < pb.npad) x = pb.blo[(long)(m - 64) * kpad + k];
-      }
-      v[u] = x;
-    }
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int e = e0 + u * blockDim.x, m = e / kpad, k = e - m * kpad;
-      if (e < 128 * kpad) Op[core_off(m, k, kpad) >> 2] = v[u];
-    }
-  }
-  fence_smem_to_async();
-  fence_before_sync();
-  __syncthreads();
-  fence_after_sync();
-  const uint32_t tmem = tmem_slot;
-  const long ntiles = (pb.rows + kTRows - 1) / kTRows;
-
-  if (warp < kTProd) {
-    /* ------------------------------------------------------------ producers */
-    /* thread p fills data row p of the tile: 16 K columns (4 float4) per stage, with four
-     * stages of loads in flight (a register ring, the loop unrolled by four so that its
-     * indices stay static) */
-    const int p = tid;
-    const uint32_t xs0 = smem_addr(Xs);
-    long ltile = blockIdx.x; /* load cursor, four stages ahead of the store cursor */
-    int lst = 0;
-    const float *rowp[4] = {nullptr, nullptr, nullptr, nullptr};
-    auto set_rows = [&]() {
-      const long r = ltile * kTRows + p;
-      const bool live = r < pb.rows;
-#pragma unroll
-      for (int c = 0; c < 4; ++c) rowp[c] = (live && c < pb.nchunks) ? pb.src(c, r, 0) : nullptr;
-    };
-    auto load = [&](float4 (&v)[4]) {
-      if (ltile >= ntiles) return;
-      if (lst == 0) set_rows();
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int e = lmap[lst][i], c = e & 0xFF;
-        v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (c != 0xFF) {
-          const float *rp = c == 0 ? rowp[0] : (c == 1 ? rowp[1] : (c == 2 ? rowp[2] : rowp[3]));
-          if (rp) v[i] = __ldg(reinterpret_cast<const float4 *>(rp + (e >> 8)));
-        }
-      }
-      if (++lst == nsteps) lst = 0, ltile += gridDim.x;
-    };
-    long tile = blockIdx.x;
-    int st = 0;
-    unsigned it = 0;
-    bool go = tile < ntiles;
-    /* one stage: wait for the ring slot, split the registers loaded four stages ago into
-     * TF32 hi / lo straight into it, refill them with the stage four ahead, signal */
-    auto step = [&](float4 (&v)[4]) {
-      if (!go) return;
-      TC_CLOCK(tp);
-      const int s = (int)(it % kTStages);
-      bool ok = true;
-      if (lane == 0) ok = t_wait(&empty[s], ((it / kTStages) & 1) ^ 1, &abort_flag, status);
-      ok = __shfl_sync(0xffffffffu, ok, 0);
-      if (!ok) {
-        go = false;
-        return;
-      }
-      TC_PHASE(2, tp);
-      const uint32_t hb = xs0 + (uint32_t)(s * 2 * kTRows * kTKs * 4), lb = hb + kTRows * kTKs * 4;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const uint32_t o = core_off(p, 4 * j, kTKs);
-        const float a0 = v[j].x, a1 = v[j].y, a2 = v[j].z, a3 = v[j].w;
-        const float h0 = tf32_rna(a0), h1 = tf32_rna(a1), h2 = tf32_rna(a2), h3 = tf32_rna(a3);
-        asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" : : "r"(hb + o), "f"(h0), "f"(h1),
-                     "f"(h2), "f"(h3) : "memory");
-        asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" : : "r"(lb + o), "f"(tf32_rna(a0 - h0)),
-                     "f"(tf32_rna(a1 - h1)), "f"(tf32_rna(a2 - h2)), "f"(tf32_rna(a3 - h3)) : "memory");
-      }
-      TC_PHASE(0, tp);
-      load(v);
-      TC_PHASE(1, tp);
-      fence_smem_to_async();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&full[s]);
-      TC_PHASE(3, tp);
-      ++it;
-      if (++st == nsteps) st = 0, tile += gridDim.x;
-      go = tile < ntiles;
-    };
-    float4 v0[4], v1[4], v2[4], v3[4];
-    load(v0), load(v1), load(v2), load(v3);
-    while (go) {
-      step(v0), step(v1), step(v2), step(v3);
-    }
-  } else if (warp < kTProd + kTEpi) {
-    /* ------------------------------------------------------------ epilogue */
-    /* per 32 rows: warp (q, h) reads lane quarter q, columns [16 h, 16 h + 16) of the chunk and
-     * writes them into staging block q / 2 (hi or lo) as [row][nout]; then all epilogue
-     * threads add the two blocks and store the rows' contiguous output with float4 */
-    const int q = warp & 3, h = (warp - kTProd) >> 2, et = tid - kTProd * 32;
-    const uint32_t lane_addr = (uint32_t)(q * 32) << 16;
-    const int nout = pb.nout;
-    const int n = (q & 1) * 32 + lane; /* output index of this lane (hi and lo quarters) */
-    float *stg = xch + (q >> 1) * 32 * 64;
-    unsigned tc = 0;
-    for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++tc) {
-      TC_CLOCK(tp);
-      const int b = (int)(tc & 1);
-      bool ok = true;
-      if (lane == 0) ok = t_wait(&dfull[b], (tc >> 1) & 1, &abort_flag, status);
-      ok = __shfl_sync(0xffffffffu, ok, 0);
-      /* all epilogue warps continue, or all leave (they meet at named barriers below) */
-      if (!named_bar_and(3, kTEpi * 32, ok)) break;
-      fence_after_sync();
-      TC_PHASE(4, tp);
-      for (int ch = 0; ch < kTRows / 32; ++ch) {
-        float t[16];
-        tmem_ld16(tmem + lane_addr + (uint32_t)(b * 256 + ch * 32 + h * 16), t);
-        if (n < nout) {
-#pragma unroll
-          for (int c = 0; c < 16; ++c) stg[(h * 16 + c) * nout + n] = t[c];
-        }
-        named_bar(1, kTEpi * 32);
-        const long rb = tile * kTRows + ch * 32;
-        const long nr = pb.rows - rb < 32 ? pb.rows - rb : 32;
-        if (nr > 0) {
-          float4 *g = reinterpret_cast<float4 *>(pb.dst(rb, 0));
-          const float4 *sh = reinterpret_cast<const float4 *>(xch);
-          const float4 *sl = reinterpret_cast<const float4 *>(xch + 32 * 64);
-          const int n4 = (int)nr * nout / 4;
-          for (int i = et; i < n4; i += kTEpi * 32) {
-            const float4 x = sh[i], y = sl[i];
-            g[i] = make_float4(x.x + y.x, x.y + y.y, x.z + y.z, x.w + y.w);
-          }
-        }
-        named_bar(1, kTEpi * 32);
-      }
-      fence_before_sync();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&dempty[b]);
-      TC_PHASE(5, tp);
-    }
-  } else {
-    if (lane == 0) {
-      /* ---------------------------------------------------------- MMA issue */
-      const uint32_t idesc = make_idesc_tf32(kTRows);
-      const uint32_t op = smem_addr(Op), xs0 = smem_addr(Xs);
-      const uint32_t op_sbo = (uint32_t)kpad * 32, x_sbo = (uint32_t)kTKs * 32;
-      unsigned it = 0, tc = 0;
-      bool ok = true;
-      for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++tc) {
-        TC_CLOCK(tp);
-        const int b = (int)(tc & 1);
-        ok = t_wait(&dempty[b], ((tc >> 1) & 1) ^ 1, &abort_flag, status);
-        if (!ok) break;
-        fence_after_sync();
-        TC_PHASE(6, tp);
-        const uint32_t d = tmem + (uint32_t)(b * 256);
-        for (int st = 0; st < nsteps; ++st, ++it) {
-          const int s = (int)(it % kTStages);
-          ok = t_wait(&full[s], (it / kTStages) & 1, &abort_flag, status);
-          if (!ok) break;
-          fence_after_sync();
-          TC_PHASE(7, tp);
-          const int k0 = st * kTKs;
-          const int ksteps = ((kpad - k0) < kTKs ? (kpad - k0) : kTKs) >> 3;
-          const uint32_t hb = xs0 + (uint32_t)(s * 2 * kTRows * kTKs * 4), lb = hb + kTRows * kTKs * 4;
-          for (int kk = 0; kk < ksteps; ++kk) {
-            const uint64_t da = make_desc(op + 256u * (uint32_t)((k0 >> 3) + kk), 128, op_sbo);
-            mma_tf32(d, da, make_desc(hb + 256u * kk, 128, x_sbo), idesc, (st | kk) != 0);
-            mma_tf32(d, da, make_desc(lb + 256u * kk, 128, x_sbo), idesc, 1);
-          }
-          mma_commit(&empty[s]);
-          TC_PHASE(8, tp);
-        }
-        if (!ok) break;
-        mma_commit(&dfull[b]);
-      }
-      /* every MMA issued has completed before TMEM is freed */
-      mma_commit(&fin);
-      if (!t_wait_time(&fin, 0)) atomicExch(status, kErrWaitTimeout);
-    }
-    __syncwarp();
-  }
-  fence_before_sync();
-  __syncthreads();
-  fence_after_sync();
-  if (warp == mma_warp) tmem_dealloc(tmem, 512);
-}
-
-
-/* ======================================================================== TMA-fed form */
-
-/* The pipelined form's operand arrangement (operator hi/lo stacked as M = 128, data rows as N)
- * with the data rows brought into shared memory by the Tensor Memory Accelerator instead of
- * per-thread loads.  Within a tile of 128 consecutive rows every A chunk is a strided 2-D block
- * of global memory (a row of the chunk every `pitch` bytes), so one cp.async.bulk.tensor.2d per
- * chunk per tile lands it densely in shared memory; rows outside the tensor (before the first
- * or after the last) are zero-filled by the TMA and patched where the tree wraps around.  Roles
- * (one CTA per SM, 17 warps):
- *   warps 0-7  split: per 16-column slice, raw FP32 rows -> TF32 hi / lo in the K-major
- *              no-swizzle core-matrix layout, into a ring of kMStages stages (mbarriers full /
- *              empty); rows whose chunk wraps around within a section (Prob::wraps) are read
- *              from global memory instead; warp 0 lane 0 also issues the TMA loads, two tiles
- *              ahead, into two raw buffers (mbarrier rawfull with expected transaction bytes;
- *              mbarrier rawempty, arrived by each split warp, frees a raw buffer);
- *   warps 8-15 epilogue, as in the pipelined form (two TMEM accumulators of 128 columns);
- *   warp 16    one thread issues the MMAs: A = the operator, resident in TMEM columns 256..
- *              (written once per CTA), B = the data stage in shared memory, M = 128, N = 128,
- *              K = 8, two MMAs (hi, lo data) per K step.
- * Waits are bounded by the global timer as in the pipelined form. */
-constexpr int kMRows = 128;
-constexpr int kMKs = 16;
-constexpr int kMSplit = 8;
-constexpr int kMEpi = 8;
-constexpr int kMThreads = (kMSplit + kMEpi + 1) * 32;
-constexpr int kMMaxSteps = 16; /* K <= 256 */
-
-struct TmaMaps {
-  CUtensorMap m[4]; /* one per A chunk (64-byte aligned in the parameter space) */
-};
-
-__host__ __device__ constexpr size_t m_smem_bytes(int kpad, int stages) {
-  return (size_t)2 * kMRows * kpad * 4 + (size_t)stages * 2 * kMRows * kMKs * 4 + (size_t)2 * 32 * 64 * 4;
-}
-
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;"
                :
@@ -1125,249 +761,6 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
                : "memory");
 }
 
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y,
-                                            uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
-      :
-      : "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
-      : "memory");
-}
-
-template <class Prob>
-__global__ void __launch_bounds__(kMThreads, 1)
-    k_tc_tma(const __grid_constant__ Prob pb, const __grid_constant__ TmaMaps maps, int stages, int *status) {
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
-  __shared__ uint64_t full[8], empty[8], dfull[2], dempty[2], rawfull[2], rawempty[2], fin;
-  __shared__ uint32_t tmem_slot;
-  __shared__ volatile int abort_flag;
-  __shared__ int lmap[kMMaxSteps][4]; /* per step and float4: chunk (low byte, 0xFF none), offset */
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int kpad = pb.kpad, nsteps = (kpad + kMKs - 1) / kMKs;
-  float *raw = reinterpret_cast<float *>(smem_raw);          /* 2 x [chunk c: 128 rows x clen] */
-  float *Xs = raw + 2 * kMRows * kpad;                        /* stage s: hi, then lo */
-  float *xch = Xs + stages * 2 * kMRows * kMKs;               /* epilogue staging */
-  const int mma_warp = kMSplit + kMEpi;
-  if (warp == mma_warp) tmem_alloc(&tmem_slot, 512);
-  if (tid == 0) {
-    for (int i = 0; i < stages; ++i) mbar_init(&full[i], kMSplit), mbar_init(&empty[i], 1);
-    for (int i = 0; i < 2; ++i)
-      mbar_init(&dfull[i], 1), mbar_init(&dempty[i], kMEpi), mbar_init(&rawfull[i], 1),
-          mbar_init(&rawempty[i], kMSplit);
-    mbar_init(&fin, 1);
-    fence_mbar_init();
-    abort_flag = 0;
-  }
-  if (tid < kMMaxSteps * 4) {
-    const int st = tid >> 2, i = tid & 3, k = st * kMKs + 4 * i;
-    int e = 0xFF;
-    if (k < kpad)
-      for (int c = 0; c < pb.nchunks; ++c)
-        if (k >= pb.coff[c] && k < pb.coff[c] + pb.clen[c]) e = c | ((k - pb.coff[c]) << 8);
-    lmap[st][i] = e;
-  }
-  fence_before_sync();
-  __syncthreads();
-  fence_after_sync();
-  const uint32_t tmem = tmem_slot;
-  /* the operator into TMEM columns 256 .. 256 + kpad: hi in lanes 0..npad-1, lo in 64.. */
-  if (warp >= kMSplit && warp < kMSplit + 4) {
-    const int q = warp & 3, m = q * 32 + lane;
-    const uint32_t lane_addr = (uint32_t)(q * 32) << 16;
-    for (int k0 = 0; k0 < kpad; k0 += 32) { /* 32 loads in flight, then four stores */
-      float v[32];
-#pragma unroll
-      for (int i = 0; i < 32; ++i) {
-        float x = 0.f;
-        if (k0 + i < kpad) {
-          if (m < pb.npad) x = pb.bhi[(long)m * kpad + k0 + i];
-          else if (m >= 64 && m - 64 < pb.npad) x = pb.blo[(long)(m - 64) * kpad + k0 + i];
-        }
-        v[i] = x;
-      }
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (k0 + 8 * q < kpad) tmem_st8(tmem + lane_addr + 256u + (uint32_t)(k0 + 8 * q), v + 8 * q);
-    }
-    tmem_st_wait();
-  }
-  fence_before_sync();
-  __syncthreads();
-  fence_after_sync();
-  const long ntiles = (pb.rows + kMRows - 1) / kMRows;
-  uint32_t tx_bytes = 0;
-  for (int c = 0; c < pb.nchunks; ++c) tx_bytes += (uint32_t)(kMRows * pb.clen[c] * 4);
-
-  if (warp < kMSplit) {
-    /* ------------------------------------------------------------ split (+ TMA issue) */
-    const uint32_t raw0 = smem_addr(raw), xs0 = smem_addr(Xs);
-    auto issue = [&](long tile, int b) {
-      mbar_expect_tx(&rawfull[b], tx_bytes);
-      const uint32_t dst = raw0 + (uint32_t)(b * kMRows * kpad * 4);
-      for (int c = 0; c < pb.nchunks; ++c)
-        tma_load_2d(dst + (uint32_t)(kMRows * pb.coff[c] * 4), &maps.m[c], 0,
-                    (int)(tile * kMRows) + pb.yoff[c], &rawfull[b]);
-    };
-    if (tid == 0) {
-      if ((long)blockIdx.x < ntiles) issue(blockIdx.x, 0);
-      if ((long)blockIdx.x + gridDim.x < ntiles) issue(blockIdx.x + gridDim.x, 1);
-    }
-    unsigned it = 0, tcount = 0;
-    bool ok = true;
-    for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++tcount) {
-      const int b = (int)(tcount & 1);
-      TC_CLOCK(tp);
-      if (lane == 0) ok = t_wait(&rawfull[b], (tcount >> 1) & 1, &abort_flag, status);
-      ok = __shfl_sync(0xffffffffu, ok, 0);
-      if (!ok) break;
-      TC_PHASE(0, tp);
-      const float *rb = raw + b * kMRows * kpad;
-      for (int st = 0; st < nsteps; ++st, ++it) {
-        const int s = (int)(it % stages);
-        if (lane == 0) ok = t_wait(&empty[s], ((it / stages) & 1) ^ 1, &abort_flag, status);
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-        if (!ok) break;
-        TC_PHASE(1, tp);
-        const uint32_t hb = xs0 + (uint32_t)(s * 2 * kMRows * kMKs * 4), lb = hb + kMRows * kMKs * 4;
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-          const int i = tid + 256 * j, row = ((i >> 5) << 3) + ((i & 31) >> 2), k4 = i & 3;
-          const int e = lmap[st][k4], c = e & 0xFF, off = e >> 8;
-          float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (c != 0xFF) {
-            const long r = tile * kMRows + row;
-            if (r < pb.rows && pb.wraps(c, r))
-              v = __ldg(reinterpret_cast<const float4 *>(pb.src(c, r, 0) + off));
-            else
-              v = *reinterpret_cast<const float4 *>(rb + kMRows * pb.coff[c] + row * pb.clen[c] + off);
-          }
-          const float h0 = tf32_rna(v.x), h1 = tf32_rna(v.y), h2 = tf32_rna(v.z), h3 = tf32_rna(v.w);
-          const uint32_t o = core_off(row, 4 * k4, kMKs);
-          asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" : : "r"(hb + o), "f"(h0), "f"(h1),
-                       "f"(h2), "f"(h3) : "memory");
-          asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" : : "r"(lb + o), "f"(tf32_rna(v.x - h0)),
-                       "f"(tf32_rna(v.y - h1)), "f"(tf32_rna(v.z - h2)), "f"(tf32_rna(v.w - h3)) : "memory");
-        }
-        TC_PHASE(9, tp);
-        fence_smem_to_async();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&full[s]);
-        TC_PHASE(2, tp);
-      }
-      if (!ok) break;
-      /* this warp is done with raw buffer b; thread 0 refills it two tiles ahead once all
-       * eight split warps are (mbarrier rawempty, bounded wait) */
-      fence_smem_to_async();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&rawempty[b]);
-      if (tid == 0 && tile + 2L * gridDim.x < ntiles) {
-        ok = t_wait(&rawempty[b], (tcount >> 1) & 1, &abort_flag, status);
-        if (ok) issue(tile + 2L * gridDim.x, b);
-      }
-      ok = __shfl_sync(0xffffffffu, ok, 0);
-      TC_PHASE(3, tp);
-    }
-  } else if (warp < kMSplit + kMEpi) {
-    /* ------------------------------------------------------------ epilogue */
-    const int q = warp & 3, h = (warp - kMSplit) >> 2, et = tid - kMSplit * 32;
-    const uint32_t lane_addr = (uint32_t)(q * 32) << 16;
-    const int nout = pb.nout;
-    const int n = (q & 1) * 32 + lane;
-    float *stg = xch + (q >> 1) * 32 * 64;
-    unsigned tc = 0;
-    for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++tc) {
-      const int b = (int)(tc & 1);
-      bool ok = true;
-      TC_CLOCK(tp);
-      if (lane == 0) ok = t_wait(&dfull[b], (tc >> 1) & 1, &abort_flag, status);
-      ok = __shfl_sync(0xffffffffu, ok, 0);
-      if (!named_bar_and(3, kMEpi * 32, ok)) break;
-      fence_after_sync();
-      TC_PHASE(4, tp);
-      for (int ch = 0; ch < kMRows / 32; ++ch) {
-        float t[16];
-        tmem_ld16(tmem + lane_addr + (uint32_t)(b * 128 + ch * 32 + h * 16), t);
-        if (n < nout) {
-#pragma unroll
-          for (int c = 0; c < 16; ++c) stg[(h * 16 + c) * nout + n] = t[c];
-        }
-        named_bar(1, kMEpi * 32);
-        const long rb = tile * kMRows + ch * 32;
-        const long nr = pb.rows - rb < 32 ? pb.rows - rb : 32;
-        if (nr > 0) {
-          float4 *g = reinterpret_cast<float4 *>(pb.dst(rb, 0));
-          const float4 *sh = reinterpret_cast<const float4 *>(xch);
-          const float4 *sl = reinterpret_cast<const float4 *>(xch + 32 * 64);
-          const int n4 = (int)nr * nout / 4;
-          for (int i = et; i < n4; i += kMEpi * 32) {
-            const float4 x = sh[i], y = sl[i];
-            g[i] = make_float4(x.x + y.x, x.y + y.y, x.z + y.z, x.w + y.w);
-          }
-        }
-        named_bar(1, kMEpi * 32);
-      }
-      fence_before_sync();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&dempty[b]);
-      TC_PHASE(5, tp);
-    }
-  } else {
-    if (lane == 0) {
-      /* ---------------------------------------------------------- MMA issue */
-      const uint32_t idesc = make_idesc_tf32(kMRows);
-      const uint32_t xs0 = smem_addr(Xs), x_sbo = (uint32_t)kMKs * 32;
-      unsigned it = 0, tc = 0;
-      bool ok = true;
-      for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++tc) {
-        const int b = (int)(tc & 1);
-        TC_CLOCK(tp);
-        ok = t_wait(&dempty[b], ((tc >> 1) & 1) ^ 1, &abort_flag, status);
-        if (!ok) break;
-        fence_after_sync();
-        TC_PHASE(6, tp);
-        const uint32_t d = tmem + (uint32_t)(b * 128);
-        for (int st = 0; st < nsteps; ++st, ++it) {
-          const int s = (int)(it % stages);
-          ok = t_wait(&full[s], (it / stages) & 1, &abort_flag, status);
-          if (!ok) break;
-          fence_after_sync();
-          TC_PHASE(7, tp);
-          const int k0 = st * kMKs;
-          const int ksteps = ((kpad - k0) < kMKs ? (kpad - k0) : kMKs) >> 3;
-          const uint32_t hb = xs0 + (uint32_t)(s * 2 * kMRows * kMKs * 4), lb = hb + kMRows * kMKs * 4;
-          for (int kk = 0; kk < ksteps; ++kk) {
-            const uint32_t a = tmem + 256u + (uint32_t)(k0 + 8 * kk);
-            mma_tf32_ts(d, a, make_desc(hb + 256u * kk, 128, x_sbo), idesc, (st | kk) != 0);
-            mma_tf32_ts(d, a, make_desc(lb + 256u * kk, 128, x_sbo), idesc, 1);
-          }
-          mma_commit(&empty[s]);
-          TC_PHASE(8, tp);
-        }
-        if (!ok) break;
-        mma_commit(&dfull[b]);
-      }
-      mma_commit(&fin);
-      if (!t_wait_time(&fin, 0)) atomicExch(status, kErrWaitTimeout);
-    }
-    __syncwarp();
-  }
-  /* TMA loads still in flight (issued for tiles that an aborted CTA never consumed) must land
-   * before the CTA's shared memory goes away */
-  if (tid == 0) {
-    unsigned tcount = 0;
-    for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) ++tcount;
-    /* loads were issued for tiles 0 .. min(tcount, consumed + 2) - 1; wait for each buffer's
-     * last issued phase */
-    for (int b = 0; b < 2; ++b) {
-      const unsigned uses = tcount > (unsigned)b ? (tcount - 1 - b) / 2 + 1 : 0;
-      if (uses) t_wait_time(&rawfull[b], (uses - 1) & 1);
-    }
-  }
-  fence_before_sync();
-  __syncthreads();
-  fence_after_sync();
-  if (warp == mma_warp) tmem_dealloc(tmem, 512);
-}
 
 /* ======================================================================== warp-specialised form */
 

@@ -2,9 +2,11 @@
 
 FMMFFT_TC_MIN_ROWS=1 (set before the plans are made) sends every eligible stage, however small,
 through the tensor-core kernel so that small cases cover it; the default threshold only routes
-stages with >= 4096 rows there.  Each test runs for the default per-stage forms (16-lane row
-form for S2M and M2M, 32-lane row form for M2L and the leaf) and for each kernel form forced on
-every stage (FMMFFT_TC_FORM row, row16, pipelined and tma), with S2M as its own stage (FMMFFT_FUSE_S2M=0) so that it runs on the tensor cores.  Tolerance: rel-L2 <= 1e-6 against FP64, as for FP32 plans.
+stages with >= 4096 rows there.  Each test runs for the default per-stage kernels (16-lane row
+form for S2M and M2M, 32-lane row form for M2L and the leaf) and for each tensor-core kernel
+forced on every stage (FMMFFT_TC_FORM row, row16 and ws, the warp-specialised one), with S2M as
+its own stage (FMMFFT_FUSE_S2M=0) so that it runs on the tensor cores.  Tolerance: rel-L2 <= 1e-6
+against FP64, as for FP32 plans.
 """
 import os
 
@@ -30,14 +32,14 @@ def fm():
     return fmmfft
 
 
-FORMS = ["default", "row", "row16", "pipelined", "tma"]
+FORMS = ["default", "row", "row16", "ws"]
 
 
 @pytest.fixture(params=FORMS)
 def force_tc(request):
     """Every eligible stage on the tensor cores, in the default per-stage forms or in one form
-    forced on every stage: the 32-lane row form, the 16-lane row form, the pipelined
-    warp-specialised form or the TMA-fed form (FMMFFT_TC_FORM=row / row16 / pipelined / tma)."""
+    forced on every stage: the 32-lane row form, the 16-lane row form or the warp-specialised
+    kernel (FMMFFT_TC_FORM=row / row16 / ws)."""
     saved = {k: os.environ.get(k) for k in ("FMMFFT_TC_MIN_ROWS", "FMMFFT_TC_FORM", "FMMFFT_FUSE_S2M")}
     os.environ["FMMFFT_TC_MIN_ROWS"] = "1"
     if request.param == "default":
