@@ -408,14 +408,9 @@ def serve_compare(rates, count=1200, seed=7, served_prec="f32_tc", plain_prec="f
                 return None
             raise
 
-    for (N, P, T, b) in shapes:
-        nbmax = max(1, min(32, (1 << 21) // N))
-        for burst in (1, 2, 4, 8, 16, 32, 32, 32):
-            if burst > nbmax and burst != 1:
-                continue
-            hs = [srv_submit(N, P, T, b, *bufs[N][j % nbuf]) for j in range(burst)]
-            for h in hs:
-                srv.wait(h)
+    for (N, P, T, b) in shapes:  # every shape's plans resident, graphs instantiated
+        srv.reserve(N, P, T, b, served_prec, 3)
+        srv.wait(srv_submit(N, P, T, b, *bufs[N][0]))
     torch.cuda.synchronize()
     served = {}
     for r in rates:

@@ -419,3 +419,73 @@ int fmmfft_server_counts(fmmfft_server s, uint64_t *requests, uint64_t *launches
   pthread_mutex_unlock(&s->mu);
   return FMMFFT_OK;
 }
+
+/* Makes `nplans` plans of a shape resident (at most the server's plans per shape), built in the
+ * caller's thread, and instantiates each batched plan's graphs for every batch size it will use
+ * (powers of two up to its capacity), so that no request of this shape later waits for a plan to
+ * be built or a graph to be captured.  Refused with FMMFFT_ERR_BUSY when the budget cannot hold
+ * them after evicting idle plans. */
+int fmmfft_server_reserve(fmmfft_server s, long N, long P, long terms, long b, int precision, int nplans) {
+  if (!s || nplans < 1) return FMMFFT_ERR_INVALID;
+  const int cap = s->nstreams < SRV_LANE_PLANS ? s->nstreams : SRV_LANE_PLANS;
+  if (nplans > cap) nplans = cap;
+  for (;;) {
+    pthread_mutex_lock(&s->mu);
+    int status = FMMFFT_OK;
+    const int l = find_lane(s, N, P, terms, b, precision, &status);
+    if (l < 0) {
+      pthread_mutex_unlock(&s->mu);
+      return status;
+    }
+    srv_lane *ln = &s->lanes[l];
+    if (ln->nplans >= nplans) {
+      pthread_mutex_unlock(&s->mu);
+      return FMMFFT_OK;
+    }
+    if (ln->creating) { /* the dispatcher is building one: wait for it */
+      pthread_mutex_unlock(&s->mu);
+      struct timespec nap = {0, 100000};
+      nanosleep(&nap, NULL);
+      continue;
+    }
+    while (s->used + ln->plan_bytes > s->budget && evict_one(s, l)) {
+    }
+    if (s->used + ln->plan_bytes > s->budget) {
+      pthread_mutex_unlock(&s->mu);
+      return FMMFFT_ERR_BUSY;
+    }
+    s->used += ln->plan_bytes;
+    ln->creating = 1;
+    const int nb = ln->nbmax;
+    pthread_mutex_unlock(&s->mu);
+    srv_plan np;
+    memset(&np, 0, sizeof np);
+    int ok = fmmfft_plan_create_batched(&np.plan, N, P, terms, b, precision, nb) == FMMFFT_OK;
+    ok = ok && cudaStreamCreateWithFlags(&np.st, cudaStreamNonBlocking) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&np.done, cudaEventDisableTiming) == cudaSuccess;
+    if (ok && nb > 1) {
+      const size_t bytes = (size_t)nb * (size_t)N * elem_bytes(precision);
+      ok = cudaMalloc(&np.bin, bytes) == cudaSuccess && cudaMalloc(&np.bout, bytes) == cudaSuccess;
+      ok = ok && cudaMemsetAsync(np.bin, 0, bytes, np.st) == cudaSuccess;
+      for (int k = 1; ok && k <= nb; k *= 2) /* every batch size's graph, captured and run once */
+        ok = fmmfft_execute_many_graph(np.plan, k, np.bin, np.bout, np.st) == FMMFFT_OK;
+      ok = ok && cudaStreamSynchronize(np.st) == cudaSuccess;
+    }
+    if (!ok) {
+      cudaGetLastError();
+      free_plan(&np);
+    }
+    pthread_mutex_lock(&s->mu);
+    ln = &s->lanes[l];
+    ln->creating = 0;
+    if (!ok) {
+      s->used -= ln->plan_bytes;
+      pthread_mutex_unlock(&s->mu);
+      return FMMFFT_ERR_NOMEM;
+    }
+    np.bytes = ln->plan_bytes;
+    np.last_use = ++s->clock;
+    ln->p[ln->nplans++] = np;
+    pthread_mutex_unlock(&s->mu);
+  }
+}

@@ -28,7 +28,7 @@ EXPORTS = ["getwlen2", "getvlen", "mfti", "mft", "fmmfft_last_error", "fmmfft_la
            "fmmfft_debug_fetch", "fmmfft_profile_start", "fmmfft_profile_stop",
            "fmmfft_stage_name", "fmmfft_execute_noalloc", "fmmfft_plan_check",
            "fmmfft_plan_selftest_wait", "fmmfft_plan_create_batched", "fmmfft_execute_many",
-           "fmmfft_execute_many_graph", "fmmfft_plan_bytes", "fmmfft_server_counts",
+           "fmmfft_execute_many_graph", "fmmfft_plan_bytes", "fmmfft_server_counts", "fmmfft_server_reserve",
            "fmmfft_plan_enable_refinement", "fmmfft_execute_refined", "fmmfft_mft_rank_mode",
            "fmmfft_execute_blocks", "fmmfft_execute_blocks_host", "fmmfft_plan_describe",
            "fmmfft_batch_create_many",
@@ -93,6 +93,8 @@ def load(path=LIB_PATH):
     lib.fmmfft_plan_bytes.restype = _I
     lib.fmmfft_server_counts.argtypes = [_VP, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     lib.fmmfft_server_counts.restype = _I
+    lib.fmmfft_server_reserve.argtypes = [_VP, _L, _L, _L, _L, _I, _I]
+    lib.fmmfft_server_reserve.restype = _I
     lib.fmmfft_plan_enable_refinement.argtypes = [_VP]
     lib.fmmfft_plan_enable_refinement.restype = _I
     lib.fmmfft_execute_refined.argtypes = [_VP, _VP, _VP, _VP]
@@ -395,6 +397,13 @@ class Server:
         if rc:
             raise FmmFftError(rc, "submit refused" if rc == 7 else "submit failed")
         return t.value
+
+    def reserve(self, N, P, terms, b, precision, nplans):
+        """Make nplans plans of a shape resident (graphs instantiated) before its requests."""
+        rc = load().fmmfft_server_reserve(self._h, int(N), int(P), int(terms), int(b),
+                                          PRECISIONS[precision], int(nplans))
+        if rc:
+            raise FmmFftError(rc, "reserve refused" if rc == 7 else "reserve failed")
 
     def counts(self):
         """-> (requests dispatched, batched launch sequences)"""

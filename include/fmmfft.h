@@ -215,19 +215,29 @@ int fmmfft_batch_launch(fmmfft_batch batch, void *stream);
 int fmmfft_batch_destroy(fmmfft_batch batch);
 
 /* ------------------------------------------------------------------ serving */
-/* A request server: transforms of mixed sizes and precisions submitted one at a time are
- * admitted onto `nstreams` CUDA streams, so that requests arriving while others run overlap on
- * the device.  Plans stay resident per (N, P, terms, b, precision) and per stream; the device
- * memory they hold is capped by hbm_budget_bytes: a request that needs a new plan evicts idle
- * plans least-recently-used, and is refused with FMMFFT_ERR_BUSY (retry later) when the plans
- * in use leave no room.  d_in / d_out are caller-owned device buffers that must stay valid
- * until the request completes.  Results do not depend on what else is in flight. */
+/* A request server with continuous batching: transforms of mixed sizes and precisions are
+ * submitted one at a time; requests of one shape (N, P, terms, b, precision) that arrive while
+ * that shape's plans are busy are queued and leave together, as ONE batched launch sequence, as
+ * soon as a plan frees up (small shapes: up to 2^21 samples per batch); each shape keeps up to
+ * `nstreams` (at most 3) resident plans on their own streams, so batches of different shapes and
+ * of one shape overlap on the device.  A dispatcher thread sends queued batches; submit, query and
+ * wait dispatch too.  The device memory of the plans is capped by hbm_budget_bytes: a plan's size
+ * is computed before anything is allocated, idle plans are evicted least-recently-used to make
+ * room, and a request whose shape cannot get a plan is refused with FMMFFT_ERR_BUSY (retry later)
+ * with nothing allocated.  d_in / d_out are caller-owned device buffers that must stay valid until
+ * the request completes.  Results do not depend on what else is in flight: a batched transform
+ * gives bitwise the output of its own execute. */
 typedef struct fmmfft_server_s *fmmfft_server;
 typedef uint64_t fmmfft_ticket;
 int fmmfft_server_create(fmmfft_server *out, size_t hbm_budget_bytes, int nstreams);
 int fmmfft_server_destroy(fmmfft_server server); /* waits for every request in flight */
 int fmmfft_server_submit(fmmfft_server server, long N, long P, long terms, long b, int precision,
                          const void *d_in, void *d_out, fmmfft_ticket *ticket);
+/* Makes nplans plans of a shape resident ahead of its requests (at most nstreams), each batched
+ * plan with its graphs for every batch size instantiated, so that no request waits for a plan to
+ * be built; FMMFFT_ERR_BUSY when the budget cannot hold them.  Blocks until they are ready. */
+int fmmfft_server_reserve(fmmfft_server server, long N, long P, long terms, long b, int precision,
+                          int nplans);
 /* FMMFFT_OK when the request is complete, FMMFFT_ERR_BUSY while it runs. */
 int fmmfft_server_query(fmmfft_server server, fmmfft_ticket ticket);
 /* Waits up to timeout_ms; FMMFFT_OK or FMMFFT_ERR_TIMEOUT. */

@@ -204,3 +204,39 @@ def test_bounded_wait_gives_up_and_reports_timeout(fm, which):
     plan.check()
     assert np.array_equal(y0, y1)
     plan.close()
+
+
+def test_server_reserve_makes_plans_resident(fm):
+    """reserve builds a shape's plans (and their batch graphs) before any request: the plan
+    count reaches the reserved number at once and requests that follow make no new plan; results
+    are bitwise those of the plan run alone.  A reserve beyond the budget is refused."""
+    import torch
+    N, P, T, b = 1 << 14, 16, 16, 32
+    srv = fm.Server(4 << 30, nstreams=3)
+    srv.reserve(N, P, T, b, "f32_tc", 2)
+    assert srv.stats()["plans"] == 2
+    srv.reserve(N, P, T, b, "f32_tc", 2)  # already resident: nothing more
+    assert srv.stats()["plans"] == 2
+    xs = [ol.seeded_input(N, 700 + i) for i in range(12)]
+    din = [_dev(x, torch.complex64) for x in xs]
+    dout = [torch.empty_like(d) for d in din]
+    ts = [srv.submit(N, P, T, b, "f32_tc", d.data_ptr(), o.data_ptr()) for d, o in zip(din, dout)]
+    for t in ts:
+        srv.wait(t)
+    assert srv.stats()["plans"] <= 3
+    plan = fm.Plan(N, P, T, b, "f32_tc")
+    s = torch.cuda.current_stream().cuda_stream
+    for d, o in zip(din, dout):
+        alone = torch.empty_like(d)
+        plan.execute_ptr(d.data_ptr(), alone.data_ptr(), s)
+        torch.cuda.synchronize()
+        assert torch.equal(alone, o)
+    plan.close()
+    srv.close()
+    big = fm.plan_bytes(1 << 22, 64, 16, 32, "f32")
+    small = fm.Server(int(big * 1.5), nstreams=3)
+    with pytest.raises(fm.FmmFftError) as ei:
+        small.reserve(1 << 22, 64, 16, 32, "f32", 3)  # room for one of the three
+    assert ei.value.status == 7
+    assert small.stats()["plans"] == 1
+    small.close()
