@@ -177,6 +177,17 @@ int fmmfft_execute_host(fmmfft_plan plan, const void *h_in, void *h_out, void *s
   return rc ? set_err(rc, err) : FMMFFT_OK;
 }
 
+int fmmfft_execute_host_many(fmmfft_plan plan, int n, const void *const *h_in, void *const *h_out,
+                             void *stream) {
+  if (!plan || n < 0 || (n > 0 && (!h_in || !h_out)))
+    return set_err(FMMFFT_ERR_INVALID, "execute_host_many: NULL argument or n < 0");
+  for (int i = 0; i < n; ++i)
+    if (!h_in[i] || !h_out[i]) return set_err(FMMFFT_ERR_INVALID, "execute_host_many: NULL buffer");
+  char err[256] = {0};
+  int rc = fmmk_execute_host_many(plan->dev, n, h_in, h_out, stream, err, sizeof err);
+  return rc ? set_err(rc == 2 ? FMMFFT_ERR_NOMEM : FMMFFT_ERR_CUDA, err) : FMMFFT_OK;
+}
+
 int fmmfft_debug_fetch(fmmfft_plan plan, double *u, double *z, double *phi, double *psi) {
   if (!plan) return set_err(FMMFFT_ERR_INVALID, "debug_fetch: NULL plan");
   int rc = fmmk_debug_fetch(plan->dev, u, z, phi, psi);

@@ -64,6 +64,8 @@ int fmmk_execute_graph_n(fmmk_state *st, const void *d_in, void *d_out, void *st
                          int nbt, char *err, size_t errlen);
 int fmmk_execute_host(fmmk_state *st, const void *h_in, void *h_out, void *stream, char *err,
                       size_t errlen);
+int fmmk_execute_host_many(fmmk_state *st, int n, const void *const *h_in, void *const *h_out,
+                           void *stream, char *err, size_t errlen);
 int fmmk_debug_fetch(fmmk_state *st, double *u, double *z, double *phi, double *psi);
 int fmmk_device_ok(char *err, size_t errlen);
 int fmmk_profile_start(fmmk_state *st, int cap);

@@ -141,14 +141,16 @@ template <typename R> struct Dev {
   float *tc_m2m[2];     /* per parent level L = 2..n-1, stride tc_m2m_stride */
   float *tc_m2l[2];     /* per child level l = 3..n, stride tc_m2l_stride */
   float *tc_leaf[2];    /* per section, stride tc_leaf_stride */
+  float *tc_lnb[2];     /* the leaf's neighbour-sum operators, per section, stride tc_lnb_stride */
   float *leaf_fix;      /* tensor-core leaf, section P/2: [2][s] first points from box-1 */
-  long tc_m2m_stride, tc_m2l_stride, tc_leaf_stride;
+  long tc_m2m_stride, tc_m2l_stride, tc_leaf_stride, tc_lnb_stride;
   /* the same operators for the warp-specialised kernel: hi rows then lo rows in the MMA's
    * core-matrix layout (tc::ws_b_index), one block per level or section */
   float *ws_s2m, *ws_m2m, *ws_m2l, *ws_leaf;
   long ws_m2m_stride, ws_m2l_stride, ws_leaf_stride;
   int kp_s2m, np_s2m, kp_m2m, np_m2m, kp_m2l, np_m2l, kp_leaf, np_leaf;
   int ok_s2m, ok_m2m, ok_m2l, ok_leaf;
+  int kp_lnb, np_lnb, ok_lnb; /* neighbour-sum leaf (tc::k_tc_nbr): the leaf's default form */
   long tc_min_rows; /* stages with fewer rows use the CUDA-core kernel */
   int fft_threads;  /* threads per block of the register FFT pass (power of two, <= 512) */
   /* tensor-core kernel: 0 row form (32 lanes), 3 row form (16 lanes), 4 warp-specialised; -1
@@ -186,13 +188,37 @@ struct Refine {
   size_t bytes;
 };
 
+/* Staging of fmmk_execute_host_many: three device buffers of one transform each, so that the
+ * copy-in of transform i+1, the execute of transform i and the copy-out of transform i-1 run at
+ * once on three streams; events order each buffer's reuse. */
+#define FMMK_HOST_SLOTS 3
+struct HostPipe {
+  void *buf[FMMK_HOST_SLOTS];
+  cudaStream_t cin, cout;
+  cudaEvent_t in_done[FMMK_HOST_SLOTS], ex_done[FMMK_HOST_SLOTS], out_done[FMMK_HOST_SLOTS];
+};
+
 struct fmmk_state {
   int precision;
   void *dev; /* Dev<float> or Dev<double> */
   Refine *refine;
   GraphSlot graphs[FMMK_GRAPHS];
   unsigned long long graph_clock;
+  HostPipe *pipe; /* made on the first fmmk_execute_host_many */
 };
+
+static void host_pipe_free(HostPipe *hp) {
+  if (!hp) return;
+  for (int i = 0; i < FMMK_HOST_SLOTS; ++i) {
+    if (hp->buf[i]) cudaFree(hp->buf[i]);
+    if (hp->in_done[i]) cudaEventDestroy(hp->in_done[i]);
+    if (hp->ex_done[i]) cudaEventDestroy(hp->ex_done[i]);
+    if (hp->out_done[i]) cudaEventDestroy(hp->out_done[i]);
+  }
+  if (hp->cin) cudaStreamDestroy(hp->cin);
+  if (hp->cout) cudaStreamDestroy(hp->cout);
+  free(hp);
+}
 
 __host__ __device__ __forceinline__ long lvl_off(long l, long S1, long T) {
   return 2 * S1 * T * ((1L << l) - 4);
@@ -595,6 +621,41 @@ struct TcLeaf : TcBase { /* batch z = section - 1; s is a power of two (log2s) *
   }
 };
 
+/* The same leaf in neighbour-sum form (tc::k_tc_nbr): row r = (transform, plane, box B) holds
+ * only box B's own data, A = [psi_B (T) | x_B (b)], and the operator of section sc has the
+ * column blocks
+ *   [0, b)     box B's targets: far field (evalm) + x_B as the window's middle box,
+ *   [b, 2b)    box B+1's targets: x_B as the first box of B+1's window,
+ *   [2b, 3b)   box B-1's targets: x_B as the last box of B-1's window,
+ *   3b .. 3b+2 (sc >= P/2) the half-shifted first point H(B) of box B+1 (evalmh, and x_B as the
+ *              middle of the window B-1..B+1), x_B's part of H(B+1), x_B's part of H(B-1);
+ * the kernel adds the blocks of rows B-1, B, B+1.  Each sample is loaded and split once per row
+ * instead of three times (K = T + b instead of T + 3b). */
+struct TcLeafNb : TcLeaf {
+  long strips;
+  __device__ const float *src(int c, long r, int z) const {
+    const long bx = r & (s - 1), pl = plane(r, z);
+    if (c == 0) return psi_n + (pl * s + bx) * T;
+    return xt + (pl + 2 * (r >> (log2s + 1)) + 2) * M + bx * b;
+  }
+  __device__ bool has_h(int z) const { return 2 * (z + 1) >= P; }
+  __device__ void put8_nb(long r, int z, int c0, const float *t) const {
+    float *dst = u + plane(r, z) * M + (r & (s - 1)) * b;
+    if (c0 == 0 && 2 * (z + 1) > P) /* the in-box first point is replaced by H(B - 1) */
+      dst[1] = t[1], dst[2] = t[2], dst[3] = t[3];
+    else
+      *reinterpret_cast<float4 *>(dst + c0) = make_float4(t[0], t[1], t[2], t[3]);
+    *reinterpret_cast<float4 *>(dst + c0 + 4) = make_float4(t[4], t[5], t[6], t[7]);
+  }
+  __device__ void put_h(long r, int z, float v) const { /* H(B): first point of box B + 1 */
+    const long nb = (r + 1) & (s - 1);
+    if (2 * (z + 1) > P)
+      u[plane(r, z) * M + nb * b] = v;
+    else
+      fixbuf[((r >> log2s) << log2s) + nb] = v;
+  }
+};
+
 template <typename R, int BM, int BN, int BK, int TM, int TN, class Prob>
 __global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_rowgemm(Prob pb) {
   constexpr int NTX = BN / TN;
@@ -751,6 +812,27 @@ static void launch_tc(const Prob &pb0, int num_sms, int *status, cudaStream_t st
     tc::k_tc_rowgemm16<Prob><<<grid, 256, smem, st>>>(pb, status);
   else
     tc::k_tc_rowgemm<Prob><<<grid, 256, smem, st>>>(pb, status);
+}
+
+/* The neighbour-sum row form (tc::k_tc_nbr), persistent, two CTAs per SM; launched like the
+ * row form (programmatic dependent launch unless pdl is 0). */
+template <class Prob> static void launch_nb(const Prob &pb, int num_sms, int *status, cudaStream_t st, int pdl) {
+  const long tps = (pb.s + tc::kNbOut - 1) / tc::kNbOut;
+  const long tiles = tps * pb.strips * pb.batches;
+  const long cap = 2L * num_sms;
+  const int grid = (int)(tiles < cap ? tiles : cap);
+  const size_t smem = tc::smem_bytes(pb.kpad, pb.npad);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, tc::k_tc_nbr<Prob>, pb, status);
 }
 
 /* First point of each leaf box for the sections whose shifted target leaves its box
@@ -1821,6 +1903,7 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
   if (d->tc_m2m_stride > cap) cap = d->tc_m2m_stride;
   if (d->tc_m2l_stride > cap) cap = d->tc_m2l_stride;
   if (d->tc_leaf_stride > cap) cap = d->tc_leaf_stride;
+  if (d->tc_lnb_stride > cap) cap = d->tc_lnb_stride;
   double *v = (double *)malloc(sizeof(double) * cap);
   if (!v) return 2;
   int rc = 0;
@@ -1880,6 +1963,30 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
       }
       rc |= tc_put(d->tc_leaf[0] + (sc - 1) * d->tc_leaf_stride, d->tc_leaf[1] + (sc - 1) * d->tc_leaf_stride,
                    d->ws_leaf + (sc - 1) * d->ws_leaf_stride, v, kp, np, err, errlen, d->bf16);
+    }
+  if (d->ok_lnb) /* neighbour-sum form (TcLeafNb): x_B's weights for boxes B, B+1, B-1 */
+    for (long sc = 1; sc < P; ++sc) {
+      const int kp = d->kp_lnb, np = d->np_lnb;
+      const double *ct = o->cot + (sc - 1) * 4 * b;
+      for (long i = 0; i < (long)kp * np; ++i) v[i] = 0;
+      for (long j = 0; j < b; ++j) {
+        for (long k = 0; k < T; ++k) v[j * kp + k] = o->evalm[(j * S1 + (sc - 1)) * T + k];
+        for (long q = 0; q < b; ++q) {
+          v[j * kp + T + q] = ct[q + 2 * b - j];           /* window middle: box B */
+          v[(b + j) * kp + T + q] = ct[q + b - j];         /* window start of box B+1 */
+          v[(2 * b + j) * kp + T + q] = ct[q + 3 * b - j]; /* window end of box B-1 */
+        }
+      }
+      if (2 * sc >= P) { /* H(B), and x_B's parts of H(B+1) and H(B-1) */
+        for (long k = 0; k < T; ++k) v[3 * b * kp + k] = o->evalmh[(sc - P / 2) * T + k];
+        for (long q = 0; q < b; ++q) {
+          v[3 * b * kp + T + q] = ct[b + q];
+          v[(3 * b + 1) * kp + T + q] = ct[q];
+          v[(3 * b + 2) * kp + T + q] = ct[2 * b + q];
+        }
+      }
+      rc |= tc_put(d->tc_lnb[0] + (sc - 1) * d->tc_lnb_stride, d->tc_lnb[1] + (sc - 1) * d->tc_lnb_stride,
+                   nullptr, v, kp, np, err, errlen, 0);
     }
   free(v);
   return rc;
@@ -1941,6 +2048,7 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
   d->kp_m2m = up8(2 * T), d->np_m2m = up16(T);
   d->kp_m2l = up8(5 * T), d->np_m2l = up16(2 * T);
   d->kp_leaf = up8(T + 3 * b), d->np_leaf = up16(b + 1); /* + the half-shifted column */
+  d->kp_lnb = up8(T + b), d->np_lnb = up16(3 * b + 3);    /* three blocks + three half-shift columns */
   auto fits = [&](int kp, int np) {
     return tc && (T % 4 == 0) && (b % 4 == 0) && np <= 256 && kp <= 256 &&
            tc::smem16_bytes(kp, np) <= (size_t)110 * 1024 && tc::tmem_cols(tc::round16(kp), np) <= 256 &&
@@ -1955,6 +2063,11 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
    * same with three TF32 parts per operand, so the split is not the cause), within the 1e-6 bar,
    * for a 1.5x faster leaf.  FMMFFT_TC_STAGES without bit 8 keeps it on the CUDA cores. */
   d->ok_leaf = fits(d->kp_leaf, d->np_leaf);
+  /* FMMFFT_LEAF_FORM=row keeps the leaf on the window-row form (TcLeaf) */
+  d->ok_lnb = tc && !d->bf16 && T % 4 == 0 && b % 8 == 0 && b <= 32 && d->kp_lnb <= 256 &&
+              d->np_lnb <= 128 && tc::smem_bytes(d->kp_lnb, d->np_lnb) <= (size_t)110 * 1024 &&
+              tc::nb_tmem_cols(d->kp_lnb, d->np_lnb) <= 256;
+  if (const char *ev = getenv("FMMFFT_LEAF_FORM")) d->ok_lnb &= strcmp(ev, "row") != 0;
   d->tc_min_rows = kTcMinRows;
   if (const char *ev = getenv("FMMFFT_TC_MIN_ROWS")) d->tc_min_rows = atol(ev), d->env_set |= KNOB_TCMIN;
   /* FMMFFT_TC_FORM=pipelined routes the tree stages that fit to the warp-specialised kernel
@@ -1986,11 +2099,14 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
   if (const char *ev = getenv("FMMFFT_TC_STAGES")) {
     long m = atol(ev);
     d->ok_s2m &= (m & 1) != 0, d->ok_m2m &= (m & 2) != 0, d->ok_m2l &= (m & 4) != 0, d->ok_leaf &= (m & 8) != 0;
+    d->ok_lnb &= (m & 8) != 0;
   }
   const long sz_s2m = d->ok_s2m ? (long)d->kp_s2m * d->np_s2m : 0;
   d->tc_m2m_stride = (long)d->kp_m2m * d->np_m2m;
   d->tc_m2l_stride = (long)d->kp_m2l * d->np_m2l;
   d->tc_leaf_stride = (long)d->kp_leaf * d->np_leaf;
+  d->tc_lnb_stride = (long)d->kp_lnb * d->np_lnb;
+  const long sz_lnb = d->ok_lnb ? S1 * d->tc_lnb_stride : 0;
   const long sz_m2m = d->ok_m2m ? nlev * d->tc_m2m_stride : 0;
   const long sz_m2l = d->ok_m2l ? nlev * d->tc_m2l_stride : 0;
   const long sz_leaf = d->ok_leaf ? S1 * d->tc_leaf_stride : 0;
@@ -2034,7 +2150,8 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
   CARVE(tcm2m, 2 * sz_m2m, float)
   CARVE(tcm2l, 2 * sz_m2l, float)
   CARVE(tcleaf, 2 * sz_leaf, float)
-  CARVE(leaffix, d->ok_leaf ? nb * 2 * s : 0, float)
+  CARVE(tclnb, 2 * sz_lnb, float)
+  CARVE(leaffix, (d->ok_leaf || d->ok_lnb) ? nb * 2 * s : 0, float)
   CARVE(wss2m, ws_s2m_n, float)
   CARVE(wsm2m, ws_m2m_n, float)
   CARVE(wsm2l, ws_m2l_n, float)
@@ -2082,6 +2199,7 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
   d->tc_m2m[0] = (float *)(base + off_tcm2m), d->tc_m2m[1] = d->tc_m2m[0] + sz_m2m;
   d->tc_m2l[0] = (float *)(base + off_tcm2l), d->tc_m2l[1] = d->tc_m2l[0] + sz_m2l;
   d->tc_leaf[0] = (float *)(base + off_tcleaf), d->tc_leaf[1] = d->tc_leaf[0] + sz_leaf;
+  d->tc_lnb[0] = (float *)(base + off_tclnb), d->tc_lnb[1] = d->tc_lnb[0] + sz_lnb;
   d->leaf_fix = (float *)(base + off_leaffix);
   d->ws_s2m = (float *)(base + off_wss2m);
   d->ws_m2m = (float *)(base + off_wsm2m);
@@ -2326,7 +2444,19 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
     pb.K = (int)(T + 3 * b), pb.N = (int)b, pb.T = (int)T, pb.b = (int)b;
     bool done = false;
     if constexpr (sizeof(R) == 4) {
-      if (d->tc && d->ok_leaf && 2 * s >= (d->tc_min_rows < 256 ? d->tc_min_rows : 256)) {
+      const bool tc_leaf_rows = d->tc && 2 * s >= (d->tc_min_rows < 256 ? d->tc_min_rows : 256);
+      if (tc_leaf_rows && d->ok_lnb && d->tc_form < 0) { /* neighbour-sum form */
+        TcLeafNb q{};
+        q.rows = 2 * s * nbt, q.batches = (int)S1, q.nchunks = 2;
+        q.clen[0] = (int)T, q.clen[1] = (int)b, q.coff[0] = 0, q.coff[1] = (int)T;
+        q.kpad = d->kp_lnb, q.npad = d->np_lnb, q.nout = (int)b;
+        q.bhi = d->tc_lnb[0], q.blo = d->tc_lnb[1], q.bstride = d->tc_lnb_stride;
+        q.fixbuf = d->leaf_fix, q.P = (int)P;
+        q.psi_n = pb.psi_n, q.xt = d->xt, q.u = d->u, q.M = M, q.s = s, q.T = (int)T, q.b = (int)b;
+        q.log2s = (int)n, q.strips = 2L * nbt;
+        launch_nb(q, d->num_sms, d->status, st, d->pdl);
+        done = true;
+      } else if (tc_leaf_rows && d->ok_leaf) {
         TcLeaf q{};
         q.rows = 2 * s * nbt, q.batches = (int)S1, q.nchunks = 4;
         q.clen[0] = (int)T, q.clen[1] = q.clen[2] = q.clen[3] = (int)b;
@@ -2625,6 +2755,7 @@ static int set_smem_limits(void) {
   allow_dyn_smem(tc::k_tc_rowgemm<TcM2M>, lim);
   allow_dyn_smem(tc::k_tc_rowgemm<TcM2L>, lim);
   allow_dyn_smem(tc::k_tc_rowgemm<TcLeaf>, lim);
+  allow_dyn_smem(tc::k_tc_nbr<TcLeafNb>, lim);
   allow_dyn_smem(tc::k_tc_rowgemm16<TcS2M>, lim);
   allow_dyn_smem(tc::k_tc_rowgemm16<TcM2M>, lim);
   allow_dyn_smem(tc::k_tc_rowgemm16<TcM2L>, lim);
@@ -2725,6 +2856,7 @@ extern "C" void fmmk_destroy(fmmk_state *st) {
   }
   for (int i = 0; i < FMMK_GRAPHS; ++i)
     if (st->graphs[i].exec) cudaGraphExecDestroy(st->graphs[i].exec);
+  host_pipe_free(st->pipe);
   if (st->precision == 0) {
     Dev<double> *d = (Dev<double> *)st->dev;
     if (d) cudaFree(d->pool), delete d;
@@ -2768,6 +2900,66 @@ extern "C" int fmmk_execute_host(fmmk_state *st, const void *h_in, void *h_out, 
   int rc = fmmk_execute(st, work, work, stream, 0, err, errlen);
   if (rc) return rc;
   FMM_CUDA_TRY(cudaMemcpyAsync(h_out, work, esz * (size_t)N, cudaMemcpyDeviceToHost, s));
+  FMM_CUDA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
+/* n transforms of host arrays h_in[i] -> h_out[i] (each N complex), pipelined: transform i is
+ * copied into staging buffer i mod 3 on the copy-in stream, executed in place there on `stream`
+ * and copied back on the copy-out stream, so that with pinned host memory the three overlap
+ * across consecutive transforms (PCIe carries both directions at once).  The buffers (3 N
+ * complex on the device) and the two copy streams are made on the first call and kept with the
+ * plan.  Each transform's bits are those of fmmk_execute.  Returns when every output is in host
+ * memory, with `stream` ordered after the last copy-out. */
+extern "C" int fmmk_execute_host_many(fmmk_state *st, int n, const void *const *h_in, void *const *h_out,
+                                      void *stream, char *err, size_t errlen) {
+  cudaStream_t s = (cudaStream_t)stream;
+  const long N = st->precision == 0 ? ((Dev<double> *)st->dev)->N : ((Dev<float> *)st->dev)->N;
+  const size_t bytes = (st->precision == 0 ? sizeof(double2) : sizeof(float2)) * (size_t)N;
+  if (!st->pipe) {
+    HostPipe *hp = (HostPipe *)calloc(1, sizeof(HostPipe));
+    if (!hp) return 2;
+    cudaError_t e = cudaStreamCreateWithFlags(&hp->cin, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&hp->cout, cudaStreamNonBlocking);
+    for (int i = 0; i < FMMK_HOST_SLOTS && e == cudaSuccess; ++i) {
+      e = cudaMalloc(&hp->buf[i], bytes);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&hp->in_done[i], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&hp->ex_done[i], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&hp->out_done[i], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) {
+      snprintf(err, errlen, "execute_host_many staging: %s", cudaGetErrorString(e));
+      host_pipe_free(hp);
+      cudaGetLastError();
+      return e == cudaErrorMemoryAllocation ? 2 : 3;
+    }
+    st->pipe = hp;
+  }
+  HostPipe *hp = st->pipe;
+  /* the caller's stream may hold work the staging buffers' last users are ordered after */
+  FMM_CUDA_TRY(cudaEventRecord(hp->out_done[0], s));
+  FMM_CUDA_TRY(cudaStreamWaitEvent(hp->cin, hp->out_done[0], 0));
+  for (int i = 0; i < n; ++i) {
+    const int k = i % FMMK_HOST_SLOTS;
+    void *buf = hp->buf[k];
+    if (i >= FMMK_HOST_SLOTS) /* buffer k's previous transform has been copied out */
+      FMM_CUDA_TRY(cudaStreamWaitEvent(hp->cin, hp->out_done[k], 0));
+    FMM_CUDA_TRY(cudaMemcpyAsync(buf, h_in[i], bytes, cudaMemcpyHostToDevice, hp->cin));
+    FMM_CUDA_TRY(cudaEventRecord(hp->in_done[k], hp->cin));
+    FMM_CUDA_TRY(cudaStreamWaitEvent(s, hp->in_done[k], 0));
+    int rc = fmmk_execute(st, buf, buf, stream, 0, err, errlen);
+    if (rc) {
+      cudaStreamSynchronize(hp->cin);
+      cudaStreamSynchronize(hp->cout);
+      return rc;
+    }
+    FMM_CUDA_TRY(cudaEventRecord(hp->ex_done[k], s));
+    FMM_CUDA_TRY(cudaStreamWaitEvent(hp->cout, hp->ex_done[k], 0));
+    FMM_CUDA_TRY(cudaMemcpyAsync(h_out[i], buf, bytes, cudaMemcpyDeviceToHost, hp->cout));
+    FMM_CUDA_TRY(cudaEventRecord(hp->out_done[k], hp->cout));
+  }
+  /* the caller's stream ends after the last copy-out */
+  if (n > 0) FMM_CUDA_TRY(cudaStreamWaitEvent(s, hp->out_done[(n - 1) % FMMK_HOST_SLOTS], 0));
   FMM_CUDA_TRY(cudaStreamSynchronize(s));
   return 0;
 }
@@ -3097,9 +3289,14 @@ extern "C" int fmmk_describe(fmmk_state *st, char *buf, size_t len) {
              d->fuse_s2m);
   } else {
     Dev<float> *d = (Dev<float> *)st->dev;
-    snprintf(buf, len, "fft_threads=%d coarse_rows=%ld tc_min_rows=%ld fuse_s2m=%d tensor_cores=%s tuned=%d",
+    const char *form = d->tc_form == 0 ? "row" : d->tc_form == 3 ? "row16" : d->tc_form == 4 ? "ws" : "per_stage";
+    snprintf(buf, len,
+             "fft_threads=%d coarse_rows=%ld tc_min_rows=%ld fuse_s2m=%d tensor_cores=%s tc_form=%s "
+             "leaf_form=%s tuned=%d",
              d->fft_threads, d->coarse_rows, d->tc_min_rows, d->fuse_s2m,
-             d->tc ? (d->bf16 ? "bf16x3" : "tf32x3") : "none", d->tuned);
+             d->tc ? (d->bf16 ? "bf16x3" : "tf32x3") : "none", form,
+             !d->tc ? "cuda_cores" : (d->ok_lnb && d->tc_form < 0) ? "neighbour_sum" : d->ok_leaf ? "window_rows" : "cuda_cores",
+             d->tuned);
   }
   return 0;
 }

@@ -447,6 +447,264 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
 }
 
 
+/* ================================================================ neighbour-sum row form */
+
+constexpr int kNbOut = kRows - 2; /* output rows of a tile: lanes 1..126 (0 and 127 are the
+                                   * neighbours of the tile's first and last output rows) */
+
+/* Tensor-memory columns of the neighbour-sum form: the accumulator (npad, rounded up to 32, all
+ * four products accumulated in place) plus A hi and A lo of one K slice, as a power of two. */
+__host__ __device__ constexpr int nb_tmem_cols(int kpad, int npad) {
+  int need = ((npad + 31) / 32) * 32 + 2 * (kpad < kSlice ? kpad : kSlice);
+  return need <= 32 ? 32 : need <= 64 ? 64 : need <= 128 ? 128 : need <= 256 ? 256 : 512;
+}
+
+/* A row contraction whose output row i is its own row's block of D plus blocks of the rows
+ * before and after it: out[i] = D[i][0, w) + D[i-1][w, 2w) + D[i+1][2w, 3w), and, where the
+ * problem has them, h[i] = D[i][3w] + D[i-1][3w+1] + D[i+1][3w+2] (w = pb.b).  A convolution-like
+ * stage whose row i needs the data of rows i-1..i+1 (a window) then loads each row's data once
+ * instead of three times.  Rows are strips of pb.s (a power of two) periodic units; a tile holds
+ * 128 consecutive units of one strip (wrapping modulo s) and outputs the middle 126.  The MMA part
+ * is k_tc_rowgemm's (A split into TF32 hi/lo in registers, written into the row's TMEM lane; B
+ * pre-split in shared memory), with the four products accumulated in place (N = npad) so that the
+ * accumulator and one K slice of A fit two CTAs per SM.  Prob supplies, beyond k_tc_rowgemm's:
+ *   long s; int b;                         units per strip, block width w (a multiple of 8, <= 32)
+ *   long strips;                           strips per batch
+ *   __device__ bool has_h(int batch) const;                 the three h columns are in use
+ *   __device__ void put8_nb(long r, int batch, int c0, const float *t) const;
+ *                                          stores out[r][c0..c0+8)
+ *   __device__ void put_h(long r, int batch, float v) const;  stores h[r]
+ * Row r of strip st is unit r - st * s; src(c, r, batch) addresses row r's chunk c. */
+template <class Prob>
+__global__ void __launch_bounds__(256, 2) k_tc_nbr(const __grid_constant__ Prob pb, int *status) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+  __shared__ int lmap[4][2][8];
+  /* warp-edge values: [half][quarter][chunk 0, 1, h][0: lane 31's next block, 1: lane 0's
+   * previous block][8] */
+  __shared__ float xch[2][4][3][2][8];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int kpad = pb.kpad, npad = pb.npad;
+  const int ks = kpad < kSlice ? kpad : kSlice;
+  const int nslices = (kpad + ks - 1) / ks;
+  float *Bhi = reinterpret_cast<float *>(smem_raw);
+  float *Blo = Bhi + npad * kpad;
+  const uint32_t ncols = (uint32_t)nb_tmem_cols(kpad, npad);
+  if (warp == 0) tmem_alloc(&tmem_slot, ncols);
+  if (tid == 0) {
+    mbar_init(&mbar, 1);
+    fence_mbar_init();
+    abort_flag = 0;
+  }
+  if (tid < 4 * 2 * 8) {
+    const int sl = tid >> 4, h = (tid >> 3) & 1, i = tid & 7;
+    const int k0 = sl * ks, k = k0 + h * 32 + 4 * i;
+    int e = 0xFF;
+    if (sl < nslices && h * 32 + 4 * i < ks && k < kpad)
+      for (int c = 0; c < pb.nchunks; ++c)
+        if (k >= pb.coff[c] && k < pb.coff[c] + pb.clen[c]) e = c | ((k - pb.coff[c]) << 8);
+    lmap[sl][h][i] = e;
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = tmem_slot;
+  const uint32_t d_cols = (uint32_t)(((npad + 31) / 32) * 32);
+  const uint32_t t_ahi = tmem + d_cols, t_alo = tmem + d_cols + (uint32_t)ks;
+  const uint32_t idesc = make_idesc_tf32(npad);
+  const uint32_t b_sbo = (uint32_t)kpad * 32, lbo = 128;
+  const uint32_t bh = smem_addr(Bhi), bl = smem_addr(Blo);
+  const long s = pb.s;
+  const int tps = (int)((s + kNbOut - 1) / kNbOut); /* tiles per strip */
+  const int tiles_per_batch = tps * (int)pb.strips;
+  const int ntiles = tiles_per_batch * pb.batches;
+  const int quarter = warp & 3, my_half = warp >> 2;
+  const int my_m = quarter * 32 + lane;
+  const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
+  const int w = pb.b, nw8 = w >> 3; /* output chunks of 8 columns */
+
+  /* row of this thread's lane in a tile: unit (t * 126 - 1 + lane) mod s of the tile's strip */
+  auto tile_row = [&](int tile, int &batch) -> long {
+    batch = tile / tiles_per_batch;
+    const int tib = tile - batch * tiles_per_batch;
+    const int strip = tib / tps, t = tib - strip * tps;
+    return (long)strip * s + (((long)t * kNbOut - 1 + my_m) & (s - 1));
+  };
+
+  float4 v[8];
+  const float *rowp[4];
+  auto load_step = [&](int tile, int slice) {
+    if (slice == 0) {
+      int batch;
+      const long r = tile_row(tile, batch);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) rowp[c] = c < pb.nchunks ? pb.src(c, r, batch) : nullptr;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int e = lmap[slice][my_half][i];
+      const int c = e & 0xFF;
+      v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (c != 0xFF) {
+        const float *rp = c == 0 ? rowp[0] : (c == 1 ? rowp[1] : (c == 2 ? rowp[2] : rowp[3]));
+        if (rp) v[i] = __ldg(reinterpret_cast<const float4 *>(rp + (e >> 8)));
+      }
+    }
+  };
+
+  int cur_batch = -1;
+  uint32_t phase = 0;
+  const bool runs = pb.batches > 1;
+  const int tile_end = runs ? (int)(((long)ntiles * (blockIdx.x + 1)) / gridDim.x) : ntiles;
+  const int tile_step = runs ? 1 : (int)gridDim.x;
+  auto stage_b = [&](int batch) {
+    const float *gbh = pb.bhi + (long)batch * pb.bstride, *gbl = pb.blo + (long)batch * pb.bstride;
+    const int nb = npad * kpad;
+    for (int e0 = tid; e0 < nb; e0 += 4 * (int)blockDim.x) {
+      float vh[4], vl[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * blockDim.x;
+        if (e < nb) vh[u] = gbh[e], vl[u] = gbl[e];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * blockDim.x;
+        if (e < nb) {
+          const int n = e / kpad, k = e - n * kpad;
+          const uint32_t o = core_off(n, k, kpad) >> 2;
+          Bhi[o] = vh[u];
+          Blo[o] = vl[u];
+        }
+      }
+    }
+    fence_smem_to_async();
+    cur_batch = batch;
+  };
+  int tile = runs ? (int)(((long)ntiles * blockIdx.x) / gridDim.x) : (int)blockIdx.x, slice = 0;
+  pdl_trigger();
+  if (tile < tile_end) stage_b(tile / tiles_per_batch);
+  pdl_wait();
+  if (tile < tile_end) load_step(tile, 0);
+  while (tile < tile_end) {
+    int batch;
+    const long r = tile_row(tile, batch);
+    const int k0 = slice * ks, k1 = k0 + ks;
+    if (batch != cur_batch) stage_b(batch);
+    if (my_half * 32 < ks) {
+      float h[32], l[32];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const float a[4] = {v[i].x, v[i].y, v[i].z, v[i].w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          h[4 * i + j] = tf32_rna(a[j]);
+          l[4 * i + j] = tf32_rna(a[j] - h[4 * i + j]);
+        }
+      }
+      const uint32_t col = (uint32_t)(my_half * 32);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (my_half * 32 + 8 * q >= ks) break;
+        tmem_st8(t_ahi + lane_addr + col + 8 * q, h + 8 * q);
+        tmem_st8(t_alo + lane_addr + col + 8 * q, l + 8 * q);
+      }
+    }
+    tmem_st_wait();
+    fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+      if (lane == 0) {
+        fence_after_sync();
+        const int ksteps = ((k1 < kpad ? k1 : kpad) - k0) >> 3, kb = k0 >> 3;
+#pragma unroll 1
+        for (int p = 0; p < 4; ++p) { /* A_hi B_hi, A_hi B_lo, A_lo B_hi, A_lo B_lo, in place */
+          uint32_t ta = (p & 2) ? t_alo : t_ahi;
+          uint64_t db = make_desc(((p & 1) ? bl : bh) + 256u * kb, lbo, b_sbo);
+#pragma unroll 1
+          for (int kk = 0; kk < ksteps; ++kk, ta += 8, db += 16)
+            mma_tf32_ts(tmem, ta, db, idesc, (k0 | p | kk) != 0);
+        }
+        mma_commit(&mbar);
+      }
+      __syncwarp();
+    }
+    const bool last_slice = slice == nslices - 1;
+    const int ntile = last_slice ? tile + tile_step : tile;
+    const int nslice = last_slice ? 0 : slice + 1;
+    if (ntile < tile_end) load_step(ntile, nslice);
+    if (tid == 0 && !mbar_wait_bounded(&mbar, phase)) {
+      atomicExch(status, kErrWaitTimeout);
+      abort_flag = 1;
+    }
+    phase ^= 1;
+    __syncthreads();
+    fence_after_sync();
+    if (abort_flag) break;
+    if (last_slice) {
+      /* epilogue: half h takes the 8-column chunks h, h + 2 of the w outputs, half 1 also the h
+       * columns; lane i's neighbours are lanes i -+ 1 (shuffles), across warps shared memory */
+      const int tib = tile - batch * tiles_per_batch;
+      const long unit = (long)(tib - (tib / tps) * tps) * kNbOut - 1 + my_m;
+      const bool out_row = my_m >= 1 && my_m <= kNbOut && unit < s;
+      const bool hcols = my_half == 1 && pb.has_h(batch);
+      /* one chunk at a time (its own exchange slot): own, next and previous blocks from TMEM,
+       * the warp-edge values to shared memory, this half's barrier, then the sums */
+      auto half_bar = [&]() {
+        if (my_half) asm volatile("bar.sync 2, 128;" ::: "memory");
+        else asm volatile("bar.sync 1, 128;" ::: "memory");
+      };
+#pragma unroll 1
+      for (int j = 0; j < 2; ++j) {
+        const int c = my_half + 2 * j;
+        if (c >= nw8) break; /* warp-uniform */
+        float cen[8], nxt[8], prv[8];
+        tmem_ld8(tmem + lane_addr + (uint32_t)(8 * c), cen);
+        tmem_ld8(tmem + lane_addr + (uint32_t)(w + 8 * c), nxt);
+        tmem_ld8(tmem + lane_addr + (uint32_t)(2 * w + 8 * c), prv);
+        if (lane == 31)
+#pragma unroll
+          for (int i = 0; i < 8; ++i) xch[my_half][quarter][j][0][i] = nxt[i];
+        if (lane == 0)
+#pragma unroll
+          for (int i = 0; i < 8; ++i) xch[my_half][quarter][j][1][i] = prv[i];
+        half_bar();
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          float fl = __shfl_up_sync(0xffffffffu, nxt[i], 1);
+          float fr = __shfl_down_sync(0xffffffffu, prv[i], 1);
+          if (lane == 0) fl = quarter > 0 ? xch[my_half][quarter - 1][j][0][i] : 0.f;
+          if (lane == 31) fr = quarter < 3 ? xch[my_half][quarter + 1][j][1][i] : 0.f;
+          cen[i] += fl + fr;
+        }
+        if (out_row) pb.put8_nb(r, batch, 8 * c, cen);
+      }
+      if (hcols) {
+        float hv[8];
+        tmem_ld8(tmem + lane_addr + (uint32_t)(3 * w), hv);
+        if (lane == 31) xch[1][quarter][2][0][0] = hv[1];
+        if (lane == 0) xch[1][quarter][2][1][0] = hv[2];
+        half_bar();
+        float fl = __shfl_up_sync(0xffffffffu, hv[1], 1);
+        float fr = __shfl_down_sync(0xffffffffu, hv[2], 1);
+        if (lane == 0) fl = quarter > 0 ? xch[1][quarter - 1][2][0][0] : 0.f;
+        if (lane == 31) fr = quarter < 3 ? xch[1][quarter + 1][2][1][0] : 0.f;
+        if (out_row) pb.put_h(r, batch, hv[0] + (fl + fr));
+      }
+      fence_before_sync();
+      __syncthreads();
+    }
+    tile = ntile, slice = nslice;
+  }
+  if (tid == 0 && abort_flag) mbar_wait_bounded(&mbar, phase ^ 1);
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
 /* ===================================================================== 16-lane row form */
 
 /* Column permutation within each group of 16 (an involution-free bijection): TMEM / shared

@@ -24,7 +24,7 @@ STATUS = {0: "OK", 1: "ERR_INVALID", 2: "ERR_NOMEM", 3: "ERR_CUDA", 4: "ERR_NO_D
 # Every symbol include/fmmfft.h declares.
 EXPORTS = ["getwlen2", "getvlen", "mfti", "mft", "fmmfft_last_error", "fmmfft_last_error_string",
            "fmmfft_plan_create", "fmmfft_plan_destroy", "fmmfft_plan_device_bytes",
-           "fmmfft_execute", "fmmfft_execute_inverse", "fmmfft_execute_host",
+           "fmmfft_execute", "fmmfft_execute_inverse", "fmmfft_execute_host", "fmmfft_execute_host_many",
            "fmmfft_debug_fetch", "fmmfft_profile_start", "fmmfft_profile_stop",
            "fmmfft_stage_name", "fmmfft_execute_noalloc", "fmmfft_plan_check",
            "fmmfft_plan_selftest_wait", "fmmfft_plan_create_batched", "fmmfft_execute_many",
@@ -72,6 +72,8 @@ def load(path=LIB_PATH):
     for f in ("fmmfft_execute", "fmmfft_execute_inverse", "fmmfft_execute_host"):
         getattr(lib, f).argtypes = [_VP, _VP, _VP, _VP]
         getattr(lib, f).restype = _I
+    lib.fmmfft_execute_host_many.argtypes = [_VP, _I, _VP, _VP, _VP]
+    lib.fmmfft_execute_host_many.restype = _I
     lib.fmmfft_debug_fetch.argtypes = [_VP, _VP, _VP, _VP, _VP]
     lib.fmmfft_profile_start.argtypes = [_VP, _I]
     lib.fmmfft_profile_stop.argtypes = [_VP, _VP, _VP, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)]
@@ -276,6 +278,14 @@ class Plan:
     def execute_graph_ptr(self, d_in, d_out, stream=0):
         """Forward transform through the plan's cached CUDA graph for (d_in, d_out)."""
         _check(load().fmmfft_execute_graph(self._h, d_in, d_out, stream or None))
+
+    def execute_host_many_ptr(self, h_ins, h_outs, stream=0):
+        """Pipelined host execute over a sequence of host buffers (pointers, N complex each)."""
+        n = len(h_ins)
+        assert len(h_outs) == n
+        ins = (ctypes.c_void_p * max(1, n))(*h_ins)
+        outs = (ctypes.c_void_p * max(1, n))(*h_outs)
+        _check(load().fmmfft_execute_host_many(self._h, n, ins, outs, stream or None))
 
     def execute_host_ptr(self, h_in, h_out, stream=0):
         """Host-memory transform (pointers, e.g. pinned buffers): H2D copy, execute, D2H copy,

@@ -158,6 +158,16 @@ int fmmfft_execute_refined(fmmfft_plan plan, const void *d_in, void *d_out, void
 
 /* Same transform from and to HOST memory: copies in, executes, copies out, synchronises. */
 int fmmfft_execute_host(fmmfft_plan plan, const void *h_in, void *h_out, void *stream);
+/* n transforms of host arrays, h_in[i] -> h_out[i] (N complex each; h_in[i] == h_out[i] is
+ * allowed), pipelined: the copy-in of transform i+1, the execute of transform i and the copy-out
+ * of transform i-1 overlap on three streams (with page-locked host memory PCIe carries both
+ * directions at once), so a sequence of host-resident transforms costs about max(copy-in,
+ * execute, copy-out) each instead of their sum.  Three device staging buffers of N complex and
+ * two copy streams are made on the first call and kept with the plan.  Each output is bitwise
+ * what fmmfft_execute_host gives.  Returns when every output is in host memory.  Replaces a loop
+ * over the reference's mft (fmmfft.c:980) for a stream of inputs. */
+int fmmfft_execute_host_many(fmmfft_plan plan, int n, const void *const *h_in, void *const *h_out,
+                             void *stream);
 
 /* Block-distributed transform: P input blocks of M = N/P complex values each (block r = rank
  * r's lq-block qr of the reference's SPMD layout, i.e. elements r*M .. r*M+M-1 of the vector)

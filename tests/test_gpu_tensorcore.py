@@ -119,18 +119,28 @@ LEAF_CASES = [(4096, 4, 8, 16), (16384, 8, 12, 32), (65536, 16, 16, 32), (65536,
               (1 << 18, 32, 24, 16), (1 << 18, 256, 12, 16), (1 << 20, 128, 24, 32), (1 << 20, 1024, 16, 8)]
 
 
+@pytest.mark.parametrize("leaf_form", ["neighbour_sum", "window_rows"])
 @pytest.mark.parametrize("N,P,T,b", LEAF_CASES)
-def test_tc_leaf_with_half_shift_column(fm, monkeypatch, N, P, T, b):
+def test_tc_leaf_with_half_shift_column(fm, monkeypatch, N, P, T, b, leaf_form):
     """The leaf contraction on the tensor cores at every size (FMMFFT_TC_MIN_ROWS=1, read when
-    the plan is made).  Its operator carries one extra output column, the next box's
-    half-shifted first point for sections sc >= P/2, which the epilogue stores in place of the
-    in-box value (sc > P/2) or leaves for the sc = P/2 mean; the half-shift stage is then that
-    mean alone.  The near-field weights grow like P/pi against O(1) sums, hence the large-P
-    cases.  u (the leaf output) and the transform against the FP64 oracle."""
+    the plan is made), in both forms.  Window rows (FMMFFT_LEAF_FORM=row): a row holds its box's
+    expansion and the 3-box sample window, and the operator carries one extra output column, the
+    next box's half-shifted first point for sections sc >= P/2, which the epilogue stores in place
+    of the in-box value (sc > P/2) or leaves for the sc = P/2 mean.  Neighbour sums (default for
+    b <= 32): a row holds its own box only, the operator has blocks for the box and its two
+    neighbours (and three half-shift columns), and the epilogue adds the blocks of adjacent rows
+    (shuffles within a warp, shared memory across warps, tiles of 126 output rows with wrap).
+    The half-shift stage is then the sc = P/2 mean alone.  The near-field weights grow like P/pi
+    against O(1) sums, hence the large-P cases.  u (the leaf output) and the transform against
+    the FP64 oracle.  The autotuner is off so that the per-stage routing under test runs."""
     monkeypatch.setenv("FMMFFT_TC_MIN_ROWS", "1")
+    monkeypatch.setenv("FMMFFT_AUTOTUNE", "0")
+    if leaf_form == "window_rows":
+        monkeypatch.setenv("FMMFFT_LEAF_FORM", "row")
     x = ol.seeded_input(N, 29 + N % 89)
     o = ol.forward_ex(x, P, T, b)
     plan = fm.Plan(N, P, T, b, "f32_tc")
+    assert "leaf_form=" + leaf_form in plan.describe(), plan.describe()
     plan.profile_start(1)
     y = run_device(plan, x)
     _, stages = plan.profile_stop()
