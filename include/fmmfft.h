@@ -49,7 +49,12 @@ typedef enum {
  * the others (interleaved re, im). */
 typedef enum {
   FMMFFT_F64 = 0,     /* FP64 everywhere (the reference's precision) */
-  FMMFFT_F32 = 1,     /* FP32 on CUDA cores: the plain GPU FMM-FFT */
+  FMMFFT_F32 = 1,     /* FP32 on CUDA cores: the plain GPU FMM-FFT.  For complex64 plans with
+                         terms >= 10 the P block-DC bins y[r M] (r < P) are the exact sums
+                         sum_n x[n] e^{-2 pi i n r / P} (FP64 on the GPU) instead of the FMM's
+                         value: at those bins the FMM's FP32 value carries the largest error of
+                         the transform (7e-5 relative at P = 64), while its truncation there is
+                         below 3.3e-8 for terms >= 10.  FP64 plans keep the FMM's value. */
   FMMFFT_F32_TC = 2,  /* operator contractions on tcgen05 tensor cores in split TF32 (operands
                          split into TF32 hi + lo, three products, FP32 accumulation), rest FP32 */
   FMMFFT_BF16X3 = 3   /* the same contractions in BF16x3 (BF16 hi + lo, three products, FP32
@@ -76,7 +81,10 @@ void mfti(long lq, long p, long terms, long b, double *w, double *v, long szkeep
 /* src/fmmfft.c:980.  Forward FMM-FFT of the full vector qr (p*lq complex128, host memory) in
  * place.  dir must be +1 (the reference's dir < 0 path is not a correct inverse,
  * fmmfft.c:976-977 vs :1080; use fmmfft_execute_inverse).  myid, w, v, sz1, szwk and
- * forward_plan are accepted for signature compatibility and not used (w may be NULL). */
+ * forward_plan are accepted for signature compatibility and not used (w may be NULL): the
+ * operators come from the device plan that mfti made for the same (lq, p, terms, b) (made here
+ * on first use if mfti was not called), which holds what mfti wrote into w; a w modified by the
+ * caller after mfti is not seen. */
 void mft(long lq, void *qr, long dir, long p, long myid, long terms, long b, double *w, double *v,
          long sz1, long szwk, void *forward_plan);
 
