@@ -162,6 +162,7 @@ template <typename R> struct Dev {
   unsigned *sync;   /* grid barrier of the coarse-tree kernel: [0] arrivals, [32] generation */
   long coarse_rows; /* levels with fewer rows go to the coarse-tree kernel (0: none) */
   int coarse_grid;  /* blocks of the coarse-tree kernel an SM holds (0: its operators do not fit) */
+  int coarse_dbuf;  /* the coarse-tree kernel's operators in two alternating buffers */
   int fuse_s2m;     /* S2M inside the sections pass where tiles hold whole boxes */
   unsigned env_set; /* knobs an environment switch fixed (the autotuner leaves them): bits below */
   int tuned;        /* the knobs come from the autotuner */
@@ -1621,38 +1622,43 @@ __global__ void k_block_dc(const typename cplx<R>::T *__restrict__ ssum,
 /* ======================================================================== coarse tree */
 
 /* The coarse levels of the tree (few boxes: every level whose row count per transform is below
- * a threshold, at most 64 boxes per plane) in one launch instead of one launch per level: the
- * upward M2M for parent levels Lm .. 2, the top flip, and the downward M2L + L2L for child levels
- * 3 .. Ll.  Every expansion plane (section, re/im, transform) is independent of the others at
- * every level (its neighbours wrap within the plane), so one block takes one plane through all
- * of these levels, with block barriers between levels and no grid-wide synchronisation.  Same
- * operators, layouts and outputs (every level's phi / psi) as the per-level launches (reference
- * fmmfft.c:476-515 upward, :620-749 top and downward).  Each level's operator is staged in shared
- * memory by the whole block (its copy issued while the level before it runs); then one warp per
- * output row, lane = output column (N / 32 columns per lane), the row's A values broadcast from
- * the lanes that loaded them; the K sum accumulates per 32-column block, then into the total
- * (two-level FP32 accumulation, as in the row kernels). */
+ * a threshold, at most 2^kCoarseMaxLevel boxes per plane) in one launch instead of one launch per
+ * level: the upward M2M for parent levels Lm .. 2, the top flip, and the downward M2L + L2L for
+ * child levels 3 .. Ll.  Every expansion plane (section, re/im, transform) is independent of the
+ * others at every level (its neighbours wrap within the plane), so one block takes one plane
+ * through all of these levels.  The plane's coarse levels stay in shared memory: phi of the
+ * levels above Lm (made by the per-level kernels) is read from global memory once, every level
+ * computed here is kept in shared memory for the levels after it and written to global memory
+ * once (the per-level kernels after this one and the debug views read it there), so a level
+ * costs one block barrier and no global round trip.  The levels' operators are copied with
+ * cp.async into two alternating buffers, the next level's while the current one computes (one
+ * buffer, copied after the barrier, when two do not fit).  Same operators, layouts and outputs
+ * as the per-level launches (reference fmmfft.c:476-515 upward, :620-749 top and downward).
+ * Compute: one warp per output row, lane = output column (N / 32 columns per lane); the K sum
+ * accumulates per 32-column block, then into the total (two-level FP32 accumulation, as in the
+ * row kernels).  Launched as a programmatic dependent launch: the first operator is staged
+ * before the wait for the kernel that made its input. */
 template <typename R> struct CoarseArgs {
   R *phi, *psi;
   const R *bm2m, *btop, *bm2l;
   long S1; /* planes / 2, all transforms of the execute */
   int T, Lm, Ll; /* coarse M2M parent levels Lm..2 (none when Lm < 2); M2L child levels 3..Ll */
+  int dbuf;      /* two operator buffers */
 };
 constexpr int kCoarseMaxLevel = 6; /* coarse M2M parents hold at most 2^6 boxes per plane */
-constexpr int kCoarseWarps = 32;   /* a block: one warp per row, a coarse level's rows in one pass */
+constexpr int kCoarseWarps = 32;   /* a block: one warp per row */
+constexpr int kCoarseTop = kCoarseMaxLevel + 1; /* highest level a block holds (M2M input, M2L) */
 
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 /* Issue the copy of a level's operator B (K x N, row-major) into the shared array Bs with
- * cp.async, in 16-byte pieces where the size and address allow, else one element per copy.
- * Nothing waits here: the level's operator does not depend on the previous level, so its copy
- * is issued before the grid barrier and lands while the block waits there; coarse_rows waits
- * for it.  The caller has finished reading Bs (coarse_rows ends on a block barrier). */
+ * cp.async, in 16-byte pieces where the size and address allow, else one element per copy;
+ * nothing waits here. */
 template <typename R>
 __device__ __forceinline__ void coarse_stage_b(int K, int N, const R *__restrict__ B, R *__restrict__ Bs) {
   const int n = K * N;
   const uint32_t sb = (uint32_t)__cvta_generic_to_shared(Bs);
-  if (((size_t)n * sizeof(R)) % 16 == 0 && ((uintptr_t)B & 15) == 0) {
+  if (((size_t)n * sizeof(R)) % 16 == 0 && ((uintptr_t)B & 15) == 0 && (sb & 15) == 0) {
     constexpr int per = 16 / sizeof(R);
     for (int e = threadIdx.x * per; e < n; e += blockDim.x * per)
       tc::cp_async16(sb + (uint32_t)(e * sizeof(R)), B + e);
@@ -1667,101 +1673,157 @@ __device__ __forceinline__ void coarse_stage_b(int K, int N, const R *__restrict
   asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
-/* out[r][n] = sum_k A(r, k) Bs[k][n] for the rows of one level of one plane, all by this block;
- * B (K x N) is in flight into the shared array Bs (coarse_stage_b), and the block stages
- * kCoarseWarps rows of A at a time into As (one row per warp), so a row costs one round of
- * loads (a coarse level's rows are one round); arow(r, k) is
- * the address of element k of row r's A.  Ends on a block barrier after the last stores, so the
- * next level reads this one's output. */
-template <typename R, class Arow>
-__device__ __forceinline__ void coarse_rows(long rows, int K, int N, R *__restrict__ Bs, R *__restrict__ As,
-                                            R *__restrict__ out, Arow arow) {
-  cp_async_wait0(); /* this thread's copies of the operator */
-  __syncthreads();  /* everyone's copies; the previous level's reads of As are done */
+/* Floats (elements) of a plane's levels 2..L: (2^(L+1) - 4) rows of T. */
+__host__ __device__ constexpr long coarse_lvl_rows(int L) { return (2L << L) - 4; }
+
+/* Shared memory of the coarse kernel: one or two operator buffers (the largest operator, the
+ * M2L one, 5T x 2T), the plane's phi and psi levels 2..kCoarseTop and the split-K partial sums
+ * (at most 32 rows x parts of 2T). */
+template <typename R> static size_t coarse_smem(long T, int dbuf) {
+  return sizeof(R) * ((dbuf ? 20 : 10) * (size_t)T * T + 2 * (size_t)coarse_lvl_rows(kCoarseTop) * T +
+                      (size_t)kCoarseWarps * 4 * T);
+}
+
+/* Rows [0, rows) of one level: out[r][n] = sum_k A(r, k) Bs[k][n].  Row r's A is up to three
+ * contiguous pieces of shared memory, segs(r, p, o) filling piece pointers p[] and their first K
+ * index o[] (o[0] = 0, pieces in K order, o[3] = K).  A level with fewer rows than warps splits
+ * each row's K range over S = warps / rows warps (S <= 8); their partial sums go to `red` and are
+ * added in a fixed order (so a plane's bits do not depend on anything else).  Lane = output
+ * column (NJ columns per lane, N <= 32 NJ).  Outputs go to the shared level Os and to global
+ * memory Og.  Ends with the outputs written by the threads that wrote them (the caller's next
+ * barrier publishes them). */
+template <typename R, int NJ, class Segs>
+__device__ __forceinline__ void coarse_level(int rows, int K, int N, const R *__restrict__ Bs, R *__restrict__ Os,
+                                             R *__restrict__ Og, R *__restrict__ red, Segs segs) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int W = kCoarseWarps;
-  for (long r0 = 0; r0 < rows; r0 += W) { /* block-uniform */
-    for (int e0 = threadIdx.x; e0 < W * K; e0 += 4 * blockDim.x) { /* 4 loads in flight */
-      R v[4];
+  int S = kCoarseWarps / rows;
+  S = S < 1 ? 1 : (S > 8 ? 8 : S);
+  const int kper = (K + S - 1) / S;
+  for (int it = warp; it < rows * S; it += kCoarseWarps) {
+    const int r = it / S, part = it - r * S;
+    const int k0 = part * kper, k1 = k0 + kper < K ? k0 + kper : K;
+    const R *pc[3];
+    int o[4];
+    segs(r, pc, o);
+    R acc[NJ];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int e = e0 + u * blockDim.x, w = e / K, k = e - w * K;
-        const long r = r0 + w;
-        v[u] = (e < W * K && r < rows) ? *arow(r, k) : R(0);
+    for (int j = 0; j < NJ; ++j) acc[j] = R(0);
+    for (int q = 0; q < 3; ++q) {
+      const int lo = k0 > o[q] ? k0 : o[q], hi = k1 < o[q + 1] ? k1 : o[q + 1];
+      const R *ap = pc[q];
+#pragma unroll 4
+      for (int k = lo; k < hi; ++k) {
+        const R av = ap[k - o[q]];
+        const R *bk = Bs + k * N + lane;
+#pragma unroll
+        for (int j = 0; j < NJ; ++j)
+          if (NJ == 1 || lane + 32 * j < N) acc[j] = fma(av, bk[32 * j], acc[j]);
       }
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-        if (e0 + u * (int)blockDim.x < W * K) As[e0 + u * blockDim.x] = v[u];
     }
+    if (S == 1) {
+#pragma unroll
+      for (int j = 0; j < NJ; ++j)
+        if (lane + 32 * j < N) Os[r * N + lane + 32 * j] = acc[j], Og[r * N + lane + 32 * j] = acc[j];
+    } else {
+#pragma unroll
+      for (int j = 0; j < NJ; ++j)
+        if (lane + 32 * j < N) red[it * N + lane + 32 * j] = acc[j];
+    }
+  }
+  if (S > 1) {
     __syncthreads();
-    const long r = r0 + warp;
-    if (r < rows) {
-      const R *ar = As + warp * K;
-      R acc[4] = {0, 0, 0, 0};
-      for (int k0 = 0; k0 < K; k0 += 32) {
-        R part[4] = {0, 0, 0, 0};
-        const int kn = K - k0 < 32 ? K - k0 : 32;
-#pragma unroll 8
-        for (int kk = 0; kk < kn; ++kk) {
-          const R a = ar[k0 + kk];
-          const R *bk = Bs + (k0 + kk) * N;
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-            if (lane + 32 * j < N) part[j] = fma(a, bk[lane + 32 * j], part[j]);
-        }
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[j] += part[j];
-      }
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (lane + 32 * j < N) out[r * N + lane + 32 * j] = acc[j];
+    for (int e = threadIdx.x; e < rows * N; e += blockDim.x) {
+      const int r = e / N, c = e - r * N;
+      R v = red[(r * S) * N + c];
+      for (int part = 1; part < S; ++part) v += red[(r * S + part) * N + c];
+      Os[e] = v;
+      Og[e] = v;
     }
-    __syncthreads(); /* As is refilled next */
   }
 }
 
-/* Shared memory of the coarse kernel: the largest operator, the M2L one (5T x 2T), and 8 rows
- * of the widest A (5T). */
-template <typename R> static size_t coarse_smem(long T) {
-  return sizeof(R) * (10 * (size_t)T * T + 5 * kCoarseWarps * (size_t)T);
+/* the same with the lane's column count chosen from N */
+template <typename R, class Segs>
+__device__ __forceinline__ void coarse_level_n(int rows, int K, int N, const R *Bs, R *Os, R *Og, R *red, Segs segs) {
+  if (N <= 32) coarse_level<R, 1>(rows, K, N, Bs, Os, Og, red, segs);
+  else if (N <= 64) coarse_level<R, 2>(rows, K, N, Bs, Os, Og, red, segs);
+  else coarse_level<R, 4>(rows, K, N, Bs, Os, Og, red, segs);
 }
 
 template <typename R> __global__ void __launch_bounds__(32 * kCoarseWarps) k_coarse(CoarseArgs<R> a) {
   extern __shared__ __align__(16) unsigned char coarse_raw[];
-  R *Bs = reinterpret_cast<R *>(coarse_raw);
-  R *As = Bs + 10L * a.T * a.T;
-  const long S1 = a.S1, pl = blockIdx.x;
   const int T = a.T;
-  /* level l of this block's plane: 2^l boxes of T values */
+  R *Bs[2];
+  Bs[0] = reinterpret_cast<R *>(coarse_raw);
+  Bs[1] = a.dbuf ? Bs[0] + 10L * T * T : Bs[0];
+  R *Ph = Bs[0] + (a.dbuf ? 20L : 10L) * T * T; /* phi levels 2..kCoarseTop of this plane */
+  R *Ps = Ph + coarse_lvl_rows(kCoarseTop) * T; /* psi levels 2..kCoarseTop */
+  R *red = Ps + coarse_lvl_rows(kCoarseTop) * T; /* split-K partial sums: 32 x 4T */
+  const long S1 = a.S1, pl = blockIdx.x;
+  /* level l of this block's plane, in global and in shared memory */
   auto lv = [&](R *base, int l) { return base + lvl_off(l, S1, T) + pl * (1L << l) * T; };
-  auto m2m_b = [&](int L) { return a.bm2m + (long)(L - 2) * 2 * T * T; };
-  auto m2l_b = [&](int l) { return a.bm2l + (long)(l - 3) * 10 * T * T; };
-  if (a.Lm >= 2)
-    coarse_stage_b<R>(2 * T, T, m2m_b(a.Lm), Bs);
-  else
-    coarse_stage_b<R>(T, T, a.btop, Bs);
-  for (int L = a.Lm; L >= 2; --L) { /* M2M: parent L from child pairs of L+1 */
-    const R *child = lv(a.phi, L + 1);
-    coarse_rows<R>(1L << L, 2 * T, T, Bs, As, lv(a.phi, L), [=](long r, int k) { return child + r * 2 * T + k; });
-    if (L > 2)
-      coarse_stage_b<R>(2 * T, T, m2m_b(L - 1), Bs);
-    else
-      coarse_stage_b<R>(T, T, a.btop, Bs);
+  auto sl = [&](R *base, int l) { return base + ((1L << l) - 4) * T; };
+  /* the levels in order: M2M parents Lm..2, the top flip, M2L children 3..Ll */
+  const int nm = a.Lm >= 2 ? a.Lm - 1 : 0, nlev = nm + 1 + (a.Ll >= 3 ? a.Ll - 2 : 0);
+  auto stage_op = [&](int i, R *dst) {
+    if (i < nm) coarse_stage_b<R>(2 * T, T, a.bm2m + (long)(a.Lm - i - 2) * 2 * T * T, dst);
+    else if (i == nm) coarse_stage_b<R>(T, T, a.btop, dst);
+    else coarse_stage_b<R>(5 * T, 2 * T, a.bm2l + (long)(i - nm - 1) * 10 * T * T, dst);
+  };
+  tc::pdl_trigger();
+  stage_op(0, Bs[0]); /* a plan constant */
+  tc::pdl_wait();
+  { /* phi of the levels this block does not make: Lm+1 .. Ltop (only Lm+1 when the M2M runs
+     * here; the top flip and M2L read levels 2..Ll) */
+    const int lo = a.Lm >= 2 ? a.Lm + 1 : 2;
+    const int hi = a.Ll > lo ? a.Ll : lo;
+    for (int l = lo; l <= hi; ++l) {
+      const R *g = lv(a.phi, l);
+      R *d = sl(Ph, l);
+      const int n = (1 << l) * T;
+      for (int e = threadIdx.x; e < n; e += blockDim.x) d[e] = g[e];
+    }
   }
-  { /* top flip: psi_2[c] = topflp . phi_2[(c + 2) mod 4] */
-    const R *phi2 = lv(a.phi, 2);
-    coarse_rows<R>(4, T, T, Bs, As, lv(a.psi, 2), [=](long r, int k) { return phi2 + ((r + 2) & 3) * T + k; });
-  }
-  if (a.Ll >= 3) coarse_stage_b<R>(5 * T, 2 * T, m2l_b(3), Bs);
-  for (int l = 3; l <= a.Ll; ++l) { /* M2L + L2L: child level l, one row per parent box */
-    const R *psi_par = lv(a.psi, l - 1), *phi = lv(a.phi, l);
-    const long mask = (1L << l) - 1;
-    coarse_rows<R>(1L << (l - 1), 5 * T, 2 * T, Bs, As, lv(a.psi, l), [=](long r, int k) {
-      if (k < T) return psi_par + r * T + k;
-      if (k < 3 * T) return phi + ((2 * r - 2) & mask) * T + (k - T);
-      return phi + ((2 * r + 2) & mask) * T + (k - 3 * T);
-    });
-    if (l < a.Ll) coarse_stage_b<R>(5 * T, 2 * T, m2l_b(l + 1), Bs);
+  for (int i = 0; i < nlev; ++i) {
+    R *B = Bs[i & 1];
+    if (a.dbuf) {
+      cp_async_wait0(); /* this thread's copies of level i's operator */
+      __syncthreads();  /* everyone's; the level before is written and done with the other buffer */
+      if (i + 1 < nlev) stage_op(i + 1, Bs[(i + 1) & 1]);
+    } else {
+      if (i > 0) {
+        __syncthreads(); /* the level before is done with the buffer */
+        stage_op(i, B);
+      }
+      cp_async_wait0();
+      __syncthreads();
+    }
+    if (i < nm) { /* M2M: parent level L from child pairs of L + 1 */
+      const int L = a.Lm - i;
+      const R *child = sl(Ph, L + 1);
+      coarse_level_n<R>(1 << L, 2 * T, T, B, sl(Ph, L), lv(a.phi, L), red, [=](int r, const R **p, int *o) {
+        p[0] = child + r * 2 * T, p[1] = p[2] = p[0];
+        o[0] = 0, o[1] = o[2] = o[3] = 2 * T;
+      });
+    } else if (i == nm) { /* top flip: psi_2[c] = topflp . phi_2[(c + 2) mod 4] */
+      const R *phi2 = sl(Ph, 2);
+      coarse_level_n<R>(4, T, T, B, sl(Ps, 2), lv(a.psi, 2), red, [=](int r, const R **p, int *o) {
+        p[0] = phi2 + ((r + 2) & 3) * T, p[1] = p[2] = p[0];
+        o[0] = 0, o[1] = o[2] = o[3] = T;
+      });
+    } else { /* M2L + L2L: child level l, one row per parent box: psi of the parent, then the
+              * child pairs 2r-2, 2r-1 and 2r+2, 2r+3 (wrapping; a pair never straddles the end) */
+      const int l = i - nm + 2;
+      const R *psi_par = sl(Ps, l - 1), *phi = sl(Ph, l);
+      const int mask = (1 << l) - 1;
+      coarse_level_n<R>(1 << (l - 1), 5 * T, 2 * T, B, sl(Ps, l), lv(a.psi, l), red,
+                        [=](int r, const R **p, int *o) {
+                          p[0] = psi_par + r * T;
+                          p[1] = phi + ((2 * r - 2) & mask) * T;
+                          p[2] = phi + ((2 * r + 2) & mask) * T;
+                          o[0] = 0, o[1] = T, o[2] = 3 * T, o[3] = 5 * T;
+                        });
+    }
   }
   cp_async_wait0();
 }
@@ -2000,7 +2062,9 @@ constexpr long kCoarseRows = 4096; /* default: tree levels with fewer rows form 
 template <typename R> static void coarse_setup(Dev<R> *d) {
   d->coarse_rows = kCoarseRows;
   if (const char *ev = getenv("FMMFFT_COARSE_ROWS")) d->coarse_rows = atol(ev), d->env_set |= KNOB_COARSE;
-  const size_t sm = coarse_smem<R>(d->T);
+  /* two operator buffers where they fit beside the plane's levels, else one */
+  d->coarse_dbuf = coarse_smem<R>(d->T, 1) <= (size_t)200 * 1024;
+  const size_t sm = coarse_smem<R>(d->T, d->coarse_dbuf);
   int nb = 0;
   if (sm <= (size_t)200 * 1024) {
     /* the attribute is the kernel's, not the plan's: always the full allowance, so that a plan
@@ -2394,9 +2458,20 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   /* 5: top flip, or the whole coarse tree (M2M Lm..2, top flip, M2L 3..Ll) */
   stage(ST_TOP);
   if (coarse) {
-    CoarseArgs<R> ca{d->phi, d->psi, d->bm2m, d->btop, d->bm2l, S1e, (int)T, (int)Lm, (int)Ll};
-    /* one block per expansion plane of every transform of the execute */
-    k_coarse<R><<<(unsigned)(2 * S1e), 32 * kCoarseWarps, coarse_smem<R>(T), st>>>(ca);
+    CoarseArgs<R> ca{d->phi, d->psi, d->bm2m, d->btop, d->bm2l, S1e, (int)T, (int)Lm, (int)Ll, d->coarse_dbuf};
+    /* one block per expansion plane of every transform of the execute; a programmatic dependent
+     * launch (it stages its first operator before waiting for the level below) */
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(2 * S1e));
+    cfg.blockDim = dim3(32 * kCoarseWarps);
+    cfg.dynamicSmemBytes = coarse_smem<R>(T, d->coarse_dbuf);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = d->pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, k_coarse<R>, ca);
     pf.launches[ST_TOP]++;
   } else {
     ProbTop<R> pb{d->phi + lvl_off(2, S1e, T), d->btop, d->psi + lvl_off(2, S1e, T), 2 * S1e * 4,
