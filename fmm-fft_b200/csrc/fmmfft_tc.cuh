@@ -174,6 +174,30 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v) {
   for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+/* 8 consecutive 32-bit TMEM columns of this thread's lane, issued without waiting: the
+ * registers hold the values only after tmem_ld_wait(), and reg_fence8 (after the wait) makes
+ * every later use of them depend on it. */
+__device__ __forceinline__ void tmem_ld8_issue(uint32_t taddr, uint32_t (&r)[8]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+      : "r"(taddr)
+      : "memory");
+}
+__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void reg_fence8(uint32_t (&r)[8]) {
+  asm volatile("" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]));
+}
+
+/* 16 lanes x 16 columns (shape 16x256b), issued without waiting (see tmem_ld8_issue). */
+__device__ __forceinline__ void tmem_ld16x2_issue(uint32_t taddr, uint32_t (&r)[8]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.16x256b.x2.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+      : "r"(taddr)
+      : "memory");
+}
+
 /* The same 16 lanes x 16 columns into registers (same register order as tmem_st16x2). */
 __device__ __forceinline__ void tmem_ld16x2(uint32_t taddr, float *v) {
   uint32_t r[8];
@@ -249,13 +273,15 @@ __host__ __device__ constexpr int tmem_cols(int kpad, int npad) {
  * loads of step i+1 are issued before the CTA waits for step i's MMAs.  Two CTAs per SM. */
 template <class Prob>
 __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ Prob pb, int *status) {
+  /* 8 warps: 4 TMEM lane quarters x NS column halves; a thread moves CW columns of a slice */
+  constexpr int NS = 2, CW = kSlice / NS, NF = CW / 4;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ uint64_t mbar;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
-  /* load map: for slice s, column half h and float4 i, the A chunk (low byte, 0xFF = zero)
+  /* load map: for slice s, column group h and float4 i, the A chunk (low byte, 0xFF = zero)
    * and the float offset within that chunk's row (high bits) */
-  __shared__ int lmap[4][2][8];
+  __shared__ int lmap[4][NS][NF];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int kpad = pb.kpad, npad = pb.npad;
   const int ks = kpad < kSlice ? kpad : kSlice;
@@ -269,11 +295,11 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
     fence_mbar_init();
     abort_flag = 0;
   }
-  if (tid < 4 * 2 * 8) {
-    const int sl = tid >> 4, h = (tid >> 3) & 1, i = tid & 7;
-    const int k0 = sl * ks, k = k0 + h * 32 + 4 * i;
+  if (tid < 4 * NS * NF) {
+    const int sl = tid / (NS * NF), h = (tid / NF) % NS, i = tid % NF;
+    const int k0 = sl * ks, k = k0 + h * CW + 4 * i;
     int e = 0xFF;
-    if (sl < nslices && h * 32 + 4 * i < ks && k < kpad)
+    if (sl < nslices && h * CW + 4 * i < ks && k < kpad)
       for (int c = 0; c < pb.nchunks; ++c)
         if (k >= pb.coff[c] && k < pb.coff[c] + pb.clen[c]) e = c | ((k - pb.coff[c]) << 8);
     lmap[sl][h][i] = e;
@@ -295,7 +321,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
   const int my_m = quarter * 32 + lane;
   const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
 
-  float4 v[8];
+  float4 v[NF];
   const float *rowp[4];
   auto load_step = [&](int tile, int slice) {
     if (slice == 0) {
@@ -306,7 +332,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
       for (int c = 0; c < 4; ++c) rowp[c] = (live && c < pb.nchunks) ? pb.src(c, r, batch) : nullptr;
     }
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
+    for (int i = 0; i < NF; ++i) {
       const int e = lmap[slice][my_half][i];
       const int c = e & 0xFF;
       v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -361,24 +387,24 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
     const long r0 = (long)(tile - batch * tiles_per_batch) * kRows;
     const int k0 = slice * ks, k1 = k0 + ks;
     if (batch != cur_batch) stage_b(batch); /* the previous step's MMAs have completed */
-    /* split into TF32 hi / lo and write both into this thread's TMEM lane */
-    if (my_half * 32 < ks) {
-      float h[32], l[32];
+    /* split into TF32 hi / lo and write both into this thread's TMEM lane, 8 columns at a time */
+    if (my_half * CW < ks) {
+      const uint32_t col = (uint32_t)(my_half * CW);
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const float a[4] = {v[i].x, v[i].y, v[i].z, v[i].w};
+      for (int q = 0; q < CW / 8; ++q) {
+        if (my_half * CW + 8 * q >= ks) break;
+        float h[8], l[8];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          h[4 * i + j] = tf32_rna(a[j]);
-          l[4 * i + j] = tf32_rna(a[j] - h[4 * i + j]);
+        for (int i = 0; i < 2; ++i) {
+          const float a[4] = {v[2 * q + i].x, v[2 * q + i].y, v[2 * q + i].z, v[2 * q + i].w};
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            h[4 * i + j] = tf32_rna(a[j]);
+            l[4 * i + j] = tf32_rna(a[j] - h[4 * i + j]);
+          }
         }
-      }
-      const uint32_t col = (uint32_t)(my_half * 32);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if (my_half * 32 + 8 * q >= ks) break;
-        tmem_st8(t_ahi + lane_addr + col + 8 * q, h + 8 * q);
-        tmem_st8(t_alo + lane_addr + col + 8 * q, l + 8 * q);
+        tmem_st8(t_ahi + lane_addr + col + 8 * q, h);
+        tmem_st8(t_alo + lane_addr + col + 8 * q, l);
       }
     }
     tmem_st_wait();
@@ -422,15 +448,20 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
       float *dst = (r < pb.rows) ? pb.dst(r, batch) : nullptr;
       /* this warp's 8-column chunks of padded N: one half each, or dealt alternately to the two
        * halves where the problem's stored columns are not split evenly by halves */
-      const int cstep = Prob::kEpiAlternate ? 16 : 8;
-      const int cbeg = Prob::kEpiAlternate ? 8 * my_half : my_half * (npad >> 1);
-      const int cend = Prob::kEpiAlternate ? npad : cbeg + (npad >> 1);
+      constexpr bool deal = Prob::kEpiAlternate;
+      const int cstep = deal ? 8 * NS : 8;
+      const int cbeg = deal ? 8 * my_half : my_half * (npad >> 1);
+      const int cend = deal ? npad : cbeg + (npad >> 1);
       for (int c0 = cbeg; c0 < cend; c0 += cstep) {
-        float t[8], tl[8];
-        tmem_ld8(tmem + lane_addr + (uint32_t)c0, t);
-        tmem_ld8(tmem + lane_addr + (uint32_t)(npad + c0), tl);
+        uint32_t th[8], tl[8];
+        tmem_ld8_issue(tmem + lane_addr + (uint32_t)c0, th);
+        tmem_ld8_issue(tmem + lane_addr + (uint32_t)(npad + c0), tl);
+        tmem_ld_wait();
+        reg_fence8(th);
+        reg_fence8(tl);
+        float t[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) t[i] += tl[i];
+        for (int i = 0; i < 8; ++i) t[i] = __uint_as_float(th[i]) + __uint_as_float(tl[i]);
         if (dst) pb.put8(dst, r, batch, c0, t);
       }
       fence_before_sync();
@@ -593,23 +624,23 @@ __global__ void __launch_bounds__(256, 2) k_tc_nbr(const __grid_constant__ Prob 
     const long r = tile_row(tile, batch);
     const int k0 = slice * ks, k1 = k0 + ks;
     if (batch != cur_batch) stage_b(batch);
-    if (my_half * 32 < ks) {
-      float h[32], l[32];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const float a[4] = {v[i].x, v[i].y, v[i].z, v[i].w};
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          h[4 * i + j] = tf32_rna(a[j]);
-          l[4 * i + j] = tf32_rna(a[j] - h[4 * i + j]);
-        }
-      }
+    if (my_half * 32 < ks) { /* split 8 columns at a time into TF32 hi / lo, both into TMEM */
       const uint32_t col = (uint32_t)(my_half * 32);
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         if (my_half * 32 + 8 * q >= ks) break;
-        tmem_st8(t_ahi + lane_addr + col + 8 * q, h + 8 * q);
-        tmem_st8(t_alo + lane_addr + col + 8 * q, l + 8 * q);
+        float h[8], l[8];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const float a[4] = {v[2 * q + i].x, v[2 * q + i].y, v[2 * q + i].z, v[2 * q + i].w};
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            h[4 * i + j] = tf32_rna(a[j]);
+            l[4 * i + j] = tf32_rna(a[j] - h[4 * i + j]);
+          }
+        }
+        tmem_st8(t_ahi + lane_addr + col + 8 * q, h);
+        tmem_st8(t_alo + lane_addr + col + 8 * q, l);
       }
     }
     tmem_st_wait();
@@ -660,10 +691,18 @@ __global__ void __launch_bounds__(256, 2) k_tc_nbr(const __grid_constant__ Prob 
       for (int j = 0; j < 2; ++j) {
         const int c = my_half + 2 * j;
         if (c >= nw8) break; /* warp-uniform */
+        uint32_t rc[8], rn[8], rp[8];
+        tmem_ld8_issue(tmem + lane_addr + (uint32_t)(8 * c), rc);
+        tmem_ld8_issue(tmem + lane_addr + (uint32_t)(w + 8 * c), rn);
+        tmem_ld8_issue(tmem + lane_addr + (uint32_t)(2 * w + 8 * c), rp);
+        tmem_ld_wait();
+        reg_fence8(rc);
+        reg_fence8(rn);
+        reg_fence8(rp);
         float cen[8], nxt[8], prv[8];
-        tmem_ld8(tmem + lane_addr + (uint32_t)(8 * c), cen);
-        tmem_ld8(tmem + lane_addr + (uint32_t)(w + 8 * c), nxt);
-        tmem_ld8(tmem + lane_addr + (uint32_t)(2 * w + 8 * c), prv);
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+          cen[i] = __uint_as_float(rc[i]), nxt[i] = __uint_as_float(rn[i]), prv[i] = __uint_as_float(rp[i]);
         if (lane == 31)
 #pragma unroll
           for (int i = 0; i < 8; ++i) xch[my_half][quarter][j][0][i] = nxt[i];
@@ -917,11 +956,17 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm16(const __grid_constant__
         dst[i] = rr[i] < pb.rows ? pb.dst(rr[i], batch) : nullptr;
       }
       for (int g = 0; g < (npad >> 4); ++g) {
-        float t[8], tl[8];
-        tmem_ld16x2(tmem + lane_addr + 16u * g, t);
-        tmem_ld16x2(tmem + lane_addr + (uint32_t)npad + 16u * g, tl);
+        float t[8];
+        {
+          uint32_t rh[8], rl[8];
+          tmem_ld16x2_issue(tmem + lane_addr + 16u * g, rh);
+          tmem_ld16x2_issue(tmem + lane_addr + (uint32_t)npad + 16u * g, rl);
+          tmem_ld_wait();
+          reg_fence8(rh);
+          reg_fence8(rl);
 #pragma unroll
-        for (int i = 0; i < 8; ++i) t[i] += tl[i];
+          for (int i = 0; i < 8; ++i) t[i] = __uint_as_float(rh[i]) + __uint_as_float(rl[i]);
+        }
         const int c = 16 * g + 4 * j4;
         if (dst[0]) pb.put4(dst[0], rr[0], batch, c, make_float4(t[0], t[1], t[4], t[5]));
         if (dst[1]) pb.put4(dst[1], rr[1], batch, c, make_float4(t[2], t[3], t[6], t[7]));
