@@ -137,13 +137,17 @@ template <typename R> struct Dev {
   /* tensor-core (FMMFFT_F32_TC) operators: pre-split TF32 hi/lo, [npad][kpad] K-major */
   int tc, num_sms;
   int *status;          /* device word: non-zero after a bounded device wait gave up */
-  float *tc_s2m[2];     /* hi, lo */
-  float *tc_m2m[2];     /* per parent level L = 2..n-1, stride tc_m2m_stride */
-  float *tc_m2l[2];     /* per child level l = 3..n, stride tc_m2l_stride */
-  float *tc_leaf[2];    /* per section, stride tc_leaf_stride */
-  float *tc_lnb[2];     /* the leaf's neighbour-sum operators, per section, stride tc_lnb_stride */
+  /* operator images: [0] the row forms' shared-memory image (hi rows then lo rows, K-major
+   * core matrices, K extent kpad; 2 kp np floats per level / section), [1] the 16-lane form's
+   * (K and N permuted, K extent round16(kp); tc_*_stride16 floats per level / section) */
+  float *tc_s2m[2];
+  float *tc_m2m[2];     /* per parent level L = 2..n-1 */
+  float *tc_m2l[2];     /* per child level l = 3..n */
+  float *tc_leaf[2];    /* per section */
+  float *tc_lnb[2];     /* the leaf's neighbour-sum operators, per section (row image only) */
   float *leaf_fix;      /* tensor-core leaf, section P/2: [2][s] first points from box-1 */
-  long tc_m2m_stride, tc_m2l_stride, tc_leaf_stride, tc_lnb_stride;
+  long tc_m2m_stride, tc_m2l_stride, tc_leaf_stride, tc_lnb_stride; /* kp np */
+  long tc_s2m_stride16, tc_m2m_stride16, tc_m2l_stride16, tc_leaf_stride16;
   /* the same operators for the warp-specialised kernel: hi rows then lo rows in the MMA's
    * core-matrix layout (tc::ws_b_index), one block per level or section */
   float *ws_s2m, *ws_m2m, *ws_m2l, *ws_leaf;
@@ -154,9 +158,11 @@ template <typename R> struct Dev {
   long tc_min_rows; /* stages with fewer rows use the CUDA-core kernel */
   int fft_threads;  /* threads per block of the register FFT pass (power of two, <= 512) */
   /* tensor-core kernel: 0 row form (32 lanes), 3 row form (16 lanes), 4 warp-specialised; -1
-   * per stage: S2M and M2M the 16-lane row form, M2L and the leaf the 32-lane one.  The autotuner
-   * chooses among -1, 3 and 4; BF16x3 plans always use 4 (the only BF16x3 kernel). */
+   * per stage: S2M, M2M and M2L the 16-lane row form (form_m2l), the leaf its neighbour-sum form
+   * (or the 32-lane window form).  The autotuner chooses among -1, 3 and 4; BF16x3 plans always
+   * use 4 (the only BF16x3 kernel). */
   int tc_form;
+  int form_m2l; /* M2L's tensor-core form when tc_form does not force one */
   int bf16;    /* FMMFFT_BF16X3: the tensor-core stages in BF16x3 instead of split TF32 */
   int pdl;     /* row-form launches as programmatic dependent launches (FMMFFT_PDL=0: off) */
   unsigned *sync;   /* grid barrier of the coarse-tree kernel: [0] arrivals, [32] generation */
@@ -507,8 +513,10 @@ template <typename R> struct ProbLeaf {
 struct TcBase {
   long rows;
   int batches, nchunks, clen[4], coff[4], kpad, npad, nout;
-  const float *bhi, *blo;
-  long bstride;
+  /* the operator of batch z as the row forms' shared-memory image (bimg + z bimg_stride) and
+   * as the 16-lane form's (bimg16 + z bimg16_stride); either may be null when its form is unused */
+  const float *bimg, *bimg16;
+  long bimg_stride, bimg16_stride;
   const float *wsb; /* warp-specialised form: operator of batch z at wsb + z * wsb_stride */
   long wsb_stride;
   int nap; /* ns an epilogue warp sleeps between failed polls (producers nap / 4, MMA nap / 8) */
@@ -1922,13 +1930,23 @@ static float bf16_to_float_host(uint16_t b) {
 /* Uploads one operator, given as FP64 [npad][kpad] K-major values, split into TF32 hi and lo:
  * as two [npad][kpad] arrays (dhi, dlo) and, when dws is given, as the warp-specialised
  * kernel's block (hi rows 0..npad-1, lo rows npad..2 npad-1, core-matrix layout). */
-static int tc_put(float *dhi, float *dlo, float *dws, const double *v, int kpad, int npad, char *err,
+/* Splits operator v ([npad][kpad], row n = output column n, zero padded) into TF32 hi / lo and
+ * uploads the images the kernels copy into shared memory as they are:
+ *   dimg   the row forms' (k_tc_rowgemm, k_tc_nbr): hi rows then lo rows, K-major core
+ *          matrices with K extent kpad (element (n, k) at byte core_off(n, k, kpad)); 2 kpad npad;
+ *   dimg16 the 16-lane form's (k_tc_rowgemm16): the same with K extent kp16 = round16(kpad) and
+ *          element (n, k) holding v(perm16(n), perm16(k)), zero for perm16(k) >= kpad; 2 kp16 npad;
+ *   dws    the warp-specialised form's (ws_b_index layout; BF16 hi / lo for BF16x3 plans).
+ * Null images are skipped. */
+static int tc_put(float *dimg, float *dimg16, float *dws, const double *v, int kpad, int npad, char *err,
                   size_t errlen, int bf16 = 0) {
   const long cnt = (long)kpad * npad;
+  const int kp16 = tc::round16(kpad);
+  const long cnt16 = (long)kp16 * npad;
   const size_t wsn = tc::ws_b_floats(kpad, npad);
-  float *h = (float *)calloc((size_t)2 * cnt + wsn + 1, sizeof(float));
+  float *h = (float *)calloc((size_t)4 * cnt + 2 * cnt16 + wsn + 1, sizeof(float));
   if (!h) return 2;
-  float *w = h + 2 * cnt;
+  float *img = h + 2 * cnt, *img16 = img + 2 * cnt, *w = img16 + 2 * cnt16;
   uint16_t *wb = (uint16_t *)w; /* BF16 block: wsn 16-bit values */
   for (long i = 0; i < cnt; ++i) {
     float f = (float)v[i];
@@ -1936,6 +1954,9 @@ static int tc_put(float *dhi, float *dlo, float *dws, const double *v, int kpad,
     h[i] = hi;
     h[cnt + i] = tf32_rna_host(f - hi);
     const int n = (int)(i / kpad), k = (int)(i % kpad);
+    const long o = (long)(tc::core_off(n, k, kpad) >> 2);
+    img[o] = h[i];
+    img[cnt + o] = h[cnt + i];
     if (bf16) {
       const uint16_t bh = bf16_rne_host(f);
       const float fh = bf16_to_float_host(bh);
@@ -1946,8 +1967,16 @@ static int tc_put(float *dhi, float *dlo, float *dws, const double *v, int kpad,
       w[tc::ws_b_index(npad + n, k, kpad)] = h[cnt + i];
     }
   }
-  cudaError_t e = cudaMemcpy(dhi, h, sizeof(float) * cnt, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(dlo, h + cnt, sizeof(float) * cnt, cudaMemcpyHostToDevice);
+  for (int n = 0; n < npad; ++n)
+    for (int k = 0; k < kp16; ++k) {
+      const int ks = tc::perm16(k);
+      const long o = (long)(tc::core_off(n, k, kp16) >> 2), src = (long)tc::perm16(n) * kpad + ks;
+      img16[o] = ks < kpad ? h[src] : 0.f;
+      img16[cnt16 + o] = ks < kpad ? h[cnt + src] : 0.f;
+    }
+  cudaError_t e = cudaSuccess;
+  if (dimg) e = cudaMemcpy(dimg, img, sizeof(float) * 2 * cnt, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && dimg16) e = cudaMemcpy(dimg16, img16, sizeof(float) * 2 * cnt16, cudaMemcpyHostToDevice);
   if (e == cudaSuccess && dws)
     e = cudaMemcpy(dws, w, (bf16 ? 2 : 4) * wsn, cudaMemcpyHostToDevice);
   free(h);
@@ -1986,7 +2015,7 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
           v[t * kp + k] = ops[FMM_SHFTFN * T * T + t * T + k];
           v[t * kp + T + k] = ops[FMM_SHFTFP * T * T + t * T + k];
         }
-      rc |= tc_put(d->tc_m2m[0] + (L - 2) * d->tc_m2m_stride, d->tc_m2m[1] + (L - 2) * d->tc_m2m_stride,
+      rc |= tc_put(d->tc_m2m[0] + (L - 2) * 2 * d->tc_m2m_stride, d->tc_m2m[1] + (L - 2) * d->tc_m2m_stride16,
                    d->ws_m2m + (L - 2) * d->ws_m2m_stride, v, kp, np, err, errlen, d->bf16);
     }
   if (d->ok_m2l)
@@ -2007,7 +2036,7 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
           v[(T + t) * kp + 4 * T + k] = OPT(FMM_FLIP2N, t, k); /* right <- phi[2B+3] */
         }
 #undef OPT
-      rc |= tc_put(d->tc_m2l[0] + (l - 3) * d->tc_m2l_stride, d->tc_m2l[1] + (l - 3) * d->tc_m2l_stride,
+      rc |= tc_put(d->tc_m2l[0] + (l - 3) * 2 * d->tc_m2l_stride, d->tc_m2l[1] + (l - 3) * d->tc_m2l_stride16,
                    d->ws_m2l + (l - 3) * d->ws_m2l_stride, v, kp, np, err, errlen, d->bf16);
     }
   if (d->ok_leaf)
@@ -2023,7 +2052,7 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
         for (long k = 0; k < T; ++k) v[b * kp + k] = o->evalmh[(sc - P / 2) * T + k];
         for (long q = 0; q < 3 * b; ++q) v[b * kp + T + q] = ct[q];
       }
-      rc |= tc_put(d->tc_leaf[0] + (sc - 1) * d->tc_leaf_stride, d->tc_leaf[1] + (sc - 1) * d->tc_leaf_stride,
+      rc |= tc_put(d->tc_leaf[0] + (sc - 1) * 2 * d->tc_leaf_stride, d->tc_leaf[1] + (sc - 1) * d->tc_leaf_stride16,
                    d->ws_leaf + (sc - 1) * d->ws_leaf_stride, v, kp, np, err, errlen, d->bf16);
     }
   if (d->ok_lnb) /* neighbour-sum form (TcLeafNb): x_B's weights for boxes B, B+1, B-1 */
@@ -2047,8 +2076,7 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
           v[(3 * b + 2) * kp + T + q] = ct[2 * b + q];
         }
       }
-      rc |= tc_put(d->tc_lnb[0] + (sc - 1) * d->tc_lnb_stride, d->tc_lnb[1] + (sc - 1) * d->tc_lnb_stride,
-                   nullptr, v, kp, np, err, errlen, 0);
+      rc |= tc_put(d->tc_lnb[0] + (sc - 1) * 2 * d->tc_lnb_stride, nullptr, nullptr, v, kp, np, err, errlen, 0);
     }
   free(v);
   return rc;
@@ -2138,6 +2166,9 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
    * (4xTF32, rel-L2 2.4e-7 at N = 2^24, P = 64, 24 terms, against 2.7e-7); the row form stays
    * the default because it is faster there (M2L 0.47 ms against 0.58 ms on a B200) */
   d->tc_form = -1;
+  /* per-stage default forms: the 16-lane row form (3) for S2M, M2M and M2L (measured at cfg2
+   * with the operators staged by bulk copy: M2L 0.218 ms against 0.240 on the 32-lane form) */
+  d->form_m2l = 3;
   if (const char *ev = getenv("FMMFFT_TC_FORM"))
     d->tc_form = strcmp(ev, "row") == 0 ? 0 : strcmp(ev, "row16") == 0 ? 3 : strcmp(ev, "ws") == 0 ? 4 : -1,
     d->env_set |= KNOB_FORM;
@@ -2166,6 +2197,10 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
     d->ok_lnb &= (m & 8) != 0;
   }
   const long sz_s2m = d->ok_s2m ? (long)d->kp_s2m * d->np_s2m : 0;
+  d->tc_s2m_stride16 = 2L * tc::round16(d->kp_s2m) * d->np_s2m;
+  d->tc_m2m_stride16 = 2L * tc::round16(d->kp_m2m) * d->np_m2m;
+  d->tc_m2l_stride16 = 2L * tc::round16(d->kp_m2l) * d->np_m2l;
+  d->tc_leaf_stride16 = 2L * tc::round16(d->kp_leaf) * d->np_leaf;
   d->tc_m2m_stride = (long)d->kp_m2m * d->np_m2m;
   d->tc_m2l_stride = (long)d->kp_m2l * d->np_m2l;
   d->tc_leaf_stride = (long)d->kp_leaf * d->np_leaf;
@@ -2215,6 +2250,10 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
   CARVE(tcm2l, 2 * sz_m2l, float)
   CARVE(tcleaf, 2 * sz_leaf, float)
   CARVE(tclnb, 2 * sz_lnb, float)
+  CARVE(tcs2m16, d->ok_s2m ? d->tc_s2m_stride16 : 0, float)
+  CARVE(tcm2m16, d->ok_m2m ? nlev * d->tc_m2m_stride16 : 0, float)
+  CARVE(tcm2l16, d->ok_m2l ? nlev * d->tc_m2l_stride16 : 0, float)
+  CARVE(tcleaf16, d->ok_leaf ? S1 * d->tc_leaf_stride16 : 0, float)
   CARVE(leaffix, (d->ok_leaf || d->ok_lnb) ? nb * 2 * s : 0, float)
   CARVE(wss2m, ws_s2m_n, float)
   CARVE(wsm2m, ws_m2m_n, float)
@@ -2259,11 +2298,11 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
   d->u = (R *)(base + off_u);
   d->status = (int *)(base + off_status);
   d->sync = (unsigned *)(base + off_sync);
-  d->tc_s2m[0] = (float *)(base + off_tcs2m), d->tc_s2m[1] = d->tc_s2m[0] + sz_s2m;
-  d->tc_m2m[0] = (float *)(base + off_tcm2m), d->tc_m2m[1] = d->tc_m2m[0] + sz_m2m;
-  d->tc_m2l[0] = (float *)(base + off_tcm2l), d->tc_m2l[1] = d->tc_m2l[0] + sz_m2l;
-  d->tc_leaf[0] = (float *)(base + off_tcleaf), d->tc_leaf[1] = d->tc_leaf[0] + sz_leaf;
-  d->tc_lnb[0] = (float *)(base + off_tclnb), d->tc_lnb[1] = d->tc_lnb[0] + sz_lnb;
+  d->tc_s2m[0] = (float *)(base + off_tcs2m), d->tc_s2m[1] = (float *)(base + off_tcs2m16);
+  d->tc_m2m[0] = (float *)(base + off_tcm2m), d->tc_m2m[1] = (float *)(base + off_tcm2m16);
+  d->tc_m2l[0] = (float *)(base + off_tcm2l), d->tc_m2l[1] = (float *)(base + off_tcm2l16);
+  d->tc_leaf[0] = (float *)(base + off_tcleaf), d->tc_leaf[1] = (float *)(base + off_tcleaf16);
+  d->tc_lnb[0] = (float *)(base + off_tclnb), d->tc_lnb[1] = nullptr;
   d->leaf_fix = (float *)(base + off_leaffix);
   d->ws_s2m = (float *)(base + off_wss2m);
   d->ws_m2m = (float *)(base + off_wsm2m);
@@ -2407,7 +2446,8 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.rows = 2 * S1 * s, q.batches = nbt, q.nchunks = 1, q.clen[0] = (int)b, q.coff[0] = 0;
         q.P = (int)P;
         q.kpad = d->kp_s2m, q.npad = d->np_s2m, q.nout = (int)T;
-        q.bhi = d->tc_s2m[0], q.blo = d->tc_s2m[1], q.bstride = 0, q.wsb = d->ws_s2m, q.wsb_stride = 0;
+        q.bimg = d->tc_s2m[0], q.bimg16 = d->tc_s2m[1], q.bimg_stride = q.bimg16_stride = 0;
+        q.wsb = d->ws_s2m, q.wsb_stride = 0;
         q.xt = d->xt, q.out = d->phi + lvl_off(n, S1e, T), q.M = M, q.b = (int)b, q.T = (int)T;
         launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 3 : d->tc_form, d->pdl, d->bf16);
         done = true;
@@ -2441,8 +2481,8 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         TcM2M q{};
         q.rows = 2 * S1e * (1L << L), q.batches = 1, q.nchunks = 1, q.clen[0] = (int)(2 * T), q.coff[0] = 0;
         q.kpad = d->kp_m2m, q.npad = d->np_m2m, q.nout = (int)T;
-        q.bhi = d->tc_m2m[0] + (L - 2) * d->tc_m2m_stride, q.blo = d->tc_m2m[1] + (L - 2) * d->tc_m2m_stride;
-        q.bstride = 0, q.wsb = d->ws_m2m + (L - 2) * d->ws_m2m_stride, q.wsb_stride = 0;
+        q.bimg = d->tc_m2m[0] + (L - 2) * 2 * d->tc_m2m_stride, q.bimg16 = d->tc_m2m[1] + (L - 2) * d->tc_m2m_stride16;
+        q.bimg_stride = q.bimg16_stride = 0, q.wsb = d->ws_m2m + (L - 2) * d->ws_m2m_stride, q.wsb_stride = 0;
         q.child = d->phi + lvl_off(L + 1, S1e, T), q.out = d->phi + lvl_off(L, S1e, T), q.T = (int)T;
         launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 3 : d->tc_form, d->pdl, d->bf16);
         done = true;
@@ -2490,11 +2530,11 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.clen[0] = (int)T, q.clen[1] = (int)(2 * T), q.clen[2] = (int)(2 * T);
         q.coff[0] = 0, q.coff[1] = (int)T, q.coff[2] = (int)(3 * T);
         q.kpad = d->kp_m2l, q.npad = d->np_m2l, q.nout = (int)(2 * T);
-        q.bhi = d->tc_m2l[0] + (l - 3) * d->tc_m2l_stride, q.blo = d->tc_m2l[1] + (l - 3) * d->tc_m2l_stride;
-        q.bstride = 0, q.wsb = d->ws_m2l + (l - 3) * d->ws_m2l_stride, q.wsb_stride = 0;
+        q.bimg = d->tc_m2l[0] + (l - 3) * 2 * d->tc_m2l_stride, q.bimg16 = d->tc_m2l[1] + (l - 3) * d->tc_m2l_stride16;
+        q.bimg_stride = q.bimg16_stride = 0, q.wsb = d->ws_m2l + (l - 3) * d->ws_m2l_stride, q.wsb_stride = 0;
         q.psi_par = d->psi + lvl_off(l - 1, S1e, T), q.phi = d->phi + lvl_off(l, S1e, T);
         q.out = d->psi + lvl_off(l, S1e, T), q.T = (int)T, q.lpar = (int)(l - 1);
-        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? 0 : d->tc_form, d->pdl, d->bf16);
+        launch_tc(q, d->num_sms, d->status, st, d->tc_form < 0 ? d->form_m2l : d->tc_form, d->pdl, d->bf16);
         done = true;
       }
     }
@@ -2525,7 +2565,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.rows = 2 * s * nbt, q.batches = (int)S1, q.nchunks = 2;
         q.clen[0] = (int)T, q.clen[1] = (int)b, q.coff[0] = 0, q.coff[1] = (int)T;
         q.kpad = d->kp_lnb, q.npad = d->np_lnb, q.nout = (int)b;
-        q.bhi = d->tc_lnb[0], q.blo = d->tc_lnb[1], q.bstride = d->tc_lnb_stride;
+        q.bimg = d->tc_lnb[0], q.bimg_stride = 2 * d->tc_lnb_stride, q.bimg16 = nullptr, q.bimg16_stride = 0;
         q.fixbuf = d->leaf_fix, q.P = (int)P;
         q.psi_n = pb.psi_n, q.xt = d->xt, q.u = d->u, q.M = M, q.s = s, q.T = (int)T, q.b = (int)b;
         q.log2s = (int)n, q.strips = 2L * nbt;
@@ -2537,7 +2577,8 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.clen[0] = (int)T, q.clen[1] = q.clen[2] = q.clen[3] = (int)b;
         q.coff[0] = 0, q.coff[1] = (int)T, q.coff[2] = (int)(T + b), q.coff[3] = (int)(T + 2 * b);
         q.kpad = d->kp_leaf, q.npad = d->np_leaf, q.nout = (int)b;
-        q.bhi = d->tc_leaf[0], q.blo = d->tc_leaf[1], q.bstride = d->tc_leaf_stride;
+        q.bimg = d->tc_leaf[0], q.bimg_stride = 2 * d->tc_leaf_stride;
+        q.bimg16 = d->tc_leaf[1], q.bimg16_stride = d->tc_leaf_stride16;
         q.wsb = d->ws_leaf, q.wsb_stride = d->ws_leaf_stride;
         q.fixbuf = d->leaf_fix, q.P = (int)P;
         q.psi_n = pb.psi_n, q.xt = d->xt, q.u = d->u, q.M = M, q.s = s, q.T = (int)T, q.b = (int)b;

@@ -136,6 +136,23 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
   }
 }
 
+/* Arrives on `bar` and adds `bytes` to the transaction count its current phase waits for. */
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;"
+               :
+               : "r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+/* Bulk copy (no tensor map) of `bytes` from global memory into this CTA's shared memory,
+ * completing on `bar`: both addresses 16-byte aligned, bytes a multiple of 16. */
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      :
+      : "r"(dst), "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
 __device__ __forceinline__ void fence_before_sync() {
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 }
@@ -221,7 +238,7 @@ __device__ __forceinline__ float tf32_rna(float a) {
 
 /* Byte offset of element (row m, column k) in a K-major no-swizzle tile whose K extent is
  * kpad floats: 8-row groups of kpad/4 core matrices, each core matrix 8 rows x 16 bytes. */
-__device__ __forceinline__ uint32_t core_off(int m, int k, int kpad) {
+__host__ __device__ __forceinline__ uint32_t core_off(int m, int k, int kpad) {
   return (uint32_t)((m >> 3) * (kpad * 32) + (k >> 2) * 128 + (m & 7) * 16 + (k & 3) * 4);
 }
 
@@ -260,7 +277,9 @@ __host__ __device__ constexpr int tmem_cols(int kpad, int npad) {
  *   long rows;  int batches;          rows per batch, number of batches
  *   int nchunks; int clen[4]; int coff[4];   A chunk lengths / K offsets (multiples of 4)
  *   int kpad, npad, nout;             padded K (multiple of 8), padded N (x16), stored columns
- *   const float *bhi, *blo; long bstride;   pre-split B, [npad][kpad] per batch
+ *   const float *bimg; long bimg_stride;   B of batch z split into TF32 hi / lo as the kernel's
+ *                                     shared-memory image (hi rows then lo rows, core matrices
+ *                                     with K extent kpad) at bimg + z bimg_stride
  *   __device__ const float *src(int c, long r, int batch) const;
  *   __device__ float *dst(long r, int batch) const;
  *   __device__ void put8(float *dst, long r, int batch, int c0, const float *t) const;
@@ -276,7 +295,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
   /* 8 warps: 4 TMEM lane quarters x NS column halves; a thread moves CW columns of a slice */
   constexpr int NS = 2, CW = kSlice / NS, NF = CW / 4;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  __shared__ uint64_t mbar;
+  __shared__ uint64_t mbar, bbar;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   /* load map: for slice s, column group h and float4 i, the A chunk (low byte, 0xFF = zero)
@@ -292,6 +311,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
   if (warp == 0) tmem_alloc(&tmem_slot, ncols);
   if (tid == 0) {
     mbar_init(&mbar, 1);
+    mbar_init(&bbar, 1);
     fence_mbar_init();
     abort_flag = 0;
   }
@@ -350,28 +370,17 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
   const bool runs = pb.batches > 1;
   const int tile_end = runs ? (int)(((long)ntiles * (blockIdx.x + 1)) / gridDim.x) : ntiles;
   const int tile_step = runs ? 1 : (int)gridDim.x;
-  auto stage_b = [&](int batch) { /* B of this batch (pre-split), core-matrix layout */
-    const float *gbh = pb.bhi + (long)batch * pb.bstride, *gbl = pb.blo + (long)batch * pb.bstride;
-    const int nb = npad * kpad;
-    for (int e0 = tid; e0 < nb; e0 += 4 * (int)blockDim.x) { /* 8 loads in flight */
-      float vh[4], vl[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int e = e0 + u * blockDim.x;
-        if (e < nb) vh[u] = gbh[e], vl[u] = gbl[e];
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int e = e0 + u * blockDim.x;
-        if (e < nb) {
-          const int n = e / kpad, k = e - n * kpad;
-          const uint32_t o = core_off(n, k, kpad) >> 2;
-          Bhi[o] = vh[u];
-          Blo[o] = vl[u];
-        }
-      }
+  /* B of a batch: its shared-memory image, one bulk copy issued by thread 0 (the MMA issuer,
+   * who waits for it before the next MMAs); the MMAs reading the previous one have completed */
+  uint32_t bphase = 0;
+  bool b_pending = false;
+  const uint32_t b_bytes = (uint32_t)(smem_bytes(kpad, npad));
+  auto stage_b = [&](int batch) {
+    if (tid == 0) {
+      mbar_expect_tx(&bbar, b_bytes);
+      bulk_g2s(smem_addr(smem_raw), pb.bimg + (long)batch * pb.bimg_stride, b_bytes, &bbar);
+      b_pending = true;
     }
-    fence_smem_to_async();
     cur_batch = batch;
   };
   int tile = runs ? (int)(((long)ntiles * blockIdx.x) / gridDim.x) : (int)blockIdx.x, slice = 0;
@@ -413,8 +422,14 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
     if (warp == 0) { /* lane 0 issues; the rest of warp 0 waits at __syncwarp */
       if (lane == 0) {
         fence_after_sync();
+        bool b_ok = true;
+        if (b_pending) { /* the operator image has landed */
+          b_ok = mbar_wait_bounded(&bbar, bphase);
+          bphase ^= 1, b_pending = !b_ok;
+          if (!b_ok) atomicExch(status, kErrWaitTimeout), abort_flag = 1;
+        }
         /* the last slice may extend past kpad: only its real K steps are issued */
-        const int ksteps = ((k1 < kpad ? k1 : kpad) - k0) >> 3, kb = k0 >> 3;
+        const int ksteps = b_ok ? ((k1 < kpad ? k1 : kpad) - k0) >> 3 : 0, kb = k0 >> 3;
 #pragma unroll 1
         for (int s = 0; s < 2; ++s) { /* A_hi x [B_hi; B_lo], A_lo x [B_hi; B_lo] */
           uint32_t ta = (s == 1) ? t_alo : t_ahi;
@@ -471,6 +486,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm(const __grid_constant__ P
   }
   /* after an expired wait, give the MMAs in flight (bounded) time to finish before TMEM goes */
   if (tid == 0 && abort_flag) mbar_wait_bounded(&mbar, phase ^ 1);
+  if (tid == 0 && b_pending) mbar_wait_bounded(&bbar, bphase); /* a copy in flight lands */
   fence_before_sync();
   __syncthreads();
   fence_after_sync();
@@ -509,7 +525,7 @@ __host__ __device__ constexpr int nb_tmem_cols(int kpad, int npad) {
 template <class Prob>
 __global__ void __launch_bounds__(256, 2) k_tc_nbr(const __grid_constant__ Prob pb, int *status) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  __shared__ uint64_t mbar;
+  __shared__ uint64_t mbar, bbar;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   __shared__ int lmap[4][2][8];
@@ -526,6 +542,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_nbr(const __grid_constant__ Prob 
   if (warp == 0) tmem_alloc(&tmem_slot, ncols);
   if (tid == 0) {
     mbar_init(&mbar, 1);
+    mbar_init(&bbar, 1);
     fence_mbar_init();
     abort_flag = 0;
   }
@@ -590,28 +607,17 @@ __global__ void __launch_bounds__(256, 2) k_tc_nbr(const __grid_constant__ Prob 
   const bool runs = pb.batches > 1;
   const int tile_end = runs ? (int)(((long)ntiles * (blockIdx.x + 1)) / gridDim.x) : ntiles;
   const int tile_step = runs ? 1 : (int)gridDim.x;
+  /* B of a batch: its shared-memory image, one bulk copy issued by thread 0 (the MMA issuer,
+   * who waits for it before the next MMAs); the MMAs reading the previous one have completed */
+  uint32_t bphase = 0;
+  bool b_pending = false;
+  const uint32_t b_bytes = (uint32_t)(smem_bytes(kpad, npad));
   auto stage_b = [&](int batch) {
-    const float *gbh = pb.bhi + (long)batch * pb.bstride, *gbl = pb.blo + (long)batch * pb.bstride;
-    const int nb = npad * kpad;
-    for (int e0 = tid; e0 < nb; e0 += 4 * (int)blockDim.x) {
-      float vh[4], vl[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int e = e0 + u * blockDim.x;
-        if (e < nb) vh[u] = gbh[e], vl[u] = gbl[e];
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int e = e0 + u * blockDim.x;
-        if (e < nb) {
-          const int n = e / kpad, k = e - n * kpad;
-          const uint32_t o = core_off(n, k, kpad) >> 2;
-          Bhi[o] = vh[u];
-          Blo[o] = vl[u];
-        }
-      }
+    if (tid == 0) {
+      mbar_expect_tx(&bbar, b_bytes);
+      bulk_g2s(smem_addr(smem_raw), pb.bimg + (long)batch * pb.bimg_stride, b_bytes, &bbar);
+      b_pending = true;
     }
-    fence_smem_to_async();
     cur_batch = batch;
   };
   int tile = runs ? (int)(((long)ntiles * blockIdx.x) / gridDim.x) : (int)blockIdx.x, slice = 0;
@@ -649,7 +655,13 @@ __global__ void __launch_bounds__(256, 2) k_tc_nbr(const __grid_constant__ Prob 
     if (warp == 0) {
       if (lane == 0) {
         fence_after_sync();
-        const int ksteps = ((k1 < kpad ? k1 : kpad) - k0) >> 3, kb = k0 >> 3;
+        bool b_ok = true;
+        if (b_pending) { /* the operator image has landed */
+          b_ok = mbar_wait_bounded(&bbar, bphase);
+          bphase ^= 1, b_pending = !b_ok;
+          if (!b_ok) atomicExch(status, kErrWaitTimeout), abort_flag = 1;
+        }
+        const int ksteps = b_ok ? ((k1 < kpad ? k1 : kpad) - k0) >> 3 : 0, kb = k0 >> 3;
 #pragma unroll 1
         for (int p = 0; p < 4; ++p) { /* A_hi B_hi, A_hi B_lo, A_lo B_hi, A_lo B_lo, in place */
           uint32_t ta = (p & 2) ? t_alo : t_ahi;
@@ -738,6 +750,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_nbr(const __grid_constant__ Prob 
     tile = ntile, slice = nslice;
   }
   if (tid == 0 && abort_flag) mbar_wait_bounded(&mbar, phase ^ 1);
+  if (tid == 0 && b_pending) mbar_wait_bounded(&bbar, bphase); /* a copy in flight lands */
   fence_before_sync();
   __syncthreads();
   fence_after_sync();
@@ -773,7 +786,7 @@ __host__ __device__ constexpr size_t smem16_bytes(int kpad, int npad) {
 template <class Prob>
 __global__ void __launch_bounds__(256, 2) k_tc_rowgemm16(const __grid_constant__ Prob pb, int *status) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  __shared__ uint64_t mbar;
+  __shared__ uint64_t mbar, bbar;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   /* load map: for slice s, 16-column group g and quad j (source columns 16g + 4j .. +3 of the
@@ -791,6 +804,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm16(const __grid_constant__
   if (warp == 0) tmem_alloc(&tmem_slot, ncols);
   if (tid == 0) {
     mbar_init(&mbar, 1);
+    mbar_init(&bbar, 1);
     fence_mbar_init();
     abort_flag = 0;
   }
@@ -856,35 +870,17 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm16(const __grid_constant__
   const int tile_step = runs ? 1 : (int)gridDim.x;
   /* B of a batch, pre-split, in the core-matrix layout with K extent kp; shared element
    * (n, k) holds operator element (perm16(n), perm16(k)), zero for k >= kpad */
+  /* B of a batch: its shared-memory image, one bulk copy issued by thread 0 (the MMA issuer,
+   * who waits for it before the next MMAs); the MMAs reading the previous one have completed */
+  uint32_t bphase = 0;
+  bool b_pending = false;
+  const uint32_t b_bytes = (uint32_t)(smem16_bytes(kpad, npad));
   auto stage_b = [&](int batch) {
-    const float *gbh = pb.bhi + (long)batch * pb.bstride, *gbl = pb.blo + (long)batch * pb.bstride;
-    const int nb = npad * kp;
-    for (int e0 = tid; e0 < nb; e0 += 4 * (int)blockDim.x) { /* 8 loads in flight */
-      float vh[4], vl[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int e = e0 + u * blockDim.x;
-        vh[u] = 0.f, vl[u] = 0.f;
-        if (e < nb) {
-          const int n = e / kp, k = e - n * kp, ks_ = perm16(k);
-          if (ks_ < kpad) {
-            const long o = (long)perm16(n) * kpad + ks_;
-            vh[u] = gbh[o], vl[u] = gbl[o];
-          }
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int e = e0 + u * blockDim.x;
-        if (e < nb) {
-          const int n = e / kp, k = e - n * kp;
-          const uint32_t o = core_off(n, k, kp) >> 2;
-          Bhi[o] = vh[u];
-          Blo[o] = vl[u];
-        }
-      }
+    if (tid == 0) {
+      mbar_expect_tx(&bbar, b_bytes);
+      bulk_g2s(smem_addr(smem_raw), pb.bimg16 + (long)batch * pb.bimg16_stride, b_bytes, &bbar);
+      b_pending = true;
     }
-    fence_smem_to_async();
     cur_batch = batch;
   };
   int tile = runs ? (int)(((long)ntiles * blockIdx.x) / gridDim.x) : (int)blockIdx.x, slice = 0;
@@ -919,7 +915,13 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm16(const __grid_constant__
     if (warp == 0) { /* lane 0 issues; the rest of warp 0 waits at __syncwarp */
       if (lane == 0) {
         fence_after_sync();
-        const int ksteps = ((k1 < kp ? k1 : kp) - k0) >> 3, kb = k0 >> 3;
+        bool b_ok = true;
+        if (b_pending) { /* the operator image has landed */
+          b_ok = mbar_wait_bounded(&bbar, bphase);
+          bphase ^= 1, b_pending = !b_ok;
+          if (!b_ok) atomicExch(status, kErrWaitTimeout), abort_flag = 1;
+        }
+        const int ksteps = b_ok ? ((k1 < kp ? k1 : kp) - k0) >> 3 : 0, kb = k0 >> 3;
 #pragma unroll 1
         for (int s = 0; s < 2; ++s) { /* A_hi x [B_hi; B_lo], A_lo x [B_hi; B_lo] */
           uint32_t ta = (s == 1) ? t_alo : t_ahi;
@@ -978,6 +980,7 @@ __global__ void __launch_bounds__(256, 2) k_tc_rowgemm16(const __grid_constant__
   }
   /* after an expired wait, give the MMAs in flight (bounded) time to finish before TMEM goes */
   if (tid == 0 && abort_flag) mbar_wait_bounded(&mbar, phase ^ 1);
+  if (tid == 0 && b_pending) mbar_wait_bounded(&bbar, bphase); /* a copy in flight lands */
   fence_before_sync();
   __syncthreads();
   fence_after_sync();
@@ -1057,12 +1060,6 @@ __device__ __forceinline__ bool t_wait_time(uint64_t *bar, uint32_t parity) {
   }
 }
 
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;"
-               :
-               : "r"(smem_addr(bar)), "r"(bytes)
-               : "memory");
-}
 
 
 /* ======================================================================== warp-specialised form */
@@ -1165,13 +1162,6 @@ __device__ __forceinline__ void cp_async16_cg(uint32_t dst, const void *src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N> __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" : : "n"(N) : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-      :
-      : "r"(dst), "l"(src), "r"(bytes), "r"(smem_addr(bar))
-      : "memory");
 }
 /* barrier `id` over `nthreads` threads that ORs a flag across them (the same answer for all) */
 __device__ __forceinline__ bool named_bar_or(int id, int nthreads, bool v) {
@@ -1472,5 +1462,6 @@ __global__ void __maxnreg__(128) k_tc_ws(const __grid_constant__ Prob pb, int *s
   fence_after_sync();
   if (warp == mma_warp) tmem_dealloc(tmem, 512);
 }
+
 
 }  // namespace tc

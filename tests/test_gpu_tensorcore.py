@@ -3,7 +3,7 @@
 FMMFFT_TC_MIN_ROWS=1 (set before the plans are made) sends every eligible stage, however small,
 through the tensor-core kernel so that small cases cover it; the default threshold only routes
 stages with >= 4096 rows there.  Each test runs for the default per-stage kernels (16-lane row
-form for S2M and M2M, 32-lane row form for M2L and the leaf) and for each tensor-core kernel
+form for S2M, M2M and M2L, the neighbour-sum form for the leaf) and for each tensor-core kernel
 forced on every stage (FMMFFT_TC_FORM row, row16 and ws, the warp-specialised one), with S2M as
 its own stage (FMMFFT_FUSE_S2M=0) so that it runs on the tensor cores.  Tolerance: rel-L2 <= 1e-6
 against FP64, as for FP32 plans.
