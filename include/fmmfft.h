@@ -236,7 +236,8 @@ int fmmfft_batch_destroy(fmmfft_batch batch);
 /* A request server with continuous batching: transforms of mixed sizes and precisions are
  * submitted one at a time; requests of one shape (N, P, terms, b, precision) that arrive while
  * that shape's plans are busy are queued and leave together, as ONE batched launch sequence, as
- * soon as a plan frees up (small shapes: up to 2^21 samples per batch); each shape keeps up to
+ * soon as a plan frees up (shapes up to 2^23 samples: up to 2^24 samples, at most 32 requests,
+ * per batch; 2^24-sample requests run one at a time); each shape keeps up to
  * `nstreams` (at most 3) resident plans on their own streams, so batches of different shapes and
  * of one shape overlap on the device.  A dispatcher thread sends queued batches; submit, query and
  * wait dispatch too.  The device memory of the plans is capped by hbm_budget_bytes: a plan's size

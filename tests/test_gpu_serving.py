@@ -113,7 +113,7 @@ def test_server_admission_by_budget(fm):
     shape, and a request whose plan cannot fit even then is refused (FMMFFT_ERR_BUSY) before
     anything is allocated: the device's free memory is the same before and after."""
     import torch
-    N, P, T, b = 1 << 21, 64, 16, 32  # 2^21 samples: a lane of one transform per launch
+    N, P, T, b = 1 << 24, 64, 16, 32  # 2^24 samples: a lane of one transform per launch
     one = fm.plan_bytes(N, P, T, b, "f32")
     x = _dev(ol.seeded_input(N, 1), torch.complex64)
     y = torch.empty_like(x)
@@ -233,10 +233,10 @@ def test_server_reserve_makes_plans_resident(fm):
         assert torch.equal(alone, o)
     plan.close()
     srv.close()
-    big = fm.plan_bytes(1 << 22, 64, 16, 32, "f32")
+    big = fm.plan_bytes(1 << 24, 64, 16, 32, "f32")  # 2^24 samples: one transform per plan
     small = fm.Server(int(big * 1.5), nstreams=3)
     with pytest.raises(fm.FmmFftError) as ei:
-        small.reserve(1 << 22, 64, 16, 32, "f32", 3)  # room for one of the three
+        small.reserve(1 << 24, 64, 16, 32, "f32", 3)  # room for one of the three
     assert ei.value.status == 7
     assert small.stats()["plans"] == 1
     small.close()
