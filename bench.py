@@ -156,14 +156,14 @@ def stage_bytes(N, P, T, b, esz):
 
 
 # DRAM bytes (read + write) per launch of the stage's kernel from one ncu capture of the bench
-# command (profiles/k_tc_rowgemm_TcLeaf_N2p24_P64_T24_b32.txt, k_sections_f32_N2p24_P64_T24_b32.txt,
-# k_tc_rowgemm_TcM2L_N2p24_P64_T24_b32.txt).  M2L: the finest of its seven launches was captured
-# (207.8 MB for 2^12 parents per section plane); the mean over the seven levels scales it by the
+# command (profiles/k_tc_nbr_TcLeafNb_N2p24_P64_T24_b32.txt, k_sections_f32_N2p24_P64_T24_b32.txt,
+# k_tc_rowgemm16_TcM2L_N2p24_P64_T24_b32.txt).  M2L: the finest of its seven launches was captured
+# (213.4 MB for 2^12 parents per section plane); the mean over the seven levels scales it by the
 # levels' rows, (2^13 - 2^6) / 2^12 / 7.  Only meaningful for the headline workload.
 TRAFFIC_PER_LAUNCH = {
-    "leaf_l2t_near": 236.550656e6 + 96.769536e6,
+    "leaf_l2t_near": 240.409344e6 + 96.509696e6,
     "sections": 134.243840e6 + 186.710528e6,
-    "m2l_l2l": (148.745984e6 + 59.072512e6) * ((1 << 13) - (1 << 6)) / (1 << 12) / 7,
+    "m2l_l2l": (148.727808e6 + 64.687360e6) * ((1 << 13) - (1 << 6)) / (1 << 12) / 7,
 }
 
 
