@@ -132,6 +132,18 @@ int fmmfft_execute_many(fmmfft_plan plan, int count, const void *d_in, void *d_o
   return rc ? set_err(rc, err) : FMMFFT_OK;
 }
 
+int fmmfft_execute_many_ptrs(fmmfft_plan plan, int count, const void *const *d_ins, void *const *d_outs,
+                             void *stream) {
+  if (!plan || !d_ins || !d_outs) return set_err(FMMFFT_ERR_INVALID, "execute_many_ptrs: NULL argument");
+  if (count < 1 || count > plan->max_transforms)
+    return set_err(FMMFFT_ERR_INVALID, "execute_many_ptrs: count outside 1..max_transforms of the plan");
+  for (int i = 0; i < count; ++i)
+    if (!d_ins[i] || !d_outs[i]) return set_err(FMMFFT_ERR_INVALID, "execute_many_ptrs: NULL buffer");
+  char err[256] = {0};
+  int rc = fmmk_execute_ptrs(plan->dev, count, d_ins, d_outs, stream, err, sizeof err);
+  return rc ? set_err(rc, err) : FMMFFT_OK;
+}
+
 int fmmfft_execute_many_graph(fmmfft_plan plan, int count, const void *d_in, void *d_out, void *stream) {
   if (!plan || !d_in || !d_out) return set_err(FMMFFT_ERR_INVALID, "execute_many_graph: NULL argument");
   if (count < 1 || count > plan->max_transforms)

@@ -52,6 +52,9 @@ int fmmk_create_n(const fmm_ops64 *ops, int precision, int nb, fmmk_state **out,
                   char *err, size_t errlen);
 int fmmk_execute_n(fmmk_state *st, const void *d_in, void *d_out, void *stream, int inverse, int nbt,
                    char *err, size_t errlen);
+/* The same with transform i read from ins[i] and written to outs[i] (nbt <= 64). */
+int fmmk_execute_ptrs(fmmk_state *st, int nbt, const void *const *ins, void *const *outs, void *stream,
+                      char *err, size_t errlen);
 int fmmk_execute_blocks(fmmk_state *st, const void *const *in, void *const *out, int host, void *stream,
                         char *err, size_t errlen);
 int fmmk_describe(fmmk_state *st, char *buf, size_t len);

@@ -58,6 +58,19 @@ template <typename R> struct cplx;
 template <> struct cplx<float> { using T = float2; };
 template <> struct cplx<double> { using T = double2; };
 
+/* Per-transform buffers of a batched execute whose inputs or outputs are not N elements apart
+ * (fmmfft_execute_many_ptrs): the sections pass reads transform tr from in[tr]; the last FFT
+ * pass and the block-DC pass write the rows of transform tr at out[tr].  Passed by value. */
+constexpr int kMaxIo = 64; /* transforms of one execute: a batched plan holds at most 64 */
+struct InTab {
+  const void *p[kMaxIo];
+  int n; /* 0: inputs N apart from the execute's d_in */
+};
+struct OutTab {
+  void *p[kMaxIo];
+  int rpp; /* the pass's rows per transform; 0: outputs N apart from the execute's d_out */
+};
+
 template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
   C r;
   r.x = a.x * b.x - a.y * b.y;
@@ -270,12 +283,13 @@ template <typename R>
 __global__ void k_sections(const typename cplx<R>::T *__restrict__ x, R *__restrict__ xt,
                            typename cplx<R>::T *__restrict__ part, long M, int P, int TMt,
                            int conj_in, const R *__restrict__ initch, R *__restrict__ phi_n, int b,
-                           int T) {
+                           int T, const InTab xin) {
   using C = typename cplx<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   { /* transform blockIdx.y of a batch: inputs N apart, workspace arrays per transform */
     const long tr = blockIdx.y;
-    x += tr * M * P, xt += tr * 2 * M * P, part += tr * (long)gridDim.x * P;
+    x = xin.n ? reinterpret_cast<const C *>(xin.p[tr]) : x + tr * M * P;
+    xt += tr * 2 * M * P, part += tr * (long)gridDim.x * P;
     if (phi_n != nullptr) phi_n += tr * 2 * (long)(P - 1) * (M / b) * T;
   }
   C *tile = reinterpret_cast<C *>(smem_raw); /* [TMt][P + 1]: the pad spreads a column over banks */
@@ -1223,7 +1237,7 @@ static FftPass fmm_pass(FftPass fp) {
 template <typename R>
 __global__ void k_fft_pass(const typename cplx<R>::T *__restrict__ in,
                            typename cplx<R>::T *__restrict__ out,
-                           const typename cplx<R>::T *__restrict__ twM, FftPass fp) {
+                           const typename cplx<R>::T *__restrict__ twM, FftPass fp, const OutTab ot = OutTab{}) {
   using C = typename cplx<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *buf = reinterpret_cast<C *>(smem_raw);
@@ -1233,7 +1247,7 @@ __global__ void k_fft_pass(const typename cplx<R>::T *__restrict__ in,
   const long row = blockIdx.y;
   const long g0 = (long)blockIdx.x * fp.W; /* first sequence of this block within the row */
   const C *src = in + row * fp.M;
-  C *dst = out + row * fp.M;
+  C *dst = ot.rpp ? reinterpret_cast<C *>(ot.p[row / ot.rpp]) + (row % ot.rpp) * fp.M : out + row * fp.M;
   const int LW = fp.L * fp.W;
   if (fp.istr == 1) {
     for (int e = threadIdx.x; e < LW; e += blockDim.x) {
@@ -1348,7 +1362,7 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
     k_fft_reg(const Ld ld, typename cplx<R>::T *__restrict__ out,
               const typename cplx<R>::T *__restrict__ twD, const typename cplx<R>::T *__restrict__ twP,
               FftPass fp, const typename cplx<R>::T *__restrict__ twD_lo = nullptr,
-              const typename cplx<R>::T *__restrict__ twP_lo = nullptr) {
+              const typename cplx<R>::T *__restrict__ twP_lo = nullptr, const OutTab ot = OutTab{}) {
   using C = typename cplx<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int L = fp.L, W = fp.W, q = L >> 3;
@@ -1447,7 +1461,7 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
     }
     Ns <<= 3, lNs += 3;
   }
-  C *dp = out + row * fp.orow;
+  C *dp = ot.rpp ? reinterpret_cast<C *>(ot.p[row / ot.rpp]) + (row % ot.rpp) * fp.orow : out + row * fp.orow;
   if (TOUT == TIN) {
     const unsigned g = g0 + w;
     C *op = dp + g * fp.oseq + t * ostr;
@@ -1505,8 +1519,9 @@ template <typename R>
 static void launch_fft_pass(const typename cplx<R>::T *in, typename cplx<R>::T *out,
                             const typename cplx<R>::T *twM, FftPass fp, long per, long rows,
                             int W_old, int reg_threads, cudaStream_t st,
-                            const typename cplx<R>::T *twM_lo = nullptr) {
+                            const typename cplx<R>::T *twM_lo = nullptr, const OutTab *ot = nullptr) {
   using C = typename cplx<R>::T;
+  const OutTab O = ot ? *ot : OutTab{}; /* the last pass of a pointer-table execute */
   const int L = fp.L;
   const bool tin = fp.istr == 1, tout = fp.ostr == 1;
   if (L >= 16 && L <= 8 * reg_threads && !(tout && !tin)) {
@@ -1525,28 +1540,28 @@ static void launch_fft_pass(const typename cplx<R>::T *in, typename cplx<R>::T *
           const size_t smc = sm + sizeof(C) * (size_t)(L + L / 16 + 1);
           if (tin && tout)
             k_fft_reg<R, true, true, StridedLd<R>, true><<<g, thr, smc, st>>>(sld, out, twM, twM, fmm_pass(fp),
-                                                                              twM_lo, twM_lo);
+                                                                              twM_lo, twM_lo, O);
           else if (tin)
             k_fft_reg<R, true, false, StridedLd<R>, true><<<g, thr, smc, st>>>(sld, out, twM, twM, fmm_pass(fp),
-                                                                               twM_lo, twM_lo);
+                                                                               twM_lo, twM_lo, O);
           else
             k_fft_reg<R, false, false, StridedLd<R>, true><<<g, thr, smc, st>>>(sld, out, twM, twM, fmm_pass(fp),
-                                                                                twM_lo, twM_lo);
+                                                                                twM_lo, twM_lo, O);
           return;
         }
       }
       if (tin && tout)
-        k_fft_reg<R, true, true><<<g, thr, sm, st>>>(sld, out, twM, twM, fmm_pass(fp));
+        k_fft_reg<R, true, true><<<g, thr, sm, st>>>(sld, out, twM, twM, fmm_pass(fp), nullptr, nullptr, O);
       else if (tin)
-        k_fft_reg<R, true, false><<<g, thr, sm, st>>>(sld, out, twM, twM, fmm_pass(fp));
+        k_fft_reg<R, true, false><<<g, thr, sm, st>>>(sld, out, twM, twM, fmm_pass(fp), nullptr, nullptr, O);
       else
-        k_fft_reg<R, false, false><<<g, thr, sm, st>>>(sld, out, twM, twM, fmm_pass(fp));
+        k_fft_reg<R, false, false><<<g, thr, sm, st>>>(sld, out, twM, twM, fmm_pass(fp), nullptr, nullptr, O);
       return;
     }
   }
   fp.W = W_old;
   dim3 g((unsigned)(per / W_old), (unsigned)rows);
-  k_fft_pass<R><<<g, 256, sizeof(C) * (size_t)L * (2 * W_old + 1), st>>>(in, out, twM, fp);
+  k_fft_pass<R><<<g, 256, sizeof(C) * (size_t)L * (2 * W_old + 1), st>>>(in, out, twM, fp, O);
 }
 
 /* ======================================================================== combine */
@@ -1600,12 +1615,14 @@ __global__ void k_combine(const R *__restrict__ xt, const R *__restrict__ u,
  * therefore evaluate them from this identity, in FP64. */
 template <typename R>
 __global__ void k_block_dc(const typename cplx<R>::T *__restrict__ ssum,
-                           typename cplx<R>::T *__restrict__ y, long M, int P, int conj_out) {
+                           typename cplx<R>::T *__restrict__ y, long M, int P, int conj_out,
+                           const OutTab yt) {
   /* one warp per output bin r; lane l sums sc = l, l + 32, ...; FP64 warp reduction */
   using C = typename cplx<R>::T;
   const int r = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (r >= P) return;
-  ssum += (long)blockIdx.y * P, y += (long)blockIdx.y * P * M; /* transform of a batch */
+  ssum += (long)blockIdx.y * P; /* transform of a batch */
+  y = yt.rpp ? reinterpret_cast<typename cplx<R>::T *>(yt.p[blockIdx.y]) : y + (long)blockIdx.y * P * M;
   double re = 0, im = 0;
   for (int sc = lane; sc < P; sc += 32) {
     double sn, cs;
@@ -2398,8 +2415,23 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
 
 template <typename R>
 static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, int inverse,
-                       int nbt, char *err, size_t errlen) {
+                       int nbt, char *err, size_t errlen, const void *const *ins = nullptr,
+                       void *const *outs = nullptr) {
   using C = typename cplx<R>::T;
+  /* ins / outs (both or neither): transform tr reads ins[tr] and writes outs[tr] instead of
+   * vin + tr N and vout + tr N */
+  InTab xin{};
+  if (ins)
+    for (int i = 0; i < nbt; ++i) xin.p[i] = ins[i];
+  xin.n = ins ? nbt : 0;
+  auto out_tab = [&](long rows) { /* the last pass's output rows, `rows` of them in all */
+    OutTab o{};
+    if (outs) {
+      for (int i = 0; i < nbt; ++i) o.p[i] = outs[i];
+      o.rpp = (int)(rows / nbt);
+    }
+    return o;
+  };
   const long M = d->M, P = d->P, T = d->T, b = d->b, s = d->s, n = d->n, S1 = d->S1;
   /* nbt transforms of this shape, inputs and outputs N apart: every tree stage runs over the
    * rows of all of them at once (the expansion planes of transform tr follow those of tr - 1
@@ -2430,7 +2462,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
     size_t sm = sizeof(C) * TMt * (P + 1) + (s2m_fused ? sizeof(R) * b * T : 0);
     k_sections<R><<<dim3((unsigned)d->ntile, (unsigned)nbt), 256, sm, st>>>(
         x, d->xt, d->part, M, (int)P, TMt, inverse, d->initch,
-        s2m_fused ? d->phi + lvl_off(n, S1e, T) : nullptr, (int)b, (int)T);
+        s2m_fused ? d->phi + lvl_off(n, S1e, T) : nullptr, (int)b, (int)T, xin);
     pf.launches[ST_SECTIONS]++;
     stage(ST_SUMS);
     k_sum_sections<R><<<dim3((unsigned)P, (unsigned)nbt), 256, 0, st>>>(d->part, d->ntile, (int)P, d->ssum);
@@ -2666,11 +2698,13 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         if (Wr > P) Wr = (int)P;
         if (Wr < 1) Wr = 1;
         fp.M = M * Wr;
+        const OutTab ot = out_tab(nbt * P / Wr);
         launch_fft_pass<R>(d->z, y, d->twM, fp, Wr, nbt * P / Wr, W, d->fft_threads, st,
-                           d->comp_tw ? d->twM_lo : nullptr);
+                           d->comp_tw ? d->twM_lo : nullptr, &ot);
       } else {
+        const OutTab ot = out_tab(nbt * P / W);
         launch_fft_pass<R>(d->z, y, d->twM, fp, W, nbt * P / W, W, d->fft_threads, st,
-                           d->comp_tw ? d->twM_lo : nullptr);
+                           d->comp_tw ? d->twM_lo : nullptr, &ot);
       }
       pf.launches[ST_FFT1]++;
     } else {
@@ -2689,8 +2723,9 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
       if (W2 > 16) W2 = 16;
       if (W2 > M2) W2 = (int)M2;
       FftPass f2{(int)M1, W2, (int)M2, M, M1, 1, 1, M2, 0, M / M1, inverse};
+      const OutTab ot = out_tab(nbt * P);
       launch_fft_pass<R>(d->tmp, y, d->twM, f2, M2, nbt * P, W2, d->fft_threads, st,
-                         d->comp_tw ? d->twM_lo : nullptr);
+                         d->comp_tw ? d->twM_lo : nullptr, &ot);
       pf.launches[ST_FFT2]++;
     }
   }
@@ -2698,7 +2733,8 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   /* below 10 terms the FMM's own truncation at these bins exceeds FP32 resolution (3e-8 at
    * 10 terms, 5e-6 at 8), and the reference's value is the FMM one, so it is kept */
   if (sizeof(R) == 4 && T >= 10) {
-    k_block_dc<R><<<dim3((unsigned)((P + 3) / 4), (unsigned)nbt), 128, 0, st>>>(d->ssum, y, M, (int)P, inverse);
+    k_block_dc<R><<<dim3((unsigned)((P + 3) / 4), (unsigned)nbt), 128, 0, st>>>(d->ssum, y, M, (int)P, inverse,
+                                                                                    out_tab(nbt));
     pf.launches[ST_DC]++;
   }
   if (slot >= 0) cudaEventRecord(pf.ev[slot * (ST_COUNT + 1) + ST_COUNT], st);
@@ -2989,6 +3025,18 @@ extern "C" int fmmk_execute_n(fmmk_state *st, const void *d_in, void *d_out, voi
   if (st->precision == 0)
     return dev_execute<double>((Dev<double> *)st->dev, d_in, d_out, s, inverse, nbt, err, errlen);
   return dev_execute<float>((Dev<float> *)st->dev, d_in, d_out, s, inverse, nbt, err, errlen);
+}
+
+extern "C" int fmmk_execute_ptrs(fmmk_state *st, int nbt, const void *const *ins, void *const *outs,
+                                 void *stream, char *err, size_t errlen) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (nbt > kMaxIo) {
+    snprintf(err, errlen, "execute of %d transforms: a pointer table holds at most %d", nbt, kMaxIo);
+    return 1;
+  }
+  if (st->precision == 0)
+    return dev_execute<double>((Dev<double> *)st->dev, ins[0], outs[0], s, 0, nbt, err, errlen, ins, outs);
+  return dev_execute<float>((Dev<float> *)st->dev, ins[0], outs[0], s, 0, nbt, err, errlen, ins, outs);
 }
 
 extern "C" int fmmk_execute(fmmk_state *st, const void *d_in, void *d_out, void *stream,

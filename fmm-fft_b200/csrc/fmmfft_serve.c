@@ -5,7 +5,8 @@
  *  - Lanes: one per request shape (N, P, terms, b, precision).  A lane owns up to
  *    SRV_LANE_PLANS resident plans, each on its own CUDA stream; small shapes get batched plans
  *    (capacity nbmax = SRV_BATCH_SAMPLES / N, at most SRV_MAX_BATCH) with contiguous staging
- *    buffers.
+ *    buffers, shapes of SRV_PTR_MIN_N samples or more batched plans of SRV_PTR_BATCH that read and
+ *    write the requests' own buffers (fmmfft_execute_many_ptrs).
  *  - Continuous batching: a request is queued on its lane; whenever one of the lane's plans is
  *    idle, every queued request (up to the plan's capacity) leaves in ONE launch sequence: their
  *    inputs are copied into the plan's staging buffer, the batched transform runs as one cached
@@ -42,6 +43,11 @@
  * 17.9 against 16.2; a batch of 2 x 2^24 gains 6% (0.93 -> 0.87 ms a transform), about what
  * its staging copies (4 x 128 MB a transform) cost, so 2^24 requests run alone */
 #define SRV_BATCH_SAMPLES (1L << 24)
+/* Shapes of at least SRV_PTR_MIN_N samples batch through fmmfft_execute_many_ptrs: each request
+ * is read and written in its own buffers (no staging copies, no graph: at these sizes a batch runs
+ * for milliseconds and its launches are a small part of that), up to SRV_PTR_BATCH requests */
+#define SRV_PTR_MIN_N (1L << 22)
+#define SRV_PTR_BATCH 4
 #define SRV_TICKETS 65536            /* outstanding tickets a server tracks (a ring) */
 
 typedef struct {
@@ -58,6 +64,7 @@ typedef struct {
   long N, P, T, b;
   int prec;
   int nbmax;
+  int ptrs;             /* batches through per-request buffers (no staging) */
   size_t plan_bytes;    /* one plan of this lane with its staging, computed before allocating */
   int nplans, creating;
   srv_plan p[SRV_LANE_PLANS];
@@ -138,8 +145,17 @@ static void dispatch_lane(struct fmmfft_server_s *s, int l) {
      * every batch a single graph launch; the rest waits for the lane's next idle plan */
     int k = 1;
     while (2 * k <= ln->qlen && 2 * k <= ln->nbmax) k *= 2;
+    if (ln->ptrs) k = ln->qlen < ln->nbmax ? ln->qlen : ln->nbmax; /* no graph per size */
     int rc = FMMFFT_OK;
-    if (ln->nbmax == 1) {
+    if (ln->ptrs) {
+      const void *ins[SRV_PTR_BATCH];
+      void *outs[SRV_PTR_BATCH];
+      for (int j = 0; j < k; ++j) {
+        srv_ticket *tk = &s->tickets[ln->queue[(ln->qhead + j) % SRV_TICKETS]];
+        ins[j] = tk->in, outs[j] = tk->out;
+      }
+      rc = fmmfft_execute_many_ptrs(p->plan, k, ins, outs, p->st);
+    } else if (ln->nbmax == 1) {
       srv_ticket *tk = &s->tickets[ln->queue[ln->qhead % SRV_TICKETS]];
       rc = fmmfft_execute(p->plan, tk->in, tk->out, p->st);
     } else {
@@ -158,7 +174,7 @@ static void dispatch_lane(struct fmmfft_server_s *s, int l) {
         tk->state = 4;
         continue;
       }
-      if (ln->nbmax > 1)
+      if (ln->nbmax > 1 && !ln->ptrs)
         cudaMemcpyAsync(tk->out, (char *)p->bout + j * nbytes, nbytes, cudaMemcpyDeviceToDevice, p->st);
       if (!tk->has_ev) {
         cudaEventCreateWithFlags(&tk->ev, cudaEventDisableTiming);
@@ -195,14 +211,14 @@ static void grow_lane(struct fmmfft_server_s *s, int l) {
   s->used += ln->plan_bytes;
   ln->creating = 1;
   const long N = ln->N, P = ln->P, T = ln->T, b = ln->b;
-  const int prec = ln->prec, nb = ln->nbmax;
+  const int prec = ln->prec, nb = ln->nbmax, ptrs = ln->ptrs;
   pthread_mutex_unlock(&s->mu);
   srv_plan np;
   memset(&np, 0, sizeof np);
   int ok = fmmfft_plan_create_batched(&np.plan, N, P, T, b, prec, nb) == FMMFFT_OK;
   ok = ok && cudaStreamCreateWithFlags(&np.st, cudaStreamNonBlocking) == cudaSuccess;
   ok = ok && cudaEventCreateWithFlags(&np.done, cudaEventDisableTiming) == cudaSuccess;
-  if (ok && nb > 1) {
+  if (ok && nb > 1 && !ptrs) {
     const size_t bytes = (size_t)nb * (size_t)N * elem_bytes(prec);
     ok = cudaMalloc(&np.bin, bytes) == cudaSuccess && cudaMalloc(&np.bout, bytes) == cudaSuccess;
   }
@@ -302,7 +318,8 @@ static int find_lane(struct fmmfft_server_s *s, long N, long P, long T, long b, 
     *status = FMMFFT_ERR_BUSY;
     return -1;
   }
-  long nb = SRV_BATCH_SAMPLES / N;
+  const int ptrs = N >= SRV_PTR_MIN_N;
+  long nb = ptrs ? SRV_PTR_BATCH : SRV_BATCH_SAMPLES / N;
   if (nb < 1) nb = 1;
   if (nb > SRV_MAX_BATCH) nb = SRV_MAX_BATCH;
   size_t bytes = 0;
@@ -311,7 +328,7 @@ static int find_lane(struct fmmfft_server_s *s, long N, long P, long T, long b, 
     *status = rc;
     return -1;
   }
-  if (nb > 1) bytes += 2 * (size_t)nb * (size_t)N * elem_bytes(prec);
+  if (nb > 1 && !ptrs) bytes += 2 * (size_t)nb * (size_t)N * elem_bytes(prec);
   int *q = (int *)malloc(sizeof(int) * SRV_TICKETS);
   if (!q) {
     *status = FMMFFT_ERR_NOMEM;
@@ -321,6 +338,7 @@ static int find_lane(struct fmmfft_server_s *s, long N, long P, long T, long b, 
   memset(ln, 0, sizeof *ln);
   ln->N = N, ln->P = P, ln->T = T, ln->b = b, ln->prec = prec;
   ln->nbmax = (int)nb;
+  ln->ptrs = ptrs;
   ln->plan_bytes = bytes;
   ln->queue = q;
   return s->nlanes++;
@@ -460,14 +478,14 @@ int fmmfft_server_reserve(fmmfft_server s, long N, long P, long terms, long b, i
     }
     s->used += ln->plan_bytes;
     ln->creating = 1;
-    const int nb = ln->nbmax;
+    const int nb = ln->nbmax, ptrs = ln->ptrs;
     pthread_mutex_unlock(&s->mu);
     srv_plan np;
     memset(&np, 0, sizeof np);
     int ok = fmmfft_plan_create_batched(&np.plan, N, P, terms, b, precision, nb) == FMMFFT_OK;
     ok = ok && cudaStreamCreateWithFlags(&np.st, cudaStreamNonBlocking) == cudaSuccess;
     ok = ok && cudaEventCreateWithFlags(&np.done, cudaEventDisableTiming) == cudaSuccess;
-    if (ok && nb > 1) {
+    if (ok && nb > 1 && !ptrs) {
       const size_t bytes = (size_t)nb * (size_t)N * elem_bytes(precision);
       ok = cudaMalloc(&np.bin, bytes) == cudaSuccess && cudaMalloc(&np.bout, bytes) == cudaSuccess;
       ok = ok && cudaMemsetAsync(np.bin, 0, bytes, np.st) == cudaSuccess;

@@ -31,7 +31,7 @@ EXPORTS = ["getwlen2", "getvlen", "mfti", "mft", "fmmfft_last_error", "fmmfft_la
            "fmmfft_execute_many_graph", "fmmfft_plan_bytes", "fmmfft_server_counts", "fmmfft_server_reserve",
            "fmmfft_plan_enable_refinement", "fmmfft_execute_refined", "fmmfft_mft_rank_mode",
            "fmmfft_execute_blocks", "fmmfft_execute_blocks_host", "fmmfft_plan_describe",
-           "fmmfft_batch_create_many",
+           "fmmfft_batch_create_many", "fmmfft_execute_many_ptrs",
            "fmmfft_execute_graph", "fmmfft_batch_create", "fmmfft_batch_launch",
            "fmmfft_batch_destroy", "fmmfft_server_create", "fmmfft_server_destroy",
            "fmmfft_server_submit", "fmmfft_server_query", "fmmfft_server_wait",
@@ -90,6 +90,8 @@ def load(path=LIB_PATH):
     lib.fmmfft_execute_many.argtypes = [_VP, _I, _VP, _VP, _VP]
     lib.fmmfft_execute_many.restype = _I
     lib.fmmfft_execute_many_graph.argtypes = [_VP, _I, _VP, _VP, _VP]
+    lib.fmmfft_execute_many_ptrs.argtypes = [_VP, _I, ctypes.POINTER(_VP), ctypes.POINTER(_VP), _VP]
+    lib.fmmfft_execute_many_ptrs.restype = _I
     lib.fmmfft_execute_many_graph.restype = _I
     lib.fmmfft_plan_bytes.argtypes = [_L, _L, _L, _L, _I, _I, ctypes.POINTER(ctypes.c_size_t)]
     lib.fmmfft_plan_bytes.restype = _I
@@ -253,6 +255,14 @@ class Plan:
         """`count` transforms in one launch sequence; transform i at d_in / d_out + i N elements."""
         f = load().fmmfft_execute_many_graph if graph else load().fmmfft_execute_many
         _check(f(self._h, int(count), d_in, d_out, stream or None))
+
+    def execute_many_ptrs(self, d_ins, d_outs, stream=0):
+        """len(d_ins) transforms in one launch sequence, transform i from device buffer d_ins[i]
+        into d_outs[i]."""
+        n = len(d_ins)
+        ins = (_VP * n)(*d_ins)
+        outs = (_VP * n)(*d_outs)
+        _check(load().fmmfft_execute_many_ptrs(self._h, n, ins, outs, stream or None))
 
     @property
     def complex_dtype(self):

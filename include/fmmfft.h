@@ -136,6 +136,13 @@ int fmmfft_plan_device_bytes(fmmfft_plan plan, size_t *bytes);
 int fmmfft_plan_create_batched(fmmfft_plan *out, long N, long P, long terms, long b, int precision,
                                int max_transforms);
 int fmmfft_execute_many(fmmfft_plan plan, int count, const void *d_in, void *d_out, void *stream);
+/* The same with each transform in a buffer of its own: transform i reads d_ins[i] and writes
+ * d_outs[i] (device pointers, N elements each; d_ins[i] == d_outs[i] runs in place).  The tables
+ * are host arrays, read during the call and passed to the kernels by value, so they may be reused
+ * as soon as the call returns.  No counterpart in the reference; the request server batches large
+ * requests this way, with no copies through staging buffers. */
+int fmmfft_execute_many_ptrs(fmmfft_plan plan, int count, const void *const *d_ins, void *const *d_outs,
+                             void *stream);
 /* The same through a CUDA graph cached per (d_in, d_out, count), as fmmfft_execute_graph. */
 int fmmfft_execute_many_graph(fmmfft_plan plan, int count, const void *d_in, void *d_out, void *stream);
 /* Device bytes a plan of this shape, precision and capacity would hold, computed without
@@ -236,8 +243,9 @@ int fmmfft_batch_destroy(fmmfft_batch batch);
 /* A request server with continuous batching: transforms of mixed sizes and precisions are
  * submitted one at a time; requests of one shape (N, P, terms, b, precision) that arrive while
  * that shape's plans are busy are queued and leave together, as ONE batched launch sequence, as
- * soon as a plan frees up (shapes up to 2^23 samples: up to 2^24 samples, at most 32 requests,
- * per batch; 2^24-sample requests run one at a time); each shape keeps up to
+ * soon as a plan frees up (shapes below 2^22 samples: up to 2^24 samples, at most 32 requests,
+ * per batch, through staging buffers; from 2^22 samples: up to 4 requests per batch, each read
+ * and written in its own buffers); each shape keeps up to
  * `nstreams` (at most 3) resident plans on their own streams, so batches of different shapes and
  * of one shape overlap on the device.  A dispatcher thread sends queued batches; submit, query and
  * wait dispatch too.  The device memory of the plans is capped by hbm_budget_bytes: a plan's size

@@ -132,3 +132,29 @@ def test_uneven_batch_grouped_by_shape_one_graph(fm):
             assert ol.rel_l2(got.cpu().numpy(), np.fft.fft(xs[i])) < 1e-6
         alone_plan.close()
     batch.close()
+
+
+@pytest.mark.parametrize("N,P,T,b,prec", [(1 << 18, 64, 24, 32, "f32_tc"), (1 << 14, 4, 12, 16, "f64"),
+                                          (4096, 8, 8, 16, "f32_tc"), (1 << 15, 8, 10, 4, "f32"),
+                                          (1 << 16, 16, 16, 32, "f32")])
+def test_execute_many_ptrs_equals_contiguous(fm, N, P, T, b, prec):
+    """fmmfft_execute_many_ptrs: transforms in buffers of their own (here scattered, one of them
+    in place) give bitwise the outputs of the contiguous batched execute, for the two-pass and the
+    one-pass local FFTs (4096 = 8 x 512), the block-DC bins of FP32 plans and an FP64 plan."""
+    import torch
+    dt = torch.complex128 if prec == "f64" else torch.complex64
+    nbt = 3
+    xs = [ol.seeded_input(N, 2000 + i) for i in range(nbt)]
+    plan = fm.Plan(N, P, T, b, prec, max_transforms=nbt)
+    s = torch.cuda.current_stream().cuda_stream
+    cin = torch.from_numpy(np.concatenate(xs)).to(dt).cuda()
+    cout = torch.empty_like(cin)
+    plan.execute_many_ptr(nbt, cin.data_ptr(), cout.data_ptr(), s)
+    ins = [torch.from_numpy(x).to(dt).cuda() for x in xs]
+    outs = [torch.empty_like(d) for d in ins]
+    outs[1] = ins[1]  # in place
+    plan.execute_many_ptrs([d.data_ptr() for d in ins], [o.data_ptr() for o in outs], s)
+    torch.cuda.synchronize()
+    for i in range(nbt):
+        assert torch.equal(outs[i], cout[i * N:(i + 1) * N]), f"transform {i} differs"
+    plan.close()

@@ -113,8 +113,8 @@ def test_server_admission_by_budget(fm):
     shape, and a request whose plan cannot fit even then is refused (FMMFFT_ERR_BUSY) before
     anything is allocated: the device's free memory is the same before and after."""
     import torch
-    N, P, T, b = 1 << 24, 64, 16, 32  # 2^24 samples: a lane of one transform per launch
-    one = fm.plan_bytes(N, P, T, b, "f32")
+    N, P, T, b = 1 << 24, 64, 16, 32
+    one = fm.plan_bytes(N, P, T, b, "f32", max_transforms=4)  # the server's plan of this shape
     x = _dev(ol.seeded_input(N, 1), torch.complex64)
     y = torch.empty_like(x)
     srv = fm.Server(int(one * 1.5), nstreams=1)  # room for one resident plan of this size
@@ -233,10 +233,37 @@ def test_server_reserve_makes_plans_resident(fm):
         assert torch.equal(alone, o)
     plan.close()
     srv.close()
-    big = fm.plan_bytes(1 << 24, 64, 16, 32, "f32")  # 2^24 samples: one transform per plan
+    big = fm.plan_bytes(1 << 24, 64, 16, 32, "f32", max_transforms=4)  # the server's plan of this shape
     small = fm.Server(int(big * 1.5), nstreams=3)
     with pytest.raises(fm.FmmFftError) as ei:
         small.reserve(1 << 24, 64, 16, 32, "f32", 3)  # room for one of the three
     assert ei.value.status == 7
     assert small.stats()["plans"] == 1
     small.close()
+
+
+def test_server_large_requests_batch_in_their_own_buffers(fm):
+    """Requests of 2^22 samples batch (up to four per launch sequence) with each request read and
+    written in its own buffers: six submitted back to back leave in fewer launches than requests,
+    and each result is bitwise that of the request run alone on a plan of its shape."""
+    import torch
+    N, P, T, b = 1 << 22, 64, 20, 32
+    xs = [ol.seeded_input(N, 900 + i) for i in range(6)]
+    din = [_dev(x, torch.complex64) for x in xs]
+    dout = [torch.empty_like(d) for d in din]
+    srv = fm.Server(32 << 30, nstreams=1)
+    srv.reserve(N, P, T, b, "f32_tc", 1)
+    ts = [srv.submit(N, P, T, b, "f32_tc", d.data_ptr(), o.data_ptr()) for d, o in zip(din, dout)]
+    for t in ts:
+        srv.wait(t)
+    nreq, nlaunch = srv.counts()
+    assert nreq == 6 and nlaunch < 6, (nreq, nlaunch)
+    plan = fm.Plan(N, P, T, b, "f32_tc")
+    s = torch.cuda.current_stream().cuda_stream
+    for d, o in zip(din, dout):
+        alone = torch.empty_like(d)
+        plan.execute_ptr(d.data_ptr(), alone.data_ptr(), s)
+        torch.cuda.synchronize()
+        assert torch.equal(alone, o)
+    plan.close()
+    srv.close()
