@@ -619,3 +619,61 @@ int fmmfft_fft_destroy(fmmfft_fft f) {
   free(f);
   return FMMFFT_OK;
 }
+
+/* ------------------------------------------------------------------ sharded transform */
+struct fmmfft_shard_s {
+  fmmk_shard *sh;
+  int phase; /* the next phase to run */
+};
+
+int fmmfft_shard_create(fmmfft_shard *out, long N, long P, long terms, long b, int precision, int G, int g) {
+  if (!out) return set_err(FMMFFT_ERR_INVALID, "shard_create: NULL output pointer");
+  *out = NULL;
+  int rc0 = check_shape(N, P, terms, b, precision, 1);
+  if (rc0) return rc0;
+  fmm_ops64 ops;
+  if (fmm_ops64_build(N / P, P, terms, b, &ops)) return set_err(FMMFFT_ERR_NOMEM, "shard_create: host allocation failed");
+  struct fmmfft_shard_s *s = (struct fmmfft_shard_s *)calloc(1, sizeof *s);
+  if (!s) {
+    fmm_ops64_free(&ops);
+    return set_err(FMMFFT_ERR_NOMEM, "shard_create: host allocation failed");
+  }
+  char err[256] = {0};
+  int rc = fmmk_shard_create(&ops, precision, G, g, &s->sh, err, sizeof err);
+  fmm_ops64_free(&ops);
+  if (rc) {
+    free(s);
+    return set_err(rc, err);
+  }
+  *out = s;
+  return set_err(FMMFFT_OK, NULL);
+}
+
+int fmmfft_shard_buffers(fmmfft_shard sh, fmmfft_shard_bufs *bufs) {
+  if (!sh || !bufs) return set_err(FMMFFT_ERR_INVALID, "shard_buffers: NULL argument");
+  void *p[7];
+  size_t c[5];
+  fmmk_shard_buffers(sh->sh, p, c);
+  bufs->x_ext = p[0], bufs->sums = p[1], bufs->phi_send = p[2], bufs->phi_all = p[3];
+  bufs->z_send = p[4], bufs->z_recv = p[5], bufs->y = p[6];
+  bufs->x_ext_elems = c[0], bufs->halo_elems = c[1], bufs->phi_elems = c[2], bufs->z_elems = c[3];
+  bufs->y_elems = c[4];
+  return FMMFFT_OK;
+}
+
+int fmmfft_shard_phase(fmmfft_shard sh, int phase, void *stream) {
+  if (!sh) return set_err(FMMFFT_ERR_INVALID, "shard_phase: NULL shard");
+  if (phase != sh->phase) return set_err(FMMFFT_ERR_INVALID, "shard_phase: phases run in the order 0, 1, 2");
+  char err[256] = {0};
+  int rc = fmmk_shard_phase(sh->sh, phase, stream, err, sizeof err);
+  if (rc) return set_err(rc, err);
+  sh->phase = (phase + 1) % 3;
+  return FMMFFT_OK;
+}
+
+int fmmfft_shard_destroy(fmmfft_shard sh) {
+  if (!sh) return FMMFFT_OK;
+  fmmk_shard_destroy(sh->sh);
+  free(sh);
+  return FMMFFT_OK;
+}

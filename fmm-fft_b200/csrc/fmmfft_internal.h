@@ -58,6 +58,15 @@ int fmmk_execute_ptrs(fmmk_state *st, int nbt, const void *const *ins, void *con
 int fmmk_execute_blocks(fmmk_state *st, const void *const *in, void *const *out, int host, void *stream,
                         char *err, size_t errlen);
 int fmmk_describe(fmmk_state *st, char *buf, size_t len);
+/* Shard g of G of one sharded transform (fmmfft_kernels.cu, "sharded transform"). */
+typedef struct fmmk_shard fmmk_shard;
+int fmmk_shard_create(const fmm_ops64 *ops, int precision, int G, int g, fmmk_shard **out, char *err,
+                      size_t errlen);
+void fmmk_shard_destroy(fmmk_shard *sh);
+/* ptr: x_ext, sums, phi_send, phi_all, z_send, z_recv, y; cnt: x_ext and halo (complex), phi_send
+ * (reals), z_send and y (complex) */
+void fmmk_shard_buffers(fmmk_shard *sh, void **ptr, size_t *cnt);
+int fmmk_shard_phase(fmmk_shard *sh, int phase, void *stream, char *err, size_t errlen);
 int fmmk_refine_enable(fmmk_state *st, const fmm_ops64 *ops, size_t *bytes, char *err, size_t errlen);
 int fmmk_execute_refined(fmmk_state *st, const void *d_in, void *d_out, void *stream, char *err,
                          size_t errlen);

@@ -1325,9 +1325,11 @@ template <typename R> struct CombineLd {
   R invM;
   int P;
   const typename cplx<R>::T *__restrict__ pretw_lo; /* compensated pre-twiddle (FP32), or null */
+  long m0; /* first column (a shard's own columns of its strip) */
   /* row = transform of a batch: its sections, fields and section sums */
-  __device__ __forceinline__ void operator()(long row, unsigned m, int t, int q,
+  __device__ __forceinline__ void operator()(long row, unsigned mc, int t, int q,
                                              typename cplx<R>::T (&v)[8]) const {
+    const long m = m0 + mc;
     const R *xt = this->xt + row * 2 * P * M, *u = this->u + row * 2 * (P - 1) * M;
     const typename cplx<R>::T *ssum = this->ssum + row * P;
 #pragma unroll
@@ -1616,11 +1618,13 @@ __global__ void k_combine(const R *__restrict__ xt, const R *__restrict__ u,
 template <typename R>
 __global__ void k_block_dc(const typename cplx<R>::T *__restrict__ ssum,
                            typename cplx<R>::T *__restrict__ y, long M, int P, int conj_out,
-                           const OutTab yt) {
-  /* one warp per output bin r; lane l sums sc = l, l + 32, ...; FP64 warp reduction */
+                           const OutTab yt, int r0 = 0, int nrows = 0) {
+  /* one warp per output bin r; lane l sums sc = l, l + 32, ...; FP64 warp reduction.  A shard of
+   * a sharded transform writes its own rows: bins r0 .. r0 + nrows - 1 at y + (r - r0) M. */
   using C = typename cplx<R>::T;
-  const int r = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-  if (r >= P) return;
+  const int rl = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (rl >= (nrows ? nrows : P)) return;
+  const int r = r0 + rl;
   ssum += (long)blockIdx.y * P; /* transform of a batch */
   y = yt.rpp ? reinterpret_cast<typename cplx<R>::T *>(yt.p[blockIdx.y]) : y + (long)blockIdx.y * P * M;
   double re = 0, im = 0;
@@ -1640,7 +1644,7 @@ __global__ void k_block_dc(const typename cplx<R>::T *__restrict__ ssum,
     C out;
     out.x = (R)re;
     out.y = (R)(conj_out ? -im : im);
-    y[(long)r * M] = out;
+    y[(long)rl * M] = out;
   }
 }
 
@@ -2413,11 +2417,25 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
   return 0;
 }
 
+/* Parts of one execute (a shard of a sharded transform runs its plan's stages in pieces, with
+ * exchanges between them); a null control runs the whole transform. */
+struct ExecCtl {
+  unsigned mask;                        /* stages to run: bit 1 << ST_* */
+  long m2m_stop, m2l_from;              /* lowest M2M parent level, first M2L child level (0: own) */
+  int no_coarse;                        /* every tree level on its own, no coarse-tree kernel */
+  long sum_t0, sum_nt;                  /* section sums over tiles [sum_t0, sum_t0 + sum_nt) */
+  void *sum_out;                        /* ... into this P-vector (null: the plan's) */
+  long comb_m0, comb_cols, comb_ostride; /* combine of columns [m0, m0 + cols) into rows of ostride */
+  void *comb_out;
+  double comb_invM;                     /* 1 / M of the whole transform */
+};
+
 template <typename R>
 static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, int inverse,
                        int nbt, char *err, size_t errlen, const void *const *ins = nullptr,
-                       void *const *outs = nullptr) {
+                       void *const *outs = nullptr, const ExecCtl *ctl = nullptr) {
   using C = typename cplx<R>::T;
+  auto run = [&](int stg) { return !ctl || ((ctl->mask >> stg) & 1u); };
   /* ins / outs (both or neither): transform tr reads ins[tr] and writes outs[tr] instead of
    * vin + tr N and vout + tr N */
   InTab xin{};
@@ -2457,20 +2475,24 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   stage(ST_SECTIONS);
   /* S2M fused into the sections pass when tiles hold whole leaf boxes */
   const bool s2m_fused = d->tileM % b == 0 && T % 4 == 0 && d->fuse_s2m;
-  {
+  if (run(ST_SECTIONS)) {
     int TMt = (int)d->tileM;
     size_t sm = sizeof(C) * TMt * (P + 1) + (s2m_fused ? sizeof(R) * b * T : 0);
     k_sections<R><<<dim3((unsigned)d->ntile, (unsigned)nbt), 256, sm, st>>>(
         x, d->xt, d->part, M, (int)P, TMt, inverse, d->initch,
         s2m_fused ? d->phi + lvl_off(n, S1e, T) : nullptr, (int)b, (int)T, xin);
     pf.launches[ST_SECTIONS]++;
-    stage(ST_SUMS);
-    k_sum_sections<R><<<dim3((unsigned)P, (unsigned)nbt), 256, 0, st>>>(d->part, d->ntile, (int)P, d->ssum);
+  }
+  stage(ST_SUMS);
+  if (run(ST_SUMS)) { /* a shard sums its own tiles only */
+    const long t0 = ctl ? ctl->sum_t0 : 0, nt = ctl ? ctl->sum_nt : d->ntile;
+    C *out = (ctl && ctl->sum_out) ? (C *)ctl->sum_out : d->ssum;
+    k_sum_sections<R><<<dim3((unsigned)P, (unsigned)nbt), 256, 0, st>>>(d->part + t0 * P, nt, (int)P, out);
     pf.launches[ST_SUMS]++;
   }
   /* 3: S2M at level n (done in stage 1 when fused) */
   stage(ST_S2M);
-  if (!s2m_fused) {
+  if (!s2m_fused && run(ST_S2M)) {
     bool done = false;
     if constexpr (sizeof(R) == 4) {
       if (d->tc && d->ok_s2m && 2 * S1 * s >= d->tc_min_rows) {
@@ -2496,7 +2518,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   if (d->tc && d->tc_min_rows < thr) thr = d->tc_min_rows; /* never take a level off the TCs */
   /* routing by the row counts of ONE transform, so that a transform takes the same kernels (and
    * gives the same bits) alone and in a batch */
-  const bool coarse = d->coarse_grid >= 1 && thr > 2 * S1 * 4;
+  const bool coarse = !(ctl && ctl->no_coarse) && d->coarse_grid >= 1 && thr > 2 * S1 * 4;
   long Lm = 1, Ll = 2;
   if (coarse) { /* and at most 2^kCoarseMaxLevel boxes per plane (one block runs a plane) */
     for (long L = 2; L <= n - 1 && L <= kCoarseMaxLevel; ++L)
@@ -2506,7 +2528,8 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   }
   /* 4: M2M, parent level L = n-1 .. 2 (.. Lm+1 with the coarse tree) */
   stage(ST_M2M);
-  for (long L = n - 1; L >= (coarse ? Lm + 1 : 2); --L) {
+  const long m2m_stop = (ctl && ctl->m2m_stop) ? ctl->m2m_stop : (coarse ? Lm + 1 : 2);
+  for (long L = n - 1; run(ST_M2M) && L >= m2m_stop; --L) {
     bool done = false;
     if constexpr (sizeof(R) == 4) {
       if (d->tc && d->ok_m2m && 2 * S1 * (1L << L) >= d->tc_min_rows) {
@@ -2529,7 +2552,8 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   }
   /* 5: top flip, or the whole coarse tree (M2M Lm..2, top flip, M2L 3..Ll) */
   stage(ST_TOP);
-  if (coarse) {
+  if (!run(ST_TOP)) {
+  } else if (coarse) {
     CoarseArgs<R> ca{d->phi, d->psi, d->bm2m, d->btop, d->bm2l, S1e, (int)T, (int)Lm, (int)Ll, d->coarse_dbuf};
     /* one block per expansion plane of every transform of the execute; a programmatic dependent
      * launch (it stages its first operator before waiting for the level below) */
@@ -2553,7 +2577,8 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   }
   /* 6: M2L + L2L, child level l = 3..n (Ll+1..n with the coarse tree; rows = parent boxes) */
   stage(ST_M2L);
-  for (long l = coarse ? Ll + 1 : 3; l <= n; ++l) {
+  const long m2l_from = (ctl && ctl->m2l_from) ? ctl->m2l_from : (coarse ? Ll + 1 : 3);
+  for (long l = m2l_from; run(ST_M2L) && l <= n; ++l) {
     bool done = false;
     if constexpr (sizeof(R) == 4) {
       if (d->tc && d->ok_m2l && 2 * S1 * (1L << (l - 1)) >= d->tc_min_rows) {
@@ -2580,7 +2605,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   }
   /* 7: leaf far + near field per section, then the half-shifted first points */
   stage(ST_LEAF);
-  {
+  if (run(ST_LEAF)) {
     ProbLeaf<R> pb{};
     pb.psi_n = d->psi + lvl_off(n, S1e, T);
     pb.xt = d->xt;
@@ -2655,28 +2680,38 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   }
   /* 8: combine -> z[P][M] */
   stage(ST_COMBINE);
-  pf.launches[ST_COMBINE]++;
-  if (P >= 16 && P * M < (1L << 32)) {
+  /* a shard combines its own columns [m0, m0 + cols) of its strip into rows of ostride */
+  const long cm0 = ctl ? ctl->comb_m0 : 0, ccols = ctl ? ctl->comb_cols : M, costr = ctl ? ctl->comb_ostride : M;
+  C *const cz = ctl ? (C *)ctl->comb_out : d->z;
+  const R cinvM = ctl ? (R)ctl->comb_invM : R(1) / R(M);
+  if (ctl && run(ST_COMBINE) && !(P >= 16 && P * M < (1L << 32))) {
+    snprintf(err, errlen, "a column window of the combine needs P >= 16");
+    return 1;
+  }
+  if (!run(ST_COMBINE)) {
+  } else if (P >= 16 && P * M < (1L << 32)) {
+    pf.launches[ST_COMBINE]++;
     /* register Stockham over sections, Wc columns per block, the pre-twiddle in the loader */
     int Wc = 512 / (int)(P / 8);
     if (Wc > 32) Wc = 32;
     if (Wc > M) Wc = (int)M;
     FftPass fp{};
     fp.L = (int)P, fp.W = Wc, fp.per = (int)(M < (1L << 30) ? M : (1L << 30)), fp.M = M;
-    fp.irow = 0, fp.orow = P * M, fp.oseq = 1, fp.ostr = M, fp.tws = 1; /* row = transform */
+    fp.irow = 0, fp.orow = P * costr, fp.oseq = 1, fp.ostr = costr, fp.tws = 1; /* row = transform */
     fp.twiddle_post = 0, fp.conj_out = 0, fp.twmul = 1, fp.twmask = 0, fp.twbits = 0;
-    const CombineLd<R> cl{d->xt, d->u, d->ssum, d->pretw, M, R(1) / R(M), (int)P,
-                          d->comp_tw ? d->pretw_lo : nullptr};
+    const CombineLd<R> cl{d->xt, d->u, d->ssum, d->pretw, M, cinvM, (int)P,
+                          d->comp_tw ? d->pretw_lo : nullptr, cm0};
     const int thr = Wc * (int)(P / 8);
     const size_t sm = sizeof(C) * ((size_t)Wc * fft_lp((int)P, Wc) + P + P / 16 + 1 + 8 * (size_t)Wc);
     if (d->comp_tw && sizeof(R) == 4)
       k_fft_reg<R, false, false, CombineLd<R>, true>
-          <<<dim3((unsigned)(M / Wc), (unsigned)nbt), thr, sm + sizeof(C) * (size_t)(P + P / 16 + 1), st>>>(
-              cl, d->z, d->twP, d->twP, fp, d->twP_lo, d->twP_lo);
+          <<<dim3((unsigned)(ccols / Wc), (unsigned)nbt), thr, sm + sizeof(C) * (size_t)(P + P / 16 + 1), st>>>(
+              cl, cz, d->twP, d->twP, fp, d->twP_lo, d->twP_lo);
     else
-      k_fft_reg<R, false, false, CombineLd<R>><<<dim3((unsigned)(M / Wc), (unsigned)nbt), thr, sm, st>>>(
-          cl, d->z, d->twP, d->twP, fp);
+      k_fft_reg<R, false, false, CombineLd<R>><<<dim3((unsigned)(ccols / Wc), (unsigned)nbt), thr, sm, st>>>(
+          cl, cz, d->twP, d->twP, fp);
   } else {
+    pf.launches[ST_COMBINE]++;
     int TMc = (int)(P >= 1024 ? 1 : (1024 / P < 32 ? 1024 / P : 32));
     if (TMc > M) TMc = (int)M;
     size_t sm = 2 * sizeof(C) * (size_t)P * TMc;
@@ -2685,7 +2720,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   }
   /* 9: size-M FFTs, z -> y */
   stage(ST_FFT1);
-  {
+  if (run(ST_FFT1)) {
     const long SMEM = 96 * 1024;
     if (d->M2 == 1) {
       int W = (int)pow2_floor(SMEM / (long)(2 * sizeof(C) * M));
@@ -2732,7 +2767,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
   stage(ST_DC);
   /* below 10 terms the FMM's own truncation at these bins exceeds FP32 resolution (3e-8 at
    * 10 terms, 5e-6 at 8), and the reference's value is the FMM one, so it is kept */
-  if (sizeof(R) == 4 && T >= 10) {
+  if (sizeof(R) == 4 && T >= 10 && run(ST_DC)) {
     k_block_dc<R><<<dim3((unsigned)((P + 3) / 4), (unsigned)nbt), 128, 0, st>>>(d->ssum, y, M, (int)P, inverse,
                                                                                     out_tab(nbt));
     pf.launches[ST_DC]++;
@@ -3852,4 +3887,259 @@ extern "C" void fmmk_fft_destroy(fmmk_fft *f) {
   if (!f) return;
   cudaFree(f->tmp);
   free(f);
+}
+
+/* ======================================================================== sharded transform */
+/* One transform of N = P M points split over G shards (one per GPU in a multi-GPU job), each
+ * holding the contiguous block y[g N/G .. (g+1) N/G) of input and output, as the reference's
+ * ranks do (src/fmmfft.c:384-978): shard g owns the leaf boxes [g s/G, (g+1) s/G) of every
+ * section.  Its plan is an ordinary single-device plan over an EXTENDED strip of s_ext = 2 s/G
+ * boxes, its own boxes with H = s/(2G) boxes of halo on either side, built from the operators of
+ * the GLOBAL tree (level l of the strip is level l + log2(G/2) of the transform; the leaf and
+ * near-field tables are the transform's).  Every box of the strip has its own multipole
+ * expansions; the coarse levels come from the other shards: the expansions of the strip's level
+ * 3 (global level lc = log2(4G), four own boxes per plane and shard) are all-gathered, each shard
+ * runs the global tree above lc on them (a small plan of 2^lc boxes) and takes the local
+ * expansions of its strip's 8 level-3 boxes from it.  Below that the strip's own M2L is exact for
+ * its own boxes and the box before them, since their interaction lists (2 to 3 boxes away at
+ * every level >= 4) stay inside the strip; so are the leaf's fields.  The combine runs over the
+ * shard's own columns (all P sections of them are local) into P rows of M/G, one all-to-all
+ * gives each shard its P/G rows whole, and a plan of P/G sections of M points runs their FFTs.
+ * Exchanges, in order: the halos of x (each shard receives the last N/(2G) points of the shard
+ * before it and the first N/(2G) of the one after it), an all-reduce of the P section sums, an
+ * all-gather of the coarse expansions, one all-to-all of the combined rows.  The stage kernels
+ * are the single-device ones (the reference's halo exchanges per level, :517-618, are replaced
+ * by the strip's halo boxes, computed redundantly). */
+
+template <typename R> struct ShardImpl {
+  using C = typename cplx<R>::T;
+  int G, g, precision;
+  long N, P, T, b, M, s, n, lc;
+  long s_loc, H, s_ext, n_ext, M_ext, M_loc;
+  Dev<R> *loc = nullptr, *crs = nullptr, *fft = nullptr;
+  void *mem = nullptr;
+  C *x_ext, *sums, *z_send, *z_recv, *y;
+  R *phi_send, *phi_all;
+  long phi_elems;
+};
+
+/* The level-3 expansions of a strip's own boxes (local boxes 2..5 of 8 per plane) into the send
+ * buffer, [plane][4][T] */
+template <typename R>
+__global__ void k_shard_pack(const R *__restrict__ lvl3, R *__restrict__ out, long planes, int T) {
+  const long total = planes * 4 * T;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long t = e % T, j = (e / T) % 4, pl = e / (4L * T);
+    out[e] = lvl3[(pl * 8 + 2 + j) * T + t];
+  }
+}
+/* The gathered expansions [shard][plane][4][T] into the global level lc, [plane][4G][T] */
+template <typename R>
+__global__ void k_shard_unpack(const R *__restrict__ all, R *__restrict__ lvl, long planes, int T, int G) {
+  const long total = (long)G * planes * 4 * T;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long t = e % T, j = (e / T) % 4, pl = (e / (4L * T)) % planes, gg = e / (4L * T * planes);
+    lvl[(pl * 4 * G + 4 * gg + j) * T + t] = all[e];
+  }
+}
+/* The local expansions of the strip's 8 level-3 boxes from the global level lc: strip box k is
+ * global box (4 g - 2 + k) mod 4G */
+template <typename R>
+__global__ void k_shard_inject(const R *__restrict__ glvl, R *__restrict__ lvl3, long planes, int T, int G,
+                               int g) {
+  const long total = planes * 8 * T;
+  const long nb = 4L * G;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long t = e % T, k = (e / T) % 8, pl = e / (8L * T);
+    const long gb = ((4L * g - 2 + k) % nb + nb) % nb;
+    lvl3[e] = glvl[(pl * nb + gb) * T + t];
+  }
+}
+
+template <typename R>
+static void shard_free(ShardImpl<R> *sh) {
+  if (!sh) return;
+  Dev<R> *ds[3] = {sh->loc, sh->crs, sh->fft};
+  for (Dev<R> *d : ds)
+    if (d) cudaFree(d->pool), delete d;
+  cudaFree(sh->mem);
+  delete sh;
+}
+
+template <typename R>
+static int shard_create(const fmm_ops64 *og, int precision, int G, int g, ShardImpl<R> **out, char *err,
+                        size_t errlen) {
+  using C = typename cplx<R>::T;
+  const long M = og->M, P = og->P, T = og->T, b = og->b, s = og->s, n = og->n;
+  auto lg2 = [](long v) { long l = 0; while ((1L << l) < v) ++l; return l; };
+  if (G < 2 || (G & (G - 1)) || g < 0 || g >= G) {
+    snprintf(err, errlen, "shard %d of %d: G must be a power of two >= 2 and 0 <= g < G", g, G);
+    return 1;
+  }
+  const long s_loc = s / G, H = s_loc / 2, s_ext = 2 * s_loc, M_loc = M / G;
+  const long tileM = P >= 2048 ? 1 : 2048 / P;
+  const int Wc = (int)(512 / (P / 8) > 32 ? 32 : 512 / (P / 8));
+  if (P < 16 || P % (2L * G) != 0 || s % G != 0 || s_loc < 8 || (H * b) % tileM != 0 || M_loc % tileM != 0 ||
+      M_loc % Wc != 0) {
+    snprintf(err, errlen,
+             "sharded transform of N = %ld, P = %ld, b = %ld over %d shards: needs P >= 16, P a multiple "
+             "of 2G and at least 8 leaf boxes per shard", M * P, P, b, G);
+    return 1;
+  }
+  ShardImpl<R> *sh = new (std::nothrow) ShardImpl<R>();
+  if (!sh) return 2;
+  sh->G = G, sh->g = g, sh->precision = precision;
+  sh->N = M * P, sh->P = P, sh->T = T, sh->b = b, sh->M = M, sh->s = s, sh->n = n;
+  sh->s_loc = s_loc, sh->H = H, sh->s_ext = s_ext, sh->n_ext = lg2(s_ext), sh->lc = lg2(4L * G);
+  sh->M_ext = s_ext * b, sh->M_loc = M_loc;
+  /* the strip: the transform's operators, its levels offset by n - n_ext */
+  fmm_ops64 ol = *og;
+  ol.M = sh->M_ext, ol.s = s_ext, ol.n = sh->n_ext;
+  ol.levops = og->levops + (n - sh->n_ext) * FMM_NLEVOPS * T * T;
+  /* the coarse tree: the transform's levels 2..lc as a tree of 4G leaf boxes */
+  fmm_ops64 oc = *og;
+  oc.s = 4L * G, oc.M = oc.s * b, oc.n = sh->lc;
+  /* the shard's rows: P/G sections of M points (only its FFT stage runs) */
+  fmm_ops64 of = *og;
+  of.P = P / G;
+  int rc = dev_create<R>(&ol, precision, 1, &sh->loc, err, errlen);
+  if (!rc) rc = dev_create<R>(&oc, precision, 1, &sh->crs, err, errlen);
+  if (!rc) rc = dev_create<R>(&of, precision, 1, &sh->fft, err, errlen);
+  if (rc) {
+    shard_free(sh);
+    return rc;
+  }
+  const long S1 = P - 1, Next = sh->M_ext * P;
+  sh->phi_elems = 2 * S1 * 4 * T;
+  size_t off = 0;
+  auto carve = [&](size_t bytes) { size_t o = off; off = align_up(off + bytes); return o; };
+  const size_t o_x = carve(sizeof(C) * Next), o_s = carve(sizeof(C) * P), o_ps = carve(sizeof(R) * sh->phi_elems),
+               o_pa = carve(sizeof(R) * sh->phi_elems * G), o_zs = carve(sizeof(C) * (sh->N / G)),
+               o_zr = carve(sizeof(C) * (sh->N / G)), o_y = carve(sizeof(C) * (sh->N / G));
+  cudaError_t ce = cudaMalloc(&sh->mem, off);
+  if (ce != cudaSuccess) {
+    snprintf(err, errlen, "cudaMalloc(%zu): %s", off, cudaGetErrorString(ce));
+    shard_free(sh);
+    return 2;
+  }
+  char *base = (char *)sh->mem;
+  sh->x_ext = (C *)(base + o_x), sh->sums = (C *)(base + o_s), sh->phi_send = (R *)(base + o_ps);
+  sh->phi_all = (R *)(base + o_pa), sh->z_send = (C *)(base + o_zs), sh->z_recv = (C *)(base + o_zr);
+  sh->y = (C *)(base + o_y);
+  *out = sh;
+  return 0;
+}
+
+/* Phase 0: the strip's sections, its own section sums, S2M and M2M up to its level 3, whose own
+ * expansions go to phi_send.  Phase 1 (after the sums were all-reduced and the expansions
+ * all-gathered): the coarse tree, the strip's M2L from level 4, the leaf and the combine of its own
+ * columns into z_send.  Phase 2 (after the all-to-all into z_recv): the P/G rows' FFTs into y. */
+template <typename R>
+static int shard_phase(ShardImpl<R> *sh, int phase, cudaStream_t st, char *err, size_t errlen) {
+  using C = typename cplx<R>::T;
+  const long P = sh->P, T = sh->T, S1 = P - 1, G = sh->G;
+  const int blocks = 4 * sh->loc->num_sms;
+  int rc = 0;
+  if (phase == 0) {
+    ExecCtl c{};
+    c.mask = (1u << ST_SECTIONS) | (1u << ST_SUMS) | (1u << ST_S2M) | (1u << ST_M2M);
+    c.m2m_stop = 3, c.no_coarse = 1;
+    c.sum_t0 = sh->H * sh->b / sh->loc->tileM, c.sum_nt = sh->M_loc / sh->loc->tileM, c.sum_out = sh->sums;
+    rc = dev_execute<R>(sh->loc, sh->x_ext, sh->y, st, 0, 1, err, errlen, nullptr, nullptr, &c);
+    if (!rc)
+      k_shard_pack<R><<<blocks, 256, 0, st>>>(sh->loc->phi + lvl_off(3, S1, T), sh->phi_send, 2 * S1, (int)T);
+  } else if (phase == 1) {
+    FMM_CUDA_TRY(cudaMemcpyAsync(sh->loc->ssum, sh->sums, sizeof(C) * P, cudaMemcpyDeviceToDevice, st));
+    k_shard_unpack<R><<<blocks, 256, 0, st>>>(sh->phi_all, sh->crs->phi + lvl_off(sh->lc, S1, T), 2 * S1,
+                                              (int)T, (int)G);
+    ExecCtl cc{};
+    cc.mask = (1u << ST_M2M) | (1u << ST_TOP) | (1u << ST_M2L);
+    rc = dev_execute<R>(sh->crs, sh->x_ext, sh->y, st, 0, 1, err, errlen, nullptr, nullptr, &cc);
+    if (rc) return rc;
+    k_shard_inject<R><<<blocks, 256, 0, st>>>(sh->crs->psi + lvl_off(sh->lc, S1, T),
+                                              sh->loc->psi + lvl_off(3, S1, T), 2 * S1, (int)T, (int)G, sh->g);
+    ExecCtl c{};
+    c.mask = (1u << ST_M2L) | (1u << ST_LEAF) | (1u << ST_COMBINE);
+    c.m2l_from = 4, c.no_coarse = 1;
+    c.comb_m0 = sh->H * sh->b, c.comb_cols = sh->M_loc, c.comb_ostride = sh->M_loc, c.comb_out = sh->z_send;
+    c.comb_invM = 1.0 / (double)sh->M;
+    rc = dev_execute<R>(sh->loc, sh->x_ext, sh->y, st, 0, 1, err, errlen, nullptr, nullptr, &c);
+  } else if (phase == 2) {
+    const long rows = P / G, M = sh->M, Ml = sh->M_loc;
+    for (long gg = 0; gg < G; ++gg) /* chunk gg: rows x columns [gg M/G, (gg+1) M/G) */
+      FMM_CUDA_TRY(cudaMemcpy2DAsync(sh->fft->z + gg * Ml, sizeof(C) * M, sh->z_recv + gg * rows * Ml,
+                                     sizeof(C) * Ml, sizeof(C) * Ml, rows, cudaMemcpyDeviceToDevice, st));
+    ExecCtl c{};
+    c.mask = 1u << ST_FFT1;
+    rc = dev_execute<R>(sh->fft, sh->y, sh->y, st, 0, 1, err, errlen, nullptr, nullptr, &c);
+    if (!rc && sizeof(R) == 4 && T >= 10) /* the block-DC bins of the shard's rows, as a plan's */
+      k_block_dc<R><<<dim3((unsigned)((rows + 3) / 4), 1), 128, 0, st>>>(sh->sums, sh->y, M, (int)P, 0, OutTab{},
+                                                                         (int)(sh->g * rows), (int)rows);
+  } else {
+    snprintf(err, errlen, "shard phase %d: 0, 1 or 2", phase);
+    return 1;
+  }
+  if (!rc) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      snprintf(err, errlen, "shard phase %d: %s", phase, cudaGetErrorString(e));
+      return 3;
+    }
+  }
+  return rc;
+}
+
+struct fmmk_shard {
+  int precision;
+  void *impl;
+};
+
+extern "C" int fmmk_shard_create(const fmm_ops64 *o, int precision, int G, int g, fmmk_shard **out, char *err,
+                                 size_t errlen) {
+  int rc = fmmk_device_ok(err, errlen);
+  if (rc) return rc;
+  set_smem_limits();
+  fmmk_shard *sh = (fmmk_shard *)calloc(1, sizeof(fmmk_shard));
+  if (!sh) return 2;
+  sh->precision = precision;
+  if (precision == 0) {
+    ShardImpl<double> *p = nullptr;
+    rc = shard_create<double>(o, precision, G, g, &p, err, errlen);
+    sh->impl = p;
+  } else {
+    ShardImpl<float> *p = nullptr;
+    rc = shard_create<float>(o, precision, G, g, &p, err, errlen);
+    sh->impl = p;
+  }
+  if (rc) {
+    free(sh);
+    return rc;
+  }
+  *out = sh;
+  return 0;
+}
+
+extern "C" void fmmk_shard_destroy(fmmk_shard *sh) {
+  if (!sh) return;
+  if (sh->precision == 0) shard_free((ShardImpl<double> *)sh->impl);
+  else shard_free((ShardImpl<float> *)sh->impl);
+  free(sh);
+}
+
+template <typename R> static void shard_bufs(ShardImpl<R> *p, void **ptr, size_t *cnt) {
+  ptr[0] = p->x_ext, ptr[1] = p->sums, ptr[2] = p->phi_send, ptr[3] = p->phi_all, ptr[4] = p->z_send;
+  ptr[5] = p->z_recv, ptr[6] = p->y;
+  cnt[0] = (size_t)(p->M_ext * p->P), cnt[1] = (size_t)(p->H * p->b * p->P), cnt[2] = (size_t)p->phi_elems;
+  cnt[3] = (size_t)(p->N / p->G), cnt[4] = (size_t)(p->N / p->G);
+}
+
+extern "C" void fmmk_shard_buffers(fmmk_shard *sh, void **ptr, size_t *cnt) {
+  if (sh->precision == 0) shard_bufs((ShardImpl<double> *)sh->impl, ptr, cnt);
+  else shard_bufs((ShardImpl<float> *)sh->impl, ptr, cnt);
+}
+
+extern "C" int fmmk_shard_phase(fmmk_shard *sh, int phase, void *stream, char *err, size_t errlen) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (sh->precision == 0) return shard_phase((ShardImpl<double> *)sh->impl, phase, st, err, errlen);
+  return shard_phase((ShardImpl<float> *)sh->impl, phase, st, err, errlen);
 }

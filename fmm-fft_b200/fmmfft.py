@@ -32,6 +32,7 @@ EXPORTS = ["getwlen2", "getvlen", "mfti", "mft", "fmmfft_last_error", "fmmfft_la
            "fmmfft_plan_enable_refinement", "fmmfft_execute_refined", "fmmfft_mft_rank_mode",
            "fmmfft_execute_blocks", "fmmfft_execute_blocks_host", "fmmfft_plan_describe",
            "fmmfft_batch_create_many", "fmmfft_execute_many_ptrs",
+           "fmmfft_shard_create", "fmmfft_shard_buffers", "fmmfft_shard_phase", "fmmfft_shard_destroy",
            "fmmfft_execute_graph", "fmmfft_batch_create", "fmmfft_batch_launch",
            "fmmfft_batch_destroy", "fmmfft_server_create", "fmmfft_server_destroy",
            "fmmfft_server_submit", "fmmfft_server_query", "fmmfft_server_wait",
@@ -47,6 +48,11 @@ class FmmFftError(RuntimeError):
 
 _lib = None
 _L, _VP, _I = ctypes.c_long, ctypes.c_void_p, ctypes.c_int
+
+
+class _ShardBufs(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in ("x_ext", "sums", "phi_send", "phi_all", "z_send", "z_recv", "y")] + \
+               [(n, ctypes.c_size_t) for n in ("x_ext_elems", "halo_elems", "phi_elems", "z_elems", "y_elems")]
 
 
 def load(path=LIB_PATH):
@@ -92,6 +98,14 @@ def load(path=LIB_PATH):
     lib.fmmfft_execute_many_graph.argtypes = [_VP, _I, _VP, _VP, _VP]
     lib.fmmfft_execute_many_ptrs.argtypes = [_VP, _I, ctypes.POINTER(_VP), ctypes.POINTER(_VP), _VP]
     lib.fmmfft_execute_many_ptrs.restype = _I
+    lib.fmmfft_shard_create.argtypes = [ctypes.POINTER(_VP), _L, _L, _L, _L, _I, _I, _I]
+    lib.fmmfft_shard_create.restype = _I
+    lib.fmmfft_shard_buffers.argtypes = [_VP, ctypes.POINTER(_ShardBufs)]
+    lib.fmmfft_shard_buffers.restype = _I
+    lib.fmmfft_shard_phase.argtypes = [_VP, _I, _VP]
+    lib.fmmfft_shard_phase.restype = _I
+    lib.fmmfft_shard_destroy.argtypes = [_VP]
+    lib.fmmfft_shard_destroy.restype = _I
     lib.fmmfft_execute_many_graph.restype = _I
     lib.fmmfft_plan_bytes.argtypes = [_L, _L, _L, _L, _I, _I, ctypes.POINTER(ctypes.c_size_t)]
     lib.fmmfft_plan_bytes.restype = _I
@@ -495,3 +509,34 @@ def level_planar(flat, P, T, n, level):
     off = 2 * (P - 1) * T * ((1 << level) - 4)
     cnt = 2 * (P - 1) * T * (1 << level)
     return flat[off:off + cnt].reshape(P - 1, 2, 1 << level, T)
+
+
+class Shard:
+    """Shard g of G of one sharded transform (fmmfft_shard_*): see include/fmmfft.h.  buffers()
+    gives the device pointers and sizes of the exchange buffers; phase(k) runs phase k."""
+
+    def __init__(self, N, P, terms, b, precision, G, g):
+        h = _VP()
+        _check(load().fmmfft_shard_create(ctypes.byref(h), int(N), int(P), int(terms), int(b),
+                                          PRECISIONS[precision], int(G), int(g)))
+        self._h = h
+        self.N, self.P, self.G, self.g, self.precision = N, P, G, g, precision
+
+    def buffers(self):
+        bb = _ShardBufs()
+        _check(load().fmmfft_shard_buffers(self._h, ctypes.byref(bb)))
+        return {n: getattr(bb, n) for n, _ in _ShardBufs._fields_}
+
+    def phase(self, k, stream=0):
+        _check(load().fmmfft_shard_phase(self._h, int(k), stream or None))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().fmmfft_shard_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -239,6 +239,34 @@ int fmmfft_batch_create_many(fmmfft_batch *out, const fmmfft_plan *plans, const 
 int fmmfft_batch_launch(fmmfft_batch batch, void *stream);
 int fmmfft_batch_destroy(fmmfft_batch batch);
 
+/* ------------------------------------------------------------------ sharded transform */
+/* One transform split over G devices (G a power of two; P >= 16, P a multiple of 2G, at least 8
+ * leaf boxes of b points per shard), replacing the reference's P-rank mft (src/fmmfft.c:384-978,
+ * its halo exchanges :517-618, section-sum reduction :452-453 and all-to-all :970).  Shard g holds
+ * the contiguous block g of N/G input points and ends with the block g of N/G outputs, as the
+ * reference's ranks hold their qr.  The library computes; the caller moves data between the
+ * shards (NCCL through torch.distributed in fmm-fft_b200/sharded.py), with the shard's buffers:
+ *   phase 0 needs x_ext = [the last halo_elems points of shard g-1's block | the shard's own N/G
+ *           points | the first halo_elems points of shard g+1's block] (cyclic in g);
+ *   between 0 and 1: `sums` (P complex) summed over the shards, in place on every shard, and
+ *           phi_all = the shards' phi_send buffers (phi_elems reals each) back to back, in shard
+ *           order;
+ *   between 1 and 2: an all-to-all: z_send holds G chunks of z_elems/G complex, chunk h for shard
+ *           h; z_recv receives the chunk for this shard from every shard, in shard order;
+ *   after phase 2: y holds the shard's y_elems outputs.
+ * Elements are complex64 (FP32 plans) or complex128 (FP64), reals float or double.  Forward only.
+ * Phases run in the order 0, 1, 2 on one stream; a stream-ordered exchange between them needs no
+ * synchronisation. */
+typedef struct fmmfft_shard_s *fmmfft_shard;
+typedef struct {
+  void *x_ext, *sums, *phi_send, *phi_all, *z_send, *z_recv, *y;
+  size_t x_ext_elems, halo_elems, phi_elems, z_elems, y_elems;
+} fmmfft_shard_bufs;
+int fmmfft_shard_create(fmmfft_shard *out, long N, long P, long terms, long b, int precision, int G, int g);
+int fmmfft_shard_buffers(fmmfft_shard sh, fmmfft_shard_bufs *bufs);
+int fmmfft_shard_phase(fmmfft_shard sh, int phase, void *stream);
+int fmmfft_shard_destroy(fmmfft_shard sh);
+
 /* ------------------------------------------------------------------ serving */
 /* A request server with continuous batching: transforms of mixed sizes and precisions are
  * submitted one at a time; requests of one shape (N, P, terms, b, precision) that arrive while
