@@ -42,12 +42,14 @@ def parse():
     ap.add_argument("--precision", default=None, help="f32 | f32_tc | f64 (default: fastest)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
-    ap.add_argument("--workload", choices=["single", "uneven-batch", "serving", "precision-sweep"],
+    ap.add_argument("--workload", choices=["single", "uneven-batch", "serving", "precision-sweep", "sharded"],
                     default="single",
                     help="single: the headline transform (default); uneven-batch: 512 transforms "
                          "of mixed N and P as one graph; serving: Poisson arrivals through the "
                          "request server; precision-sweep: N = 2^26, P = 256, tones + noise, every "
-                         "order and arithmetic, error against throughput")
+                         "order and arithmetic, error against throughput; sharded: the headline "
+                         "transform as G shards (emulated in this process), each shard's device time")
+    ap.add_argument("--shards", type=int, default=8, help="sharded: G")
     ap.add_argument("--rate", type=float, default=2000.0, help="serving: arrivals per second")
     ap.add_argument("--requests", type=int, default=1200, help="serving: requests per rate")
     ap.add_argument("--no-served", action="store_true", help="skip the served-vs-plain object")
@@ -549,8 +551,83 @@ def run_precision_sweep(a):
     return 0
 
 
+# ------------------------------------------------------------------------ sharded transform
+def run_sharded(a):
+    """The headline transform as G shards of fmmfft_shard_*, all on this device in turn (the
+    exchanges as device copies): each shard's phases timed with CUDA events, L2 flushed before
+    every phase.  On G GPUs the shards' phases run at once, so a transform's device time there is
+    the slowest shard's phases plus the exchanges (whose bytes are reported, not timed here)."""
+    import numpy as np
+    import torch
+    import fmmfft
+    import sharded
+    torch.cuda.set_device(0)
+    N, P, T, b = WORKLOAD["N"], WORKLOAD["P"], WORKLOAD["terms"], WORKLOAD["b"]
+    G, prec = a.shards, a.precision or "f32_tc"
+    x = torch.from_numpy(seeded(N, 0, np.complex64)).cuda()
+    shards = [fmmfft.Shard(N, P, T, b, prec, G, g) for g in range(G)]
+    views = [sharded._views(s) for s in shards]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.current_stream()
+    tr = sharded.LocalTransport(G)
+    blocks = list(x.chunk(G))
+
+    def step(timed):
+        times = np.zeros((G, 3))
+        for v, blk in zip(views, blocks):
+            v["x_ext"][v["halo"]:v["halo"] + blk.numel()].copy_(blk)
+        tr.halos(blocks, [v["x_ext"][:v["halo"]] for v in views],
+                 [v["x_ext"][v["halo"] + blk.numel():] for v, blk in zip(views, blocks)])
+        evs = []
+        for k in range(3):
+            for g, s in enumerate(shards):
+                flush.fill_(k + 1)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                s.phase(k, st.cuda_stream)
+                e1.record()
+                evs.append((g, k, e0, e1))
+            if k == 0:
+                tr.sum([v["sums"] for v in views])
+                tr.gather([v["phi_send"] for v in views], [v["phi_all"] for v in views])
+            elif k == 1:
+                tr.alltoall([v["z_send"] for v in views], [v["z_recv"] for v in views])
+        torch.cuda.synchronize()
+        for g, k, e0, e1 in evs:
+            times[g, k] = e0.elapsed_time(e1)
+        return times
+
+    for _ in range(max(a.warmup, 3)):
+        step(False)
+    per = [step(True) for _ in range(a.steps)]
+    worst = sorted(t.sum(axis=1).max() for t in per)[len(per) // 2]
+    y = torch.cat([v["y"] for v in views]).cpu().numpy().astype(np.complex128)
+    ref = np.fft.fft(x.cpu().numpy().astype(np.complex128))
+    err = float(np.linalg.norm(y - ref) / np.linalg.norm(ref))
+    bb = shards[0].buffers()
+    esz = 8
+    line = {"metric": "device time per transform, sharded over G shards (slowest shard's phases)",
+            "value": worst, "unit": "ms", "higher_is_better": False, "n_gpus": 1, "steps": a.steps,
+            "warmup": max(a.warmup, 3), "dtype": "fp32 (split-TF32 tcgen05)", "data": "synthetic",
+            "config": {"workload": "sharded single transform", "N": N, "P": P, "terms": T, "b": b,
+                       "shards": G, "precision": prec, "how": "G shards emulated on one B200, phases in turn, "
+                       "256 MB L2 flush before every phase"},
+            "phase_ms_median": {f"shard{g}": [float(np.median([t[g, k] for t in per])) for k in range(3)]
+                                for g in range(G)},
+            "exchange_bytes_per_shard": {"x_halos_in": 2 * bb["halo_elems"] * esz, "section_sums": 2 * P * esz,
+                                         "coarse_allgather_in": (G - 1) * bb["phi_elems"] * 4,
+                                         "alltoall_out": (G - 1) * bb["z_elems"] // G * esz},
+            "accuracy": {"rel_l2_vs_fp64": err}}
+    print(json.dumps(line))
+    for sh in shards:
+        sh.close()
+    return 0
+
+
 def main():
     a = parse()
+    if a.workload == "sharded":
+        return run_sharded(a)
     if a.workload == "precision-sweep":
         return run_precision_sweep(a)
     if a.workload == "uneven-batch":
