@@ -159,6 +159,8 @@ template <typename R> struct Dev {
   float *tc_leaf[2];    /* per section */
   float *tc_lnb[2];     /* the leaf's neighbour-sum operators, per section (row image only) */
   float *leaf_fix;      /* tensor-core leaf, section P/2: [2][s] first points from box-1 */
+  float *lnb_w01;       /* neighbour-sum leaf: per section the near-field weights of offsets 0
+                         * and -1, applied in FP32 in the epilogue (not in the operator) */
   long tc_m2m_stride, tc_m2l_stride, tc_leaf_stride, tc_lnb_stride; /* kp np */
   long tc_s2m_stride16, tc_m2m_stride16, tc_m2l_stride16, tc_leaf_stride16;
   /* the same operators for the warp-specialised kernel: hi rows then lo rows in the MMA's
@@ -607,9 +609,27 @@ struct TcLeaf : TcBase { /* batch z = section - 1; s is a power of two (log2s) *
     return xt + (pl + 2 * (r >> (log2s + 1)) + 2) * M + (((bx - 2 + c) * b) & (M - 1));
   }
   __device__ float *dst(long r, int z) const { return u + plane(r, z) * M + (r & (s - 1)) * b; }
-  __device__ void put8(float *dst, long r, int z, int c0, const float *t) const {
+  const float *w01; /* per section z: the near-field weights of offsets 0 and -1 (not in B) */
+  /* adds w0 x[j] + w1 x[j-1] (FP32) to outputs j = c .. c+n-1 (those below b) of row r's box */
+  __device__ void near01(long r, int z, int c, int n, float *t) const {
+    const long bx = r & (s - 1), pl = plane(r, z);
+    const float *xp = xt + (pl + 2 * (r >> (log2s + 1)) + 2) * M;
+    const long j0 = bx * b + c;
+    const float w0 = w01[2 * z], w1 = w01[2 * z + 1];
+    float prev = xp[(j0 - 1) & (M - 1)];
+    for (int i = 0; i < n && c + i < b; ++i) {
+      const float xi = xp[j0 + i];
+      t[i] = fmaf(w0, xi, fmaf(w1, prev, t[i]));
+      prev = xi;
+    }
+  }
+  __device__ void put8(float *dst, long r, int z, int c0, const float *t0) const {
     const int sc = z + 1;
     const bool shifted = 2 * sc > P; /* the in-box first point is replaced */
+    float t[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) t[i] = t0[i];
+    near01(r, z, c0, 8, t);
     if (c0 + 4 <= b) {
       if (c0 == 0 && shifted) {
         dst[1] = t[1], dst[2] = t[2], dst[3] = t[3];
@@ -630,6 +650,9 @@ struct TcLeaf : TcBase { /* batch z = section - 1; s is a power of two (log2s) *
   __device__ void put4(float *dst, long r, int z, int c, float4 v) const { /* c a multiple of 4 */
     const int sc = z + 1;
     if (c < b) {
+      float t[4] = {v.x, v.y, v.z, v.w};
+      near01(r, z, c, 4, t);
+      v = make_float4(t[0], t[1], t[2], t[3]);
       if (c == 0 && 2 * sc > P) /* the in-box first point is replaced */
         dst[1] = v.y, dst[2] = v.z, dst[3] = v.w;
       else
@@ -656,6 +679,12 @@ struct TcLeaf : TcBase { /* batch z = section - 1; s is a power of two (log2s) *
  * instead of three times (K = T + b instead of T + 3b). */
 struct TcLeafNb : TcLeaf {
   long strips;
+  /* adds w0 x[j] + w1 x[j-1] (FP32) to targets j = c0 .. c0+7 of a row, x = x[c0-1 .. c0+7] */
+  __device__ void fix_apply(int z, const float (&x)[9], float *t) const {
+    const float w0 = w01[2 * z], w1 = w01[2 * z + 1];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) t[i] = fmaf(w0, x[i + 1], fmaf(w1, x[i], t[i]));
+  }
   __device__ const float *src(int c, long r, int z) const {
     const long bx = r & (s - 1), pl = plane(r, z);
     if (c == 0) return psi_n + (pl * s + bx) * T;
@@ -2060,7 +2089,19 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
       rc |= tc_put(d->tc_m2l[0] + (l - 3) * 2 * d->tc_m2l_stride, d->tc_m2l[1] + (l - 3) * d->tc_m2l_stride16,
                    d->ws_m2l + (l - 3) * d->ws_m2l_stride, v, kp, np, err, errlen, d->bf16);
     }
-  if (d->ok_leaf)
+  /* The two near-field weights of largest magnitude, source offsets d = 0 and d = -1 from the
+   * target (|w| up to ~P / pi), are left out of both leaf operators and applied in FP32 when the
+   * kernels store the leaf's outputs: split into TF32 parts and summed in the tensor core's FP32
+   * accumulator they set the leaf's rounding error (4 x that of FP32 products); without them the
+   * remaining terms are O(1) and the leaf's error is that of the FP32 stores' two FMAs. */
+  float *w01 = (d->ok_lnb || d->ok_leaf) ? (float *)malloc(sizeof(float) * 2 * S1) : nullptr;
+  if ((d->ok_lnb || d->ok_leaf) && !w01) rc = 2;
+  if (w01)
+    for (long sc = 1; sc < P; ++sc) {
+      const double *ct = o->cot + (sc - 1) * 4 * b;
+      w01[2 * (sc - 1)] = (float)ct[2 * b], w01[2 * (sc - 1) + 1] = (float)ct[2 * b - 1];
+    }
+  if (d->ok_leaf && w01)
     for (long sc = 1; sc < P; ++sc) {
       const int kp = d->kp_leaf, np = d->np_leaf;
       const double *ct = o->cot + (sc - 1) * 4 * b;
@@ -2068,6 +2109,7 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
       for (long j = 0; j < b; ++j) {
         for (long k = 0; k < T; ++k) v[j * kp + k] = o->evalm[(j * S1 + (sc - 1)) * T + k];
         for (long q = 0; q < 3 * b; ++q) v[j * kp + T + q] = ct[q + b - j];
+        v[j * kp + T + j + b] = 0, v[j * kp + T + j + b - 1] = 0; /* d = 0, -1: in FP32 */
       }
       if (2 * sc >= P) { /* column b: the next box's half-shifted first point (TcLeaf) */
         for (long k = 0; k < T; ++k) v[b * kp + k] = o->evalmh[(sc - P / 2) * T + k];
@@ -2076,7 +2118,7 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
       rc |= tc_put(d->tc_leaf[0] + (sc - 1) * 2 * d->tc_leaf_stride, d->tc_leaf[1] + (sc - 1) * d->tc_leaf_stride16,
                    d->ws_leaf + (sc - 1) * d->ws_leaf_stride, v, kp, np, err, errlen, d->bf16);
     }
-  if (d->ok_lnb) /* neighbour-sum form (TcLeafNb): x_B's weights for boxes B, B+1, B-1 */
+  if (d->ok_lnb && w01) /* neighbour-sum form (TcLeafNb): x_B's weights for boxes B, B+1, B-1 */
     for (long sc = 1; sc < P; ++sc) {
       const int kp = d->kp_lnb, np = d->np_lnb;
       const double *ct = o->cot + (sc - 1) * 4 * b;
@@ -2089,6 +2131,11 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
           v[(2 * b + j) * kp + T + q] = ct[q + 3 * b - j]; /* window end of box B-1 */
         }
       }
+      for (long j = 0; j < b; ++j) {
+        v[j * kp + T + j] = 0;                        /* d = 0 */
+        if (j > 0) v[j * kp + T + j - 1] = 0;         /* d = -1 within box B */
+      }
+      v[b * kp + T + b - 1] = 0;                      /* d = -1: the last point of B, first target of B+1 */
       if (2 * sc >= P) { /* H(B), and x_B's parts of H(B+1) and H(B-1) */
         for (long k = 0; k < T; ++k) v[3 * b * kp + k] = o->evalmh[(sc - P / 2) * T + k];
         for (long q = 0; q < b; ++q) {
@@ -2099,6 +2146,10 @@ template <typename R> static int tc_upload_ops(Dev<R> *d, const fmm_ops64 *o, ch
       }
       rc |= tc_put(d->tc_lnb[0] + (sc - 1) * 2 * d->tc_lnb_stride, nullptr, nullptr, v, kp, np, err, errlen, 0);
     }
+  if (w01) {
+    if (!rc && cudaMemcpy(d->lnb_w01, w01, sizeof(float) * 2 * S1, cudaMemcpyHostToDevice) != cudaSuccess) rc = 3;
+    free(w01);
+  }
   free(v);
   return rc;
 }
@@ -2276,6 +2327,7 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
   CARVE(tcm2l16, d->ok_m2l ? nlev * d->tc_m2l_stride16 : 0, float)
   CARVE(tcleaf16, d->ok_leaf ? S1 * d->tc_leaf_stride16 : 0, float)
   CARVE(leaffix, (d->ok_leaf || d->ok_lnb) ? nb * 2 * s : 0, float)
+  CARVE(lnbw, (d->ok_lnb || d->ok_leaf) ? 2 * S1 : 0, float)
   CARVE(wss2m, ws_s2m_n, float)
   CARVE(wsm2m, ws_m2m_n, float)
   CARVE(wsm2l, ws_m2l_n, float)
@@ -2325,6 +2377,7 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
   d->tc_leaf[0] = (float *)(base + off_tcleaf), d->tc_leaf[1] = (float *)(base + off_tcleaf16);
   d->tc_lnb[0] = (float *)(base + off_tclnb), d->tc_lnb[1] = nullptr;
   d->leaf_fix = (float *)(base + off_leaffix);
+  d->lnb_w01 = (float *)(base + off_lnbw);
   d->ws_s2m = (float *)(base + off_wss2m);
   d->ws_m2m = (float *)(base + off_wsm2m);
   d->ws_m2l = (float *)(base + off_wsm2l);
@@ -2623,6 +2676,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.clen[0] = (int)T, q.clen[1] = (int)b, q.coff[0] = 0, q.coff[1] = (int)T;
         q.kpad = d->kp_lnb, q.npad = d->np_lnb, q.nout = (int)b;
         q.bimg = d->tc_lnb[0], q.bimg_stride = 2 * d->tc_lnb_stride, q.bimg16 = nullptr, q.bimg16_stride = 0;
+        q.w01 = d->lnb_w01;
         q.fixbuf = d->leaf_fix, q.P = (int)P;
         q.psi_n = pb.psi_n, q.xt = d->xt, q.u = d->u, q.M = M, q.s = s, q.T = (int)T, q.b = (int)b;
         q.log2s = (int)n, q.strips = 2L * nbt;
@@ -2634,7 +2688,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
         q.clen[0] = (int)T, q.clen[1] = q.clen[2] = q.clen[3] = (int)b;
         q.coff[0] = 0, q.coff[1] = (int)T, q.coff[2] = (int)(T + b), q.coff[3] = (int)(T + 2 * b);
         q.kpad = d->kp_leaf, q.npad = d->np_leaf, q.nout = (int)b;
-        q.bimg = d->tc_leaf[0], q.bimg_stride = 2 * d->tc_leaf_stride;
+        q.bimg = d->tc_leaf[0], q.bimg_stride = 2 * d->tc_leaf_stride, q.w01 = d->lnb_w01;
         q.bimg16 = d->tc_leaf[1], q.bimg16_stride = d->tc_leaf_stride16;
         q.wsb = d->ws_leaf, q.wsb_stride = d->ws_leaf_stride;
         q.fixbuf = d->leaf_fix, q.P = (int)P;

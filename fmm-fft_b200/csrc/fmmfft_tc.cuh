@@ -518,6 +518,10 @@ __host__ __device__ constexpr int nb_tmem_cols(int kpad, int npad) {
  *   long s; int b;                         units per strip, block width w (a multiple of 8, <= 32)
  *   long strips;                           strips per batch
  *   __device__ bool has_h(int batch) const;                 the three h columns are in use
+ *   __device__ void fix_apply(int batch, const float (&x)[9], float *t) const;
+ *                                          adds to out[r][c0..c0+8) what the operator leaves out,
+ *                                          from the row's samples x[c0-1 .. c0+7] (A chunk 1,
+ *                                          which the kernel keeps in shared memory in FP32)
  *   __device__ void put8_nb(long r, int batch, int c0, const float *t) const;
  *                                          stores out[r][c0..c0+8)
  *   __device__ void put_h(long r, int batch, float v) const;  stores h[r]
@@ -532,6 +536,9 @@ __global__ void __launch_bounds__(256, 2) k_tc_nbr(const __grid_constant__ Prob 
   /* warp-edge values: [half][quarter][chunk 0, 1, h][0: lane 31's next block, 1: lane 0's
    * previous block][8] */
   __shared__ float xch[2][4][3][2][8];
+  /* the tile's samples (A chunk 1, b <= 32 of them a row) in FP32, for the terms the operator
+   * leaves to the epilogue; rows padded to 36 floats against bank conflicts */
+  __shared__ __align__(16) float xstage[kRows][36];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int kpad = pb.kpad, npad = pb.npad;
   const int ks = kpad < kSlice ? kpad : kSlice;
@@ -648,6 +655,11 @@ __global__ void __launch_bounds__(256, 2) k_tc_nbr(const __grid_constant__ Prob 
         tmem_st8(t_ahi + lane_addr + col + 8 * q, h);
         tmem_st8(t_alo + lane_addr + col + 8 * q, l);
       }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) { /* this thread's samples of the row, kept in FP32 */
+        const int e = lmap[slice][my_half][i];
+        if ((e & 0xFF) == 1) *reinterpret_cast<float4 *>(&xstage[my_m][e >> 8]) = v[i];
+      }
     }
     tmem_st_wait();
     fence_before_sync();
@@ -699,7 +711,21 @@ __global__ void __launch_bounds__(256, 2) k_tc_nbr(const __grid_constant__ Prob 
         if (my_half) asm volatile("bar.sync 2, 128;" ::: "memory");
         else asm volatile("bar.sync 1, 128;" ::: "memory");
       };
-#pragma unroll 1
+      /* the samples the FP32 terms need, x[j-1 .. j+7] of each chunk (the one before the box's
+       * first is the previous row's last) */
+      float fx[2][9];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int c = my_half + 2 * j;
+        if (out_row && c < nw8) {
+          fx[j][0] = c == 0 ? xstage[my_m - 1][w - 1] : xstage[my_m][8 * c - 1];
+          const float4 a = *reinterpret_cast<const float4 *>(&xstage[my_m][8 * c]);
+          const float4 e = *reinterpret_cast<const float4 *>(&xstage[my_m][8 * c + 4]);
+          fx[j][1] = a.x, fx[j][2] = a.y, fx[j][3] = a.z, fx[j][4] = a.w;
+          fx[j][5] = e.x, fx[j][6] = e.y, fx[j][7] = e.z, fx[j][8] = e.w;
+        }
+      }
+#pragma unroll
       for (int j = 0; j < 2; ++j) {
         const int c = my_half + 2 * j;
         if (c >= nw8) break; /* warp-uniform */
@@ -730,7 +756,10 @@ __global__ void __launch_bounds__(256, 2) k_tc_nbr(const __grid_constant__ Prob 
           if (lane == 31) fr = quarter < 3 ? xch[my_half][quarter + 1][j][1][i] : 0.f;
           cen[i] += fl + fr;
         }
-        if (out_row) pb.put8_nb(r, batch, 8 * c, cen);
+        if (out_row) {
+          pb.fix_apply(batch, fx[j], cen); /* the terms the operator leaves to FP32 */
+          pb.put8_nb(r, batch, 8 * c, cen);
+        }
       }
       if (hcols) {
         float hv[8];
