@@ -163,7 +163,7 @@ def stage_bytes(N, P, T, b, esz):
 # (213.4 MB for 2^12 parents per section plane); the mean over the seven levels scales it by the
 # levels' rows, (2^13 - 2^6) / 2^12 / 7.  Only meaningful for the headline workload.
 TRAFFIC_PER_LAUNCH = {
-    "leaf_l2t_near": 240.409344e6 + 96.509696e6,
+    "leaf_l2t_near": 240.520704e6 + 98.922752e6,
     "sections": 134.243840e6 + 186.710528e6,
     "m2l_l2l": (148.727808e6 + 64.687360e6) * ((1 << 13) - (1 << 6)) / (1 << 12) / 7,
 }
