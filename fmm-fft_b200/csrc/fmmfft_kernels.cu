@@ -150,6 +150,10 @@ template <typename R> struct Dev {
   /* tensor-core (FMMFFT_F32_TC) operators: pre-split TF32 hi/lo, [npad][kpad] K-major */
   int tc, num_sms;
   int *status;          /* device word: non-zero after a bounded device wait gave up */
+  /* the section sums run on a stream of their own, forked after the sections pass and joined
+   * before the combine (their only reader), so they overlap the tree stages; null: in line */
+  cudaStream_t side;
+  cudaEvent_t ev_fork, ev_join;
   /* operator images: [0] the row forms' shared-memory image (hi rows then lo rows, K-major
    * core matrices, K extent kpad; 2 kp np floats per level / section), [1] the 16-lane form's
    * (K and N permuted, K extent round16(kp); tc_*_stride16 floats per level / section) */
@@ -2466,8 +2470,26 @@ static int dev_create(const fmm_ops64 *o, int precision, int nb, Dev<R> **out, c
     delete d;
     return rc;
   }
+  if (cudaStreamCreateWithFlags(&d->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&d->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&d->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError(); /* no side stream: the sums run in line */
+    if (d->side) cudaStreamDestroy(d->side);
+    if (d->ev_fork) cudaEventDestroy(d->ev_fork);
+    d->side = nullptr, d->ev_fork = d->ev_join = nullptr;
+  }
   *out = d;
   return 0;
+}
+
+/* Frees a plan's device state. */
+template <typename R> static void dev_release(Dev<R> *d) {
+  if (!d) return;
+  if (d->side) cudaStreamDestroy(d->side);
+  if (d->ev_fork) cudaEventDestroy(d->ev_fork);
+  if (d->ev_join) cudaEventDestroy(d->ev_join);
+  cudaFree(d->pool);
+  delete d;
 }
 
 /* Parts of one execute (a shard of a sharded transform runs its plan's stages in pieces, with
@@ -2537,10 +2559,18 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
     pf.launches[ST_SECTIONS]++;
   }
   stage(ST_SUMS);
+  bool sums_forked = false;
   if (run(ST_SUMS)) { /* a shard sums its own tiles only */
     const long t0 = ctl ? ctl->sum_t0 : 0, nt = ctl ? ctl->sum_nt : d->ntile;
     C *out = (ctl && ctl->sum_out) ? (C *)ctl->sum_out : d->ssum;
-    k_sum_sections<R><<<dim3((unsigned)P, (unsigned)nbt), 256, 0, st>>>(d->part + t0 * P, nt, (int)P, out);
+    cudaStream_t ss = st;
+    if (!ctl && d->side) { /* off the critical path until the combine */
+      cudaEventRecord(d->ev_fork, st);
+      cudaStreamWaitEvent(d->side, d->ev_fork, 0);
+      ss = d->side, sums_forked = true;
+    }
+    k_sum_sections<R><<<dim3((unsigned)P, (unsigned)nbt), 256, 0, ss>>>(d->part + t0 * P, nt, (int)P, out);
+    if (sums_forked) cudaEventRecord(d->ev_join, ss);
     pf.launches[ST_SUMS]++;
   }
   /* 3: S2M at level n (done in stage 1 when fused) */
@@ -2742,6 +2772,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
     snprintf(err, errlen, "a column window of the combine needs P >= 16");
     return 1;
   }
+  if (sums_forked) cudaStreamWaitEvent(st, d->ev_join, 0); /* the combine reads the sums */
   if (!run(ST_COMBINE)) {
   } else if (P >= 16 && P * M < (1L << 32)) {
     pf.launches[ST_COMBINE]++;
@@ -3061,7 +3092,7 @@ extern "C" int fmmk_create_n(const fmm_ops64 *ops, int precision, int nb, fmmk_s
     const char *ev = getenv("FMMFFT_AUTOTUNE");
     if (!rc && !(ev && atoi(ev) == 0)) {
       rc = dev_autotune<float>(d, err, errlen);
-      if (rc) cudaFree(d->pool), delete d;
+      if (rc) dev_release(d);
     }
   }
   if (rc) {
@@ -3100,10 +3131,10 @@ extern "C" void fmmk_destroy(fmmk_state *st) {
   host_pipe_free(st->pipe);
   if (st->precision == 0) {
     Dev<double> *d = (Dev<double> *)st->dev;
-    if (d) cudaFree(d->pool), delete d;
+    dev_release(d);
   } else {
     Dev<float> *d = (Dev<float> *)st->dev;
-    if (d) cudaFree(d->pool), delete d;
+    dev_release(d);
   }
   free(st);
 }
@@ -4014,8 +4045,7 @@ template <typename R>
 static void shard_free(ShardImpl<R> *sh) {
   if (!sh) return;
   Dev<R> *ds[3] = {sh->loc, sh->crs, sh->fft};
-  for (Dev<R> *d : ds)
-    if (d) cudaFree(d->pool), delete d;
+  for (Dev<R> *d : ds) dev_release(d);
   cudaFree(sh->mem);
   delete sh;
 }
