@@ -1316,23 +1316,37 @@ __global__ void k_fft_pass(const typename cplx<R>::T *__restrict__ in,
 
 /* Register-resident Stockham pass: one thread per radix-8 butterfly column (L/8 threads per
  * sequence, W sequences per block) keeps its 8 values in registers through every stage; the
- * stages exchange through ONE shared buffer laid out per sequence, buf[w*LP + i + i/8] with
- * the pitch LP of fft_lp, which keeps both thread orders below free of bank conflicts.  The first
+ * stages exchange through ONE shared buffer laid out per sequence, element i of sequence w at
+ * w*LP + fft_swz(i, kw) (pitch LP of fft_lp, an XOR swizzle within 16-element rows), which
+ * keeps every exchange of both thread orders free of bank conflicts at the FMM-FFT's shapes
+ * (L = 512 with W = 8; the combine's L = P with W = 32 / 16).  The first
  * stage reads global memory directly and the last stage writes it directly.  Thread order:
  * along the sequence (TIN) when the input is contiguous in i, across sequences otherwise, so
  * that a warp's loads are coalesced either way; when the output wants the other order
  * (TOUT != TIN) the result goes once through the shared buffer.  The 4-step twiddle of output
  * i = t + r L/8 of sequence g factors as exp(-2 pi i g t / M) exp(-2 pi i g (L/8) r / M): one
- * gather per thread and 8 W steps in shared memory.  Shared: W*LP + L + L/16 + 1 + 8 W
- * elements; needs 16 <= L and W*L/8 <= 512; offsets within a row fit 32 bits (M <= 2^26). */
-/* Row pitch (in complex elements) of a sequence in the register pass's exchange buffer:
- * >= L + L/8, and == 32/W (mod 16) so that a warp's W sequences x 32/W positions fall on
- * distinct 8-byte bank slots in both thread orders (every slot hit twice: the minimum for a
- * warp of 8-byte accesses). */
+ * gather per thread and 8 W steps in shared memory.  Shared: fft_smem_elems(L, W) elements
+ * (more for compensated twiddles); needs 16 <= L and W*L/8 <= 512; offsets within a row fit 32
+ * bits (M <= 2^26). */
+/* Exchange-buffer layout.  A half-warp's 16 8-byte accesses are conflict-free when they fall on
+ * 16 distinct slots (element index mod 16).  Across sequences (thread order w-fastest) the
+ * pitch LP = L + 16/W puts W sequences 16/W slots apart, and for W = 8 the XOR of bit 0 by
+ * w bit 2 separates the pairs {c, c+8} that a radix-8 store's two threads of one sequence hit;
+ * along a sequence the row swizzle h(R) = (R & 7) ^ ((R & 4) << 1) of row R = i / 16 spreads
+ * the stride-8 stores 8t + r (rows t/2) and the stage-8 stores (rows R, R + 4) over both
+ * halves of the row.  The swizzle permutes within each 16-element row, so indices stay in
+ * [w LP, w LP + L). */
 __host__ __device__ __forceinline__ int fft_lp(int L, int W) {
-  const int base = L + L / 8;
-  const int a = W >= 2 ? (32 / W) & 15 : 1;
-  return base + ((a - base % 16) + 16) % 16;
+  return L + (W >= 16 ? 1 : W == 1 ? 0 : 16 / W);
+}
+__device__ __forceinline__ int fft_swz(int i, int kw) {
+  const int R = i >> 4;
+  return i ^ (R & 7) ^ ((R & 4) << 1) ^ kw;
+}
+/* Shared elements of a register pass: exchange buffer, stage twiddles (L - Ns0 <= L used, the
+ * region kept at L + L/16 + 1), 4-step twiddle steps [w][9]. */
+__host__ __device__ __forceinline__ size_t fft_smem_elems(int L, int W) {
+  return (size_t)W * fft_lp(L, W) + L + L / 16 + 1 + 9 * (size_t)W;
 }
 
 /* Input of a register pass: element t + r q (r < 8) of sequence g of row `row` into v[r]. */
@@ -1404,9 +1418,12 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
   const int lq = __ffs(q) - 1, lW = __ffs(W) - 1;
   const int LP = fft_lp(L, W);
   C *buf = reinterpret_cast<C *>(smem_raw);
-  C *twl = buf + W * LP;    /* exp(-2 pi i m / L) at m + m/16 */
-  C *twq = twl + L + L / 16 + 1; /* 4-step twiddle steps exp(-2 pi i g q r / M), [w][r] */
-  C *twl_lo = twq + 8 * W;       /* COMP: the remainders of twl */
+  /* stage twiddles, stage-major: for the stage of span Ns (Ns0, 8 Ns0, ..., L/8; Ns0 the first
+   * stage's radix), exp(-2 pi i r k / (8 Ns)) at (Ns - Ns0) + 7 k + r - 1 (k < Ns, 1 <= r < 8):
+   * a thread's 7 twiddles are consecutive and a half-warp's threads 7 apart */
+  C *twl = buf + W * LP;
+  C *twq = twl + L + L / 16 + 1; /* 4-step twiddle steps exp(-2 pi i g q r / M), [w][9] */
+  C *twl_lo = twq + 9 * W;       /* COMP: the remainders of twl */
   const int tid = threadIdx.x;
   const unsigned g0 = blockIdx.x * (unsigned)W;
   /* post-twiddle exp(-2 pi i e / T) for e = g * i */
@@ -1416,12 +1433,18 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
     const unsigned lo = (1u << fp.twbits) - 1;
     return cmul(twP[lo + 1 + (e >> fp.twbits)], twP[e & lo]);
   };
-  for (int m = tid; m < L; m += blockDim.x) twl[m + (m >> 4)] = twD[(long)m * fp.tws];
-  if constexpr (COMP)
-    for (int m = tid; m < L; m += blockDim.x) twl_lo[m + (m >> 4)] = twD_lo[(long)m * fp.tws];
+  const int lg = __ffs(L) - 1;
+  const int ns0 = lg % 3 == 0 ? 8 : lg % 3 == 2 ? 4 : 2;
+  for (int Ns = ns0; Ns <= q; Ns <<= 3)
+    for (int m = tid; m < 7 * Ns; m += blockDim.x) {
+      const int k = m / 7, r = m - 7 * k + 1;
+      const long e = (long)(r * k * (q / Ns)) * fp.tws; /* r k L / (8 Ns) of L */
+      twl[Ns - ns0 + m] = twD[e];
+      if constexpr (COMP) twl_lo[Ns - ns0 + m] = twD_lo[e];
+    }
   if (fp.twiddle_post && !COMP)
     for (int m = tid; m < 8 * W; m += blockDim.x)
-      twq[m] = post((g0 + (m >> 3)) * (unsigned)q * (unsigned)(m & 7));
+      twq[(m >> 3) * 9 + (m & 7)] = post((g0 + (m >> 3)) * (unsigned)q * (unsigned)(m & 7));
   /* COMP: x times exp(-2 pi i e / T), e = g i twmul mod T, from the hi / lo tables */
   auto post_comp = [&](C x, unsigned gi) -> C {
     if constexpr (COMP) {
@@ -1439,14 +1462,13 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
   C v[8];
   ld(row, g0 + w, t, q, v);
   C *bw = buf + w * LP;
-  const int lg = __ffs(L) - 1;
+  const int kw = W == 8 ? (w >> 2) & 1 : 0;
   int Ns, lNs;
   if (lg % 3 == 0) { /* radix-8 first stage: outputs 8t + r */
     dft8(v);
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
-      const int i = 8 * t + r;
-      bw[i + (i >> 3)] = v[r];
+      bw[fft_swz(8 * t + r, kw)] = v[r];
     }
     Ns = 8, lNs = 3;
   } else if (lg % 3 == 2) { /* radix 4: butterflies t (v0,2,4,6) and t+q (v1,3,5,7) */
@@ -1454,46 +1476,38 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
     dft4(v[1], v[3], v[5], v[7]);
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-      const int i0 = 4 * t + r, i1 = 4 * (t + q) + r;
-      bw[i0 + (i0 >> 3)] = v[2 * r];
-      bw[i1 + (i1 >> 3)] = v[2 * r + 1];
+      bw[fft_swz(4 * t + r, kw)] = v[2 * r];
+      bw[fft_swz(4 * (t + q) + r, kw)] = v[2 * r + 1];
     }
     Ns = 4, lNs = 2;
   } else { /* radix 2: butterflies t + m q, inputs v[m], v[m+4] */
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
       const int i = 2 * (t + m * q);
-      bw[i + (i >> 3)] = cadd(v[m], v[m + 4]);
-      bw[i + 1 + ((i + 1) >> 3)] = csub(v[m], v[m + 4]);
+      bw[fft_swz(i, kw)] = cadd(v[m], v[m + 4]);
+      bw[fft_swz(i + 1, kw)] = csub(v[m], v[m + 4]);
     }
     Ns = 2, lNs = 1;
   }
   for (;;) {
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const int i = t + r * q;
-      v[r] = bw[i + (i >> 3)];
-    }
+    for (int r = 0; r < 8; ++r) v[r] = bw[fft_swz(t + r * q, kw)];
     const int k = t & (Ns - 1);
-    const int ts = k << (lg - 3 - lNs); /* k L / (8 Ns) */
+    const int tb = Ns - ns0 + 7 * k - 1;
 #pragma unroll
     for (int r = 1; r < 8; ++r) {
-      const int m = r * ts;
       if constexpr (COMP)
-        v[r] = cmul_comp(v[r], twl[m + (m >> 4)], twl_lo[m + (m >> 4)]);
+        v[r] = cmul_comp(v[r], twl[tb + r], twl_lo[tb + r]);
       else
-        v[r] = cmul(v[r], twl[m + (m >> 4)]);
+        v[r] = cmul(v[r], twl[tb + r]);
     }
     dft8(v);
     if (lNs + 3 == lg) break; /* v[r] = output t + r q */
     __syncthreads();
     const int o = ((t >> lNs) << (lNs + 3)) + k;
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const int i = o + (r << lNs);
-      bw[i + (i >> 3)] = v[r];
-    }
+    for (int r = 0; r < 8; ++r) bw[fft_swz(o + (r << lNs), kw)] = v[r];
     Ns <<= 3, lNs += 3;
   }
   C *dp = ot.rpp ? reinterpret_cast<C *>(ot.p[row / ot.rpp]) + (row % ot.rpp) * fp.orow : out + row * fp.orow;
@@ -1510,7 +1524,7 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
         if constexpr (COMP)
           x = post_comp(x, g * (unsigned)(t + r * q));
         else
-          x = cmul(x, cmul(a, twq[w * 8 + r]));
+          x = cmul(x, cmul(a, twq[w * 9 + r]));
       }
       if (fp.conj_out) x.y = -x.y;
       op[r * qs] = x;
@@ -1518,16 +1532,14 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
   } else {
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const int i = t + r * q;
-      bw[i + (i >> 3)] = v[r];
-    }
+    for (int r = 0; r < 8; ++r) bw[fft_swz(t + r * q, kw)] = v[r];
     __syncthreads();
     int t2, w2;
     if (TOUT) t2 = tid & (q - 1), w2 = tid >> lq;
     else w2 = tid & (W - 1), t2 = tid >> lW;
     const unsigned g = g0 + w2;
     const C *b2 = buf + w2 * LP;
+    const int kw2 = W == 8 ? (w2 >> 2) & 1 : 0;
     C *op = dp + g * fp.oseq + t2 * ostr;
     const unsigned qs = (unsigned)q * ostr;
     C a;
@@ -1535,12 +1547,12 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
       const int i = t2 + r * q;
-      C x = b2[i + (i >> 3)];
+      C x = b2[fft_swz(i, kw2)];
       if (fp.twiddle_post) {
         if constexpr (COMP)
           x = post_comp(x, g * (unsigned)i);
         else
-          x = cmul(x, cmul(a, twq[w2 * 8 + r]));
+          x = cmul(x, cmul(a, twq[w2 * 9 + r]));
       }
       if (fp.conj_out) x.y = -x.y;
       op[r * qs] = x;
@@ -1568,7 +1580,7 @@ static void launch_fft_pass(const typename cplx<R>::T *in, typename cplx<R>::T *
       fp.W = W;
       const StridedLd<R> sld{in, fp.M, fp.iseq, (unsigned)fp.istr};
       const int thr = W * (L / 8);
-      const size_t sm = sizeof(C) * ((size_t)W * fft_lp(L, W) + L + L / 16 + 1 + 8 * W);
+      const size_t sm = sizeof(C) * fft_smem_elems(L, W);
       dim3 g((unsigned)(per / W), (unsigned)rows);
       if constexpr (sizeof(R) == 4) {
         if (twM_lo) { /* compensated twiddles */
@@ -2787,7 +2799,7 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
     const CombineLd<R> cl{d->xt, d->u, d->ssum, d->pretw, M, cinvM, (int)P,
                           d->comp_tw ? d->pretw_lo : nullptr, cm0};
     const int thr = Wc * (int)(P / 8);
-    const size_t sm = sizeof(C) * ((size_t)Wc * fft_lp((int)P, Wc) + P + P / 16 + 1 + 8 * (size_t)Wc);
+    const size_t sm = sizeof(C) * fft_smem_elems((int)P, Wc);
     if (d->comp_tw && sizeof(R) == 4)
       k_fft_reg<R, false, false, CombineLd<R>, true>
           <<<dim3((unsigned)(ccols / Wc), (unsigned)nbt), thr, sm + sizeof(C) * (size_t)(P + P / 16 + 1), st>>>(
@@ -3938,7 +3950,7 @@ static int fft_run(fmmk_fft *f, const void *in, void *out, cudaStream_t st, char
     const C *src = (const C *)(f->src[k] == 0 ? in : (f->src[k] == 1 ? out : f->tmp));
     C *dst = (C *)(f->dst[k] == 1 ? out : f->tmp);
     const int thr = fp.W * (fp.L / 8);
-    const size_t sm = sizeof(C) * ((size_t)fp.W * fft_lp(fp.L, fp.W) + fp.L + fp.L / 16 + 1 + 8 * fp.W);
+    const size_t sm = sizeof(C) * fft_smem_elems(fp.L, fp.W);
     dim3 g((unsigned)(f->per[k] / fp.W), (unsigned)f->rows[k]);
     const StridedLd<R> sld{src, fp.irow, fp.iseq, (unsigned)fp.istr};
     if (f->tin[k] && f->tout[k])
