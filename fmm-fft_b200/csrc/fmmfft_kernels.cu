@@ -323,11 +323,14 @@ __global__ void k_sections(const typename cplx<R>::T *__restrict__ x, R *__restr
   if (phi_n != nullptr)
     for (int e = threadIdx.x; e < b * T; e += blockDim.x) ich[e] = initch[e];
   __syncthreads();
-  /* planar store: plane (2sc+ri), TMt contiguous points */
-  for (int e = threadIdx.x; e < 2 * E; e += blockDim.x) {
-    int mm = e & (TMt - 1), q = e >> lt, sc = q >> 1, ri = q & 1;
-    C v = tile[mm * PP + sc];
-    xt[(long)q * M + m0 + mm] = ri ? v.y : v.x;
+  /* planar stores: point mm of section sc to planes 2sc (re) and 2sc+1 (im), TMt contiguous
+   * points a plane */
+  for (int e = threadIdx.x; e < E; e += blockDim.x) {
+    const int mm = e & (TMt - 1), sc = e >> lt;
+    const C v = tile[mm * PP + sc];
+    R *dst = xt + (long)(2 * sc) * M + m0 + mm;
+    dst[0] = v.x;
+    dst[M] = v.y;
   }
   /* S2M of the tile's leaf boxes (reference initmm, fmmfft.c:199-211), when the tile holds
    * whole boxes (b | TMt) and T % 4 == 0: phi_n[(2(sc-1) + ri) s + box][k] =
