@@ -1408,8 +1408,10 @@ template <typename R> struct CombineLd {
  * entry's remainder; the stage twiddles are applied with cmul_comp from a second shared table,
  * and the 4-step post-twiddle of output i of sequence g is read directly as twP[(g i) mod T]
  * (hi and lo; single-level tables, twbits = 0) instead of as a product of two rounded factors.
- * Shared memory: L + L/16 + 1 more elements. */
-template <typename R, bool TIN, bool TOUT, class Ld = StridedLd<R>, bool COMP = false>
+ * Shared memory: L + L/16 + 1 more elements.
+ * LGT != 0: a build for L = 2^LGT only (fp.L must equal it), so that the stage loop unrolls and
+ * every exchange index is folded at compile time; LGT = 0 serves any L. */
+template <typename R, bool TIN, bool TOUT, class Ld = StridedLd<R>, bool COMP = false, int LGT = 0>
 __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
     k_fft_reg(const Ld ld, typename cplx<R>::T *__restrict__ out,
               const typename cplx<R>::T *__restrict__ twD, const typename cplx<R>::T *__restrict__ twP,
@@ -1417,8 +1419,8 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
               const typename cplx<R>::T *__restrict__ twP_lo = nullptr, const OutTab ot = OutTab{}) {
   using C = typename cplx<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int L = fp.L, W = fp.W, q = L >> 3;
-  const int lq = __ffs(q) - 1, lW = __ffs(W) - 1;
+  const int L = LGT ? 1 << LGT : fp.L, W = fp.W, q = L >> 3;
+  const int lq = LGT ? LGT - 3 : __ffs(q) - 1, lW = __ffs(W) - 1;
   const int LP = fft_lp(L, W);
   C *buf = reinterpret_cast<C *>(smem_raw);
   /* stage twiddles, stage-major: for the stage of span Ns (Ns0, 8 Ns0, ..., L/8; Ns0 the first
@@ -1436,7 +1438,7 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
     const unsigned lo = (1u << fp.twbits) - 1;
     return cmul(twP[lo + 1 + (e >> fp.twbits)], twP[e & lo]);
   };
-  const int lg = __ffs(L) - 1;
+  const int lg = LGT ? LGT : __ffs(L) - 1;
   const int ns0 = lg % 3 == 0 ? 8 : lg % 3 == 2 ? 4 : 2;
   for (int Ns = ns0; Ns <= q; Ns <<= 3)
     for (int m = tid; m < 7 * Ns; m += blockDim.x) {
@@ -1492,7 +1494,10 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
     }
     Ns = 2, lNs = 1;
   }
-  for (;;) {
+  /* the stages after the first; their count is a constant in an L-specific build */
+  const int nst = LGT ? (LGT - (LGT % 3 == 0 ? 3 : LGT % 3)) / 3 : (lg - lNs) / 3;
+#pragma unroll
+  for (int si = 0; si < nst; ++si) {
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < 8; ++r) v[r] = bw[fft_swz(t + r * q, kw)];
@@ -1506,7 +1511,7 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 3 : 1)
         v[r] = cmul(v[r], twl[tb + r]);
     }
     dft8(v);
-    if (lNs + 3 == lg) break; /* v[r] = output t + r q */
+    if (si == nst - 1) break; /* v[r] = output t + r q */
     __syncthreads();
     const int o = ((t >> lNs) << (lNs + 3)) + k;
 #pragma unroll
@@ -1599,6 +1604,18 @@ static void launch_fft_pass(const typename cplx<R>::T *in, typename cplx<R>::T *
                                                                                 twM_lo, twM_lo, O);
           return;
         }
+      }
+      if (L == 512) { /* the size-2^18 FFTs' two passes: a build for L = 512 */
+        if (tin && tout)
+          k_fft_reg<R, true, true, StridedLd<R>, false, 9><<<g, thr, sm, st>>>(sld, out, twM, twM, fmm_pass(fp),
+                                                                               nullptr, nullptr, O);
+        else if (tin)
+          k_fft_reg<R, true, false, StridedLd<R>, false, 9><<<g, thr, sm, st>>>(sld, out, twM, twM, fmm_pass(fp),
+                                                                                nullptr, nullptr, O);
+        else
+          k_fft_reg<R, false, false, StridedLd<R>, false, 9><<<g, thr, sm, st>>>(sld, out, twM, twM, fmm_pass(fp),
+                                                                                 nullptr, nullptr, O);
+        return;
       }
       if (tin && tout)
         k_fft_reg<R, true, true><<<g, thr, sm, st>>>(sld, out, twM, twM, fmm_pass(fp), nullptr, nullptr, O);
@@ -2807,6 +2824,9 @@ static int dev_execute(Dev<R> *d, const void *vin, void *vout, cudaStream_t st, 
       k_fft_reg<R, false, false, CombineLd<R>, true>
           <<<dim3((unsigned)(ccols / Wc), (unsigned)nbt), thr, sm + sizeof(C) * (size_t)(P + P / 16 + 1), st>>>(
               cl, cz, d->twP, d->twP, fp, d->twP_lo, d->twP_lo);
+    else if (P == 64) /* a build for 64 sections */
+      k_fft_reg<R, false, false, CombineLd<R>, false, 6><<<dim3((unsigned)(ccols / Wc), (unsigned)nbt), thr, sm, st>>>(
+          cl, cz, d->twP, d->twP, fp);
     else
       k_fft_reg<R, false, false, CombineLd<R>><<<dim3((unsigned)(ccols / Wc), (unsigned)nbt), thr, sm, st>>>(
           cl, cz, d->twP, d->twP, fp);
@@ -3032,6 +3052,14 @@ static int set_smem_limits(void) {
   cudaFuncSetAttribute(k_fft_reg<double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_fft_reg<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_fft_reg<double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<float, true, true, StridedLd<float>, false, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<float, true, false, StridedLd<float>, false, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<float, false, false, StridedLd<float>, false, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<double, true, true, StridedLd<double>, false, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<double, true, false, StridedLd<double>, false, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<double, false, false, StridedLd<double>, false, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<float, false, false, CombineLd<float>, false, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fft_reg<double, false, false, CombineLd<double>, false, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_combine<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_combine<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_sections<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
